@@ -1,0 +1,24 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import __graft_entry__  # noqa: E402
+
+__graft_entry__.load_package()
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built extension")
+    config.addinivalue_line("markers", "slow: takes more than ~20 s on 8 CPU cores")
+
+
+@pytest.fixture(scope="session")
+def golden_dir():
+    return GOLDEN

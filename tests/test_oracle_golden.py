@@ -1,0 +1,85 @@
+"""Pins the CPU oracle against the reference's own known-answer tests.
+
+src/tests.sh:38-117 runs ESOLO240 and ESOLO2160 and checks the dynamic output
+with src/dtester.c (max row 1-norm of the difference <= EPS = 1e-3 for the
+boundary displacements, tractions, interior displacements and stresses).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from bem_mececcs_b200 import formats
+
+EPS = 1.0e-3  # src/dtester.c:24
+
+
+def _run(golden_dir, tag):
+    s = formats.read_static(os.path.join(golden_dir, f"ESOLO{tag}E_-5+5.DAT"))
+    d = formats.read_dynamic(os.path.join(golden_dir, f"ESOLO{tag}D_-5+5.DAT"), s.nbe)
+    p = oracle.OracleProblem(s, d)
+    p.ghmatece()
+    fr = d.freqs[0]
+    disp, tr, _ = p.solve(fr)
+    zdsol, zssol = p.interior(fr, disp, tr)
+    mine = formats.Results(fr, disp.reshape(-1, 3), tr.reshape(-1, 3),
+                           zdsol.reshape(-1, 3), zssol.reshape(-1, 9))
+    gold = formats.parse_results(os.path.join(golden_dir, f"SSOLO{tag}D_-5+5.SOL"))
+    assert len(gold) == 1 and gold[0].disp.shape == (s.nbe, 3)
+    return mine, gold[0]
+
+
+def test_oracle_matches_golden_240(golden_dir):
+    mine, gold = _run(golden_dir, "240")
+    err = formats.dtester_errors(mine, gold)
+    assert all(np.isfinite(list(err.values())))
+    assert all(v <= EPS for v in err.values()), err
+
+
+@pytest.mark.slow
+def test_oracle_matches_golden_2160(golden_dir):
+    mine, gold = _run(golden_dir, "2160")
+    err = formats.dtester_errors(mine, gold)
+    assert all(v <= EPS for v in err.values()), err
+
+
+def test_gauleg_matches_exact_rule():
+    # Gauss-Legendre nodes/weights are known to double precision.
+    for npg in (2, 4, 8):
+        gi, ome = oracle.gauleg(npg)
+        x, w = np.polynomial.legendre.leggauss(npg)
+        assert np.allclose(gi, x, atol=1e-14) and np.allclose(ome, w, atol=1e-14)
+
+
+def test_restated_zgesv_matches_lapack():
+    rng = np.random.default_rng(7)
+    n = 300
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    x1 = oracle.zgesv(a, b, use_openblas=False)
+    x2 = oracle.zgesv(a, b, use_openblas=True)
+    assert np.linalg.norm(x1 - x2) / np.linalg.norm(x2) < 1e-12
+    assert np.linalg.norm(a @ x1 - b) / np.linalg.norm(b) < 1e-12
+
+
+def test_parser_roundtrip(tmp_path, golden_dir):
+    s = formats.read_static(os.path.join(golden_dir, "ESOLO240E_-5+5.DAT"))
+    d = formats.read_dynamic(os.path.join(golden_dir, "ESOLO240D_-5+5.DAT"), s.nbe)
+    formats.write_static(tmp_path / "e.dat", s)
+    formats.write_dynamic(tmp_path / "d.dat", d)
+    s2 = formats.read_static(tmp_path / "e.dat")
+    d2 = formats.read_dynamic(tmp_path / "d.dat", s2.nbe)
+    assert (s2.n, s2.nbe, s2.np, s2.npg) == (s.n, s.nbe, s.np, s.npg)
+    assert np.array_equal(s2.cone, s.cone) and np.array_equal(s2.cx, s.cx)
+    assert np.array_equal(d2.kode, d.kode) and np.array_equal(d2.bc, d.bc)
+    assert np.array_equal(d2.cxi, d.cxi) and d2.freqs.tolist() == d.freqs.tolist()
+
+
+def test_results_format_roundtrip(tmp_path, golden_dir):
+    gold = formats.parse_results(os.path.join(golden_dir, "SSOLO240D_-5+5.SOL"))[0]
+    path = tmp_path / "out.sol"
+    path.write_text(formats.format_results(gold), encoding="latin-1")
+    back = formats.parse_results(path)[0]
+    err = formats.dtester_errors(back, gold)
+    assert max(err.values()) == 0.0
