@@ -1,0 +1,116 @@
+"""The reference's per-mesh / per-frequency pipeline on the GPU.
+
+`BemSolver` mirrors the reference driver (src/Main.for:108-194) and its
+routines, each backed by the C-ABI of libbem_b200.so:
+
+  ghmatece()   GHMATECE   (src/Ghmatece.for:9-256): HESTdiag, GESTdiag
+  set_bc()     send_dyn_data_gpu_ (ZDFI = BC, KODE; src/Main.for:151-163)
+  ghmatecd()   GHMATECD   (src/Ghmatecd.for:11-239): swapped ZH, ZFI = ZG*ZDFI
+  linsolve()   LINSOLVE   (src/Linsolve.for:1-66): ZFI <- ZH^-1 ZFI
+  interec()    INTEREC un-swap (src/Interec.for:59-67): displacements, tractions
+
+Errors: a degenerate Jacobian raises BemError(BEM_ERR_DEGENERATE) where the
+reference prints "Matriz Singular" / STOPs; a singular ZH raises
+BemError(BEM_ERR_SINGULAR) where the reference's lu_assert exits.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import host
+from .capi import (BEM_FAST_SINGULAR, BEM_KEEP_PRESWAP, BemError, Context, c128, f64, i32,
+                   ptr)
+
+
+class BemSolver:
+    def __init__(self, static, device: int = 0, ctx: Context | None = None):
+        self.s = static
+        self.ctx = ctx or Context(device)
+        s = static
+        self.nn = 3 * s.nbe
+        self.gi, self.ome = host.gauleg(s.npg)
+        self.cone = i32(s.cone_fortran())
+        self.cx, self.cy, self.cz = f64(s.cx), f64(s.cy), f64(s.cz)
+        self.etas = host.normvec(s.cone, self.cx, self.cy, self.cz)
+        self.cxm, self.cym, self.czm = (f64(a) for a in s.centroids())
+        self.c = host.static_consts(s.ge, s.rnu)
+        L = self.ctx.L
+        self.ctx.check(L.bem_mesh_upload(self.ctx.h, s.n, s.nbe, s.np, s.npg, ptr(self.cone),
+                                         ptr(self.cx), ptr(self.cy), ptr(self.cz), ptr(self.cxm),
+                                         ptr(self.cym), ptr(self.czm), ptr(self.etas),
+                                         ptr(f64(self.gi)), ptr(f64(self.ome))),
+                       "bem_mesh_upload")
+        self.kode = None
+        self.zdfi = None
+        self.material = None
+
+    def ghmatece(self, compute_gest: bool = True):
+        hd = np.zeros(9 * self.s.nbe)
+        gd = np.zeros(9 * self.s.nbe)
+        self.ctx.check(self.ctx.L.bem_ghmatece(self.ctx.h, ptr(f64(self.c)), int(compute_gest),
+                                               ptr(hd), ptr(gd)), "bem_ghmatece")
+        return hd, (gd if compute_gest else None)
+
+    def static_h(self):
+        out = np.zeros(9 * self.s.nbe * self.s.n)
+        self.ctx.check(self.ctx.L.bem_static_h(self.ctx.h, ptr(f64(self.c)), ptr(out)),
+                       "bem_static_h")
+        return out
+
+    def set_gestdiag(self, gd):
+        self.ctx.check(self.ctx.L.bem_set_gestdiag(self.ctx.h, ptr(f64(gd))), "bem_set_gestdiag")
+
+    def set_bc(self, kode, zdfi, dam: float, rho: float):
+        self.kode = i32(kode)
+        self.zdfi = c128(zdfi)
+        self.material = host.material(self.s.ge, self.s.rnu, dam, rho)
+        self.ctx.check(self.ctx.L.bem_dyn_upload(self.ctx.h, ptr(self.zdfi), ptr(self.kode)),
+                       "bem_dyn_upload")
+
+    def ghmatecd(self, fr: float, *, keep_preswap: bool = False, fast_singular: bool = True):
+        zge, zcs, zcp = self.material
+        flags = (BEM_FAST_SINGULAR if fast_singular else 0) | (BEM_KEEP_PRESWAP if keep_preswap else 0)
+        self.ctx.check(self.ctx.L.bem_ghmatecd(
+            self.ctx.h, ptr(f64([zge.real, zge.imag])), ptr(f64([zcs.real, zcs.imag])),
+            ptr(f64([zcp.real, zcp.imag])), ptr(f64(self.c)), float(fr), flags), "bem_ghmatecd")
+
+    def get_system(self):
+        zh = np.zeros(self.nn * self.nn, dtype=np.complex128)
+        zfi = np.zeros(self.nn, dtype=np.complex128)
+        self.ctx.check(self.ctx.L.bem_get_system(self.ctx.h, ptr(zh), ptr(zfi)), "bem_get_system")
+        return zh, zfi
+
+    def get_preswap(self):
+        zh = np.zeros(self.nn * self.nn, dtype=np.complex128)
+        zg = np.zeros(self.nn * self.nn, dtype=np.complex128)
+        self.ctx.check(self.ctx.L.bem_get_preswap(self.ctx.h, ptr(zh), ptr(zg)), "bem_get_preswap")
+        return zh, zg
+
+    def linsolve(self):
+        zfi = np.zeros(self.nn, dtype=np.complex128)
+        self.ctx.check(self.ctx.L.bem_linsolve(self.ctx.h, ptr(zfi)), "bem_linsolve")
+        return zfi
+
+    def interec(self):
+        disp = np.zeros(self.nn, dtype=np.complex128)
+        trac = np.zeros(self.nn, dtype=np.complex128)
+        self.ctx.check(self.ctx.L.bem_unswap(self.ctx.h, ptr(disp), ptr(trac)), "bem_unswap")
+        return disp, trac
+
+    def solve_frequency(self, fr: float):
+        """GHMATECD + LINSOLVE + un-swap: boundary displacements and tractions."""
+        self.ghmatecd(fr)
+        self.linsolve()
+        return self.interec()
+
+
+def solve_dense(ctx: Context, a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """ZGESV on the device for one right-hand side; a is (n, n)."""
+    n = b.shape[0]
+    af = c128(np.asarray(a).reshape(n, n).ravel(order="F"))
+    x = np.zeros(n, dtype=np.complex128)
+    ctx.check(ctx.L.bem_solve_dense(ctx.h, n, ptr(af), ptr(c128(b)), ptr(x)), "bem_solve_dense")
+    return x
+
+
+__all__ = ["BemSolver", "BemError", "solve_dense"]

@@ -1,0 +1,188 @@
+/*
+ * bem_capi.h -- C-ABI of libbem_b200.so, the B200 (sm_100a) implementation
+ * of the BEM-MECECCS hot path: H/G assembly (GHMATECE/GHMATECD) and the
+ * dense complex solve (LINSOLVE).
+ *
+ * Two layers:
+ *
+ *  1. The drop-in seam.  The exact gfortran-mangled entry points that the
+ *     reference's Fortran driver calls when built with -DUSE_GPU (lower case
+ *     plus '_', every argument by reference, no hidden lengths).  A Fortran
+ *     build of the reference links against this library instead of its own
+ *     CUDA sources under src/kernels/.  FP64 form only (FREAL=double, COMPLEX = 16-byte
+ *     interleaved re/im, INTEGER = int32).  State lives in one process-wide
+ *     context, like the reference's device globals (src/kernels/shared.cu:6-31).
+ *     Errors follow the reference: *status = 1 on a degenerate Jacobian, and
+ *     CUDA / solver failures print a message and exit(1).
+ *
+ *  2. The native API (bem_*).  An explicit context per mesh, status codes
+ *     instead of exit(), device-resident state that can be kept across
+ *     frequencies, and an optional caller stream.
+ *
+ * Layouts follow the reference (Fortran column-major):
+ *   cone[k*n + i]            CONE(i+1,k+1), 1-based node numbers, n x 4
+ *   etas[3*j + c]            ETAS(c+1,j+1)
+ *   hestdiag[9*a + 3*j + i]  HESTdiag(i+1,j+1,a+1)  (same for gestdiag)
+ *   zh[col*nn + row]         ZH(row+1,col+1), nn = 3*nbe, complex interleaved
+ */
+#ifndef BEM_CAPI_H
+#define BEM_CAPI_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* 1. Drop-in seam (gfortran name mangling, all arguments by reference).     */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces send_shared_data_to_gpu_, src/kernels/shared.cu:84-99.
+ * Uploads the mesh and the Gauss rule; precomputes Gauss-point geometry. */
+void send_shared_data_to_gpu_(double cx[], double cy[], double cz[],
+                              double cxm[], double cym[], double czm[],
+                              double etas[], double gi[], double ome[],
+                              int cone[], int *np, int *npg, int *n, int *nbe);
+
+/* Replaces send_dyn_data_gpu_, src/kernels/shared.cu:168-182.
+ * zdfi: 3*nbe complex (re,im pairs); kode: 3*nbe. */
+void send_dyn_data_gpu_(int *nbe, double zdfi[], int kode[]);
+
+/* Replaces cuda_ghmatece_, src/kernels/Ghmatece_cu.cu:264-371.
+ * Static Kelvin T over NBE x N element pairs with the rigid-body row sum
+ * fused; HESTdiag stays on the device (hestdiag is not written, as in the
+ * reference without TEST_CUDA).  *status = 1 on DET < 1e-5. */
+void cuda_ghmatece_(int *nbe, int *npg, int *n, int *np, double *c3,
+                    double *c4, double *fr, double hestdiag[], int *status);
+
+/* Replaces cuda_send_gest_data_, src/kernels/Ghmatece_cu.cu:373-380.
+ * Uploads the CPU-computed GESTdiag (3,3,NBE). */
+void cuda_send_gest_data_(int *nbe, double *gestdiag);
+
+/* Replaces cuda_ghmatecd_, src/kernels/Ghmatecd_cu.cu:305-483.
+ * Assembles ZH with the boundary-condition column swap applied and the
+ * right-hand side ZFI = ZG*ZDFI on the device; both stay there for
+ * cuda_linsolve_ (zfi and zhp are not written, as in the reference without
+ * TEST_CUDA).  fast_singular = 1 integrates Stokes minus Kelvin on the
+ * diagonal and adds the static diagonals.  *status = 1 on DET < 1e-5. */
+void cuda_ghmatecd_(int *nbe, int *npg, int *n, int *np, double zge[2],
+                    double zcs[2], double zcp[2], double *c1, double *c2,
+                    double *c3, double *c4, double *fr, double hestdiag[],
+                    double gestdiag[], double zfi[], double zhp[],
+                    int kode[], int *fast_singular, int *status);
+
+/* Replaces cuda_linsolve_, src/kernels/Linsolve_cu.cu:53-126.
+ * LU with partial pivoting of the device-resident ZH and solve for ZFI;
+ * copies the solution into zfi (nn complex).  zh is not read.  A singular
+ * matrix prints an error and exits, as the reference's lu_assert does. */
+void cuda_linsolve_(int *nn, int *n, double zh[], double zfi[]);
+
+/* Replaces deallocate_shared_gpu_data_, src/kernels/shared.cu:184-214. */
+void deallocate_shared_gpu_data_(void);
+
+/* ------------------------------------------------------------------------ */
+/* 2. Native API.                                                            */
+/* ------------------------------------------------------------------------ */
+
+enum bem_status {
+  BEM_OK = 0,
+  BEM_ERR_DEGENERATE = 1, /* DET < 1e-5 at some Gauss point */
+  BEM_ERR_SINGULAR = 2,   /* zero pivot in the LU */
+  BEM_ERR_ARG = 3,        /* bad argument or size */
+  BEM_ERR_CUDA = 4,       /* CUDA runtime error */
+  BEM_ERR_NOMEM = 5,      /* device allocation failed */
+  BEM_ERR_STATE = 6,      /* call out of order (e.g. solve before assembly) */
+  BEM_ERR_TIMEOUT = 7     /* a bounded device-side wait gave up */
+};
+
+typedef struct bem_ctx bem_ctx;
+
+/* Flags of bem_ghmatecd. */
+#define BEM_FAST_SINGULAR 1  /* the reference's fast_singular = 1 */
+#define BEM_KEEP_PRESWAP 2   /* also keep pre-swap H and G for read-back */
+
+int bem_ctx_create(int device, bem_ctx **out);
+int bem_ctx_destroy(bem_ctx *ctx);
+/* Runs every kernel of ctx on `stream` (a cudaStream_t); NULL restores the
+ * context's own stream. */
+int bem_ctx_set_stream(bem_ctx *ctx, void *stream);
+const char *bem_status_string(int status);
+const char *bem_last_error(bem_ctx *ctx);
+/* Number of kernels this library launched on ctx since creation. */
+long long bem_ctx_launch_count(bem_ctx *ctx);
+
+/* Mesh upload, as send_shared_data_to_gpu_. */
+int bem_mesh_upload(bem_ctx *ctx, int n, int nbe, int np, int npg,
+                    const int *cone, const double *cx, const double *cy,
+                    const double *cz, const double *cxm, const double *cym,
+                    const double *czm, const double *etas, const double *gi,
+                    const double *ome);
+
+/* GHMATECE on the device.  c = {C1,C2,C3,C4} (src/Ghmatece.for:60-63).
+ * Computes HESTdiag (rigid body) and, if compute_gest, GESTdiag (SINGGE on
+ * the device).  Outputs may be NULL; results stay resident. */
+int bem_ghmatece(bem_ctx *ctx, const double c[4], int compute_gest,
+                 double *hestdiag_out, double *gestdiag_out);
+
+/* Upload host static diagonals (cuda_send_gest_data_ and its H twin). */
+int bem_set_gestdiag(bem_ctx *ctx, const double *gestdiag);
+int bem_set_hestdiag(bem_ctx *ctx, const double *hestdiag);
+
+/* Full static H (3nbe x 3n, column-major) for checking; may be slow. */
+int bem_static_h(bem_ctx *ctx, const double c[4], double *hest_out);
+
+/* Boundary conditions, as send_dyn_data_gpu_. zdfi: 3nbe complex. */
+int bem_dyn_upload(bem_ctx *ctx, const double *zdfi, const int *kode);
+
+/* GHMATECD on the device: swapped ZH and RHS ZFI assembled in place. */
+int bem_ghmatecd(bem_ctx *ctx, const double zge[2], const double zcs[2],
+                 const double zcp[2], const double c[4], double fr,
+                 int flags);
+
+/* Read back the assembled system: zh nn x nn (after the swap), zfi nn.
+ * Either may be NULL.  Valid after bem_ghmatecd, before bem_linsolve. */
+int bem_get_system(bem_ctx *ctx, double *zh, double *zfi);
+/* Pre-swap H and G (needs BEM_KEEP_PRESWAP at assembly). */
+int bem_get_preswap(bem_ctx *ctx, double *zh, double *zg);
+
+/* LINSOLVE on the device: factor the assembled ZH, solve for ZFI, copy the
+ * solution (nn complex) to zfi_out (may be NULL to keep it on the device). */
+int bem_linsolve(bem_ctx *ctx, double *zfi_out);
+
+/* ZGESV on the device for one right-hand side (src/Linsolve.for:94-100):
+ * a is nn x nn column-major complex (host), b nn complex (host); the
+ * solution is written to x (host).  Uses the same LU as bem_linsolve and
+ * replaces any assembled system of ctx. */
+int bem_solve_dense(bem_ctx *ctx, int nn, const double *a, const double *b,
+                    double *x);
+
+/* The Interec.for:59-67 un-swap of the last solution: boundary
+ * displacements into disp_out and tractions into trac_out (nn complex). */
+int bem_unswap(bem_ctx *ctx, double *disp_out, double *trac_out);
+
+/* Synchronise ctx's stream; returns the first pending error. */
+int bem_sync(bem_ctx *ctx);
+
+/* bem_linsolve without the read-back and without synchronising: the
+ * factorisation and solve are only enqueued on ctx's stream; errors are
+ * reported by the next bem_sync. */
+int bem_linsolve_async(bem_ctx *ctx);
+
+/* Kernel-class timing with CUDA events on ctx's stream.  Classes:
+ * 0 assembly, 1 LU panel, 2 row interchange + triangular solve,
+ * 3 trailing-update GEMM, 4 back substitution.  work[c] is the algorithmic
+ * work of the class: Stokes evaluations for 0, real flops for 3 (8 m n k
+ * per complex update), 0 otherwise. */
+#define BEM_PROF_CLASSES 5
+int bem_prof_enable(bem_ctx *ctx, int on);
+int bem_prof_reset(bem_ctx *ctx);
+int bem_prof_read(bem_ctx *ctx, double *ms, long long *launches,
+                  double *work);
+
+/* Measures this GPU's FP64 tensor-core (DMMA) throughput with a
+ * register-resident mma.sync loop; writes TFLOP/s. */
+int bem_measure_fp64_peak(bem_ctx *ctx, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BEM_CAPI_H */

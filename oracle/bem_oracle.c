@@ -464,15 +464,29 @@ int orc_ghmatecd(int n, int nbe, int np, int npg, const int *cone,
                  const double *zcp, double fr, const double *hestdiag,
                  const double *gestdiag, double *zh_, double *zg_)
 {
+    return orc_ghmatecd_cols(n, nbe, np, npg, cone, cx, cy, cz, cxm, cym, czm,
+                             etas, gi, ome, c, zge, zcs, zcp, fr, hestdiag,
+                             gestdiag, 0, nbe, zh_, zg_);
+}
+
+int orc_ghmatecd_cols(int n, int nbe, int np, int npg, const int *cone,
+                      const double *cx, const double *cy, const double *cz,
+                      const double *cxm, const double *cym, const double *czm,
+                      const double *etas, const double *gi, const double *ome,
+                      const double *c, const double *zge, const double *zcs,
+                      const double *zcp, double fr, const double *hestdiag,
+                      const double *gestdiag, int jlo, int jhi, double *zh_,
+                      double *zg_)
+{
     (void)np;
     const int nn = 3 * nbe;
     zc *zh = (zc *)zh_, *zg = (zc *)zg_;
     dyn_consts d = make_dyn(zge[0] + I * zge[1], zcs[0] + I * zcs[1],
                             zcp[0] + I * zcp[1], fr);
     int status = ORC_OK;
-    /* Ghmatecd.for:113-166. */
+    /* Ghmatecd.for:113-166 (element columns jlo..jhi-1). */
 #pragma omp parallel for schedule(dynamic, 4) reduction(max : status)
-    for (int j = 0; j < nbe; ++j) {
+    for (int j = jlo; j < jhi; ++j) {
         double co[4][3];
         load_co(n, j, cone, cx, cy, cz, co);
         for (int i = 0; i < nbe; ++i) {

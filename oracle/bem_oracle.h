@@ -61,6 +61,16 @@ int orc_ghmatecd(int n, int nbe, int np, int npg, const int *cone,
                  const double *zcp, double fr, const double *hestdiag,
                  const double *gestdiag, double *zh, double *zg);
 
+/* The same for element columns jlo..jhi-1 only (a bounded sample). */
+int orc_ghmatecd_cols(int n, int nbe, int np, int npg, const int *cone,
+                      const double *cx, const double *cy, const double *cz,
+                      const double *cxm, const double *cym, const double *czm,
+                      const double *etas, const double *gi, const double *ome,
+                      const double *c, const double *zge, const double *zcs,
+                      const double *zcp, double fr, const double *hestdiag,
+                      const double *gestdiag, int jlo, int jhi, double *zh,
+                      double *zg);
+
 /* Ghmatecd.for:316-333 as called at :168 (effective semantics:
  * column j with KODE=0: ZH(:,j) <- -ZG(:,j); ZG(:,j) <- -ZH(:,j)*ZGE). */
 void orc_boundary_conditions(int nn, double *zh, double *zg, const int *kode,

@@ -50,6 +50,8 @@ def lib():
                                          ctypes.c_void_p]
         L.orc_ghmatecd.argtypes = geo + [_d, _d, _d, _d, _d, _d, _d, _d, _d, _d, _dbl,
                                          _d, _d, _c, _c]
+        L.orc_ghmatecd_cols.argtypes = geo + [_d, _d, _d, _d, _d, _d, _d, _d, _d, _d, _dbl,
+                                              _d, _d, _int, _int, _c, _c]
         L.orc_boundary_conditions.argtypes = [_int, _c, _c, _i, _d]
         L.orc_zgemv.argtypes = [_int, _c, _c, _c]
         L.orc_zgesv.argtypes = [_int, _c, _i, _c]
@@ -154,6 +156,21 @@ class OracleProblem:
         st = lib().orc_ghmatecd(*self._geo(), self.cxm, self.cym, self.czm, self.etas,
                                 self.gi, self.ome, self.c, self.zge, self.zcs, self.zcp,
                                 float(fr), self.hestdiag, self.gestdiag, zh, zg)
+        if st != 0:
+            raise RuntimeError(f"GHMATECD status {st}")
+        return zh, zg
+
+    def ghmatecd_cols(self, fr: float, jlo: int, jhi: int, zh=None, zg=None):
+        """GHMATECD restricted to element columns jlo..jhi-1 (timing samples)."""
+        if self.hestdiag is None:
+            self.ghmatece()
+        nn = self.nn
+        zh = np.zeros(nn * nn, dtype=np.complex128) if zh is None else zh
+        zg = np.zeros(nn * nn, dtype=np.complex128) if zg is None else zg
+        st = lib().orc_ghmatecd_cols(*self._geo(), self.cxm, self.cym, self.czm, self.etas,
+                                     self.gi, self.ome, self.c, self.zge, self.zcs, self.zcp,
+                                     float(fr), self.hestdiag, self.gestdiag, int(jlo), int(jhi),
+                                     zh, zg)
         if st != 0:
             raise RuntimeError(f"GHMATECD status {st}")
         return zh, zg
