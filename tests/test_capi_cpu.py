@@ -49,12 +49,40 @@ def test_host_setup_matches_oracle():
 
 def test_meshgen_configs():
     s, d = meshgen.config_mesh("c1_240")
-    assert (s.n, s.nbe, s.np, s.npg) == (240, 240, 272, 4)
+    # 240 boundary elements + bottom 240 + walls 2*(16+15)*4.
+    assert (s.nbe, s.n, s.npg) == (240, 240 + 240 + 248, 4)
     assert d.kode.min() == 1 and d.bc[2::3].sum() > 0
     s2, _ = meshgen.config_mesh("c2_2160")
-    assert (s2.n, s2.np) == (2160, 2254)
+    assert s2.nbe == 2160 and s2.n == 2160 * 2 + 2 * (48 + 45) * 4
     # Jitter keeps the domain boundary fixed and moves interior nodes.
     assert s2.cx.min() == -5.0 and s2.cx.max() == 5.0
-    s0 = meshgen.planar_grid(48, 45)
+    s0 = meshgen.enclosed_grid(48, 45, depth=2.5, layers=4)
     assert not np.array_equal(s0.cx, s2.cx)
     assert np.max(np.abs(s0.cx - s2.cx)) <= 0.1 * 10 / 48 + 1e-12
+
+
+def test_enclosure_normals_point_outward():
+    s, _ = meshgen.config_mesh("c1_240")
+    et = host.normvec(s.cone, s.cx, s.cy, s.cz).reshape(-1, 3)
+    cxm, cym, czm = s.centroids()
+    assert np.allclose(et[: s.nbe], [0, 0, 1])  # boundary surface: +z
+    mid = np.stack([cxm, cym, czm + 1.25], 1)   # box centre at z = -1.25
+    assert np.all(np.sum(et[s.nbe:] * mid[s.nbe:], axis=1) > 0)
+
+
+def test_planar_mesh_alone_is_singular():
+    """Why the synthetic meshes are enclosed: an open planar surface with
+    N = NBE gives a singular H (no free term from the rigid-body sum)."""
+    s = meshgen.planar_grid(6, 5)
+    d = meshgen.traction_patch(s, radius=2.0)
+    p = oracle.OracleProblem(s, d)
+    p.ghmatece()
+    zh, _, _, _ = p.system(1.0)
+    sv = np.linalg.svd(zh.reshape(p.nn, p.nn, order="F"), compute_uv=False)
+    assert sv[0] / sv[-1] > 1e12
+    s = meshgen.enclosed_grid(6, 5, depth=2.5, layers=4)
+    p = oracle.OracleProblem(s, meshgen.traction_patch(s, radius=2.0))
+    p.ghmatece()
+    zh, _, _, _ = p.system(1.0)
+    sv = np.linalg.svd(zh.reshape(p.nn, p.nn, order="F"), compute_uv=False)
+    assert sv[0] / sv[-1] < 100
