@@ -514,6 +514,8 @@ int launch_static(bem_ctx* ctx, const double c[4], int compute_gest, double* hes
   Mesh& m = ctx->mesh;
   const int jc = jc_for(m.ng);
   const int chunks = (m.n + jc - 1) / jc;
+  // static_chunks holds the capacity of static_part in chunks of nbe*9 doubles
+  // for the current mesh (reset to 0 by bem_mesh_upload).
   if (chunks > ctx->static_chunks) {
     if (ctx->static_part) cudaFree(ctx->static_part);
     ctx->static_part = nullptr;

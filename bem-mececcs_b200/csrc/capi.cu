@@ -235,6 +235,14 @@ int bem_mesh_upload(bem_ctx* ctx, int n, int nbe, int np, int npg, const int* co
   BEM_CUDA(ctx, cudaMemcpy(flags, ctx->d_status + ST_COUNT, sizeof flags, cudaMemcpyDeviceToHost));
   ctx->have_mesh = true;
   ctx->have_hest = ctx->have_gest = ctx->have_dyn = false;
+  // Per-mesh buffers sized by nbe are reallocated on the next use.
+  cudaFree(ctx->zdfi);
+  cudaFree(ctx->kode);
+  ctx->zdfi = nullptr;
+  ctx->kode = nullptr;
+  cudaFree(ctx->static_part);
+  ctx->static_part = nullptr;
+  ctx->static_chunks = 0;
   ctx->sys.assembled = ctx->sys.solved = false;
   cudaFree(ctx->hestdiag);
   cudaFree(ctx->gestdiag);
