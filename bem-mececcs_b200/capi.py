@@ -25,6 +25,9 @@ BEM_ERR_STATE = 6
 BEM_ERR_TIMEOUT = 7
 BEM_FAST_SINGULAR = 1
 BEM_KEEP_PRESWAP = 2
+BEM_FORM_PLAIN = 0
+BEM_FORM_MIXED = 1
+PROF_CLASSES = ["assembly", "panel", "laswp_trsm", "gemm", "solves", "residual"]
 
 _lib = None
 
@@ -80,6 +83,7 @@ def lib():
     L.bem_prof_reset.argtypes = [vp]
     L.bem_prof_read.argtypes = [vp, vp, vp, vp]
     L.bem_measure_fp64_peak.argtypes = [vp, vp]
+    L.bem_sweep.argtypes = [vp, vp, vp, vp, vp, vp, ip, ip, ip, ip, vp, vp]
     _lib = L
     return L
 
@@ -137,13 +141,13 @@ class Context:
         self.check(self.L.bem_prof_reset(self.h), "bem_prof_reset")
 
     def prof_read(self) -> dict:
-        ms = np.zeros(5)
-        n = np.zeros(5, dtype=np.int64)
-        work = np.zeros(5)
+        nc = len(PROF_CLASSES)
+        ms = np.zeros(nc)
+        n = np.zeros(nc, dtype=np.int64)
+        work = np.zeros(nc)
         self.check(self.L.bem_prof_read(self.h, ptr(ms), ptr(n), ptr(work)), "bem_prof_read")
-        names = ["assembly", "panel", "laswp_trsm", "gemm", "backsub"]
         return {k: {"ms": float(ms[i]), "launches": int(n[i]), "work": float(work[i])}
-                for i, k in enumerate(names)}
+                for i, k in enumerate(PROF_CLASSES)}
 
     def fp64_peak_tflops(self) -> float:
         out = np.zeros(1)

@@ -247,9 +247,9 @@ __global__ void k_gest(int nbe, const double* __restrict__ corner, const double4
 // Dynamic assembly.
 // ---------------------------------------------------------------------------
 struct DynParams {
-  int nbe, nn, ng, jc;
+  int nbe, nn, ng, jc, chunks;
   size_t lda;
-  StokesConsts<double> k;
+  size_t a_stride;  // elements between the systems of consecutive problems
   double2 zge;
   double c1, c2, c3, c4;
   int fast_singular;
@@ -260,13 +260,15 @@ struct DynParams {
   const double* gestdiag;
   const int* kode;
   const double2* zdfi;
-  double2* A;
-  double2* zh_pre;  // optional
-  double2* zg_pre;  // optional
-  double2* diag_h;
+  double2* A;       // problem b: A + b*a_stride, nn x (nn+1)
+  float2* A32;      // optional complex64 copy (same layout)
+  double2* zh_pre;  // optional, problem 0 only
+  double2* zg_pre;  // optional, problem 0 only
+  double2* diag_h;  // [batch][nbe][9]
   double2* diag_g;
-  double2* rhs_part;
+  double2* rhs_part;  // [batch][chunks][nn]
   int* status;
+  StokesConsts<double> kb[kMaxBatch];  // per problem (frequency)
 };
 
 __device__ __forceinline__ zd ld(const double2* p) {
@@ -281,6 +283,10 @@ __device__ __forceinline__ void st(double2* p, zd z) { *p = make_double2(z.re, z
 __global__ void __launch_bounds__(128) k_dyn_diag(DynParams p) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= p.nbe) return;
+  const int prob = blockIdx.z;
+  const StokesConsts<double>& kc = p.kb[prob];
+  double2* diag_h = p.diag_h + (size_t)prob * p.nbe * 9;
+  double2* diag_g = p.diag_g + (size_t)prob * p.nbe * 9;
   const double4 P = p.colloc[j];
   const double4 nv = p.eta[j];
   const double rn0 = nv.x, rn1 = nv.y, rn2 = nv.z;
@@ -296,15 +302,15 @@ __global__ void __launch_bounds__(128) k_dyn_diag(DynParams p) {
     double drn = (r1 * rn0 + r2 * rn1 + r3 * rn2) * ir;
     const double rd[3] = {r1 * ir, r2 * ir, r3 * ir};
     const double rn[3] = {rn0, rn1, rn2};
-    StokesRadial<double> s = stokes_radial(p.k, r, ir);
+    StokesRadial<double> s = stokes_radial(kc, r, ir);
 #pragma unroll
     for (int jj = 0; jj < 3; ++jj)
 #pragma unroll
       for (int ii = 0; ii < 3; ++ii) {
         const double dl = (ii == jj) ? 1.0 : 0.0;
-        zd u = p.k.zc0 * (s.fhi * dl - s.cappa * (rd[jj] * rd[ii]));
-        zd t = p.k.inv4pi * ((s.aa * (drn * dl + rd[jj] * rn[ii])) + s.bb * (rd[ii] * rd[jj] * drn) +
-                             s.cc * (rd[ii] * rn[jj]));
+        zd u = kc.zc0 * (s.fhi * dl - s.cappa * (rd[jj] * rd[ii]));
+        zd t = kc.inv4pi * ((s.aa * (drn * dl + rd[jj] * rn[ii])) + s.bb * (rd[ii] * rd[jj] * drn) +
+                            s.cc * (rd[ii] * rn[jj]));
         if (p.fast_singular) {
           u.re -= (p.c1 / r) * (p.c2 * dl + rd[ii] * rd[jj]);
           t.re -= (p.c3 * ir * ir) * (drn * (p.c4 * dl + 3.0 * rd[ii] * rd[jj]) +
@@ -320,8 +326,8 @@ __global__ void __launch_bounds__(128) k_dyn_diag(DynParams p) {
       zg[k].re += p.gestdiag[(size_t)j * 9 + k];
       zh[k].re += p.hestdiag[(size_t)j * 9 + k];
     }
-    st(&p.diag_h[(size_t)j * 9 + k], zh[k]);
-    st(&p.diag_g[(size_t)j * 9 + k], zg[k]);
+    st(&diag_h[(size_t)j * 9 + k], zh[k]);
+    st(&diag_g[(size_t)j * 9 + k], zg[k]);
   }
 }
 
@@ -345,6 +351,13 @@ __global__ void __launch_bounds__(128) k_dyn_offdiag(DynParams p) {
   const int I = blockIdx.x * kRowsPerCta + lane;
   const int J0 = blockIdx.y * p.jc;
   const int jn = min(p.jc, p.nbe - J0);
+  const int prob = blockIdx.z;
+  const StokesConsts<double>& kc = p.kb[prob];
+  double2* A = p.A + (size_t)prob * p.a_stride;
+  float2* A32 = p.A32 ? p.A32 + (size_t)prob * p.a_stride : nullptr;
+  const double2* diag_h = p.diag_h + (size_t)prob * p.nbe * 9;
+  const double2* diag_g = p.diag_g + (size_t)prob * p.nbe * 9;
+  const bool preswap = p.zh_pre && prob == 0;
 
   if (threadIdx.x == 0) mbar_init(&s_bar, 1);
   __syncthreads();
@@ -384,7 +397,7 @@ __global__ void __launch_bounds__(128) k_dyn_offdiag(DynParams p) {
         const double ir = 1.0 / r;
         const double d0 = r1 * ir, d1 = r2 * ir, d2 = r3 * ir;
         const double drn = (r1 * n3[0] + r2 * n3[1] + r3 * n3[2]) * ir;
-        const StokesRadial<double> s = stokes_radial(p.k, r, ir);
+        const StokesRadial<double> s = stokes_radial(kc, r, ir);
         const double wt = qq.w;
         const double w0 = wt * d0, w1 = wt * d1, w2 = wt * d2, wd = wt * drn;
         cfma(F, s.fhi, wt);
@@ -416,20 +429,20 @@ __global__ void __launch_bounds__(128) k_dyn_offdiag(DynParams p) {
         for (int j = 0; j < 3; ++j) {
           const int sy = sym3(i, j);
           zd u = (i == j) ? F - K[sy] : -K[sy];
-          U[i][j] = p.k.zc0 * u;
+          U[i][j] = kc.zc0 * u;
           zd t = B[sy];
           cfma(t, A1[j], n3[i]);
           cfma(t, C[i], n3[j]);
           if (i == j) t = t + A0;
-          T[i][j] = t * p.k.inv4pi;
+          T[i][j] = t * kc.inv4pi;
         }
     } else if (valid) {
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-          U[i][j] = ld(&p.diag_g[(size_t)J * 9 + 3 * j + i]);
-          T[i][j] = ld(&p.diag_h[(size_t)J * 9 + 3 * j + i]);
+          U[i][j] = ld(&diag_g[(size_t)J * 9 + 3 * j + i]);
+          T[i][j] = ld(&diag_h[(size_t)J * 9 + 3 * j + i]);
         }
     }
     if (valid) {
@@ -443,7 +456,7 @@ __global__ void __launch_bounds__(128) k_dyn_offdiag(DynParams p) {
         for (int i = 0; i < 3; ++i) {
           const size_t row = (size_t)3 * I + i;
           zd h = T[i][j], g = U[i][j];
-          if (p.zh_pre) {
+          if (preswap) {
             st(&p.zh_pre[(size_t)col * p.nn + row], h);
             st(&p.zg_pre[(size_t)col * p.nn + row], g);
           }
@@ -452,7 +465,8 @@ __global__ void __launch_bounds__(128) k_dyn_offdiag(DynParams p) {
             h = -g;
             g = -hg;
           }
-          st(&p.A[(size_t)col * p.lda + row], h);
+          st(&A[(size_t)col * p.lda + row], h);
+          if (A32) A32[(size_t)col * p.lda + row] = make_float2((float)h.re, (float)h.im);
           cfma(rhs[i], g, x);
         }
       }
@@ -467,19 +481,23 @@ __global__ void __launch_bounds__(128) k_dyn_offdiag(DynParams p) {
       zd acc = s_rhs[0][t];
 #pragma unroll
       for (int v = 1; v < kWarpsPerCta; ++v) acc = acc + s_rhs[v][t];
-      st(&p.rhs_part[(size_t)blockIdx.y * p.nn + row], acc);
+      st(&p.rhs_part[((size_t)prob * p.chunks + blockIdx.y) * p.nn + row], acc);
     }
   }
 }
 
 // RHS column of A: sum of the per-chunk partials in chunk order.
-__global__ void k_rhs_reduce(int nn, int chunks, size_t lda, const double2* __restrict__ part,
-                             double2* A) {
+__global__ void k_rhs_reduce(int nn, int chunks, size_t lda, size_t a_stride, const double2* __restrict__ part,
+                             double2* A, float2* A32) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= nn) return;
+  const int prob = blockIdx.y;
+  const double2* pp = part + (size_t)prob * chunks * nn;
   zd acc{0.0, 0.0};
-  for (int c = 0; c < chunks; ++c) acc = acc + ld(&part[(size_t)c * nn + r]);
-  st(&A[(size_t)nn * lda + r], acc);
+  for (int c = 0; c < chunks; ++c) acc = acc + ld(&pp[(size_t)c * nn + r]);
+  const size_t idx = (size_t)prob * a_stride + (size_t)nn * lda + r;
+  st(&A[idx], acc);
+  if (A32) A32[idx] = make_float2((float)acc.re, (float)acc.im);
 }
 
 // ---------------------------------------------------------------------------
@@ -585,31 +603,25 @@ static StokesConsts<double> make_consts(const double zge_[2], const double zcs_[
   return k;
 }
 
-int launch_dynamic(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2],
-                   const double c[4], double fr, int flags) {
+int launch_dynamic_batch(bem_ctx* ctx, const DynBatch& b) {
   Mesh& m = ctx->mesh;
-  System& s = ctx->sys;
   const int jc = jc_for(m.ng);
   const int chunks = (m.nbe + jc - 1) / jc;
-  if (chunks > s.rhs_chunks) {
-    if (s.rhs_part) cudaFree(s.rhs_part);
-    s.rhs_part = nullptr;
-    BEM_CUDA(ctx, cudaMalloc(&s.rhs_part, (size_t)chunks * s.nn * sizeof(double2)));
-    s.rhs_chunks = chunks;
-  }
+  if (b.batch < 1 || b.batch > kMaxBatch) return fail(ctx, BEM_ERR_ARG, "batch size out of range");
   DynParams p{};
   p.nbe = m.nbe;
-  p.nn = s.nn;
+  p.nn = 3 * m.nbe;
   p.ng = m.ng;
   p.jc = jc;
-  p.lda = s.lda;
-  p.k = make_consts(zge, zcs, zcp, fr);
-  p.zge = make_double2(zge[0], zge[1]);
-  p.c1 = c[0];
-  p.c2 = c[1];
-  p.c3 = c[2];
-  p.c4 = c[3];
-  p.fast_singular = (flags & BEM_FAST_SINGULAR) ? 1 : 0;
+  p.chunks = chunks;
+  p.lda = b.lda;
+  p.a_stride = b.a_stride;
+  p.zge = make_double2(b.zge[0], b.zge[1]);
+  p.c1 = b.c[0];
+  p.c2 = b.c[1];
+  p.c3 = b.c[2];
+  p.c4 = b.c[3];
+  p.fast_singular = (b.flags & BEM_FAST_SINGULAR) ? 1 : 0;
   p.gq = m.gq;
   p.eta = m.eta;
   p.colloc = m.colloc;
@@ -617,27 +629,67 @@ int launch_dynamic(bem_ctx* ctx, const double zge[2], const double zcs[2], const
   p.gestdiag = ctx->gestdiag;
   p.kode = ctx->kode;
   p.zdfi = ctx->zdfi;
-  p.A = s.A;
-  p.zh_pre = (flags & BEM_KEEP_PRESWAP) ? s.zh_pre : nullptr;
-  p.zg_pre = (flags & BEM_KEEP_PRESWAP) ? s.zg_pre : nullptr;
-  p.diag_h = s.diag_h;
-  p.diag_g = s.diag_g;
-  p.rhs_part = s.rhs_part;
+  p.A = b.A;
+  p.A32 = b.A32;
+  p.zh_pre = b.zh_pre;
+  p.zg_pre = b.zg_pre;
+  p.diag_h = b.diag_h;
+  p.diag_g = b.diag_g;
+  p.rhs_part = b.rhs_part;
   p.status = ctx->d_status;
+  for (int i = 0; i < b.batch; ++i) p.kb[i] = make_consts(b.zge, b.zcs, b.zcp, b.freqs[i]);
 
-  ProfScope ps(ctx, 0, (double)m.nbe * (double)m.nbe * (double)m.ng);
-  k_dyn_diag<<<(m.nbe + 127) / 128, 128, 0, ctx->stream>>>(p);
+  ProfScope ps(ctx, 0, (double)m.nbe * (double)m.nbe * (double)m.ng * b.batch);
+  k_dyn_diag<<<dim3((m.nbe + 127) / 128, 1, b.batch), 128, 0, ctx->stream>>>(p);
   ctx->launches++;
   BEM_CUDA(ctx, cudaGetLastError());
   const size_t smem = (size_t)jc * m.ng * sizeof(double4);
-  dim3 grid((m.nbe + kRowsPerCta - 1) / kRowsPerCta, chunks);
+  dim3 grid((m.nbe + kRowsPerCta - 1) / kRowsPerCta, chunks, b.batch);
   k_dyn_offdiag<<<grid, 128, smem, ctx->stream>>>(p);
   ctx->launches++;
   BEM_CUDA(ctx, cudaGetLastError());
-  k_rhs_reduce<<<(s.nn + 255) / 256, 256, 0, ctx->stream>>>(s.nn, chunks, s.lda, s.rhs_part, s.A);
+  k_rhs_reduce<<<dim3((p.nn + 255) / 256, b.batch), 256, 0, ctx->stream>>>(p.nn, chunks, b.lda, b.a_stride,
+                                                                           b.rhs_part, b.A, b.A32);
   ctx->launches++;
   BEM_CUDA(ctx, cudaGetLastError());
   return BEM_OK;
+}
+
+int rhs_chunks(bem_ctx* ctx) {
+  const int jc = jc_for(ctx->mesh.ng);
+  return (ctx->mesh.nbe + jc - 1) / jc;
+}
+
+int launch_dynamic(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2],
+                   const double c[4], double fr, int flags) {
+  Mesh& m = ctx->mesh;
+  System& s = ctx->sys;
+  const int chunks = rhs_chunks(ctx);
+  if (chunks > s.rhs_chunks) {
+    if (s.rhs_part) cudaFree(s.rhs_part);
+    s.rhs_part = nullptr;
+    BEM_CUDA(ctx, cudaMalloc(&s.rhs_part, (size_t)chunks * s.nn * sizeof(double2)));
+    s.rhs_chunks = chunks;
+  }
+  (void)m;
+  DynBatch b{};
+  b.zge = zge;
+  b.zcs = zcs;
+  b.zcp = zcp;
+  b.c = c;
+  b.freqs = &fr;
+  b.batch = 1;
+  b.flags = flags;
+  b.A = s.A;
+  b.lda = s.lda;
+  b.a_stride = 0;
+  b.A32 = nullptr;
+  b.zh_pre = (flags & BEM_KEEP_PRESWAP) ? s.zh_pre : nullptr;
+  b.zg_pre = (flags & BEM_KEEP_PRESWAP) ? s.zg_pre : nullptr;
+  b.diag_h = s.diag_h;
+  b.diag_g = s.diag_g;
+  b.rhs_part = s.rhs_part;
+  return launch_dynamic_batch(ctx, b);
 }
 
 }  // namespace bem

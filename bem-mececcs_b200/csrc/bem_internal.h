@@ -5,6 +5,7 @@
 
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "bem_capi.h"
@@ -14,6 +15,37 @@ namespace bem {
 
 // Largest Gauss rule per direction (the reference's fixtures use 8).
 constexpr int kMaxNpg = 8;
+// Largest number of problems assembled or factored in lockstep.
+constexpr int kMaxBatch = 16;
+// Largest number of iterative-refinement steps of the mixed form.
+constexpr int kMaxRefine = 8;
+
+// Device buffers of bem_sweep (per batch of problems).
+struct SweepBuf {
+  int nn = 0, batch = 0, rhs_chunks = 0, resid_chunks = 0;
+  size_t lda = 0, a_stride = 0;
+  double2* A64 = nullptr;       // [batch] x nn x (nn+1)
+  float2* A32 = nullptr;        // complex64 copies (mixed form)
+  double2* x64 = nullptr;       // [batch][nn] refined solutions
+  float2* v32 = nullptr;        // [batch][nn] refinement right-hand sides
+  double2* part = nullptr;      // [batch][resid_chunks][nn] residual partials
+  double2 *diag_h = nullptr, *diag_g = nullptr;  // [batch][nbe][9]
+  double2* rhs_part = nullptr;  // [batch][rhs_chunks][nn]
+  unsigned long long* norm = nullptr;  // [kMaxRefine][batch][2] max|d|, max|x|
+};
+
+// One batched dynamic assembly: `batch` frequencies of the resident mesh.
+struct DynBatch {
+  const double *zge, *zcs, *zcp, *c;
+  const double* freqs;
+  int batch, flags;
+  double2* A;          // problem b at A + b*a_stride
+  size_t lda, a_stride;
+  float2* A32;         // optional complex64 copy, same layout
+  double2 *zh_pre, *zg_pre;
+  double2 *diag_h, *diag_g;  // [batch][nbe][9]
+  double2* rhs_part;         // [batch][chunks][nn]
+};
 
 struct Mesh {
   int n = 0, nbe = 0, np = 0, npg = 0, ng = 0;  // ng = npg^2
@@ -39,11 +71,16 @@ struct System {
   bool assembled = false, solved = false, have_preswap = false;
 };
 
+// Gather list of one panel's row interchanges: count, then dst/src pairs.
+constexpr int kPermStride = 1 + 2 * 128;
+
 struct LuWork {
-  int cap_nn = 0;
-  int* ipiv = nullptr;          // [nn] 1-based pivot rows
-  int* perm = nullptr;          // [2 + 4*64] count, then dst/src pairs of one panel
-  double* slot_val = nullptr;   // [2][kMaxGrid]
+  int cap_nn = 0, cap_batch = 0;
+  int cluster_cs = 0;           // CTAs per panel cluster (16 or 8)
+  int* ipiv = nullptr;          // [batch][nn] 1-based pivot rows
+  int* perm = nullptr;          // [panel][batch][kPermStride]
+  std::vector<std::pair<int, int>> panels;  // (k, w) of every panel of the last factorisation
+  double* slot_val = nullptr;   // grid-panel fallback: [2][kMaxGrid]
   int* slot_row = nullptr;      // [2][kMaxGrid]
   double2* cand = nullptr;      // [2][kMaxGrid][64]
   double2* drow = nullptr;      // [2][64]
@@ -106,6 +143,7 @@ struct bem_ctx {
   double* static_part = nullptr;  // [chunks][nbe][9] rigid-body partial sums
   int static_chunks = 0;
   bem::Profiler prof;
+  bem::SweepBuf sweep;
 };
 
 namespace bem {
@@ -126,10 +164,24 @@ int launch_geometry(bem_ctx* ctx, const double* d_cx, const double* d_cy, const 
 int launch_static(bem_ctx* ctx, const double c[4], int compute_gest, double* hest_full);
 int launch_dynamic(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2],
                    const double c[4], double fr, int flags);
+int launch_dynamic_batch(bem_ctx* ctx, const DynBatch& b);
+int rhs_chunks(bem_ctx* ctx);
 
 // LU (lu.cu).
-int lu_ensure_workspace(bem_ctx* ctx, int nn);
+int lu_ensure_workspace(bem_ctx* ctx, int nn, int batch);
 int lu_factor_solve(bem_ctx* ctx);
+// Factor and solve `batch` problems A + b*bstride (elements of complex64 when
+// fp32, else complex128), each nn x (nn+1) with the right-hand side last.
+int lu_factor_solve_batch(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int batch, bool fp32);
+// Solves with the factors of the last lu_factor_solve_batch for right-hand
+// sides v + b*vstride (overwritten by the solutions).
+int lu_solve_vec(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int batch, void* v, size_t vstride,
+                 bool fp32);
+
+// Frequency sweep (mixed.cu).
+int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], const double c[4],
+          const double* freqs, int nfreq, int form, int batch, int iters, double* x_out, double* corr_out);
+void release_sweep(bem_ctx* ctx);
 int measure_fp64_peak(bem_ctx* ctx, double* tflops);
 
 int check_status(bem_ctx* ctx);

@@ -161,6 +161,7 @@ int bem_ctx_destroy(bem_ctx* ctx) {
   cudaFree(L.cand);
   cudaFree(L.drow);
   cudaFree(L.barrier);
+  release_sweep(ctx);
   for (cudaEvent_t e : ctx->prof.pool) cudaEventDestroy(e);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
@@ -243,6 +244,7 @@ int bem_mesh_upload(bem_ctx* ctx, int n, int nbe, int np, int npg, const int* co
   cudaFree(ctx->static_part);
   ctx->static_part = nullptr;
   ctx->static_chunks = 0;
+  release_sweep(ctx);
   ctx->sys.assembled = ctx->sys.solved = false;
   cudaFree(ctx->hestdiag);
   cudaFree(ctx->gestdiag);
@@ -427,6 +429,19 @@ int bem_linsolve_async(bem_ctx* ctx) {
   int rc = lu_factor_solve(ctx);
   if (rc) return rc;
   ctx->sys.solved = true;
+  return BEM_OK;
+}
+
+int bem_sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], const double c[4],
+              const double* freqs, int nfreq, int form, int batch, int refine, double* x_out, double* corr_out) {
+  if (!ctx || !zge || !zcs || !zcp || !c || (nfreq > 0 && !freqs)) return BEM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!ctx->have_mesh || !ctx->have_dyn || !ctx->have_hest || !ctx->have_gest)
+    return fail(ctx, BEM_ERR_STATE, "bem_sweep needs the mesh, BCs and static diagonals");
+  cudaSetDevice(ctx->device);
+  int rc = sweep(ctx, zge, zcs, zcp, c, freqs, nfreq, form, batch, refine, x_out, corr_out);
+  if (rc) return rc;
+  if (ctx->mesh_flag_bnd) return fail(ctx, BEM_ERR_DEGENERATE, "Jacobian below 1e-5 on a boundary element");
   return BEM_OK;
 }
 

@@ -1,23 +1,31 @@
-// lu.cu -- dense complex LU with partial pivoting and solve (FP64 form).
+// lu.cu -- dense complex LU with partial pivoting and solve, FP64 and FP32.
 //
 // Replaces LINSOLVE's ZGESV (src/Linsolve.for:94-100) and the reference's
 // magma_zgesv_gpu (src/kernels/Linsolve_cu.cu:86-89).  Blocked right-looking
-// factorisation of A = [ZH | ZFI] (the right-hand side rides along as column
-// nn, so the forward substitution happens during the factorisation):
+// factorisation of A = [ZH | ZFI]: the right-hand side rides along as column
+// nn, so the forward substitution happens during the factorisation.  A batch
+// of B equal-size problems (A_b = A + b * bstride) is factored in lockstep.
 //
-//   for each panel of NB columns starting at k:
-//     k_panel        cooperative kernel; the panel's rows live in shared
-//                    memory spread over up to one CTA per SM; one bounded
-//                    grid barrier per column; pivot = first row of largest
-//                    |re|+|im| (LAPACK IZAMAX), rows interchanged as ZGETF2.
-//     k_laswp_trsm   the panel's row interchanges applied to every column
-//                    to the right (as one gather) and U12 = L11^-1 A12.
-//     k_gemm_update  A22 -= L21 U12 on the FP64 tensor cores (DMMA
-//                    m8n8k4), complex as 4 real products.
-//   k_backsub        U x = y, one launch per NB-row block.
+//   for each panel of w columns starting at k (w adapts to the panel height):
+//     k_panel_cluster  one thread-block cluster (16 CTAs) per problem holds the
+//                      panel rows in shared memory; per column the pivot
+//                      candidates and rows are exchanged over distributed
+//                      shared memory with one hardware cluster barrier.  Pivot =
+//                      first row of largest |re|+|im| (LAPACK IZAMAX); rows are
+//                      interchanged as ZGETF2 does.
+//     k_panel_grid     fallback for panels too tall for one cluster: the same
+//                      algorithm over a cooperative grid with a bounded
+//                      software grid barrier.
+//     k_laswp_trsm     the panel's row interchanges applied to every column to
+//                      the right (one gather per column) and U12 = L11^-1 A12.
+//     k_gemm_f64       A22 -= L21 U12 on the FP64 tensor cores (DMMA m8n8k4).
+//     k_gemm_tf32      the same for FP32 storage on the TF32 tensor cores.
+//   k_backsub          U x = y, one launch per 64-row block, the diagonal
+//                      block staged in shared memory.
 //
-// Row interchanges are never applied to the columns left of a panel: the
-// solve does not need L in LAPACK's final row order.
+// Row interchanges are never applied to columns left of a panel; each panel's
+// interchanges are kept (ipiv and a dst/src gather list) so that later solves
+// can replay them in panel order.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -28,55 +36,327 @@
 namespace bem {
 
 constexpr int kPanelThreads = 256;
-constexpr int kPermMax = 2 * 64;  // perm list capacity of one panel
 
-struct PanelArgs {
-  double2* A;
-  size_t lda;
-  int nn, k, w, G, R;
-  int* ipiv;
-  int* perm;
-  double* slot_val;
-  int* slot_row;
-  double2* cand;
-  double2* drow;
-  unsigned* bar;
-  int* status;
+template <typename R>
+struct Elt;
+template <>
+struct Elt<double> {
+  using T = double2;
+};
+template <>
+struct Elt<float> {
+  using T = float2;
 };
 
-__device__ __forceinline__ zd ldz(const double2* p) {
-  double2 v = *p;
-  return zd{v.x, v.y};
+template <typename R>
+__device__ __forceinline__ cpx<R> ldc(const typename Elt<R>::T* p) {
+  const auto v = *p;
+  return cpx<R>{v.x, v.y};
 }
-__device__ __forceinline__ zd ldz_cg(const double2* p) {
-  double2 v = __ldcg(p);
-  return zd{v.x, v.y};
+template <typename R>
+__device__ __forceinline__ cpx<R> ldc_cg(const typename Elt<R>::T* p) {
+  const auto v = __ldcg(p);
+  return cpx<R>{v.x, v.y};
 }
-__device__ __forceinline__ void stz(double2* p, zd z) { *p = make_double2(z.re, z.im); }
+template <typename R>
+__device__ __forceinline__ void stc(typename Elt<R>::T* p, cpx<R> z) {
+  typename Elt<R>::T v;
+  v.x = z.re;
+  v.y = z.im;
+  *p = v;
+}
+// a -= l * u
+template <typename R>
+__device__ __forceinline__ void cfms(cpx<R>& a, cpx<R> l, cpx<R> u) {
+  a.re = fma(-l.re, u.re, fma(l.im, u.im, a.re));
+  a.im = fma(-l.re, u.im, fma(-l.im, u.re, a.im));
+}
 
-__device__ __forceinline__ bool better(double v, int r, double bv, int br) {
+template <typename R>
+__device__ __forceinline__ bool better(R v, int r, R bv, int br) {
   return v > bv || (v == bv && r < br);
 }
 
-template <int NB>
-__global__ void __launch_bounds__(kPanelThreads) k_panel(PanelArgs a) {
-  extern __shared__ __align__(16) double2 s_raw[];
-  zd* s_a = reinterpret_cast<zd*>(s_raw);  // [NB][R], column-major panel rows
-  __shared__ zd s_piv[NB], s_drow[NB];
-  __shared__ double s_rv[kPanelThreads / 32];
+// ---- thread-block cluster helpers (distributed shared memory) ----
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ unsigned map_rank(const void* p, unsigned rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ int dsm_ld(const int* p, unsigned rank) {
+  int v;
+  asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(map_rank(p, rank)) : "memory");
+  return v;
+}
+__device__ __forceinline__ double dsm_ld(const double* p, unsigned rank) {
+  double v;
+  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(map_rank(p, rank)) : "memory");
+  return v;
+}
+__device__ __forceinline__ float dsm_ld(const float* p, unsigned rank) {
+  float v;
+  asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(map_rank(p, rank)) : "memory");
+  return v;
+}
+__device__ __forceinline__ zd dsm_ld(const zd* p, unsigned rank) {
+  zd v;
+  asm volatile("ld.shared::cluster.v2.f64 {%0,%1}, [%2];" : "=d"(v.re), "=d"(v.im) : "r"(map_rank(p, rank)) : "memory");
+  return v;
+}
+__device__ __forceinline__ zf dsm_ld(const zf* p, unsigned rank) {
+  zf v;
+  asm volatile("ld.shared::cluster.v2.f32 {%0,%1}, [%2];" : "=f"(v.re), "=f"(v.im) : "r"(map_rank(p, rank)) : "memory");
+  return v;
+}
+
+// Shared state of one problem's panel step.
+struct PanelArgs {
+  void* A;
+  size_t lda, bstride;
+  int nn, k, w;
+  int rp;          // panel rows per CTA
+  int cs;          // CTAs per problem (cluster size or grid size)
+  int* ipiv;       // [B][nn] 1-based pivot rows
+  int ipiv_stride;
+  int* perm;       // [B][kPermStride]: count, then dst/src pairs
+  int perm_stride;
+  int* status;
+  // grid fallback only:
+  void* slot_val;
+  int* slot_row;
+  void* cand;
+  void* drow;
+  unsigned* bar;
+};
+
+// Per-column bookkeeping of the gather list that replays the panel's row
+// interchanges on other columns: entries 0..w-1 are rows k..k+w-1, entries
+// beyond w are displaced rows below the panel.  Called by one thread.
+__device__ __forceinline__ void perm_swap(int* pdst, int* psrc, int& pcount, int k, int w, int j, int prow) {
+  int ip;
+  if (prow < k + w) {
+    ip = prow - k;
+  } else {
+    ip = -1;
+    for (int e = w; e < pcount; ++e)
+      if (pdst[e] == prow) {
+        ip = e;
+        break;
+      }
+    if (ip < 0) {
+      ip = pcount++;
+      pdst[ip] = prow;
+      psrc[ip] = prow;
+    }
+  }
+  const int t = psrc[j];
+  psrc[j] = psrc[ip];
+  psrc[ip] = t;
+}
+
+// Local part of every column step: candidate search over the CTA's rows.
+template <typename R>
+__device__ __forceinline__ void local_argmax(const cpx<R>* col, int rcount, int rbase, int gj, R* s_rv, int* s_rr,
+                                             R& out_v, int& out_r) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  R bv = R(-1);
+  int br = INT_MAX;
+  for (int r = tid; r < rcount; r += blockDim.x) {
+    const int gr = rbase + r;
+    if (gr >= gj) {
+      const R v = cabs1(col[r]);
+      if (better(v, gr, bv, br)) {
+        bv = v;
+        br = gr;
+      }
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const R ov = __shfl_xor_sync(0xffffffffu, bv, off);
+    const int orr = __shfl_xor_sync(0xffffffffu, br, off);
+    if (better(ov, orr, bv, br)) {
+      bv = ov;
+      br = orr;
+    }
+  }
+  if (lane == 0) {
+    s_rv[warp] = bv;
+    s_rr[warp] = br;
+  }
+  __syncthreads();
+  R v = s_rv[0];
+  int rr = s_rr[0];
+  for (int q = 1; q < kPanelThreads / 32; ++q)
+    if (better(s_rv[q], s_rr[q], v, rr)) {
+      v = s_rv[q];
+      rr = s_rr[q];
+    }
+  out_v = v;
+  out_r = rr;
+}
+
+// Scale column j and apply the rank-1 update to the panel columns right of j.
+template <typename R>
+__device__ __forceinline__ void eliminate(cpx<R>* s_a, int rp, int rcount, int rbase, int gj, int j, int w,
+                                          const cpx<R>* s_piv, int* status, bool report) {
+  const int tid = threadIdx.x;
+  const cpx<R> pv = s_piv[j];
+  const bool zero = (pv.re == R(0) && pv.im == R(0));
+  if (zero && report && tid == 0) atomicCAS(&status[ST_SINGULAR], 0, gj + 1);
+  const cpx<R> rpv = zero ? cpx<R>{R(0), R(0)} : crcp(pv);
+  for (int r = tid; r < rcount; r += blockDim.x)
+    if (rbase + r > gj) s_a[j * rp + r] = s_a[j * rp + r] * rpv;
+  __syncthreads();
+  const int ncol = w - j - 1;
+  for (int idx = tid; idx < ncol * rcount; idx += blockDim.x) {
+    const int c = j + 1 + idx / rcount, r = idx % rcount;
+    if (rbase + r > gj) cfms(s_a[c * rp + r], s_a[j * rp + r], s_piv[c]);
+  }
+  __syncthreads();
+}
+
+template <typename R, int NB>
+__global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(PanelArgs a) {
+  using E = typename Elt<R>::T;
+  using C = cpx<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s_a = reinterpret_cast<C*>(smem_raw);   // [NB][rp] panel rows, column-major
+  C* s_pub = s_a + (size_t)NB * a.rp;        // [2][2][NB]: candidate row, row gj
+  __shared__ R s_pval[2];
+  __shared__ int s_prow[2];
+  __shared__ C s_piv[NB], s_drow[NB];
+  __shared__ R s_rv[kPanelThreads / 32];
   __shared__ int s_rr[kPanelThreads / 32];
-  __shared__ int s_best, s_win_row, s_win_cta;
-  __shared__ int s_pdst[kPermMax], s_psrc[kPermMax];
+  __shared__ int s_win_row, s_win_rank;
+  __shared__ int s_pdst[2 * NB], s_psrc[2 * NB];
   __shared__ int s_pcount;
 
-  const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int R = a.R, w = a.w, k = a.k;
-  const int rbase = k + b * R;
-  const int rcount = max(0, min(R, a.nn - rbase));
+  const unsigned rank = cluster_rank();
+  const int prob = blockIdx.y, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  E* A = static_cast<E*>(a.A) + (size_t)prob * a.bstride;
+  int* ipiv = a.ipiv + (size_t)prob * a.ipiv_stride;
+  int* perm = a.perm + (size_t)prob * a.perm_stride;
+  const int rp = a.rp, w = a.w, k = a.k;
+  const int rbase = k + (int)rank * rp;
+  const int rcount = max(0, min(rp, a.nn - rbase));
 
   for (int idx = tid; idx < w * rcount; idx += blockDim.x) {
     const int c = idx / rcount, r = idx % rcount;
-    s_a[c * R + r] = ldz(&a.A[(size_t)(k + c) * a.lda + rbase + r]);
+    s_a[c * rp + r] = ldc<R>(&A[(size_t)(k + c) * a.lda + rbase + r]);
+  }
+  if (rank == 0 && tid < w) {
+    s_pdst[tid] = k + tid;
+    s_psrc[tid] = k + tid;
+  }
+  if (rank == 0 && tid == 0) s_pcount = w;
+  __syncthreads();
+
+  for (int j = 0; j < w; ++j) {
+    const int gj = k + j, par = j & 1;
+    const int owner = (gj - k) / rp;
+    R bv;
+    int br;
+    local_argmax<R>(s_a + j * rp, rcount, rbase, gj, s_rv, s_rr, bv, br);
+    C* cand = s_pub + (size_t)par * 2 * NB;
+    C* drow = cand + NB;
+    if (tid == 0) {
+      s_pval[par] = bv;
+      s_prow[par] = br;
+    }
+    if (br != INT_MAX && tid < w) cand[tid] = s_a[tid * rp + (br - rbase)];
+    if ((int)rank == owner && tid < w) drow[tid] = s_a[tid * rp + (gj - rbase)];
+    cluster_sync();
+    if (warp == 0) {
+      R v = R(-1);
+      int rr = INT_MAX, cb = 0;
+      if (lane < a.cs) {
+        v = dsm_ld(&s_pval[par], lane);
+        rr = dsm_ld(&s_prow[par], lane);
+        cb = lane;
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const R ov = __shfl_xor_sync(0xffffffffu, v, off);
+        const int orr = __shfl_xor_sync(0xffffffffu, rr, off);
+        const int ocb = __shfl_xor_sync(0xffffffffu, cb, off);
+        if (better(ov, orr, v, rr)) {
+          v = ov;
+          rr = orr;
+          cb = ocb;
+        }
+      }
+      if (lane == 0) {
+        s_win_row = rr;
+        s_win_rank = cb;
+      }
+    }
+    __syncthreads();
+    const int prow = s_win_row;
+    if (tid < w) {
+      s_piv[tid] = dsm_ld(&cand[tid], (unsigned)s_win_rank);
+      s_drow[tid] = dsm_ld(&drow[tid], (unsigned)owner);
+    }
+    __syncthreads();
+    if (prow != gj && prow >= rbase && prow < rbase + rcount && tid < w) s_a[tid * rp + (prow - rbase)] = s_drow[tid];
+    if ((int)rank == owner && tid < w) s_a[tid * rp + (gj - rbase)] = s_piv[tid];
+    if (rank == 0 && tid == 0) {
+      ipiv[gj] = prow + 1;
+      perm_swap(s_pdst, s_psrc, s_pcount, k, w, j, prow);
+    }
+    __syncthreads();
+    eliminate<R>(s_a, rp, rcount, rbase, gj, j, w, s_piv, a.status, rank == 0);
+  }
+  for (int idx = tid; idx < w * rcount; idx += blockDim.x) {
+    const int c = idx / rcount, r = idx % rcount;
+    stc<R>(&A[(size_t)(k + c) * a.lda + rbase + r], s_a[c * rp + r]);
+  }
+  if (rank == 0) {
+    if (tid == 0) perm[0] = s_pcount;
+    for (int e = tid; e < s_pcount; e += blockDim.x) {
+      perm[1 + 2 * e] = s_pdst[e];
+      perm[2 + 2 * e] = s_psrc[e];
+    }
+  }
+  cluster_sync();  // no CTA leaves while others may still read its shared memory
+}
+
+// Fallback for panels too tall for one cluster: the same column steps over a
+// cooperative grid of cs CTAs, exchanging candidates through global memory
+// (double-buffered by column parity) with one bounded grid barrier per column.
+template <typename R, int NB>
+__global__ void __launch_bounds__(kPanelThreads) k_panel_grid(PanelArgs a) {
+  using E = typename Elt<R>::T;
+  using C = cpx<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s_a = reinterpret_cast<C*>(smem_raw);
+  __shared__ C s_piv[NB], s_drow[NB];
+  __shared__ R s_rv[kPanelThreads / 32];
+  __shared__ int s_rr[kPanelThreads / 32];
+  __shared__ int s_best, s_win_row, s_win_cta;
+  __shared__ int s_pdst[2 * NB], s_psrc[2 * NB];
+  __shared__ int s_pcount;
+
+  const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  E* A = static_cast<E*>(a.A);
+  const int rp = a.rp, w = a.w, k = a.k, G = a.cs;
+  const int rbase = k + b * rp;
+  const int rcount = max(0, min(rp, a.nn - rbase));
+  R* slot_val = static_cast<R*>(a.slot_val);
+  C* cand = static_cast<C*>(a.cand);
+  C* drow = static_cast<C*>(a.drow);
+
+  for (int idx = tid; idx < w * rcount; idx += blockDim.x) {
+    const int c = idx / rcount, r = idx % rcount;
+    s_a[c * rp + r] = ldc<R>(&A[(size_t)(k + c) * a.lda + rbase + r]);
   }
   if (b == 0 && tid < w) {
     s_pdst[tid] = k + tid;
@@ -86,63 +366,27 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(PanelArgs a) {
   __syncthreads();
 
   for (int j = 0; j < w; ++j) {
-    const int gj = k + j;
-    const int par = j & 1;
-    // 1. Local candidate: first row of largest |re|+|im| in column j.
-    double bv = -1.0;
-    int br = INT_MAX;
-    for (int r = tid; r < rcount; r += blockDim.x) {
-      const int gr = rbase + r;
-      if (gr >= gj) {
-        const double v = cabs1(s_a[j * R + r]);
-        if (better(v, gr, bv, br)) {
-          bv = v;
-          br = gr;
-        }
-      }
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-      const int orr = __shfl_xor_sync(0xffffffffu, br, off);
-      if (better(ov, orr, bv, br)) {
-        bv = ov;
-        br = orr;
-      }
-    }
-    if (lane == 0) {
-      s_rv[warp] = bv;
-      s_rr[warp] = br;
-    }
-    __syncthreads();
+    const int gj = k + j, par = j & 1;
+    R bv;
+    int br;
+    local_argmax<R>(s_a + j * rp, rcount, rbase, gj, s_rv, s_rr, bv, br);
     if (tid == 0) {
-      double v = s_rv[0];
-      int rr = s_rr[0];
-      for (int q = 1; q < kPanelThreads / 32; ++q)
-        if (better(s_rv[q], s_rr[q], v, rr)) {
-          v = s_rv[q];
-          rr = s_rr[q];
-        }
-      a.slot_val[par * a.G + b] = v;
-      a.slot_row[par * a.G + b] = rr;
-      s_best = rr;
+      slot_val[par * G + b] = bv;
+      a.slot_row[par * G + b] = br;
+      s_best = br;
     }
     __syncthreads();
-    // 2. Publish the candidate row and, from its owner, the current row gj.
     const int lbr = s_best;
-    if (lbr != INT_MAX && tid < w)
-      stz(&a.cand[((size_t)par * a.G + b) * NB + tid], s_a[tid * R + (lbr - rbase)]);
-    if (gj >= rbase && gj < rbase + rcount && tid < w)
-      stz(&a.drow[par * NB + tid], s_a[tid * R + (gj - rbase)]);
-    // 3. Everyone's candidates are visible after the barrier.
-    if (!grid_barrier(a.bar, (unsigned)(j + 1), (unsigned)a.G, a.status)) return;
+    if (lbr != INT_MAX && tid < w) cand[((size_t)par * G + b) * NB + tid] = s_a[tid * rp + (lbr - rbase)];
+    if (gj >= rbase && gj < rbase + rcount && tid < w) drow[par * NB + tid] = s_a[tid * rp + (gj - rbase)];
+    if (!grid_barrier(a.bar, (unsigned)(j + 1), (unsigned)G, a.status)) return;
     if (tid == 0) __threadfence();
     if (warp == 0) {
-      double v = -1.0;
+      R v = R(-1);
       int rr = INT_MAX, cb = 0;
-      for (int t = lane; t < a.G; t += 32) {
-        const double tv = __ldcg(&a.slot_val[par * a.G + t]);
-        const int tr = __ldcg(&a.slot_row[par * a.G + t]);
+      for (int t = lane; t < G; t += 32) {
+        const R tv = __ldcg(&slot_val[par * G + t]);
+        const int tr = __ldcg(&a.slot_row[par * G + t]);
         if (better(tv, tr, v, rr)) {
           v = tv;
           rr = tr;
@@ -151,7 +395,7 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(PanelArgs a) {
       }
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, v, off);
+        const R ov = __shfl_xor_sync(0xffffffffu, v, off);
         const int orr = __shfl_xor_sync(0xffffffffu, rr, off);
         const int ocb = __shfl_xor_sync(0xffffffffu, cb, off);
         if (better(ov, orr, v, rr)) {
@@ -168,63 +412,22 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(PanelArgs a) {
     __syncthreads();
     const int prow = s_win_row, pcta = s_win_cta;
     if (tid < w) {
-      s_piv[tid] = ldz_cg(&a.cand[((size_t)par * a.G + pcta) * NB + tid]);
-      s_drow[tid] = ldz_cg(&a.drow[par * NB + tid]);
+      s_piv[tid] = ldc_cg<R>(reinterpret_cast<const E*>(&cand[((size_t)par * G + pcta) * NB + tid]));
+      s_drow[tid] = ldc_cg<R>(reinterpret_cast<const E*>(&drow[par * NB + tid]));
     }
     __syncthreads();
-    // 4. Interchange rows gj and prow (ZGETF2 swaps whole panel rows).
-    if (prow != gj && prow >= rbase && prow < rbase + rcount && tid < w)
-      s_a[tid * R + (prow - rbase)] = s_drow[tid];
-    if (gj >= rbase && gj < rbase + rcount && tid < w) s_a[tid * R + (gj - rbase)] = s_piv[tid];
+    if (prow != gj && prow >= rbase && prow < rbase + rcount && tid < w) s_a[tid * rp + (prow - rbase)] = s_drow[tid];
+    if (gj >= rbase && gj < rbase + rcount && tid < w) s_a[tid * rp + (gj - rbase)] = s_piv[tid];
     if (b == 0 && tid == 0) {
       a.ipiv[gj] = prow + 1;
-      int ip;
-      if (prow < k + w) {
-        ip = prow - k;
-      } else {
-        ip = -1;
-        for (int e = w; e < s_pcount; ++e)
-          if (s_pdst[e] == prow) {
-            ip = e;
-            break;
-          }
-        if (ip < 0) {
-          ip = s_pcount++;
-          s_pdst[ip] = prow;
-          s_psrc[ip] = prow;
-        }
-      }
-      const int t = s_psrc[j];
-      s_psrc[j] = s_psrc[ip];
-      s_psrc[ip] = t;
+      perm_swap(s_pdst, s_psrc, s_pcount, k, w, j, prow);
     }
     __syncthreads();
-    // 5. Multipliers L(:,j) = A(:,j) / pivot, then the rank-1 update of the
-    //    panel columns right of j.  A zero pivot leaves the column as is and
-    //    records the first such column (ZGETF2's INFO).
-    const zd pv = s_piv[j];
-    const bool zero = (pv.re == 0.0 && pv.im == 0.0);
-    if (zero && b == 0 && tid == 0) atomicCAS(&a.status[ST_SINGULAR], 0, gj + 1);
-    const zd rp = zero ? zd{0.0, 0.0} : crcp(pv);
-    for (int r = tid; r < rcount; r += blockDim.x)
-      if (rbase + r > gj) s_a[j * R + r] = s_a[j * R + r] * rp;
-    __syncthreads();
-    const int ncol = w - j - 1;
-    for (int idx = tid; idx < ncol * rcount; idx += blockDim.x) {
-      const int c = j + 1 + idx / rcount, r = idx % rcount;
-      if (rbase + r > gj) {
-        zd v = s_a[c * R + r];
-        const zd l = s_a[j * R + r], u = s_piv[c];
-        v.re = fma(-l.re, u.re, fma(l.im, u.im, v.re));
-        v.im = fma(-l.re, u.im, fma(-l.im, u.re, v.im));
-        s_a[c * R + r] = v;
-      }
-    }
-    __syncthreads();
+    eliminate<R>(s_a, rp, rcount, rbase, gj, j, w, s_piv, a.status, b == 0);
   }
   for (int idx = tid; idx < w * rcount; idx += blockDim.x) {
     const int c = idx / rcount, r = idx % rcount;
-    stz(&a.A[(size_t)(k + c) * a.lda + rbase + r], s_a[c * R + r]);
+    stc<R>(&A[(size_t)(k + c) * a.lda + rbase + r], s_a[c * rp + r]);
   }
   if (b == 0) {
     if (tid == 0) a.perm[0] = s_pcount;
@@ -236,91 +439,77 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(PanelArgs a) {
 }
 
 // Row interchanges of one panel applied to columns [c0, ncols) as a gather,
-// then U12 = L11^-1 A12 (unit lower).  One warp per column.
-template <int NB>
-__global__ void __launch_bounds__(256) k_laswp_trsm(double2* A, size_t lda, int k, int w, int c0, int ncols,
-                                                    const int* __restrict__ perm) {
-  extern __shared__ __align__(16) double2 s_raw[];
-  zd* s_L = reinterpret_cast<zd*>(s_raw);  // [NB][NB] column-major
+// then U12 = L11^-1 A12 (unit lower).  One warp per column; problem = blockIdx.y.
+template <typename R>
+__global__ void __launch_bounds__(256) k_laswp_trsm(void* Av, size_t lda, size_t bstride, int k, int w, int c0,
+                                                    int ncols, const int* __restrict__ perm, int perm_stride) {
+  using E = typename Elt<R>::T;
+  using C = cpx<R>;
+  constexpr int NB = 64;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s_L = reinterpret_cast<C*>(smem_raw);  // [NB][NB] column-major
+  E* A = static_cast<E*>(Av) + (size_t)blockIdx.y * bstride;
+  const int* pl = perm + (size_t)blockIdx.y * perm_stride;
   for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
     const int c = idx / w, r = idx % w;
-    s_L[c * NB + r] = ldz(&A[(size_t)(k + c) * lda + k + r]);
+    s_L[c * NB + r] = ldc<R>(&A[(size_t)(k + c) * lda + k + r]);
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int count = perm[0];
-  const int* pl = perm + 1;
-  constexpr int V = NB / 32;
+  const int count = pl[0];
+  pl += 1;
   for (int col = c0 + blockIdx.x * 8 + warp; col < ncols; col += gridDim.x * 8) {
-    double2* cp = A + (size_t)col * lda;
-    zd v[V];
-#pragma unroll
-    for (int q = 0; q < V; ++q) {
-      const int e = lane + 32 * q;
-      v[q] = (e < w) ? ldz(&cp[pl[2 * e + 1]]) : zd{0.0, 0.0};
-    }
-    zd x[2];
+    E* cp = A + (size_t)col * lda;
+    C v0 = lane < w ? ldc<R>(&cp[pl[2 * lane + 1]]) : C{R(0), R(0)};
+    C v1 = lane + 32 < w ? ldc<R>(&cp[pl[2 * (lane + 32) + 1]]) : C{R(0), R(0)};
+    C x[2];
     int xd[2] = {-1, -1};
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
       const int e = w + lane + 32 * q;
       if (e < count) {
         xd[q] = pl[2 * e];
-        x[q] = ldz(&cp[pl[2 * e + 1]]);
+        x[q] = ldc<R>(&cp[pl[2 * e + 1]]);
       }
     }
     __syncwarp();
 #pragma unroll
     for (int q = 0; q < 2; ++q)
-      if (xd[q] >= 0) stz(&cp[xd[q]], x[q]);
-    // Forward substitution with the unit lower L11.
+      if (xd[q] >= 0) stc<R>(&cp[xd[q]], x[q]);
+    // Forward substitution with the unit lower L11: rows lane and lane+32.
     for (int i = 0; i < w; ++i) {
-      const int src = i & 31;
-      zd ui;
-#pragma unroll
-      for (int q = 0; q < V; ++q)
-        if ((i >> 5) == q) {
-          ui.re = __shfl_sync(0xffffffffu, v[q].re, src);
-          ui.im = __shfl_sync(0xffffffffu, v[q].im, src);
-        }
-#pragma unroll
-      for (int q = 0; q < V; ++q) {
-        const int r = lane + 32 * q;
-        if (r > i && r < w) {
-          const zd l = s_L[i * NB + r];
-          v[q].re = fma(-l.re, ui.re, fma(l.im, ui.im, v[q].re));
-          v[q].im = fma(-l.re, ui.im, fma(-l.im, ui.re, v[q].im));
-        }
-      }
+      const C src = (i < 32) ? v0 : v1;
+      C ui;
+      ui.re = __shfl_sync(0xffffffffu, src.re, i & 31);
+      ui.im = __shfl_sync(0xffffffffu, src.im, i & 31);
+      if (lane > i && lane < w) cfms(v0, s_L[i * NB + lane], ui);
+      if (lane + 32 > i && lane + 32 < w) cfms(v1, s_L[i * NB + lane + 32], ui);
     }
-#pragma unroll
-    for (int q = 0; q < V; ++q) {
-      const int r = lane + 32 * q;
-      if (r < w) stz(&cp[k + r], v[q]);
-    }
+    if (lane < w) stc<R>(&cp[k + lane], v0);
+    if (lane + 32 < w) stc<R>(&cp[k + lane + 32], v1);
   }
 }
 
 // ---------------------------------------------------------------------------
-// Trailing update C -= A B on the FP64 tensor cores.
-// C: rows [r0, nn), cols [c0, ncols); A = L21 (cols k..k+w); B = U12.
-// CTA tile 64x64 complex, 8 warps of 32x16, k chunks of 16 double-buffered
-// through cp.async.  Shared layouts keep every fragment load conflict-free:
-// As[k][m] with row stride 66 and Bs[n][k] with stride 20 (complex units).
+// Trailing update C -= L21 U12 on the tensor cores, complex as 4 real products.
+// C: rows [r0, nn), cols [c0, ncols) of problem blockIdx.z; L21 = columns
+// k..k+w-1 of the same rows; U12 = rows k..k+w-1 of the same columns.
 // ---------------------------------------------------------------------------
-constexpr int GBM = 64, GBN = 64, GBK = 16;
-constexpr int AS_STRIDE = GBM + 2;  // == 2 mod 8
-constexpr int BS_STRIDE = GBK + 4;  // == 4 mod 8
-constexpr size_t kGemmSmem = (size_t)2 * (GBK * AS_STRIDE + GBN * BS_STRIDE) * sizeof(double2);
-
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
   const unsigned s = smem_u32(smem);
   const int n = valid ? 16 : 0;
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(n) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+  const unsigned s = smem_u32(smem);
+  const int n = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(gmem), "r"(n) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
@@ -328,36 +517,41 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(256) k_gemm_update(double2* A, size_t lda, int nn, int k, int w, int r0,
-                                                     int c0, int ncols) {
+// FP64: CTA tile 64x64 complex, 8 warps of 32x16, k chunks of 16 double-buffered
+// through cp.async.  As[k][m] (row stride 66) and Bs[n][k] (stride 20), in
+// complex units, keep every fragment load conflict-free.
+constexpr int GBM = 64, GBN = 64, GBK = 16;
+constexpr int AS_STRIDE = GBM + 2;  // == 2 mod 8
+constexpr int BS_STRIDE = GBK + 4;  // == 4 mod 8
+constexpr size_t kGemmSmem = (size_t)2 * (GBK * AS_STRIDE + GBN * BS_STRIDE) * sizeof(double2);
+
+__global__ void __launch_bounds__(256) k_gemm_f64(double2* Abase, size_t lda, size_t bstride, int nn, int k, int w,
+                                                  int r0, int c0, int ncols) {
   extern __shared__ __align__(16) double2 g_smem[];
   auto As = reinterpret_cast<double2(*)[GBK][AS_STRIDE]>(g_smem);
   auto Bs = reinterpret_cast<double2(*)[GBN][BS_STRIDE]>(g_smem + 2 * GBK * AS_STRIDE);
+  double2* A = Abase + (size_t)blockIdx.z * bstride;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warps
   const int row0 = r0 + blockIdx.x * GBM, col0 = c0 + blockIdx.y * GBN;
 
   auto load_chunk = [&](int stage, int kc) {
-    // A tile: 16 k x 64 rows = 1024 complex, 4 per thread.
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int idx = tid + q * 256;
       const int kk = idx >> 6, m = idx & 63;
       const int gr = row0 + m, gk = kc + kk;
       const bool ok = gr < nn && gk < w;
-      const double2* src = ok ? &A[(size_t)(k + gk) * lda + gr] : A;
-      cp_async16(&As[stage][kk][m], src, ok);
+      cp_async16(&As[stage][kk][m], ok ? &A[(size_t)(k + gk) * lda + gr] : A, ok);
     }
-    // B tile: 64 cols x 16 k = 1024 complex.
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int idx = tid + q * 256;
       const int n = idx >> 4, kk = idx & 15;
       const int gc = col0 + n, gk = kc + kk;
       const bool ok = gc < ncols && gk < w;
-      const double2* src = ok ? &A[(size_t)gc * lda + k + gk] : A;
-      cp_async16(&Bs[stage][n][kk], src, ok);
+      cp_async16(&Bs[stage][n][kk], ok ? &A[(size_t)gc * lda + k + gk] : A, ok);
     }
     cp_async_commit();
   };
@@ -416,23 +610,169 @@ __global__ void __launch_bounds__(256) k_gemm_update(double2* A, size_t lda, int
       }
 }
 
+// FP32 storage, TF32 tensor cores (mma.sync m16n8k8, operands rounded to
+// TF32, FP32 accumulation).  CTA tile 128x64 complex, 8 warps of 32x32,
+// k chunks of 16.  As[k][m] row stride 136 float2 and Bs[n][k] stride 20.
+constexpr int TBM = 128, TBN = 64, TBK = 16;
+constexpr int TAS = TBM + 8;   // float2 units
+constexpr int TBS = TBK + 4;
+constexpr size_t kGemmTf32Smem = (size_t)2 * (TBK * TAS + TBN * TBS) * sizeof(float2);
+
+__device__ __forceinline__ unsigned to_tf32(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(256) k_gemm_tf32(float2* Abase, size_t lda, size_t bstride, int nn, int k, int w,
+                                                   int r0, int c0, int ncols) {
+  extern __shared__ __align__(16) float2 t_smem[];
+  auto As = reinterpret_cast<float2(*)[TBK][TAS]>(t_smem);
+  auto Bs = reinterpret_cast<float2(*)[TBN][TBS]>(t_smem + 2 * TBK * TAS);
+  float2* A = Abase + (size_t)blockIdx.z * bstride;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = warp >> 1, wn = warp & 1;  // 4 x 2 warps of 32x32
+  const int row0 = r0 + blockIdx.x * TBM, col0 = c0 + blockIdx.y * TBN;
+
+  auto load_chunk = [&](int stage, int kc) {
+    // A: 16 k x 128 rows = 2048 float2, 8 per thread.
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int idx = tid + q * 256;
+      const int kk = idx >> 7, m = idx & 127;
+      const int gr = row0 + m, gk = kc + kk;
+      const bool ok = gr < nn && gk < w;
+      cp_async8(&As[stage][kk][m], ok ? &A[(size_t)(k + gk) * lda + gr] : A, ok);
+    }
+    // B: 64 cols x 16 k = 1024 float2, 4 per thread.
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int idx = tid + q * 256;
+      const int n = idx >> 4, kk = idx & 15;
+      const int gc = col0 + n, gk = kc + kk;
+      const bool ok = gc < ncols && gk < w;
+      cp_async8(&Bs[stage][n][kk], ok ? &A[(size_t)gc * lda + k + gk] : A, ok);
+    }
+    cp_async_commit();
+  };
+
+  float acc_re[2][4][4], acc_im[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc_re[i][j][e] = acc_im[i][j][e] = 0.f;
+
+  const int nchunks = (w + TBK - 1) / TBK;
+  load_chunk(0, 0);
+  for (int c = 0; c < nchunks; ++c) {
+    if (c + 1 < nchunks) {
+      load_chunk((c + 1) & 1, (c + 1) * TBK);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const int st = c & 1;
+#pragma unroll
+    for (int ks = 0; ks < TBK / 8; ++ks) {
+      unsigned ar[2][4], ai[2][4], an[2][4], br_[4][2], bi[4][2];
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+        const int rb = wm * 32 + mt * 16 + g;
+        const float2 x0 = As[st][ks * 8 + t][rb];
+        const float2 x1 = As[st][ks * 8 + t][rb + 8];
+        const float2 x2 = As[st][ks * 8 + t + 4][rb];
+        const float2 x3 = As[st][ks * 8 + t + 4][rb + 8];
+        ar[mt][0] = to_tf32(x0.x);
+        ar[mt][1] = to_tf32(x1.x);
+        ar[mt][2] = to_tf32(x2.x);
+        ar[mt][3] = to_tf32(x3.x);
+        ai[mt][0] = to_tf32(x0.y);
+        ai[mt][1] = to_tf32(x1.y);
+        ai[mt][2] = to_tf32(x2.y);
+        ai[mt][3] = to_tf32(x3.y);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) an[mt][e] = ai[mt][e] ^ 0x80000000u;
+      }
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int cb = wn * 32 + nt * 8 + g;
+        const float2 y0 = Bs[st][cb][ks * 8 + t];
+        const float2 y1 = Bs[st][cb][ks * 8 + t + 4];
+        br_[nt][0] = to_tf32(y0.x);
+        br_[nt][1] = to_tf32(y1.x);
+        bi[nt][0] = to_tf32(y0.y);
+        bi[nt][1] = to_tf32(y1.y);
+      }
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          mma_tf32(acc_re[mt][nt], ar[mt], br_[nt]);
+          mma_tf32(acc_re[mt][nt], an[mt], bi[nt]);
+          mma_tf32(acc_im[mt][nt], ar[mt], bi[nt]);
+          mma_tf32(acc_im[mt][nt], ai[mt], br_[nt]);
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int gr = row0 + wm * 32 + mt * 16 + g + ((e >> 1) << 3);
+        const int gc = col0 + wn * 32 + nt * 8 + 2 * t + (e & 1);
+        if (gr < nn && gc < ncols) {
+          float2* p = &A[(size_t)gc * lda + gr];
+          float2 v = *p;
+          v.x -= acc_re[mt][nt][e];
+          v.y -= acc_im[mt][nt][e];
+          *p = v;
+        }
+      }
+}
+
 // ---------------------------------------------------------------------------
 // Back substitution U x = y (y = column nn of A after the factorisation).
-// Launch s handles block s (rows [s*NB, ...)): every row above block s+1
-// first subtracts U(row, block s+1) x_{s+1}; CTA 0 owns the rows of block s
-// and then solves its upper-triangular diagonal block.
+// Launch s handles block s (rows [s*64, ...)): every row above block s+1
+// subtracts U(row, block s+1) x_{s+1}; CTA 0 owns the rows of block s, stages
+// the block's upper triangle in shared memory and solves it.
 // ---------------------------------------------------------------------------
-template <int NB>
-__global__ void __launch_bounds__(256) k_backsub(double2* A, size_t lda, int nn, int s) {
-  __shared__ zd s_x[NB];
-  __shared__ zd s_y[NB];
-  double2* y = A + (size_t)nn * lda;
-  const int b0 = s * NB, b1 = min(b0 + NB, nn);   // block s
-  const int n0 = b1, n1 = min(b1 + NB, nn);       // block s+1 (already solved)
-  const int wn = n1 - n0;
-  for (int i = threadIdx.x; i < wn; i += blockDim.x) s_x[i] = ldz(&y[n0 + i]);
+template <typename R>
+__global__ void __launch_bounds__(256) k_backsub(void* Av, size_t lda, size_t bstride, int nn, int s, void* yv,
+                                                 size_t ystride) {
+  using E = typename Elt<R>::T;
+  using C = cpx<R>;
+  constexpr int NB = 64;
+  __shared__ C s_x[NB];
+  __shared__ C s_y[NB];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s_U = reinterpret_cast<C*>(smem_raw);  // column-major diagonal block (CTA 0)
+  E* A = static_cast<E*>(Av) + (size_t)blockIdx.y * bstride;
+  // The right-hand side: column nn of A, or a separate vector per problem.
+  E* y = yv ? static_cast<E*>(yv) + (size_t)blockIdx.y * ystride : A + (size_t)nn * lda;
+  const int b0 = s * NB, b1 = min(b0 + NB, nn);
+  const int n0 = b1, n1 = min(b1 + NB, nn);
+  const int wn = n1 - n0, wb = b1 - b0;
+  for (int i = threadIdx.x; i < wn; i += blockDim.x) s_x[i] = ldc<R>(&y[n0 + i]);
+  if (blockIdx.x == 0)
+    for (int idx = threadIdx.x; idx < wb * wb; idx += blockDim.x) {
+      const int c = idx / wb, r = idx % wb;
+      s_U[c * NB + r] = ldc<R>(&A[(size_t)(b0 + c) * lda + b0 + r]);
+    }
   __syncthreads();
-  // Rows handled by this CTA.
   int lo, hi;
   if (blockIdx.x == 0) {
     lo = b0;
@@ -442,74 +782,52 @@ __global__ void __launch_bounds__(256) k_backsub(double2* A, size_t lda, int nn,
     hi = min(lo + (int)blockDim.x, b0);
   }
   const int r = lo + threadIdx.x;
-  zd acc{0.0, 0.0};
+  C acc{R(0), R(0)};
   if (r < hi) {
-    acc = ldz(&y[r]);
-    for (int c = 0; c < wn; ++c) {
-      const zd u = ldz(&A[(size_t)(n0 + c) * lda + r]);
-      const zd xc = s_x[c];
-      acc.re = fma(-u.re, xc.re, fma(u.im, xc.im, acc.re));
-      acc.im = fma(-u.re, xc.im, fma(-u.im, xc.re, acc.im));
-    }
-    if (blockIdx.x != 0) stz(&y[r], acc);
+    acc = ldc<R>(&y[r]);
+    for (int c = 0; c < wn; ++c) cfms(acc, ldc<R>(&A[(size_t)(n0 + c) * lda + r]), s_x[c]);
+    if (blockIdx.x != 0) stc<R>(&y[r], acc);
   }
   if (blockIdx.x != 0) return;
   if (r < hi) s_y[r - b0] = acc;
   __syncthreads();
-  // Upper-triangular solve of block s by warp 0 (2 rows per lane for NB=64).
   if (threadIdx.x >= 32) return;
   const int lane = threadIdx.x;
-  const int wb = b1 - b0;
-  constexpr int V = NB / 32;
-  zd v[V];
-#pragma unroll
-  for (int q = 0; q < V; ++q) {
-    const int rr = lane + 32 * q;
-    v[q] = rr < wb ? s_y[rr] : zd{0.0, 0.0};
-  }
+  C v0 = lane < wb ? s_y[lane] : C{R(0), R(0)};
+  C v1 = lane + 32 < wb ? s_y[lane + 32] : C{R(0), R(0)};
   for (int i = wb - 1; i >= 0; --i) {
-    const int srcl = i & 31;
-    zd yi;
-#pragma unroll
-    for (int q = 0; q < V; ++q)
-      if ((i >> 5) == q) {
-        yi.re = __shfl_sync(0xffffffffu, v[q].re, srcl);
-        yi.im = __shfl_sync(0xffffffffu, v[q].im, srcl);
-      }
-    const zd d = ldz(&A[(size_t)(b0 + i) * lda + b0 + i]);
-    // x_i = y_i / U_ii
-    const double den = 1.0 / fma(d.re, d.re, d.im * d.im);
-    const zd xi{(yi.re * d.re + yi.im * d.im) * den, (yi.im * d.re - yi.re * d.im) * den};
-#pragma unroll
-    for (int q = 0; q < V; ++q) {
-      const int rr = lane + 32 * q;
-      if (rr == i) v[q] = xi;
-      if (rr < i) {
-        const zd u = ldz(&A[(size_t)(b0 + i) * lda + b0 + rr]);
-        v[q].re = fma(-u.re, xi.re, fma(u.im, xi.im, v[q].re));
-        v[q].im = fma(-u.re, xi.im, fma(-u.im, xi.re, v[q].im));
-      }
-    }
+    const C src = (i < 32) ? v0 : v1;
+    C yi;
+    yi.re = __shfl_sync(0xffffffffu, src.re, i & 31);
+    yi.im = __shfl_sync(0xffffffffu, src.im, i & 31);
+    const C d = s_U[i * NB + i];
+    const R den = R(1) / fma(d.re, d.re, d.im * d.im);
+    const C xi{(yi.re * d.re + yi.im * d.im) * den, (yi.im * d.re - yi.re * d.im) * den};
+    if (lane == i) v0 = xi;
+    if (lane + 32 == i) v1 = xi;
+    if (lane < i) cfms(v0, s_U[i * NB + lane], xi);
+    if (lane + 32 < i) cfms(v1, s_U[i * NB + lane + 32], xi);
   }
-#pragma unroll
-  for (int q = 0; q < V; ++q) {
-    const int rr = lane + 32 * q;
-    if (rr < wb) stz(&y[b0 + rr], v[q]);
-  }
+  if (lane < wb) stc<R>(&y[b0 + lane], v0);
+  if (lane + 32 < wb) stc<R>(&y[b0 + lane + 32], v1);
 }
 
 // ---------------------------------------------------------------------------
 // Host side.
 // ---------------------------------------------------------------------------
-int lu_ensure_workspace(bem_ctx* ctx, int nn) {
+int lu_ensure_workspace(bem_ctx* ctx, int nn, int batch) {
   LuWork& L = ctx->lu;
-  if (L.cap_nn >= nn && L.ipiv) return BEM_OK;
+  if (L.cap_nn >= nn && L.cap_batch >= batch && L.ipiv) return BEM_OK;
   cudaFree(L.ipiv);
+  cudaFree(L.perm);
   L.ipiv = nullptr;
-  BEM_CUDA(ctx, cudaMalloc(&L.ipiv, (size_t)nn * sizeof(int)));
+  L.perm = nullptr;
+  BEM_CUDA(ctx, cudaMalloc(&L.ipiv, (size_t)nn * batch * sizeof(int)));
+  const int max_panels = (nn + 15) / 16 + 1;
+  BEM_CUDA(ctx, cudaMalloc(&L.perm, (size_t)max_panels * kPermStride * batch * sizeof(int)));
   L.cap_nn = nn;
-  if (!L.perm) {
-    BEM_CUDA(ctx, cudaMalloc(&L.perm, (1 + 2 * kPermMax) * sizeof(int)));
+  L.cap_batch = batch;
+  if (!L.slot_val) {
     BEM_CUDA(ctx, cudaMalloc(&L.slot_val, 2 * kMaxGrid * sizeof(double)));
     BEM_CUDA(ctx, cudaMalloc(&L.slot_row, 2 * kMaxGrid * sizeof(int)));
     BEM_CUDA(ctx, cudaMalloc(&L.cand, (size_t)2 * kMaxGrid * 64 * sizeof(double2)));
@@ -519,71 +837,295 @@ int lu_ensure_workspace(bem_ctx* ctx, int nn) {
   return BEM_OK;
 }
 
-template <int NB>
-static int lu_run(bem_ctx* ctx) {
-  System& s = ctx->sys;
-  LuWork& L = ctx->lu;
-  const int nn = s.nn;
-  const int ncols = nn + 1;
-  {
-    BEM_CUDA(ctx, cudaFuncSetAttribute(k_panel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_trsm<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       NB * NB * (int)sizeof(double2)));
-    BEM_CUDA(ctx, cudaFuncSetAttribute(k_gemm_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kGemmSmem));
+constexpr size_t kPanelSmemBudget = 220 * 1024;
+
+template <typename R, int NB>
+static int launch_cluster_panel(bem_ctx* ctx, const PanelArgs& pa, int batch) {
+  const size_t smem = ((size_t)NB * pa.rp + 4 * NB) * sizeof(cpx<R>);
+  auto kern = k_panel_cluster<R, NB>;
+  BEM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  BEM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(pa.cs, batch, 1);
+  cfg.blockDim = dim3(kPanelThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = pa.cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  BEM_CUDA(ctx, cudaLaunchKernelEx(&cfg, kern, pa));
+  return BEM_OK;
+}
+
+template <typename R, int NB>
+static int launch_grid_panel(bem_ctx* ctx, PanelArgs pa) {
+  auto kern = k_panel_grid<R, NB>;
+  const size_t smem = (size_t)pa.rp * NB * sizeof(cpx<R>);
+  BEM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  BEM_CUDA(ctx, cudaMemsetAsync(pa.bar, 0, sizeof(unsigned), ctx->stream));
+  void* args[] = {&pa};
+  BEM_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)kern, dim3(pa.cs), dim3(kPanelThreads), args, smem,
+                                            ctx->stream));
+  return BEM_OK;
+}
+
+// Largest cluster size the device accepts for the panel kernel (16, else 8).
+static int cluster_size(bem_ctx* ctx) {
+  if (ctx->lu.cluster_cs) return ctx->lu.cluster_cs;
+  int cs = 8;
+  auto kern = k_panel_cluster<double, 32>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemBudget);
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(16, 1, 1);
+    cfg.blockDim = dim3(kPanelThreads, 1, 1);
+    cfg.dynamicSmemBytes = kPanelSmemBudget;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 16;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg) == cudaSuccess && nclusters >= 1) cs = 16;
   }
-  const int max_rows = (200 * 1024) / (NB * (int)sizeof(double2));
-  for (int k = 0; k < nn; k += NB) {
-    const int w = std::min(NB, nn - k);
+  cudaGetLastError();
+  ctx->lu.cluster_cs = cs;
+  return cs;
+}
+
+template <typename R>
+static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int batch) {
+  LuWork& L = ctx->lu;
+  const int ncols = nn + 1;
+  const size_t es = sizeof(cpx<R>);
+  const int cs = cluster_size(ctx);
+  const size_t lsmem = 64 * 64 * es;
+  const size_t bsmem = 64 * 64 * es;
+  BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_trsm<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem));
+  BEM_CUDA(ctx, cudaFuncSetAttribute(k_backsub<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem));
+  BEM_CUDA(ctx, cudaFuncSetAttribute(k_gemm_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
+  BEM_CUDA(ctx, cudaFuncSetAttribute(k_gemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmTf32Smem));
+  L.panels.clear();
+  for (int k = 0; k < nn;) {
     const int m = nn - k;
-    int G = std::min({ctx->num_sms, kMaxGrid, (m + 15) / 16});
-    G = std::max(G, 1);
-    int R = (m + G - 1) / G;
-    if (R > max_rows) return fail(ctx, BEM_ERR_ARG, "matrix too large for the FP64 panel kernel");
-    G = (m + R - 1) / R;
-    PanelArgs pa{s.A, s.lda, nn, k, w, G, R, L.ipiv, L.perm, L.slot_val, L.slot_row, L.cand, L.drow,
-                 L.barrier, ctx->d_status};
-    BEM_CUDA(ctx, cudaMemsetAsync(L.barrier, 0, sizeof(unsigned), ctx->stream));
-    void* args[] = {&pa};
-    const size_t smem = (size_t)R * NB * sizeof(double2);
+    int* perm_p = L.perm + L.panels.size() * (size_t)batch * kPermStride;  // this panel's lists
+    PanelArgs pa{};
+    pa.A = A;
+    pa.lda = lda;
+    pa.bstride = bstride;
+    pa.nn = nn;
+    pa.k = k;
+    pa.ipiv = L.ipiv;
+    pa.ipiv_stride = nn;
+    pa.perm = perm_p;
+    pa.perm_stride = kPermStride;
+    pa.status = ctx->d_status;
+    // Panel width: the widest of 64/32/16 whose rows fit one cluster.
+    const int rp_c = (m + cs - 1) / cs;
+    int nb = 0;
+    for (int cand : {64, 32, 16})
+      if (((size_t)cand * rp_c + 4 * cand) * es <= kPanelSmemBudget) {
+        nb = cand;
+        break;
+      }
+    int w;
     {
       ProfScope ps(ctx, 1, 0.0);
-      BEM_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)k_panel<NB>, dim3(G), dim3(kPanelThreads), args,
-                                                smem, ctx->stream));
+      if (nb) {
+        w = std::min(nb, m);
+        pa.w = w;
+        pa.rp = rp_c;
+        pa.cs = cs;  // CTAs past the last row own no rows but join every barrier
+        int rc = (nb == 64) ? launch_cluster_panel<R, 64>(ctx, pa, batch)
+                 : (nb == 32) ? launch_cluster_panel<R, 32>(ctx, pa, batch)
+                              : launch_cluster_panel<R, 16>(ctx, pa, batch);
+        if (rc) return rc;
+        ctx->launches++;
+      } else {
+        // Panel taller than one cluster holds: cooperative grid, one problem at a time.
+        int G = std::min({ctx->num_sms, kMaxGrid, (m + 15) / 16});
+        const int rp = (m + G - 1) / G;
+        int nbg = 64;
+        if ((size_t)rp * 64 * es > kPanelSmemBudget) nbg = 32;
+        if ((size_t)rp * nbg * es > kPanelSmemBudget)
+          return fail(ctx, BEM_ERR_ARG, "matrix too large for the panel kernels");
+        w = std::min(nbg, m);
+        G = (m + rp - 1) / rp;
+        pa.w = w;
+        pa.rp = rp;
+        pa.cs = G;
+        pa.slot_val = L.slot_val;
+        pa.slot_row = L.slot_row;
+        pa.cand = L.cand;
+        pa.drow = L.drow;
+        pa.bar = L.barrier;
+        for (int b = 0; b < batch; ++b) {
+          PanelArgs pb = pa;
+          pb.A = static_cast<char*>(A) + (size_t)b * bstride * es;
+          pb.ipiv = L.ipiv + (size_t)b * nn;
+          pb.perm = perm_p + (size_t)b * kPermStride;
+          int rc = (nbg == 64) ? launch_grid_panel<R, 64>(ctx, pb) : launch_grid_panel<R, 32>(ctx, pb);
+          if (rc) return rc;
+          ctx->launches++;
+        }
+      }
     }
-    ctx->launches++;
+    BEM_CUDA(ctx, cudaGetLastError());
     const int c0 = k + w;
     if (c0 < ncols) {
       const int cols = ncols - c0;
-      const int blocks = std::min((cols + 7) / 8, 4 * ctx->num_sms);
+      const int blocks = std::max(1, std::min((cols + 7) / 8, (4 * ctx->num_sms + batch - 1) / batch));
       {
         ProfScope ps(ctx, 2, 0.0);
-        k_laswp_trsm<NB><<<blocks, 256, NB * NB * sizeof(double2), ctx->stream>>>(s.A, s.lda, k, w, c0, ncols,
-                                                                                L.perm);
+        k_laswp_trsm<R><<<dim3(blocks, batch), 256, lsmem, ctx->stream>>>(A, lda, bstride, k, w, c0, ncols, perm_p,
+                                                                           kPermStride);
       }
       ctx->launches++;
       BEM_CUDA(ctx, cudaGetLastError());
       if (c0 < nn) {
-        dim3 grid((nn - c0 + GBM - 1) / GBM, (cols + GBN - 1) / GBN);
-        {
-          ProfScope ps(ctx, 3, 8.0 * (double)(nn - c0) * (double)cols * (double)w);
-          k_gemm_update<<<grid, 256, kGemmSmem, ctx->stream>>>(s.A, s.lda, nn, k, w, c0, c0, ncols);
+        ProfScope ps(ctx, 3, 8.0 * (double)(nn - c0) * (double)cols * (double)w * batch);
+        if (sizeof(R) == 8) {
+          dim3 grid((nn - c0 + GBM - 1) / GBM, (cols + GBN - 1) / GBN, batch);
+          k_gemm_f64<<<grid, 256, kGemmSmem, ctx->stream>>>(static_cast<double2*>(A), lda, bstride, nn, k, w, c0, c0,
+                                                           ncols);
+        } else {
+          dim3 grid((nn - c0 + TBM - 1) / TBM, (cols + TBN - 1) / TBN, batch);
+          k_gemm_tf32<<<grid, 256, kGemmTf32Smem, ctx->stream>>>(static_cast<float2*>(A), lda, bstride, nn, k, w, c0,
+                                                                c0, ncols);
         }
         ctx->launches++;
         BEM_CUDA(ctx, cudaGetLastError());
       }
     }
+    L.panels.push_back({k, w});
+    k += w;
   }
-  const int nblocks = (nn + NB - 1) / NB;
+  const int nblocks = (nn + 63) / 64;
   ProfScope ps(ctx, 4, 0.0);
   for (int sblk = nblocks - 1; sblk >= 0; --sblk) {
-    const int b0 = sblk * NB;
-    const int grid = 1 + (b0 + 255) / 256;
-    k_backsub<NB><<<grid, 256, 0, ctx->stream>>>(s.A, s.lda, nn, sblk);
+    const int b0 = sblk * 64;
+    k_backsub<R><<<dim3(1 + (b0 + 255) / 256, batch), 256, bsmem, ctx->stream>>>(A, lda, bstride, nn, sblk,
+                                                                                  nullptr, 0);
     ctx->launches++;
     BEM_CUDA(ctx, cudaGetLastError());
   }
   return BEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Solves with the stored factors for a new right-hand side v (per problem):
+// panel by panel, replay the panel's interchanges on v (one gather), solve
+// with the unit lower L11, update the rows below with L21; then the upper
+// back substitution.  Used by iterative refinement.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(256) k_fwd_panel(void* Av, size_t lda, size_t bstride, void* vv, size_t vstride,
+                                                   int k, int w, const int* __restrict__ perm, int perm_stride) {
+  using E = typename Elt<R>::T;
+  using C = cpx<R>;
+  constexpr int NB = 64;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s_L = reinterpret_cast<C*>(smem_raw);  // [NB][NB]
+  __shared__ C s_tmp[2 * NB];
+  const int prob = blockIdx.x;
+  E* A = static_cast<E*>(Av) + (size_t)prob * bstride;
+  E* v = static_cast<E*>(vv) + (size_t)prob * vstride;
+  const int* pl = perm + (size_t)prob * perm_stride;
+  const int count = pl[0];
+  for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
+    const int c = idx / w, r = idx % w;
+    s_L[c * NB + r] = ldc<R>(&A[(size_t)(k + c) * lda + k + r]);
+  }
+  for (int e = threadIdx.x; e < count; e += blockDim.x) s_tmp[e] = ldc<R>(&v[pl[2 + 2 * e]]);
+  __syncthreads();
+  for (int e = threadIdx.x; e < count; e += blockDim.x)
+    if (e >= w) stc<R>(&v[pl[1 + 2 * e]], s_tmp[e]);
+  if (threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
+  C v0 = lane < w ? s_tmp[lane] : C{R(0), R(0)};
+  C v1 = lane + 32 < w ? s_tmp[lane + 32] : C{R(0), R(0)};
+  for (int i = 0; i < w; ++i) {
+    const C src = (i < 32) ? v0 : v1;
+    C ui;
+    ui.re = __shfl_sync(0xffffffffu, src.re, i & 31);
+    ui.im = __shfl_sync(0xffffffffu, src.im, i & 31);
+    if (lane > i && lane < w) cfms(v0, s_L[i * NB + lane], ui);
+    if (lane + 32 > i && lane + 32 < w) cfms(v1, s_L[i * NB + lane + 32], ui);
+  }
+  if (lane < w) stc<R>(&v[k + lane], v0);
+  if (lane + 32 < w) stc<R>(&v[k + lane + 32], v1);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_fwd_update(void* Av, size_t lda, size_t bstride, void* vv, size_t vstride,
+                                                    int k, int w, int nn) {
+  using E = typename Elt<R>::T;
+  using C = cpx<R>;
+  __shared__ C s_x[64];
+  E* A = static_cast<E*>(Av) + (size_t)blockIdx.y * bstride;
+  E* v = static_cast<E*>(vv) + (size_t)blockIdx.y * vstride;
+  for (int i = threadIdx.x; i < w; i += blockDim.x) s_x[i] = ldc<R>(&v[k + i]);
+  __syncthreads();
+  const int r = k + w + blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nn) return;
+  C acc = ldc<R>(&v[r]);
+  for (int c = 0; c < w; ++c) cfms(acc, ldc<R>(&A[(size_t)(k + c) * lda + r]), s_x[c]);
+  stc<R>(&v[r], acc);
+}
+
+template <typename R>
+static int lu_solve_vec_t(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int batch, void* v,
+                          size_t vstride) {
+  LuWork& L = ctx->lu;
+  const size_t es = sizeof(cpx<R>);
+  const size_t lsmem = 64 * 64 * es;
+  BEM_CUDA(ctx, cudaFuncSetAttribute(k_fwd_panel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem));
+  BEM_CUDA(ctx, cudaFuncSetAttribute(k_backsub<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem));
+  ProfScope ps(ctx, 4, 0.0);
+  for (size_t p = 0; p < L.panels.size(); ++p) {
+    const int k = L.panels[p].first, w = L.panels[p].second;
+    const int* perm_p = L.perm + p * (size_t)batch * kPermStride;
+    k_fwd_panel<R><<<batch, 256, lsmem, ctx->stream>>>(A, lda, bstride, v, vstride, k, w, perm_p, kPermStride);
+    ctx->launches++;
+    if (k + w < nn) {
+      k_fwd_update<R><<<dim3((nn - k - w + 255) / 256, batch), 256, 0, ctx->stream>>>(A, lda, bstride, v, vstride,
+                                                                                     k, w, nn);
+      ctx->launches++;
+    }
+  }
+  const int nblocks = (nn + 63) / 64;
+  for (int sblk = nblocks - 1; sblk >= 0; --sblk) {
+    const int b0 = sblk * 64;
+    k_backsub<R><<<dim3(1 + (b0 + 255) / 256, batch), 256, lsmem, ctx->stream>>>(A, lda, bstride, nn, sblk, v,
+                                                                                  vstride);
+    ctx->launches++;
+  }
+  BEM_CUDA(ctx, cudaGetLastError());
+  return BEM_OK;
+}
+
+int lu_solve_vec(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int batch, void* v, size_t vstride,
+                 bool fp32) {
+  return fp32 ? lu_solve_vec_t<float>(ctx, A, lda, bstride, nn, batch, v, vstride)
+              : lu_solve_vec_t<double>(ctx, A, lda, bstride, nn, batch, v, vstride);
+}
+
+int lu_factor_solve(bem_ctx* ctx) {
+  int rc = lu_ensure_workspace(ctx, ctx->sys.nn, 1);
+  if (rc) return rc;
+  return lu_run<double>(ctx, ctx->sys.A, ctx->sys.lda, 0, ctx->sys.nn, 1);
+}
+
+int lu_factor_solve_batch(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int batch, bool fp32) {
+  int rc = lu_ensure_workspace(ctx, nn, batch);
+  if (rc) return rc;
+  return fp32 ? lu_run<float>(ctx, A, lda, bstride, nn, batch) : lu_run<double>(ctx, A, lda, bstride, nn, batch);
 }
 
 // FP64 tensor-core throughput probe: independent DMMA chains in registers.
@@ -623,12 +1165,6 @@ int measure_fp64_peak(bem_ctx* ctx, double* tflops) {
   cudaEventDestroy(e1);
   cudaFree(out);
   return BEM_OK;
-}
-
-int lu_factor_solve(bem_ctx* ctx) {
-  int rc = lu_ensure_workspace(ctx, ctx->sys.nn);
-  if (rc) return rc;
-  return lu_run<64>(ctx);
 }
 
 }  // namespace bem

@@ -1,0 +1,241 @@
+// mixed.cu -- the batching and precision forms of the frequency sweep.
+//
+// bem_sweep assembles and solves a list of frequencies on the resident mesh,
+// `batch` problems at a time in lockstep (one launch per kernel for the whole
+// batch: assembly, every LU step, every refinement step).
+//
+//   plain form:  FP64 assembly, FP64 LU (as bem_ghmatecd + bem_linsolve).
+//   mixed form:  FP64 assembly that also stores a complex64 copy of the
+//                system; LU of the copy in FP32 with TF32 tensor-core trailing
+//                updates; then iterative refinement in FP64:
+//                  x <- x0;  repeat: r = b - A x (FP64, the FP64 matrix),
+//                                    d = LU32^-1 r (FP32 factors),
+//                                    x <- x + d (FP64).
+//                The relative size of the last correction, max|d| / max|x|,
+//                is reported per frequency.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "bem_internal.h"
+
+namespace bem {
+
+namespace {
+
+constexpr int kResidRows = 256, kResidCols = 256;
+
+// partial[prob][chunk][r] = sum over the chunk's columns c of A(r,c) x(c).
+__global__ void __launch_bounds__(kResidRows) k_resid_partial(const double2* __restrict__ A, size_t lda,
+                                                              size_t a_stride, const double2* __restrict__ x,
+                                                              size_t x_stride, int nn, int chunks, double2* part) {
+  __shared__ double2 s_x[kResidCols];
+  const int prob = blockIdx.z;
+  const double2* Ap = A + (size_t)prob * a_stride;
+  const double2* xp = x + (size_t)prob * x_stride;
+  const int c0 = blockIdx.y * kResidCols;
+  const int cn = min(kResidCols, nn - c0);
+  for (int i = threadIdx.x; i < cn; i += blockDim.x) s_x[i] = xp[c0 + i];
+  __syncthreads();
+  const int r = blockIdx.x * kResidRows + threadIdx.x;
+  if (r >= nn) return;
+  double re = 0.0, im = 0.0;
+  for (int c = 0; c < cn; ++c) {
+    const double2 a = Ap[(size_t)(c0 + c) * lda + r];
+    const double2 xv = s_x[c];
+    re = fma(a.x, xv.x, fma(-a.y, xv.y, re));
+    im = fma(a.x, xv.y, fma(a.y, xv.x, im));
+  }
+  part[((size_t)prob * chunks + blockIdx.y) * nn + r] = make_double2(re, im);
+}
+
+// v32 = (complex64)(b - sum of partials), b = column nn of A.
+__global__ void k_resid_final(const double2* __restrict__ A, size_t lda, size_t a_stride,
+                              const double2* __restrict__ part, int nn, int chunks, float2* v, size_t v_stride) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nn) return;
+  const int prob = blockIdx.y;
+  const double2 b = A[(size_t)prob * a_stride + (size_t)nn * lda + r];
+  double re = b.x, im = b.y;
+  const double2* pp = part + (size_t)prob * chunks * nn;
+  for (int c = 0; c < chunks; ++c) {
+    const double2 q = pp[(size_t)c * nn + r];
+    re -= q.x;
+    im -= q.y;
+  }
+  v[(size_t)prob * v_stride + r] = make_float2((float)re, (float)im);
+}
+
+// x = (complex128) column nn of the FP32 system (the first, FP32, solution).
+__global__ void k_x_init(const float2* __restrict__ A32, size_t lda, size_t a_stride, int nn, double2* x,
+                         size_t x_stride) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nn) return;
+  const int prob = blockIdx.y;
+  const float2 v = A32[(size_t)prob * a_stride + (size_t)nn * lda + r];
+  x[(size_t)prob * x_stride + r] = make_double2(v.x, v.y);
+}
+
+// x += d; tracks max|d| and max|x| (|re|+|im|) per problem in norm[prob][2].
+__global__ void k_ir_update(double2* x, size_t x_stride, const float2* __restrict__ d, size_t d_stride, int nn,
+                            unsigned long long* norm) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int prob = blockIdx.y;
+  double dm = 0.0, xm = 0.0;
+  if (r < nn) {
+    const float2 dv = d[(size_t)prob * d_stride + r];
+    double2 xv = x[(size_t)prob * x_stride + r];
+    xv.x += dv.x;
+    xv.y += dv.y;
+    x[(size_t)prob * x_stride + r] = xv;
+    dm = fabs((double)dv.x) + fabs((double)dv.y);
+    xm = fabs(xv.x) + fabs(xv.y);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    dm = fmax(dm, __shfl_xor_sync(0xffffffffu, dm, off));
+    xm = fmax(xm, __shfl_xor_sync(0xffffffffu, xm, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    // Non-negative doubles order like their bit patterns.
+    atomicMax(&norm[2 * prob], __double_as_longlong(dm));
+    atomicMax(&norm[2 * prob + 1], __double_as_longlong(xm));
+  }
+}
+
+void free_sweep(SweepBuf& S) {
+  cudaFree(S.A64);
+  cudaFree(S.A32);
+  cudaFree(S.x64);
+  cudaFree(S.v32);
+  cudaFree(S.part);
+  cudaFree(S.diag_h);
+  cudaFree(S.diag_g);
+  cudaFree(S.rhs_part);
+  cudaFree(S.norm);
+  S = SweepBuf{};
+}
+
+int ensure_sweep(bem_ctx* ctx, int batch, bool mixed) {
+  SweepBuf& S = ctx->sweep;
+  const int nn = 3 * ctx->mesh.nbe;
+  const int nbe = ctx->mesh.nbe;
+  const int chunks = rhs_chunks(ctx);
+  if (S.nn == nn && S.batch >= batch && (!mixed || S.A32) && S.rhs_chunks >= chunks) return BEM_OK;
+  free_sweep(S);
+  S.nn = nn;
+  S.batch = batch;
+  S.lda = (size_t)nn;
+  S.a_stride = S.lda * (size_t)(nn + 1);
+  S.rhs_chunks = chunks;
+  S.resid_chunks = (nn + kResidCols - 1) / kResidCols;
+  BEM_CUDA(ctx, cudaMalloc(&S.A64, S.a_stride * batch * sizeof(double2)));
+  if (mixed) BEM_CUDA(ctx, cudaMalloc(&S.A32, S.a_stride * batch * sizeof(float2)));
+  BEM_CUDA(ctx, cudaMalloc(&S.x64, (size_t)nn * batch * sizeof(double2)));
+  BEM_CUDA(ctx, cudaMalloc(&S.v32, (size_t)nn * batch * sizeof(float2)));
+  BEM_CUDA(ctx, cudaMalloc(&S.part, (size_t)S.resid_chunks * nn * batch * sizeof(double2)));
+  BEM_CUDA(ctx, cudaMalloc(&S.diag_h, (size_t)nbe * 9 * batch * sizeof(double2)));
+  BEM_CUDA(ctx, cudaMalloc(&S.diag_g, (size_t)nbe * 9 * batch * sizeof(double2)));
+  BEM_CUDA(ctx, cudaMalloc(&S.rhs_part, (size_t)chunks * nn * batch * sizeof(double2)));
+  BEM_CUDA(ctx, cudaMalloc(&S.norm, (size_t)2 * batch * kMaxRefine * sizeof(unsigned long long)));
+  return BEM_OK;
+}
+
+}  // namespace
+
+void release_sweep(bem_ctx* ctx) { free_sweep(ctx->sweep); }
+
+int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], const double c[4],
+          const double* freqs, int nfreq, int form, int batch, int iters, double* x_out, double* corr_out) {
+  const bool mixed = form == BEM_FORM_MIXED;
+  if (!mixed && form != BEM_FORM_PLAIN) return fail(ctx, BEM_ERR_ARG, "unknown form");
+  if (batch < 1 || batch > kMaxBatch || nfreq < 0 || iters < 0 || iters > kMaxRefine)
+    return fail(ctx, BEM_ERR_ARG, "bem_sweep: batch, count or refinement steps out of range");
+  int rc = ensure_sweep(ctx, batch, mixed);
+  if (rc) return rc;
+  SweepBuf& S = ctx->sweep;
+  const int nn = S.nn;
+  BEM_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->stream));
+  std::vector<unsigned long long> hnorm;
+  for (int f0 = 0; f0 < nfreq; f0 += batch) {
+    const int bsz = std::min(batch, nfreq - f0);
+    DynBatch db{};
+    db.zge = zge;
+    db.zcs = zcs;
+    db.zcp = zcp;
+    db.c = c;
+    db.freqs = freqs + f0;
+    db.batch = bsz;
+    db.flags = BEM_FAST_SINGULAR;
+    db.A = S.A64;
+    db.lda = S.lda;
+    db.a_stride = S.a_stride;
+    db.A32 = mixed ? S.A32 : nullptr;
+    db.diag_h = S.diag_h;
+    db.diag_g = S.diag_g;
+    db.rhs_part = S.rhs_part;
+    rc = launch_dynamic_batch(ctx, db);
+    if (rc) return rc;
+    const dim3 vgrid((nn + 255) / 256, bsz);
+    if (mixed) {
+      rc = lu_factor_solve_batch(ctx, S.A32, S.lda, S.a_stride, nn, bsz, true);
+      if (rc) return rc;
+      k_x_init<<<vgrid, 256, 0, ctx->stream>>>(S.A32, S.lda, S.a_stride, nn, S.x64, nn);
+      ctx->launches++;
+      BEM_CUDA(ctx, cudaMemsetAsync(S.norm, 0, (size_t)2 * bsz * kMaxRefine * sizeof(unsigned long long),
+                                    ctx->stream));
+      for (int it = 0; it < iters; ++it) {
+        {
+          ProfScope ps(ctx, 5, 8.0 * (double)nn * nn * bsz);
+          k_resid_partial<<<dim3((nn + kResidRows - 1) / kResidRows, S.resid_chunks, bsz), kResidRows, 0,
+                            ctx->stream>>>(S.A64, S.lda, S.a_stride, S.x64, nn, nn, S.resid_chunks, S.part);
+          k_resid_final<<<vgrid, 256, 0, ctx->stream>>>(S.A64, S.lda, S.a_stride, S.part, nn, S.resid_chunks, S.v32,
+                                                        nn);
+        }
+        ctx->launches += 2;
+        rc = lu_solve_vec(ctx, S.A32, S.lda, S.a_stride, nn, bsz, S.v32, nn, true);
+        if (rc) return rc;
+        k_ir_update<<<vgrid, 256, 0, ctx->stream>>>(S.x64, nn, S.v32, nn, nn, S.norm + (size_t)2 * bsz * it);
+        ctx->launches++;
+        BEM_CUDA(ctx, cudaGetLastError());
+      }
+    } else {
+      rc = lu_factor_solve_batch(ctx, S.A64, S.lda, S.a_stride, nn, bsz, false);
+      if (rc) return rc;
+    }
+    if (x_out) {
+      double* dst = x_out + (size_t)2 * nn * f0;
+      if (mixed)
+        BEM_CUDA(ctx, cudaMemcpyAsync(dst, S.x64, (size_t)nn * bsz * sizeof(double2), cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+      else
+        BEM_CUDA(ctx, cudaMemcpy2DAsync(dst, (size_t)nn * sizeof(double2), S.A64 + (size_t)nn * S.lda,
+                                        S.a_stride * sizeof(double2), (size_t)nn * sizeof(double2), bsz,
+                                        cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    if (corr_out) {
+      if (mixed && iters > 0) {
+        hnorm.assign((size_t)2 * bsz * kMaxRefine, 0ull);
+        BEM_CUDA(ctx, cudaMemcpyAsync(hnorm.data(), S.norm, (size_t)2 * bsz * iters * sizeof(unsigned long long),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+        BEM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        const size_t last = (size_t)2 * bsz * (iters - 1);
+        for (int b = 0; b < bsz; ++b) {
+          double dm, xm;
+          const unsigned long long du = hnorm[last + 2 * b], xu = hnorm[last + 2 * b + 1];
+          memcpy(&dm, &du, sizeof dm);
+          memcpy(&xm, &xu, sizeof xm);
+          corr_out[f0 + b] = xm > 0 ? dm / xm : 0.0;
+        }
+      } else {
+        for (int b = 0; b < bsz; ++b) corr_out[f0 + b] = 0.0;
+      }
+    }
+  }
+  if (x_out || corr_out) return check_status(ctx);
+  return BEM_OK;
+}
+
+}  // namespace bem

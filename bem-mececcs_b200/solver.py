@@ -18,8 +18,8 @@ from __future__ import annotations
 import numpy as np
 
 from . import host
-from .capi import (BEM_FAST_SINGULAR, BEM_KEEP_PRESWAP, BemError, Context, c128, f64, i32,
-                   ptr)
+from .capi import (BEM_FAST_SINGULAR, BEM_FORM_MIXED, BEM_FORM_PLAIN, BEM_KEEP_PRESWAP, BemError,
+                   Context, c128, f64, i32, ptr)
 
 
 class BemSolver:
@@ -96,6 +96,22 @@ class BemSolver:
         trac = np.zeros(self.nn, dtype=np.complex128)
         self.ctx.check(self.ctx.L.bem_unswap(self.ctx.h, ptr(disp), ptr(trac)), "bem_unswap")
         return disp, trac
+
+    def sweep(self, freqs, *, form: str = "mixed", batch: int = 8, refine: int = 3,
+              want_x: bool = True):
+        """Frequency sweep on the resident mesh (bem_sweep).  Returns
+        (x[nfreq, nn] raw solutions or None, last relative correction)."""
+        freqs = f64(freqs)
+        nf = freqs.size
+        zge, zcs, zcp = self.material
+        x = np.zeros((nf, self.nn), dtype=np.complex128) if want_x else None
+        corr = np.zeros(nf) if want_x else None
+        fm = BEM_FORM_MIXED if form == "mixed" else BEM_FORM_PLAIN
+        self.ctx.check(self.ctx.L.bem_sweep(
+            self.ctx.h, ptr(f64([zge.real, zge.imag])), ptr(f64([zcs.real, zcs.imag])),
+            ptr(f64([zcp.real, zcp.imag])), ptr(f64(self.c)), ptr(freqs), nf, fm, batch, refine,
+            ptr(x), ptr(corr)), "bem_sweep")
+        return x, corr
 
     def solve_frequency(self, fr: float):
         """GHMATECD + LINSOLVE + un-swap: boundary displacements and tractions."""

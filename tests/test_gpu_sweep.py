@@ -1,0 +1,95 @@
+"""The batching and precision forms (bem_sweep) against the FP64 oracle.
+
+Plain form: FP64 batched assembly + lockstep FP64 LU, <= 1e-10 relative.
+Mixed form: FP32 LU on TF32 tensor cores + FP64 iterative refinement; the
+target is <= 1e-8 relative error on the solution; with 3 refinement steps it
+reaches the FP64 level, checked here at 1e-10.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from bem_mececcs_b200 import meshgen
+from bem_mececcs_b200.capi import Context
+from bem_mececcs_b200.solver import BemSolver
+from gpu_util import rel
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def c1():
+    s, d = meshgen.config_mesh("c1_240")
+    p = oracle.OracleProblem(s, d)
+    p.ghmatece()
+    ctx = Context(0)
+    sol = BemSolver(s, ctx=ctx)
+    sol.ghmatece(compute_gest=True)
+    sol.set_bc(d.kode, d.bc.astype(np.complex128), d.dam, d.rho)
+    yield s, d, p, sol
+    ctx.close()
+
+
+FREQS = [0.1, 0.37, 1.0, 2.5, 6.0, 10.0, 0.8]
+
+
+def _oracle_x(p, fr):
+    zh, zfi, _, _ = p.system(fr)
+    return oracle.zgesv(zh, zfi, use_openblas=False)
+
+
+@pytest.mark.parametrize("batch", [1, 3, 8])
+def test_sweep_plain_batched(c1, batch):
+    s, d, p, sol = c1
+    x, _ = sol.sweep(FREQS, form="plain", batch=batch)
+    for i, fr in enumerate(FREQS):
+        assert rel(x[i], _oracle_x(p, fr)) < 1e-10, (batch, fr)
+
+
+@pytest.mark.parametrize("batch", [1, 4, 8])
+def test_sweep_mixed_refined(c1, batch):
+    s, d, p, sol = c1
+    x, corr = sol.sweep(FREQS, form="mixed", batch=batch, refine=3)
+    for i, fr in enumerate(FREQS):
+        e = rel(x[i], _oracle_x(p, fr))
+        assert e < 1e-10, (batch, fr, e)
+        assert corr[i] < 1e-9
+
+
+def test_sweep_mixed_refinement_converges(c1):
+    """No refinement: the FP32/TF32 LU alone is far from 1e-8; each FP64
+    refinement step shrinks the error."""
+    s, d, p, sol = c1
+    errs = []
+    for it in range(0, 4):
+        x, _ = sol.sweep(FREQS[:2], form="mixed", batch=2, refine=it)
+        errs.append(max(rel(x[i], _oracle_x(p, fr)) for i, fr in enumerate(FREQS[:2])))
+    assert errs[0] > 1e-7
+    assert errs[1] < errs[0] * 1e-2 and errs[2] < errs[1] and errs[3] < 1e-10, errs
+
+
+def test_sweep_matches_single_solve(c1):
+    s, d, p, sol = c1
+    x, _ = sol.sweep([1.3], form="plain", batch=1)
+    sol.ghmatecd(1.3)
+    xs = sol.linsolve()
+    assert rel(x[0], xs) < 1e-13
+
+
+@pytest.mark.slow
+def test_sweep_mixed_c2_2160():
+    s, d = meshgen.config_mesh("c2_2160")
+    ctx = Context(0)
+    sol = BemSolver(s, ctx=ctx)
+    sol.ghmatece(compute_gest=True)
+    sol.set_bc(d.kode, d.bc.astype(np.complex128), d.dam, d.rho)
+    freqs = [0.5, 2.0, 8.0]
+    xm, corr = sol.sweep(freqs, form="mixed", batch=3, refine=3)
+    xp, _ = sol.sweep(freqs, form="plain", batch=3)
+    p = oracle.OracleProblem(s, d)
+    p.ghmatece()
+    ox = oracle.zgesv(*p.system(2.0)[:2], use_openblas=True)
+    assert rel(xp[1], ox) < 1e-10
+    for i in range(3):
+        assert rel(xm[i], xp[i]) < 1e-8, (freqs[i], rel(xm[i], xp[i]))
+    ctx.close()
