@@ -224,19 +224,30 @@ __device__ __forceinline__ void eliminate(cpx<R>* s_a, int rp, int rcount, int r
   __syncthreads();
 }
 
-template <typename R, int NB>
-__global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(PanelArgs a) {
+// Panel factorisation in one thread-block cluster per problem.  CTA `rank`
+// owns panel rows [k + rank*rp, ...) in shared memory; thread t owns local
+// rows t, t+256, ... (RPT of them).  The panel is processed in sub-panels of
+// 8 columns held in registers, so the per-column rank-1 updates never touch
+// shared memory; the columns right of a sub-panel are updated once per
+// sub-panel (a triangular solve of the sub-panel's 8 pivot rows, then a
+// rank-8 update).  Per column: one CTA barrier and one cluster barrier; the
+// pivot candidates and the pivot row are read over distributed shared
+// memory from double-buffered publish areas.
+template <typename R, int NB, int NT>
+__global__ void __launch_bounds__(NT, 1) k_panel_cluster(PanelArgs a) {
+  constexpr int RPT = 1;
   using E = typename Elt<R>::T;
   using C = cpx<R>;
+  constexpr int SW = 8;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* s_a = reinterpret_cast<C*>(smem_raw);   // [NB][rp] panel rows, column-major
-  C* s_pub = s_a + (size_t)NB * a.rp;        // [2][2][NB]: candidate row, row gj
+  C* s_a = reinterpret_cast<C*>(smem_raw);  // [NB][rp] panel rows, column-major
+  C* s_pub = s_a + (size_t)NB * a.rp;       // [2][2][NB]: candidate row, row gj
+  C* s_blk = s_pub + 4 * NB;                // [2][SW][NB]: a sub-panel's pivot rows
+  __shared__ C s_u[SW][NB];                 // U of the sub-panel's pivot rows
   __shared__ R s_pval[2];
   __shared__ int s_prow[2];
-  __shared__ C s_piv[NB], s_drow[NB];
-  __shared__ R s_rv[kPanelThreads / 32];
-  __shared__ int s_rr[kPanelThreads / 32];
-  __shared__ int s_win_row, s_win_rank;
+  __shared__ R s_rv[NT / 32];
+  __shared__ int s_rr[NT / 32];
   __shared__ int s_pdst[2 * NB], s_psrc[2 * NB];
   __shared__ int s_pcount;
 
@@ -245,7 +256,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(PanelArgs a)
   E* A = static_cast<E*>(a.A) + (size_t)prob * a.bstride;
   int* ipiv = a.ipiv + (size_t)prob * a.ipiv_stride;
   int* perm = a.perm + (size_t)prob * a.perm_stride;
-  const int rp = a.rp, w = a.w, k = a.k;
+  const int rp = a.rp, w = a.w, k = a.k, cs = a.cs;
   const int rbase = k + (int)rank * rp;
   const int rcount = max(0, min(rp, a.nn - rbase));
 
@@ -260,61 +271,232 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(PanelArgs a)
   if (rank == 0 && tid == 0) s_pcount = w;
   __syncthreads();
 
-  for (int j = 0; j < w; ++j) {
-    const int gj = k + j, par = j & 1;
-    const int owner = (gj - k) / rp;
-    R bv;
-    int br;
-    local_argmax<R>(s_a + j * rp, rcount, rbase, gj, s_rv, s_rr, bv, br);
-    C* cand = s_pub + (size_t)par * 2 * NB;
-    C* drow = cand + NB;
-    if (tid == 0) {
-      s_pval[par] = bv;
-      s_prow[par] = br;
-    }
-    if (br != INT_MAX && tid < w) cand[tid] = s_a[tid * rp + (br - rbase)];
-    if ((int)rank == owner && tid < w) drow[tid] = s_a[tid * rp + (gj - rbase)];
-    cluster_sync();
-    if (warp == 0) {
-      R v = R(-1);
-      int rr = INT_MAX, cb = 0;
-      if (lane < a.cs) {
-        v = dsm_ld(&s_pval[par], lane);
-        rr = dsm_ld(&s_prow[par], lane);
-        cb = lane;
+  // Global row of my q-th local row (INT_MAX when it does not exist).
+  int grow[RPT];
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) {
+    const int lr = tid + NT * q;
+    grow[q] = lr < rcount ? rbase + lr : INT_MAX;
+  }
+  C v[RPT][SW];
+
+  for (int s0 = 0; s0 < w; s0 += SW) {
+    const int sw = min(SW, w - s0);
+#pragma unroll
+    for (int q = 0; q < RPT; ++q)
+#pragma unroll
+      for (int c = 0; c < SW; ++c)
+        v[q][c] = (grow[q] != INT_MAX && c < sw) ? s_a[(s0 + c) * rp + (grow[q] - rbase)] : C{R(0), R(0)};
+
+    for (int jj = 0; jj < sw; ++jj) {
+      const int j = s0 + jj, gj = k + j, par = j & 1;
+      const int owner = j / rp;  // (gj - k) / rp
+      // 1. Candidate over my rows, then over the CTA.
+      R bv = R(-1);
+      int br = INT_MAX;
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        if (grow[q] != INT_MAX && grow[q] >= gj) {
+          C x = v[q][0];
+#pragma unroll
+          for (int c = 1; c < SW; ++c)
+            if (c == jj) x = v[q][c];
+          const R val = cabs1(x);
+          if (better(val, grow[q], bv, br)) {
+            bv = val;
+            br = grow[q];
+          }
+        }
       }
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {
-        const R ov = __shfl_xor_sync(0xffffffffu, v, off);
-        const int orr = __shfl_xor_sync(0xffffffffu, rr, off);
-        const int ocb = __shfl_xor_sync(0xffffffffu, cb, off);
-        if (better(ov, orr, v, rr)) {
-          v = ov;
-          rr = orr;
-          cb = ocb;
+        const R ov = __shfl_xor_sync(0xffffffffu, bv, off);
+        const int orr = __shfl_xor_sync(0xffffffffu, br, off);
+        if (better(ov, orr, bv, br)) {
+          bv = ov;
+          br = orr;
         }
       }
       if (lane == 0) {
-        s_win_row = rr;
-        s_win_rank = cb;
+        s_rv[warp] = bv;
+        s_rr[warp] = br;
+      }
+      __syncthreads();
+      R cv = s_rv[0];
+      int cr = s_rr[0];
+#pragma unroll
+      for (int q = 1; q < NT / 32; ++q)
+        if (better(s_rv[q], s_rr[q], cv, cr)) {
+          cv = s_rv[q];
+          cr = s_rr[q];
+        }
+      // 2. Publish the candidate row and, from its owner, row gj.
+      C* cand = s_pub + (size_t)par * 2 * NB;
+      C* drow = cand + NB;
+      if (tid == 0) {
+        s_pval[par] = cv;
+        s_prow[par] = cr;
+      }
+      if (cr != INT_MAX) {
+        const int lr = cr - rbase;
+        if (tid < w && (tid < s0 || tid >= s0 + sw)) cand[tid] = s_a[tid * rp + lr];
+        if (tid == (lr & (NT - 1))) {
+#pragma unroll
+          for (int q = 0; q < RPT; ++q)
+            if (q == (lr / NT))
+#pragma unroll
+              for (int c = 0; c < SW; ++c)
+                if (c < sw) cand[s0 + c] = v[q][c];
+        }
+      }
+      if ((int)rank == owner) {
+        const int lr = gj - rbase;
+        if (tid < w && (tid < s0 || tid >= s0 + sw)) drow[tid] = s_a[tid * rp + lr];
+        if (tid == (lr & (NT - 1))) {
+#pragma unroll
+          for (int q = 0; q < RPT; ++q)
+            if (q == (lr / NT))
+#pragma unroll
+              for (int c = 0; c < SW; ++c)
+                if (c < sw) drow[s0 + c] = v[q][c];
+        }
+      }
+      cluster_sync();
+      // 3. Winner (every warp reduces the cs candidates redundantly).
+      R wv = R(-1);
+      int wr = INT_MAX, wk = 0;
+      if (lane < cs) {
+        wv = dsm_ld(&s_pval[par], lane);
+        wr = dsm_ld(&s_prow[par], lane);
+        wk = lane;
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const R ov = __shfl_xor_sync(0xffffffffu, wv, off);
+        const int orr = __shfl_xor_sync(0xffffffffu, wr, off);
+        const int ok = __shfl_xor_sync(0xffffffffu, wk, off);
+        if (better(ov, orr, wv, wr)) {
+          wv = ov;
+          wr = orr;
+          wk = ok;
+        }
+      }
+      const int prow = wr;
+      const unsigned wrank = (unsigned)wk;
+      // Pivot row values of the sub-panel columns, broadcast to the warp.
+      C pl = (lane < sw) ? dsm_ld(&cand[s0 + lane], wrank) : C{R(0), R(0)};
+      C piv[SW];
+#pragma unroll
+      for (int c = 0; c < SW; ++c) {
+        piv[c].re = __shfl_sync(0xffffffffu, pl.re, c);
+        piv[c].im = __shfl_sync(0xffffffffu, pl.im, c);
+      }
+      // 4. Interchange rows gj and prow (whole panel rows).
+      if ((int)rank == owner) {  // row gj <- pivot row
+        const int lr = gj - rbase;
+        if (tid < w && (tid < s0 || tid >= s0 + sw)) s_a[tid * rp + lr] = dsm_ld(&cand[tid], wrank);
+        if (tid == (lr & (NT - 1))) {
+#pragma unroll
+          for (int q = 0; q < RPT; ++q)
+            if (q == (lr / NT))
+#pragma unroll
+              for (int c = 0; c < SW; ++c) v[q][c] = piv[c];
+        }
+      }
+      if (prow != gj && prow >= rbase && prow < rbase + rcount) {  // row prow <- old row gj
+        const int lr = prow - rbase;
+        if (tid < w && (tid < s0 || tid >= s0 + sw)) s_a[tid * rp + lr] = dsm_ld(&drow[tid], (unsigned)owner);
+        if (tid == (lr & (NT - 1))) {
+#pragma unroll
+          for (int q = 0; q < RPT; ++q)
+            if (q == (lr / NT))
+#pragma unroll
+              for (int c = 0; c < SW; ++c)
+                if (c < sw) v[q][c] = dsm_ld(&drow[s0 + c], (unsigned)owner);
+        }
+      }
+      if (rank == 0 && tid == 0) {
+        ipiv[gj] = prow + 1;
+        perm_swap(s_pdst, s_psrc, s_pcount, k, w, j, prow);
+      }
+      // 5. Multipliers and the rank-1 update of the sub-panel, in registers.
+      C pj = piv[0];
+#pragma unroll
+      for (int c = 1; c < SW; ++c)
+        if (c == jj) pj = piv[c];
+      const bool zero = (pj.re == R(0) && pj.im == R(0));
+      if (zero && rank == 0 && tid == 0) atomicCAS(&a.status[ST_SINGULAR], 0, gj + 1);
+      const C rpv = zero ? C{R(0), R(0)} : crcp(pj);
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        if (grow[q] != INT_MAX && grow[q] > gj) {
+          C l = v[q][0];
+#pragma unroll
+          for (int c = 1; c < SW; ++c)
+            if (c == jj) l = v[q][c];
+          l = l * rpv;
+#pragma unroll
+          for (int c = 0; c < SW; ++c) {
+            if (c == jj) v[q][c] = l;
+            if (c > jj) cfms(v[q][c], l, piv[c]);
+          }
+        }
+      }
+    }
+    // End of the sub-panel: registers back to shared memory.
+#pragma unroll
+    for (int q = 0; q < RPT; ++q)
+      if (grow[q] != INT_MAX)
+#pragma unroll
+        for (int c = 0; c < SW; ++c)
+          if (c < sw) s_a[(s0 + c) * rp + (grow[q] - rbase)] = v[q][c];
+    if (s0 + sw >= w) break;
+    // Publish this sub-panel's pivot rows (global rows k+s0 .. k+s0+sw-1).
+    const int bpar = (s0 / SW) & 1;
+    C* blk = s_blk + (size_t)bpar * SW * NB;
+    __syncthreads();
+    for (int idx = tid; idx < sw * w; idx += blockDim.x) {
+      const int i = idx / w, c = idx % w;
+      const int gr = k + s0 + i;
+      if (gr >= rbase && gr < rbase + rcount) blk[i * NB + c] = s_a[c * rp + (gr - rbase)];
+    }
+    cluster_sync();
+    for (int idx = tid; idx < sw * w; idx += blockDim.x) {
+      const int i = idx / w, c = idx % w;
+      s_u[i][c] = dsm_ld(&blk[i * NB + c], (unsigned)((s0 + i) / rp));
+    }
+    __syncthreads();
+    // U of the pivot rows for the columns right of the sub-panel:
+    // U(i,c) = A(i,c) - sum_{t<i} L(i,t) U(t,c), L = the sub-panel's unit lower.
+    for (int c = s0 + sw + tid; c < w; c += blockDim.x)
+      for (int i = 1; i < sw; ++i) {
+        C x = s_u[i][c];
+        for (int t = 0; t < i; ++t) cfms(x, s_u[i][s0 + t], s_u[t][c]);
+        s_u[i][c] = x;
+      }
+    __syncthreads();
+    // Rank-sw update of my rows in the columns right of the sub-panel; the
+    // pivot rows themselves take their U values.
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      const int gr = grow[q];
+      const int lr = gr - rbase;
+      if (gr != INT_MAX && gr >= k + s0 + sw) {
+        for (int c = s0 + sw; c < w; ++c) {
+          C x = s_a[c * rp + lr];
+#pragma unroll
+          for (int t = 0; t < SW; ++t)
+            if (t < sw) cfms(x, v[q][t], s_u[t][c]);
+          s_a[c * rp + lr] = x;
+        }
+      } else if (gr != INT_MAX && gr >= k + s0) {
+        const int i = gr - k - s0;
+        for (int c = s0 + sw; c < w; ++c) s_a[c * rp + lr] = s_u[i][c];
       }
     }
     __syncthreads();
-    const int prow = s_win_row;
-    if (tid < w) {
-      s_piv[tid] = dsm_ld(&cand[tid], (unsigned)s_win_rank);
-      s_drow[tid] = dsm_ld(&drow[tid], (unsigned)owner);
-    }
-    __syncthreads();
-    if (prow != gj && prow >= rbase && prow < rbase + rcount && tid < w) s_a[tid * rp + (prow - rbase)] = s_drow[tid];
-    if ((int)rank == owner && tid < w) s_a[tid * rp + (gj - rbase)] = s_piv[tid];
-    if (rank == 0 && tid == 0) {
-      ipiv[gj] = prow + 1;
-      perm_swap(s_pdst, s_psrc, s_pcount, k, w, j, prow);
-    }
-    __syncthreads();
-    eliminate<R>(s_a, rp, rcount, rbase, gj, j, w, s_piv, a.status, rank == 0);
   }
+  __syncthreads();
   for (int idx = tid; idx < w * rcount; idx += blockDim.x) {
     const int c = idx / rcount, r = idx % rcount;
     stc<R>(&A[(size_t)(k + c) * a.lda + rbase + r], s_a[c * rp + r]);
@@ -839,15 +1021,15 @@ int lu_ensure_workspace(bem_ctx* ctx, int nn, int batch) {
 
 constexpr size_t kPanelSmemBudget = 220 * 1024;
 
-template <typename R, int NB>
+template <typename R, int NB, int NT>
 static int launch_cluster_panel(bem_ctx* ctx, const PanelArgs& pa, int batch) {
-  const size_t smem = ((size_t)NB * pa.rp + 4 * NB) * sizeof(cpx<R>);
-  auto kern = k_panel_cluster<R, NB>;
+  const size_t smem = ((size_t)NB * pa.rp + 4 * NB + 2 * 8 * NB) * sizeof(cpx<R>);
+  auto kern = k_panel_cluster<R, NB, NT>;
   BEM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   BEM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(pa.cs, batch, 1);
-  cfg.blockDim = dim3(kPanelThreads, 1, 1);
+  cfg.blockDim = dim3(NT, 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = ctx->stream;
   cudaLaunchAttribute attr[1];
@@ -859,6 +1041,37 @@ static int launch_cluster_panel(bem_ctx* ctx, const PanelArgs& pa, int batch) {
   cfg.numAttrs = 1;
   BEM_CUDA(ctx, cudaLaunchKernelEx(&cfg, kern, pa));
   return BEM_OK;
+}
+
+// Does a panel of width NB with rp rows per CTA fit one CTA's shared memory?
+template <typename R, int NB, int NT>
+static bool cluster_panel_fits(int rp) {
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, k_panel_cluster<R, NB, NT>) != cudaSuccess) return false;
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const size_t dyn = ((size_t)NB * rp + 4 * NB + 2 * 8 * NB) * sizeof(cpx<R>);
+  return dyn + fa.sharedSizeBytes + 1024 <= (size_t)optin;
+}
+
+template <typename R>
+static bool cluster_panel_fits_any(int nb, int rp) {
+  const bool big = rp > 256;
+  if (nb == 64) return big ? cluster_panel_fits<R, 64, 512>(rp) : cluster_panel_fits<R, 64, 256>(rp);
+  if (nb == 32) return big ? cluster_panel_fits<R, 32, 512>(rp) : cluster_panel_fits<R, 32, 256>(rp);
+  if (nb == 16) return big ? cluster_panel_fits<R, 16, 512>(rp) : cluster_panel_fits<R, 16, 256>(rp);
+  return false;
+}
+
+// Dispatch on (panel width, threads = rows per CTA rounded up to 256 or 512).
+template <typename R>
+static int launch_cluster_panel_any(bem_ctx* ctx, const PanelArgs& pa, int batch, int nb) {
+  const bool big = pa.rp > 256;
+  if (nb == 64) return big ? launch_cluster_panel<R, 64, 512>(ctx, pa, batch) : launch_cluster_panel<R, 64, 256>(ctx, pa, batch);
+  if (nb == 32) return big ? launch_cluster_panel<R, 32, 512>(ctx, pa, batch) : launch_cluster_panel<R, 32, 256>(ctx, pa, batch);
+  if (nb == 16) return big ? launch_cluster_panel<R, 16, 512>(ctx, pa, batch) : launch_cluster_panel<R, 16, 256>(ctx, pa, batch);
+  return fail(ctx, BEM_ERR_ARG, "no cluster panel variant for this size");
 }
 
 template <typename R, int NB>
@@ -877,12 +1090,12 @@ static int launch_grid_panel(bem_ctx* ctx, PanelArgs pa) {
 static int cluster_size(bem_ctx* ctx) {
   if (ctx->lu.cluster_cs) return ctx->lu.cluster_cs;
   int cs = 8;
-  auto kern = k_panel_cluster<double, 32>;
+  auto kern = k_panel_cluster<double, 32, 512>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemBudget);
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(16, 1, 1);
-    cfg.blockDim = dim3(kPanelThreads, 1, 1);
+    cfg.blockDim = dim3(512, 1, 1);
     cfg.dynamicSmemBytes = kPanelSmemBudget;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -926,14 +1139,16 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     pa.perm = perm_p;
     pa.perm_stride = kPermStride;
     pa.status = ctx->d_status;
-    // Panel width: the widest of 64/32/16 whose rows fit one cluster.
+    // Panel width: the widest of 64/32/16 whose rows fit one cluster, at most
+    // 512 rows per CTA (one row per thread).
     const int rp_c = (m + cs - 1) / cs;
     int nb = 0;
-    for (int cand : {64, 32, 16})
-      if (((size_t)cand * rp_c + 4 * cand) * es <= kPanelSmemBudget) {
-        nb = cand;
-        break;
-      }
+    if (rp_c <= 512)
+      for (int cand : {64, 32, 16})
+        if (cluster_panel_fits_any<R>(cand, rp_c)) {
+          nb = cand;
+          break;
+        }
     int w;
     {
       ProfScope ps(ctx, 1, 0.0);
@@ -942,9 +1157,7 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
         pa.w = w;
         pa.rp = rp_c;
         pa.cs = cs;  // CTAs past the last row own no rows but join every barrier
-        int rc = (nb == 64) ? launch_cluster_panel<R, 64>(ctx, pa, batch)
-                 : (nb == 32) ? launch_cluster_panel<R, 32>(ctx, pa, batch)
-                              : launch_cluster_panel<R, 16>(ctx, pa, batch);
+        int rc = launch_cluster_panel_any<R>(ctx, pa, batch, nb);
         if (rc) return rc;
         ctx->launches++;
       } else {
