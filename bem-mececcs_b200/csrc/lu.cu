@@ -250,6 +250,9 @@ __global__ void __launch_bounds__(NT, 1) k_panel_cluster(PanelArgs a) {
   __shared__ int s_rr[NT / 32];
   __shared__ int s_pdst[2 * NB], s_psrc[2 * NB];
   __shared__ int s_pcount;
+  __shared__ int s_ipiv[NB];
+  __shared__ C s_pv[8];        // pivot row, sub-panel columns
+  __shared__ int s_win[2];     // winner row, winner rank
 
   const unsigned rank = cluster_rank();
   const int prob = blockIdx.y, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -362,35 +365,52 @@ __global__ void __launch_bounds__(NT, 1) k_panel_cluster(PanelArgs a) {
         }
       }
       cluster_sync();
-      // 3. Winner (every warp reduces the cs candidates redundantly).
-      R wv = R(-1);
-      int wr = INT_MAX, wk = 0;
-      if (lane < cs) {
-        wv = dsm_ld(&s_pval[par], lane);
-        wr = dsm_ld(&s_prow[par], lane);
-        wk = lane;
-      }
+      // 3. Winner: warp 0 reads every CTA's candidate (value, row and its 8
+      //    sub-panel values) in one round of remote loads, reduces, and
+      //    broadcasts through shared memory.
+      if (warp == 0) {
+        R wv = R(-1);
+        int wr = INT_MAX, wk = 0;
+        C cvals[SW];
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const R ov = __shfl_xor_sync(0xffffffffu, wv, off);
-        const int orr = __shfl_xor_sync(0xffffffffu, wr, off);
-        const int ok = __shfl_xor_sync(0xffffffffu, wk, off);
-        if (better(ov, orr, wv, wr)) {
-          wv = ov;
-          wr = orr;
-          wk = ok;
+        for (int c = 0; c < SW; ++c) cvals[c] = C{R(0), R(0)};
+        if (lane < cs) {
+          wv = dsm_ld(&s_pval[par], lane);
+          wr = dsm_ld(&s_prow[par], lane);
+          wk = lane;
+#pragma unroll
+          for (int c = 0; c < SW; ++c)
+            if (c < sw) cvals[c] = dsm_ld(&cand[s0 + c], lane);
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          const R ov = __shfl_xor_sync(0xffffffffu, wv, off);
+          const int orr = __shfl_xor_sync(0xffffffffu, wr, off);
+          const int ok = __shfl_xor_sync(0xffffffffu, wk, off);
+          if (better(ov, orr, wv, wr)) {
+            wv = ov;
+            wr = orr;
+            wk = ok;
+          }
+        }
+        // Lane wk holds the winner's values.
+#pragma unroll
+        for (int c = 0; c < SW; ++c) {
+          const R re = __shfl_sync(0xffffffffu, cvals[c].re, wk);
+          const R im = __shfl_sync(0xffffffffu, cvals[c].im, wk);
+          if (lane == c) s_pv[c] = C{re, im};
+        }
+        if (lane == 0) {
+          s_win[0] = wr;
+          s_win[1] = wk;
         }
       }
-      const int prow = wr;
-      const unsigned wrank = (unsigned)wk;
-      // Pivot row values of the sub-panel columns, broadcast to the warp.
-      C pl = (lane < sw) ? dsm_ld(&cand[s0 + lane], wrank) : C{R(0), R(0)};
+      __syncthreads();
+      const int prow = s_win[0];
+      const unsigned wrank = (unsigned)s_win[1];
       C piv[SW];
 #pragma unroll
-      for (int c = 0; c < SW; ++c) {
-        piv[c].re = __shfl_sync(0xffffffffu, pl.re, c);
-        piv[c].im = __shfl_sync(0xffffffffu, pl.im, c);
-      }
+      for (int c = 0; c < SW; ++c) piv[c] = s_pv[c];
       // 4. Interchange rows gj and prow (whole panel rows).
       if ((int)rank == owner) {  // row gj <- pivot row
         const int lr = gj - rbase;
@@ -416,7 +436,7 @@ __global__ void __launch_bounds__(NT, 1) k_panel_cluster(PanelArgs a) {
         }
       }
       if (rank == 0 && tid == 0) {
-        ipiv[gj] = prow + 1;
+        s_ipiv[j] = prow + 1;
         perm_swap(s_pdst, s_psrc, s_pcount, k, w, j, prow);
       }
       // 5. Multipliers and the rank-1 update of the sub-panel, in registers.
@@ -502,6 +522,7 @@ __global__ void __launch_bounds__(NT, 1) k_panel_cluster(PanelArgs a) {
     stc<R>(&A[(size_t)(k + c) * a.lda + rbase + r], s_a[c * rp + r]);
   }
   if (rank == 0) {
+    if (tid < w) ipiv[k + tid] = s_ipiv[tid];
     if (tid == 0) perm[0] = s_pcount;
     for (int e = tid; e < s_pcount; e += blockDim.x) {
       perm[1 + 2 * e] = s_pdst[e];
