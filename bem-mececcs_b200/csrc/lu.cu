@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(NT, 1) k_panel_cluster(PanelArgs a) {
 #pragma unroll
       for (int c = 0; c < SW; ++c) piv[c] = s_pv[c];
       // 4. Interchange rows gj and prow (whole panel rows).
-      if ((int)rank == owner) {  // row gj <- pivot row
+      if ((int)rank == owner && prow != gj) {  // row gj <- pivot row
         const int lr = gj - rbase;
         if (tid < w && (tid < s0 || tid >= s0 + sw)) s_a[tid * rp + lr] = dsm_ld(&cand[tid], wrank);
         if (tid == (lr & (NT - 1))) {
