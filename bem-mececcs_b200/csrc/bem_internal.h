@@ -89,6 +89,15 @@ struct LuWork {
 
 constexpr int kMaxGrid = 160;
 
+// Packed operands of the tensor-core FP32 trailing update (gemm_tc.cu).
+struct TcWork {
+  int nn = 0, batch = 0;
+  float* lhat = nullptr;  // [batch][2nn][64]  re/im rows of L21, TF32
+  float* ure = nullptr;   // [batch][nn+1][64] Re U12, K-major, TF32
+  float* uim = nullptr;   // [batch][nn+1][64] Im U12
+  void* maps = nullptr;   // 3 TMA tensor maps (host copies, passed by value)
+};
+
 // CUDA-event timing per kernel class (off unless enabled).
 struct Profiler {
   bool on = false;
@@ -144,6 +153,8 @@ struct bem_ctx {
   int static_chunks = 0;
   bem::Profiler prof;
   bem::SweepBuf sweep;
+  bem::TcWork tc;
+  bool use_tcgen05 = true;  // FP32 trailing update on tcgen05 (else TF32 mma.sync)
 };
 
 namespace bem {
@@ -182,6 +193,11 @@ int lu_solve_vec(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int 
 int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], const double c[4],
           const double* freqs, int nfreq, int form, int batch, int iters, double* x_out, double* corr_out);
 void release_sweep(bem_ctx* ctx);
+
+// Tensor-core FP32 trailing update (gemm_tc.cu).
+int tc_ensure(bem_ctx* ctx, int nn, int batch);
+void tc_release(bem_ctx* ctx);
+int tc_trailing_update(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int k, int w, int batch);
 int measure_fp64_peak(bem_ctx* ctx, double* tflops);
 
 int check_status(bem_ctx* ctx);

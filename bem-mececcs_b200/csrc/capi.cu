@@ -137,6 +137,7 @@ int bem_ctx_create(int device, bem_ctx** out) {
     return e == cudaErrorMemoryAllocation ? BEM_ERR_NOMEM : BEM_ERR_CUDA;
   }
   ctx->stream = ctx->own_stream;
+  if (const char* env = getenv("BEM_TF32_MMA_SYNC")) ctx->use_tcgen05 = env[0] != '1';
   *out = ctx;
   return BEM_OK;
 }
@@ -162,6 +163,7 @@ int bem_ctx_destroy(bem_ctx* ctx) {
   cudaFree(L.drow);
   cudaFree(L.barrier);
   release_sweep(ctx);
+  tc_release(ctx);
   for (cudaEvent_t e : ctx->prof.pool) cudaEventDestroy(e);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;

@@ -1,0 +1,372 @@
+// gemm_tc.cu -- FP32 LU trailing update on the 5th-generation tensor cores.
+//
+// C (complex64, column-major) -= L21 * U12 for one panel step of the FP32 LU,
+// with TF32 operands and FP32 accumulation in tensor memory.
+//
+// Complex as real GEMMs: the panel L21 (m x k complex) is viewed as a real
+// matrix Lhat of 2m rows (row 2r = Re L(r,:), row 2r+1 = Im L(r,:)); U12 is
+// split into U_re and U_im (k x n each).  Then
+//   D1 = Lhat * U_re,   D2 = Lhat * U_im        (2m x n real, FP32)
+//   Re C(r,j) -= D1(2r,j) - D2(2r+1,j),  Im C(r,j) -= D2(2r,j) + D1(2r+1,j).
+// Both operands are packed K-major (64 FP32 per row, rounded to TF32) once
+// per panel step: Lhat by k_pack_l21, U_re/U_im by the row-interchange +
+// triangular-solve kernel.
+//
+// k_gemm_tc: persistent, one CTA per SM, 8 warps.  Warp 0 issues TMA loads
+// (128-byte swizzle, no multicast) into a 2-stage ring; warp 1 allocates 512
+// TMEM columns and one elected thread issues tcgen05.mma (M=128, N=128, K=8,
+// kind::tf32) into double-buffered accumulators; warps 4-7 read the
+// accumulators with tcgen05.ld, combine real and imaginary parts with one
+// lane shuffle and update C in place.  Every mbarrier wait is bounded; on
+// timeout the kernel records ST_TIMEOUT and drains.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "bem_internal.h"
+
+namespace bem {
+
+namespace {
+
+constexpr int kTcRows = 64;        // complex rows per tile (UMMA M = 128 real rows)
+constexpr int kTcCols = 128;       // columns per tile (UMMA N)
+constexpr uint32_t kBox = 128 * 128;  // one box: 128 rows x 32 floats = 16 KB
+constexpr uint32_t kStageBytes = 6 * kBox;  // Lhat, U_re, U_im, 2 K-halves each
+constexpr int kStages = 2;
+constexpr uint32_t kTmemCols = 512;
+constexpr size_t kTcSmem = (size_t)kStages * kStageBytes + 1024;
+
+__device__ __forceinline__ uint32_t idesc_tf32_128x128() {
+  // c_format F32 (bit 4), a/b format TF32 = 2 (bits 7, 10), K-major A and B,
+  // N >> 3 at bit 17, M >> 4 at bit 24.
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcCols >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (SBO), version 1.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+struct TcArgs {
+  float2* A;        // the systems (complex64), problem b at A + b*bstride
+  size_t lda, bstride;
+  int nn, r0, c0, ncols, kw;
+  int mtiles, ntiles, batch;
+  int lrows;        // Lhat rows per problem (2*nn)
+  int urows;        // U rows per problem (nn+1)
+  int* status;
+};
+
+// Bounded wait; on timeout raise the kernel-wide abort flag and the status word.
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* status) {
+  if (*abort_flag) return false;
+  if (mbar_wait(bar, parity)) return true;
+  *abort_flag = 1;
+  atomicExch(&status[ST_TIMEOUT], 1);
+  return false;
+}
+
+__global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUtensorMap tm_l,
+                                                    const __grid_constant__ CUtensorMap tm_ure,
+                                                    const __grid_constant__ CUtensorMap tm_uim, TcArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  __shared__ uint64_t full_bar[kStages], empty_bar[kStages], tfull_bar[2], tempty_bar[2];
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_abort;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int total = a.mtiles * a.ntiles * a.batch;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&tfull_bar[s], 1);
+      mbar_init(&tempty_bar[s], 4);
+    }
+    s_abort = 0;
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  const int ksteps = (a.kw + 7) / 8;
+  const int boxes = (a.kw + 31) / 32;
+  volatile int* abort_flag = &s_abort;
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer ----
+    int it = 0;
+    for (int t = blockIdx.x; t < total; t += gridDim.x, ++it) {
+      const int s = it % kStages;
+      const uint32_t ph = (uint32_t)(it / kStages) & 1u;
+      if (!wait_or_abort(&empty_bar[s], ph ^ 1u, abort_flag, a.status)) break;
+      const int b = t / (a.mtiles * a.ntiles);
+      const int rem = t % (a.mtiles * a.ntiles);
+      const int tm = rem % a.mtiles, tn = rem / a.mtiles;
+      unsigned char* st = smem + (size_t)s * kStageBytes;
+      mbar_expect_tx(&full_bar[s], (uint32_t)boxes * 3u * kBox);
+      const int ly = b * a.lrows + 2 * tm * kTcRows;
+      const int uy = b * a.urows + tn * kTcCols;
+      for (int h = 0; h < boxes; ++h) {
+        tma_load_2d(st + (0 + h) * kBox, &tm_l, 32 * h, ly, &full_bar[s]);
+        tma_load_2d(st + (2 + h) * kBox, &tm_ure, 32 * h, uy, &full_bar[s]);
+        tma_load_2d(st + (4 + h) * kBox, &tm_uim, 32 * h, uy, &full_bar[s]);
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer ----
+    const uint32_t idesc = idesc_tf32_128x128();
+    int it = 0;
+    for (int t = blockIdx.x; t < total; t += gridDim.x, ++it) {
+      const int s = it % kStages;
+      const uint32_t ph = (uint32_t)(it / kStages) & 1u;
+      const int buf = it & 1;
+      const uint32_t bph = (uint32_t)(it >> 1) & 1u;
+      if (!wait_or_abort(&tempty_bar[buf], bph ^ 1u, abort_flag, a.status)) break;
+      tc_fence_after();
+      if (!wait_or_abort(&full_bar[s], ph, abort_flag, a.status)) break;
+      tc_fence_after();
+      const uint32_t sbase = smem_u32(smem + (size_t)s * kStageBytes);
+      const uint32_t d1 = tmem + (uint32_t)buf * 256u, d2 = d1 + 128u;
+      for (int kk = 0; kk < ksteps; ++kk) {
+        const uint32_t off = (uint32_t)(kk >> 2) * kBox + (uint32_t)(kk & 3) * 32u;
+        const uint64_t da = sdesc(sbase + 0 * kBox + off);
+        const uint64_t dre = sdesc(sbase + 2 * kBox + off);
+        const uint64_t dim = sdesc(sbase + 4 * kBox + off);
+        umma_tf32(d1, da, dre, idesc, kk > 0 ? 1u : 0u);
+        umma_tf32(d2, da, dim, idesc, kk > 0 ? 1u : 0u);
+      }
+      umma_commit(&empty_bar[s]);
+      umma_commit(&tfull_bar[buf]);
+    }
+  } else if (warp >= 4) {
+    // ---- epilogue: TMEM -> registers -> C -= D ----
+    const int e = warp - 4;
+    int it = 0;
+    for (int t = blockIdx.x; t < total; t += gridDim.x, ++it) {
+      const int buf = it & 1;
+      const uint32_t bph = (uint32_t)(it >> 1) & 1u;
+      bool ok = true;
+      if (lane == 0) ok = wait_or_abort(&tfull_bar[buf], bph, abort_flag, a.status);
+      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+      if (!ok) break;
+      tc_fence_after();
+      const int b = t / (a.mtiles * a.ntiles);
+      const int rem = t % (a.mtiles * a.ntiles);
+      const int tm = rem % a.mtiles, tn = rem / a.mtiles;
+      const int r = a.r0 + tm * kTcRows + 16 * e + (lane >> 1);
+      const int p = lane & 1;
+      float* C = reinterpret_cast<float*>(a.A + (size_t)b * a.bstride);
+      const uint32_t tbase = tmem + (uint32_t)buf * 256u + ((uint32_t)(32 * e) << 16);
+      for (int c = 0; c < kTcCols; c += 16) {
+        float v1[16], v2[16];
+        tmem_ld16(tbase + (uint32_t)c, v1);
+        tmem_ld16(tbase + 128u + (uint32_t)c, v2);
+        tmem_ld_wait();
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const float x = __shfl_xor_sync(0xffffffffu, v2[i], 1);
+          const float val = p ? (v1[i] + x) : (v1[i] - x);
+          const int col = a.c0 + tn * kTcCols + c + i;
+          if (r < a.nn && col < a.ncols) {
+            float* q = C + 2 * ((size_t)col * a.lda + r) + p;
+            *q -= val;
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty_bar[buf]);
+    }
+  }
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  }
+}
+
+// Lhat: rows 2(r - r0) + p of problem b hold part p of L(r, k..k+kw-1),
+// rounded to TF32, zero-padded to 64 columns.  32 rows x 64 columns per CTA
+// through a shared transpose so reads and writes are both coalesced.
+__global__ void __launch_bounds__(256) k_pack_l21(const float2* __restrict__ A, size_t lda, size_t bstride, int nn,
+                                                  int k, int kw, int r0, float* lhat, int lrows) {
+  __shared__ float2 tile[64][33];
+  const int b = blockIdx.y;
+  const float2* Ap = A + (size_t)b * bstride;
+  const int rbase = r0 + blockIdx.x * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 8 x 32
+  for (int c = ty; c < 64; c += 8) {
+    const int r = rbase + tx;
+    float2 v = make_float2(0.f, 0.f);
+    if (c < kw && r < nn) v = Ap[(size_t)(k + c) * lda + r];
+    tile[c][tx] = v;
+  }
+  __syncthreads();
+  float* out = lhat + (size_t)b * lrows * 64;
+  for (int idx = threadIdx.x; idx < 32 * 2 * 64; idx += blockDim.x) {
+    const int c = idx & 63, rr = idx >> 6;  // rr = 2*local_row + part
+    const int lr = rr >> 1, p = rr & 1;
+    const int r = rbase + lr;
+    if (r >= nn) continue;
+    const float2 v = tile[c][lr];
+    const float x = p ? v.y : v.x;
+    unsigned t;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(x));
+    out[(size_t)(2 * (r - r0) + p) * 64 + c] = __uint_as_float(t);
+  }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// 2-D map over `rows` rows of 64 floats (256-byte rows), 32 x 128 boxes, 128B swizzle.
+bool make_map(CUtensorMap* m, float* base, size_t rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {64, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {64 * sizeof(float)};
+  cuuint32_t box[2] = {32, 128};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+int tc_ensure(bem_ctx* ctx, int nn, int batch) {
+  TcWork& W = ctx->tc;
+  if (W.nn == nn && W.batch >= batch && W.lhat) return BEM_OK;
+  cudaFree(W.lhat);
+  cudaFree(W.ure);
+  cudaFree(W.uim);
+  W = TcWork{};
+  const size_t lrows = (size_t)2 * nn * batch, urows = (size_t)(nn + 1) * batch;
+  BEM_CUDA(ctx, cudaMalloc(&W.lhat, lrows * 64 * sizeof(float)));
+  BEM_CUDA(ctx, cudaMalloc(&W.ure, urows * 64 * sizeof(float)));
+  BEM_CUDA(ctx, cudaMalloc(&W.uim, urows * 64 * sizeof(float)));
+  BEM_CUDA(ctx, cudaMemset(W.lhat, 0, lrows * 64 * sizeof(float)));
+  BEM_CUDA(ctx, cudaMemset(W.ure, 0, urows * 64 * sizeof(float)));
+  BEM_CUDA(ctx, cudaMemset(W.uim, 0, urows * 64 * sizeof(float)));
+  W.maps = new CUtensorMap[3];
+  CUtensorMap* maps = static_cast<CUtensorMap*>(W.maps);
+  if (!make_map(&maps[0], W.lhat, lrows) || !make_map(&maps[1], W.ure, urows) || !make_map(&maps[2], W.uim, urows))
+    return fail(ctx, BEM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  W.nn = nn;
+  W.batch = batch;
+  BEM_CUDA(ctx, cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+  return BEM_OK;
+}
+
+void tc_release(bem_ctx* ctx) {
+  TcWork& W = ctx->tc;
+  cudaFree(W.lhat);
+  cudaFree(W.ure);
+  cudaFree(W.uim);
+  delete[] static_cast<CUtensorMap*>(W.maps);
+  W = TcWork{};
+}
+
+// C -= L21 U12 for rows [r0, nn) and columns [c0, ncols) of `batch` FP32
+// systems; U_re/U_im must already hold the step's U12 (rows c - c0).
+int tc_trailing_update(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int k, int w, int batch) {
+  TcWork& W = ctx->tc;
+  const int r0 = k + w, c0 = k + w, ncols = nn + 1;
+  if (r0 >= nn) return BEM_OK;
+  k_pack_l21<<<dim3((nn - r0 + 31) / 32, batch), 256, 0, ctx->stream>>>(A, lda, bstride, nn, k, w, r0, W.lhat,
+                                                                        2 * nn);
+  ctx->launches++;
+  TcArgs t{};
+  t.A = A;
+  t.lda = lda;
+  t.bstride = bstride;
+  t.nn = nn;
+  t.r0 = r0;
+  t.c0 = c0;
+  t.ncols = ncols;
+  t.kw = w;
+  t.mtiles = (nn - r0 + kTcRows - 1) / kTcRows;
+  t.ntiles = (ncols - c0 + kTcCols - 1) / kTcCols;
+  t.batch = batch;
+  t.lrows = 2 * nn;
+  t.urows = nn + 1;
+  t.status = ctx->d_status;
+  const int total = t.mtiles * t.ntiles * batch;
+  const int grid = std::min(total, ctx->num_sms);
+  CUtensorMap* maps = static_cast<CUtensorMap*>(W.maps);
+  k_gemm_tc<<<grid, 256, kTcSmem, ctx->stream>>>(maps[0], maps[1], maps[2], t);
+  ctx->launches++;
+  BEM_CUDA(ctx, cudaGetLastError());
+  return BEM_OK;
+}
+
+}  // namespace bem

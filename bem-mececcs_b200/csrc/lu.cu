@@ -645,7 +645,8 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel_grid(PanelArgs a) {
 // then U12 = L11^-1 A12 (unit lower).  One warp per column; problem = blockIdx.y.
 template <typename R>
 __global__ void __launch_bounds__(256) k_laswp_trsm(void* Av, size_t lda, size_t bstride, int k, int w, int c0,
-                                                    int ncols, const int* __restrict__ perm, int perm_stride) {
+                                                    int ncols, const int* __restrict__ perm, int perm_stride,
+                                                    float* ure, float* uim, int urows) {
   using E = typename Elt<R>::T;
   using C = cpx<R>;
   constexpr int NB = 64;
@@ -690,6 +691,21 @@ __global__ void __launch_bounds__(256) k_laswp_trsm(void* Av, size_t lda, size_t
     }
     if (lane < w) stc<R>(&cp[k + lane], v0);
     if (lane + 32 < w) stc<R>(&cp[k + lane + 32], v1);
+    if (ure) {
+      // Packed K-major copies of U12 for the tensor-core update, rounded to TF32.
+      const size_t row = ((size_t)blockIdx.y * urows + (col - c0)) * 64;
+      const float r0 = lane < w ? (float)v0.re : 0.f, i0 = lane < w ? (float)v0.im : 0.f;
+      const float r1 = lane + 32 < w ? (float)v1.re : 0.f, i1 = lane + 32 < w ? (float)v1.im : 0.f;
+      unsigned t0, t1, t2, t3;
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t0) : "f"(r0));
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t1) : "f"(r1));
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t2) : "f"(i0));
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t3) : "f"(i1));
+      ure[row + lane] = __uint_as_float(t0);
+      ure[row + lane + 32] = __uint_as_float(t1);
+      uim[row + lane] = __uint_as_float(t2);
+      uim[row + lane + 32] = __uint_as_float(t3);
+    }
   }
 }
 
@@ -1145,6 +1161,10 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
   BEM_CUDA(ctx, cudaFuncSetAttribute(k_backsub<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem));
   BEM_CUDA(ctx, cudaFuncSetAttribute(k_gemm_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
   BEM_CUDA(ctx, cudaFuncSetAttribute(k_gemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmTf32Smem));
+  if (sizeof(R) == 4 && ctx->use_tcgen05) {
+    int rc = tc_ensure(ctx, nn, batch);
+    if (rc) return rc;
+  }
   L.panels.clear();
   for (int k = 0; k < nn;) {
     const int m = nn - k;
@@ -1215,16 +1235,21 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     if (c0 < ncols) {
       const int cols = ncols - c0;
       const int blocks = std::max(1, std::min((cols + 7) / 8, (4 * ctx->num_sms + batch - 1) / batch));
+      const bool tc = sizeof(R) == 4 && ctx->use_tcgen05;
       {
         ProfScope ps(ctx, 2, 0.0);
-        k_laswp_trsm<R><<<dim3(blocks, batch), 256, lsmem, ctx->stream>>>(A, lda, bstride, k, w, c0, ncols, perm_p,
-                                                                           kPermStride);
+        k_laswp_trsm<R><<<dim3(blocks, batch), 256, lsmem, ctx->stream>>>(
+            A, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, tc ? ctx->tc.ure : nullptr,
+            tc ? ctx->tc.uim : nullptr, nn + 1);
       }
       ctx->launches++;
       BEM_CUDA(ctx, cudaGetLastError());
       if (c0 < nn) {
         ProfScope ps(ctx, 3, 8.0 * (double)(nn - c0) * (double)cols * (double)w * batch);
-        if (sizeof(R) == 8) {
+        if (tc) {
+          int rc = tc_trailing_update(ctx, static_cast<float2*>(A), lda, bstride, nn, k, w, batch);
+          if (rc) return rc;
+        } else if (sizeof(R) == 8) {
           dim3 grid((nn - c0 + GBM - 1) / GBM, (cols + GBN - 1) / GBN, batch);
           k_gemm_f64<<<grid, 256, kGemmSmem, ctx->stream>>>(static_cast<double2*>(A), lda, bstride, nn, k, w, c0, c0,
                                                            ncols);
