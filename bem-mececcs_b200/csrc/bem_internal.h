@@ -95,7 +95,10 @@ struct TcWork {
   float* lhat = nullptr;  // [batch][2nn][64]  re/im rows of L21, TF32
   float* ure = nullptr;   // [batch][nn+1][64] Re U12, K-major, TF32
   float* uim = nullptr;   // [batch][nn+1][64] Im U12
-  void* maps = nullptr;   // 3 TMA tensor maps (host copies, passed by value)
+  void* maps = nullptr;   // 4 TMA tensor maps (host copies, passed by value)
+  float2* cbase = nullptr;  // systems the C map (maps[3]) was made for
+  size_t clda = 0, cbstride = 0;
+  int cbatch = 0;
 };
 
 // CUDA-event timing per kernel class (off unless enabled).

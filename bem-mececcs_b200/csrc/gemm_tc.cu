@@ -12,13 +12,17 @@
 // per panel step: Lhat by k_pack_l21, U_re/U_im by the row-interchange +
 // triangular-solve kernel.
 //
-// k_gemm_tc: persistent, one CTA per SM, 8 warps.  Warp 0 issues TMA loads
-// (128-byte swizzle, no multicast) into a 2-stage ring; warp 1 allocates 512
-// TMEM columns and one elected thread issues tcgen05.mma (M=128, N=128, K=8,
-// kind::tf32) into double-buffered accumulators; warps 4-7 read the
-// accumulators with tcgen05.ld, combine real and imaginary parts with one
-// lane shuffle and update C in place.  Every mbarrier wait is bounded; on
-// timeout the kernel records ST_TIMEOUT and drains.
+// k_gemm_tc: persistent, one CTA per SM, 8 warps, one 64 x 128 complex tile
+// of C at a time.  Warp 0 issues TMA loads (no multicast): the C tile through
+// a 3-D map (floats of a column x columns x problems, so edges and padding
+// are clipped) into one of two shared-memory buffers, and the operands
+// (128-byte swizzle) into one stage.  Warp 1 allocates 512 TMEM columns and
+// one elected thread issues tcgen05.mma (M=128, N=128, K=8, kind::tf32) into
+// double-buffered accumulators.  Warps 4-7 read the accumulators with
+// tcgen05.ld, combine real and imaginary parts with one lane shuffle,
+// subtract into the shared C tile and write it back with one TMA store, so C
+// moves through HBM as 64 KB bulk copies in each direction.  Every mbarrier
+// wait is bounded; on timeout the kernel records ST_TIMEOUT and drains.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -33,11 +37,11 @@ namespace {
 
 constexpr int kTcRows = 64;        // complex rows per tile (UMMA M = 128 real rows)
 constexpr int kTcCols = 128;       // columns per tile (UMMA N)
-constexpr uint32_t kBox = 128 * 128;  // one box: 128 rows x 32 floats = 16 KB
+constexpr uint32_t kBox = 128 * 128;  // one operand box: 128 rows x 32 floats = 16 KB
 constexpr uint32_t kStageBytes = 6 * kBox;  // Lhat, U_re, U_im, 2 K-halves each
-constexpr int kStages = 2;
+constexpr uint32_t kCBytes = 128 * 128 * 4;  // C tile: 64 complex rows x 128 columns
 constexpr uint32_t kTmemCols = 512;
-constexpr size_t kTcSmem = (size_t)kStages * kStageBytes + 1024;
+constexpr size_t kTcSmem = (size_t)kStageBytes + 2 * kCBytes + 1024;
 
 __device__ __forceinline__ uint32_t idesc_tf32_128x128() {
   // c_format F32 (bit 4), a/b format TF32 = 2 (bits 7, 10), K-major A and B,
@@ -63,6 +67,24 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
       "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
       : "memory");
 }
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int x, int y, int z, const void* src) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(map), "r"(x),
+               "r"(y), "r"(z), "r"(smem_u32(src))
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void tma_store_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void tma_store_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void epi_bar_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
 __device__ __forceinline__ void umma_tf32(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                           uint32_t accumulate) {
@@ -114,23 +136,26 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, vo
 
 __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUtensorMap tm_l,
                                                     const __grid_constant__ CUtensorMap tm_ure,
-                                                    const __grid_constant__ CUtensorMap tm_uim, TcArgs a) {
+                                                    const __grid_constant__ CUtensorMap tm_uim,
+                                                    const __grid_constant__ CUtensorMap tm_c, TcArgs a) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  __shared__ uint64_t full_bar[kStages], empty_bar[kStages], tfull_bar[2], tempty_bar[2];
+  unsigned char* ops = smem;                     // one operand stage
+  float* cbuf = reinterpret_cast<float*>(smem + kStageBytes);  // 2 C tiles [col][128 floats]
+  __shared__ uint64_t op_full, op_empty, c_full[2], c_empty[2], t_full[2], t_empty[2];
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int total = a.mtiles * a.ntiles * a.batch;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
-      mbar_init(&full_bar[s], 1);
-      mbar_init(&empty_bar[s], 1);
-    }
+    mbar_init(&op_full, 1);
+    mbar_init(&op_empty, 1);
     for (int s = 0; s < 2; ++s) {
-      mbar_init(&tfull_bar[s], 1);
-      mbar_init(&tempty_bar[s], 4);
+      mbar_init(&c_full[s], 1);
+      mbar_init(&c_empty[s], 1);
+      mbar_init(&t_full[s], 1);
+      mbar_init(&t_empty[s], 4);
     }
     s_abort = 0;
   }
@@ -149,23 +174,25 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
   volatile int* abort_flag = &s_abort;
 
   if (warp == 0 && lane == 0) {
-    // ---- TMA producer ----
+    // ---- TMA producer: C tile (2 buffers) and operands (1 stage) ----
     int it = 0;
     for (int t = blockIdx.x; t < total; t += gridDim.x, ++it) {
-      const int s = it % kStages;
-      const uint32_t ph = (uint32_t)(it / kStages) & 1u;
-      if (!wait_or_abort(&empty_bar[s], ph ^ 1u, abort_flag, a.status)) break;
       const int b = t / (a.mtiles * a.ntiles);
       const int rem = t % (a.mtiles * a.ntiles);
       const int tm = rem % a.mtiles, tn = rem / a.mtiles;
-      unsigned char* st = smem + (size_t)s * kStageBytes;
-      mbar_expect_tx(&full_bar[s], (uint32_t)boxes * 3u * kBox);
+      const int cb = it & 1;
+      if (!wait_or_abort(&c_empty[cb], ((uint32_t)(it >> 1) & 1u) ^ 1u, abort_flag, a.status)) break;
+      mbar_expect_tx(&c_full[cb], kCBytes);
+      tma_load_3d(cbuf + (size_t)cb * (kCBytes / 4), &tm_c, 2 * (a.r0 + tm * kTcRows), a.c0 + tn * kTcCols, b,
+                  &c_full[cb]);
+      if (!wait_or_abort(&op_empty, ((uint32_t)it & 1u) ^ 1u, abort_flag, a.status)) break;
+      mbar_expect_tx(&op_full, (uint32_t)boxes * 3u * kBox);
       const int ly = b * a.lrows + 2 * tm * kTcRows;
       const int uy = b * a.urows + tn * kTcCols;
       for (int h = 0; h < boxes; ++h) {
-        tma_load_2d(st + (0 + h) * kBox, &tm_l, 32 * h, ly, &full_bar[s]);
-        tma_load_2d(st + (2 + h) * kBox, &tm_ure, 32 * h, uy, &full_bar[s]);
-        tma_load_2d(st + (4 + h) * kBox, &tm_uim, 32 * h, uy, &full_bar[s]);
+        tma_load_2d(ops + (0 + h) * kBox, &tm_l, 32 * h, ly, &op_full);
+        tma_load_2d(ops + (2 + h) * kBox, &tm_ure, 32 * h, uy, &op_full);
+        tma_load_2d(ops + (4 + h) * kBox, &tm_uim, 32 * h, uy, &op_full);
       }
     }
   } else if (warp == 1 && lane == 0) {
@@ -173,15 +200,12 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
     const uint32_t idesc = idesc_tf32_128x128();
     int it = 0;
     for (int t = blockIdx.x; t < total; t += gridDim.x, ++it) {
-      const int s = it % kStages;
-      const uint32_t ph = (uint32_t)(it / kStages) & 1u;
       const int buf = it & 1;
-      const uint32_t bph = (uint32_t)(it >> 1) & 1u;
-      if (!wait_or_abort(&tempty_bar[buf], bph ^ 1u, abort_flag, a.status)) break;
+      if (!wait_or_abort(&t_empty[buf], ((uint32_t)(it >> 1) & 1u) ^ 1u, abort_flag, a.status)) break;
       tc_fence_after();
-      if (!wait_or_abort(&full_bar[s], ph, abort_flag, a.status)) break;
+      if (!wait_or_abort(&op_full, (uint32_t)it & 1u, abort_flag, a.status)) break;
       tc_fence_after();
-      const uint32_t sbase = smem_u32(smem + (size_t)s * kStageBytes);
+      const uint32_t sbase = smem_u32(ops);
       const uint32_t d1 = tmem + (uint32_t)buf * 256u, d2 = d1 + 128u;
       for (int kk = 0; kk < ksteps; ++kk) {
         const uint32_t off = (uint32_t)(kk >> 2) * kBox + (uint32_t)(kk & 3) * 32u;
@@ -191,27 +215,27 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
         umma_tf32(d1, da, dre, idesc, kk > 0 ? 1u : 0u);
         umma_tf32(d2, da, dim, idesc, kk > 0 ? 1u : 0u);
       }
-      umma_commit(&empty_bar[s]);
-      umma_commit(&tfull_bar[buf]);
+      umma_commit(&op_empty);
+      umma_commit(&t_full[buf]);
     }
   } else if (warp >= 4) {
-    // ---- epilogue: TMEM -> registers -> C -= D ----
+    // ---- epilogue: C tile in shared memory -= combined accumulators ----
     const int e = warp - 4;
     int it = 0;
     for (int t = blockIdx.x; t < total; t += gridDim.x, ++it) {
-      const int buf = it & 1;
-      const uint32_t bph = (uint32_t)(it >> 1) & 1u;
-      bool ok = true;
-      if (lane == 0) ok = wait_or_abort(&tfull_bar[buf], bph, abort_flag, a.status);
-      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
-      if (!ok) break;
+      const int buf = it & 1, cb = it & 1;
+      const uint32_t ph = (uint32_t)(it >> 1) & 1u;
+      // every lane observes both barriers, so the TMA-written C tile is visible to it
+      int ok = wait_or_abort(&t_full[buf], ph, abort_flag, a.status) &&
+               wait_or_abort(&c_full[cb], ph, abort_flag, a.status);
+      if (!__all_sync(0xffffffffu, ok)) break;
       tc_fence_after();
       const int b = t / (a.mtiles * a.ntiles);
       const int rem = t % (a.mtiles * a.ntiles);
       const int tm = rem % a.mtiles, tn = rem / a.mtiles;
-      const int r = a.r0 + tm * kTcRows + 16 * e + (lane >> 1);
+      const int rho = 32 * e + lane;  // real row in the tile = float index in the C column
       const int p = lane & 1;
-      float* C = reinterpret_cast<float*>(a.A + (size_t)b * a.bstride);
+      float* ct = cbuf + (size_t)cb * (kCBytes / 4);
       const uint32_t tbase = tmem + (uint32_t)buf * 256u + ((uint32_t)(32 * e) << 16);
       for (int c = 0; c < kTcCols; c += 16) {
         float v1[16], v2[16];
@@ -222,17 +246,21 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
         for (int i = 0; i < 16; ++i) {
           const float x = __shfl_xor_sync(0xffffffffu, v2[i], 1);
           const float val = p ? (v1[i] + x) : (v1[i] - x);
-          const int col = a.c0 + tn * kTcCols + c + i;
-          if (r < a.nn && col < a.ncols) {
-            float* q = C + 2 * ((size_t)col * a.lda + r) + p;
-            *q -= val;
-          }
+          ct[(c + i) * 128 + rho] -= val;
         }
       }
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(&tempty_bar[buf]);
+      if (lane == 0) mbar_arrive(&t_empty[buf]);
+      fence_proxy_async();
+      epi_bar_sync();
+      if (e == 0 && lane == 0) {
+        tma_store_3d(&tm_c, 2 * (a.r0 + tm * kTcRows), a.c0 + tn * kTcCols, b, ct);
+        tma_store_wait_read();
+        mbar_arrive(&c_empty[cb]);
+      }
     }
+    if (e == 0 && lane == 0) tma_store_wait_all();
   }
   __syncthreads();
   if (warp == 1) {
@@ -301,6 +329,20 @@ bool make_map(CUtensorMap* m, float* base, size_t rows) {
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// 3-D map over the FP32 systems: floats of a column (2*nn, the rest of lda is
+// padding), nn+1 columns, batch problems; 128 x 128 boxes, no swizzle.
+bool make_cmap(CUtensorMap* m, float2* base, int nn, size_t lda, size_t bstride, int batch) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)2 * nn, (cuuint64_t)nn + 1, (cuuint64_t)batch};
+  cuuint64_t strides[2] = {(cuuint64_t)lda * sizeof(float2), (cuuint64_t)bstride * sizeof(float2)};
+  cuuint32_t box[3] = {128, 128, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 }  // namespace
 
 int tc_ensure(bem_ctx* ctx, int nn, int batch) {
@@ -317,7 +359,7 @@ int tc_ensure(bem_ctx* ctx, int nn, int batch) {
   BEM_CUDA(ctx, cudaMemset(W.lhat, 0, lrows * 64 * sizeof(float)));
   BEM_CUDA(ctx, cudaMemset(W.ure, 0, urows * 64 * sizeof(float)));
   BEM_CUDA(ctx, cudaMemset(W.uim, 0, urows * 64 * sizeof(float)));
-  W.maps = new CUtensorMap[3];
+  W.maps = new CUtensorMap[4];
   CUtensorMap* maps = static_cast<CUtensorMap*>(W.maps);
   if (!make_map(&maps[0], W.lhat, lrows) || !make_map(&maps[1], W.ure, urows) || !make_map(&maps[2], W.uim, urows))
     return fail(ctx, BEM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
@@ -342,6 +384,15 @@ int tc_trailing_update(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int 
   TcWork& W = ctx->tc;
   const int r0 = k + w, c0 = k + w, ncols = nn + 1;
   if (r0 >= nn) return BEM_OK;
+  CUtensorMap* maps = static_cast<CUtensorMap*>(W.maps);
+  if (W.cbase != A || W.clda != lda || W.cbstride != bstride || W.cbatch != batch) {
+    if ((lda % 2) != 0 || (bstride % 2) != 0 || !make_cmap(&maps[3], A, nn, lda, bstride, batch))
+      return fail(ctx, BEM_ERR_ARG, "tensor-core update needs an even leading dimension");
+    W.cbase = A;
+    W.clda = lda;
+    W.cbstride = bstride;
+    W.cbatch = batch;
+  }
   k_pack_l21<<<dim3((nn - r0 + 31) / 32, batch), 256, 0, ctx->stream>>>(A, lda, bstride, nn, k, w, r0, W.lhat,
                                                                         2 * nn);
   ctx->launches++;
@@ -362,8 +413,7 @@ int tc_trailing_update(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int 
   t.status = ctx->d_status;
   const int total = t.mtiles * t.ntiles * batch;
   const int grid = std::min(total, ctx->num_sms);
-  CUtensorMap* maps = static_cast<CUtensorMap*>(W.maps);
-  k_gemm_tc<<<grid, 256, kTcSmem, ctx->stream>>>(maps[0], maps[1], maps[2], t);
+  k_gemm_tc<<<grid, 256, kTcSmem, ctx->stream>>>(maps[0], maps[1], maps[2], maps[3], t);
   ctx->launches++;
   BEM_CUDA(ctx, cudaGetLastError());
   return BEM_OK;

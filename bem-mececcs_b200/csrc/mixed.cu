@@ -127,7 +127,7 @@ int ensure_sweep(bem_ctx* ctx, int batch, bool mixed) {
   free_sweep(S);
   S.nn = nn;
   S.batch = batch;
-  S.lda = (size_t)nn;
+  S.lda = (size_t)((nn + 1) & ~1);  // even: 16-byte aligned column strides for the FP32 TMA maps
   S.a_stride = S.lda * (size_t)(nn + 1);
   S.rhs_chunks = chunks;
   S.resid_chunks = (nn + kResidCols - 1) / kResidCols;

@@ -363,7 +363,10 @@ def _roofline(name, k, peaks, peak64):
         bf16 = peaks.get("bf16_tflops")
         peak = 0.5 * bf16 if bf16 else 0.5 * 1590.0
         ach = k["work"] / secs / 1e12
-        return {"bound": "tensor", "kernel": "k_gemm_tf32 (FP32 LU trailing update, TF32 mma.sync)",
+        kern = ("k_gemm_tf32 (FP32 LU trailing update, TF32 mma.sync)"
+                if os.environ.get("BEM_TF32_MMA_SYNC") == "1" else
+                "k_pack_l21 + k_gemm_tc (FP32 LU trailing update, tcgen05 kind::tf32, TMEM accumulators)")
+        return {"bound": "tensor", "kernel": kern,
                 "achieved": round(ach, 3), "peak": round(peak, 1), "unit": "TFLOP/s",
                 "frac": round(ach / peak, 4), "traffic": None,
                 "peak_source": ("dense TF32 = half the measured dense BF16 cuBLAS figure of "
