@@ -74,6 +74,7 @@ def lib():
     L.bem_ghmatecd.argtypes = [vp, vp, vp, vp, vp, dp, ip]
     L.bem_get_system.argtypes = [vp, vp, vp]
     L.bem_get_preswap.argtypes = [vp, vp, vp]
+    L.bem_ghmatecd_noalloc.argtypes = [vp, vp, vp, vp, vp, dp, ip, vp, ctypes.c_size_t]
     L.bem_linsolve.argtypes = [vp, vp]
     L.bem_solve_dense.argtypes = [vp, ip, vp, vp, vp]
     L.bem_unswap.argtypes = [vp, vp, vp]

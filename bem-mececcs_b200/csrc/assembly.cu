@@ -13,6 +13,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <mutex>
 #include <vector>
 
 #include "bem_internal.h"
@@ -692,4 +694,130 @@ int launch_dynamic(bem_ctx* ctx, const double zge[2], const double zcs[2], const
   return launch_dynamic_batch(ctx, b);
 }
 
+// ---------------------------------------------------------------------------
+// GHMATECD without allocation (bem_ghmatecd_noalloc).
+//
+// The assembly needs two scratch buffers besides its inputs and outputs: the
+// pre-swap diagonal blocks written by k_dyn_diag and read by k_dyn_offdiag
+// (2 x 9 x nbe complex), and the per-chunk partial sums of the right-hand side
+// written by k_dyn_offdiag and summed by k_rhs_reduce (chunks x 3nbe
+// complex).  This variant takes both from one fixed array that every device
+// holds from the moment the library's kernels are loaded on it until the
+// process exits, so a call allocates nothing.  Every scratch word the kernels
+// read is first written by the same call, so nothing in it needs to start at
+// zero; the status words live in the context and are cleared per call.
+// ---------------------------------------------------------------------------
+
+constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;  // 8 MiB per device
+static __device__ __align__(256) double2 g_noalloc_scratch[kNoAllocScratchBytes / sizeof(double2)];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double2* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device, looked up on the
+// first call per device.  On the host the array's name stands for a host-side
+// shadow, never for device memory, so only this address goes to kernels.
+int noalloc_scratch(bem_ctx* ctx, double2** out) {
+  if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices)
+    return fail(ctx, BEM_ERR_ARG, "bem_ghmatecd_noalloc: device index out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[ctx->device]) {
+    void* addr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+    if (e != cudaSuccess || !addr) return cuda_fail(ctx, e, "cudaGetSymbolAddress(no-allocation scratch)");
+    g_noalloc_addr[ctx->device] = static_cast<double2*>(addr);
+  }
+  *out = g_noalloc_addr[ctx->device];
+  return BEM_OK;
+}
+
+// Scratch layout in complex128 words: diagonal H blocks, diagonal G blocks,
+// then the RHS partials starting on a 256-byte boundary.
+size_t noalloc_part_offset(int nbe) { return ((size_t)18 * nbe + 15) & ~(size_t)15; }
+size_t noalloc_words(int nbe, int chunks) { return noalloc_part_offset(nbe) + (size_t)chunks * 3 * nbe; }
+
+}  // namespace
+
 }  // namespace bem
+
+using namespace bem;
+
+int bem_ghmatecd_noalloc(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2],
+                         const double c[4], double fr, int flags, double* a, size_t lda) {
+  if (!ctx || !zge || !zcs || !zcp || !c || !a) return BEM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (flags & ~BEM_FAST_SINGULAR)
+    return fail(ctx, BEM_ERR_ARG, "bem_ghmatecd_noalloc: only BEM_FAST_SINGULAR is accepted");
+  if (!ctx->have_mesh || !ctx->have_dyn) return fail(ctx, BEM_ERR_STATE, "bem_ghmatecd_noalloc needs mesh and BCs");
+  if ((flags & BEM_FAST_SINGULAR) && (!ctx->have_hest || !ctx->have_gest))
+    return fail(ctx, BEM_ERR_STATE, "bem_ghmatecd_noalloc needs HESTdiag and GESTdiag");
+  const Mesh& m = ctx->mesh;
+  if (m.ng * (int)sizeof(double4) > 1024 * 32) return fail(ctx, BEM_ERR_ARG, "Gauss rule too large");
+  const int nn = 3 * m.nbe;
+  if (lda < (size_t)nn) return fail(ctx, BEM_ERR_ARG, "bem_ghmatecd_noalloc: lda < 3*nbe");
+  if (reinterpret_cast<uintptr_t>(a) % alignof(double2) != 0)
+    return fail(ctx, BEM_ERR_ARG, "bem_ghmatecd_noalloc: a must be 16-byte aligned");
+  const int jc = jc_for(m.ng);
+  const int chunks = (m.nbe + jc - 1) / jc;
+  const size_t need = noalloc_words(m.nbe, chunks) * sizeof(double2);
+  if (need > kNoAllocScratchBytes) {
+    char msg[200];
+    std::snprintf(msg, sizeof msg,
+                  "bem_ghmatecd_noalloc: this mesh needs %zu bytes of scratch, the fixed limit is %zu bytes; "
+                  "use bem_ghmatecd",
+                  need, kNoAllocScratchBytes);
+    return fail(ctx, BEM_ERR_ARG, msg);
+  }
+  BEM_CUDA(ctx, cudaSetDevice(ctx->device));
+  double2* scratch = nullptr;
+  int rc = noalloc_scratch(ctx, &scratch);
+  if (rc) return rc;
+  BEM_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->stream));
+
+  DynParams p{};
+  p.nbe = m.nbe;
+  p.nn = nn;
+  p.ng = m.ng;
+  p.jc = jc;
+  p.chunks = chunks;
+  p.lda = lda;
+  p.a_stride = 0;
+  p.zge = make_double2(zge[0], zge[1]);
+  p.c1 = c[0];
+  p.c2 = c[1];
+  p.c3 = c[2];
+  p.c4 = c[3];
+  p.fast_singular = (flags & BEM_FAST_SINGULAR) ? 1 : 0;
+  p.gq = m.gq;
+  p.eta = m.eta;
+  p.colloc = m.colloc;
+  p.hestdiag = ctx->hestdiag;
+  p.gestdiag = ctx->gestdiag;
+  p.kode = ctx->kode;
+  p.zdfi = ctx->zdfi;
+  p.A = reinterpret_cast<double2*>(a);
+  p.A32 = nullptr;
+  p.zh_pre = nullptr;
+  p.zg_pre = nullptr;
+  p.diag_h = scratch;
+  p.diag_g = scratch + (size_t)9 * m.nbe;
+  p.rhs_part = scratch + noalloc_part_offset(m.nbe);
+  p.status = ctx->d_status;
+  p.kb[0] = make_consts(zge, zcs, zcp, fr);
+
+  k_dyn_diag<<<dim3((m.nbe + 127) / 128, 1, 1), 128, 0, ctx->stream>>>(p);
+  ctx->launches++;
+  BEM_CUDA(ctx, cudaGetLastError());
+  const size_t smem = (size_t)jc * m.ng * sizeof(double4);
+  k_dyn_offdiag<<<dim3((m.nbe + kRowsPerCta - 1) / kRowsPerCta, chunks, 1), 128, smem, ctx->stream>>>(p);
+  ctx->launches++;
+  BEM_CUDA(ctx, cudaGetLastError());
+  k_rhs_reduce<<<dim3((nn + 255) / 256, 1), 256, 0, ctx->stream>>>(nn, chunks, lda, 0, p.rhs_part, p.A, nullptr);
+  ctx->launches++;
+  BEM_CUDA(ctx, cudaGetLastError());
+  if (ctx->mesh_flag_bnd) return fail(ctx, BEM_ERR_DEGENERATE, "Jacobian below 1e-5 on a boundary element");
+  return BEM_OK;
+}

@@ -28,6 +28,8 @@
 #ifndef BEM_CAPI_H
 #define BEM_CAPI_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -143,6 +145,29 @@ int bem_ghmatecd(bem_ctx *ctx, const double zge[2], const double zcs[2],
 int bem_get_system(bem_ctx *ctx, double *zh, double *zfi);
 /* Pre-swap H and G (needs BEM_KEEP_PRESWAP at assembly). */
 int bem_get_preswap(bem_ctx *ctx, double *zh, double *zg);
+
+/* GHMATECD that allocates nothing.  No counterpart in the reference: it is an
+ * addition for callers that must not allocate device memory once set up --
+ * a serving process that has handed its free HBM to its own pool or cache
+ * (bem_ghmatecd would add a 16 nn^2-byte system behind its back), or a loop
+ * that cannot afford cudaFree's device-wide synchronisation.
+ * Same assembly as bem_ghmatecd (flags: 0 or BEM_FAST_SINGULAR), written to
+ * the caller's device buffer a: nn x (nn + 1) complex128, column-major with
+ * leading dimension lda >= nn (complex elements), 16-byte aligned; columns
+ * 0..nn-1 receive ZH after the BC swap, column nn the RHS ZFI -- the values
+ * bem_get_system returns.  ctx's own system is left untouched.  The
+ * assembly's scratch (2 x 9 nbe + chunks x nn complex128 words, chunks =
+ * ceil(nbe / min(64, 1024 / npg^2))) comes from one fixed 8 MiB array that
+ * each device holds until the process exits; a larger mesh is rejected with
+ * BEM_ERR_ARG (nbe <= 3136 at npg <= 4, 1618 at npg = 8).  The first call on a device
+ * looks up that array's device address; make it before any stream capture.
+ * All calls on a device share the array: calls that overlap on the GPU
+ * (other streams, other contexts of the same device) race.  Asynchronous on
+ * ctx's stream; a device-side timeout shows at the next bem_sync. */
+int bem_ghmatecd_noalloc(bem_ctx *ctx, const double zge[2],
+                         const double zcs[2], const double zcp[2],
+                         const double c[4], double fr, int flags, double *a,
+                         size_t lda);
 
 /* LINSOLVE on the device: factor the assembled ZH, solve for ZFI, copy the
  * solution (nn complex) to zfi_out (may be NULL to keep it on the device). */
