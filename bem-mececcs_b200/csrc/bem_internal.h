@@ -85,6 +85,13 @@ struct LuWork {
   double2* cand = nullptr;      // [2][kMaxGrid][64]
   double2* drow = nullptr;      // [2][64]
   unsigned* barrier = nullptr;  // grid barrier counter
+  // cooperative triangular solves (k_trsv)
+  void* trsv_w = nullptr;       // [batch][2][nn] scratch vectors
+  size_t trsv_w_bytes = 0;
+  unsigned* trsv_ctr = nullptr;  // [kMaxBatch] group barrier counters
+  int* pstart = nullptr;         // device copy of pstart_host
+  int pstart_cap = 0;
+  std::vector<int> pstart_host;  // first row of each panel of the last factorisation, then nn
 };
 
 constexpr int kMaxGrid = 160;
@@ -158,6 +165,7 @@ struct bem_ctx {
   bem::SweepBuf sweep;
   bem::TcWork tc;
   bool use_tcgen05 = true;  // FP32 trailing update on tcgen05 (else TF32 mma.sync)
+  bool use_trsv_coop = true;  // one cooperative launch per triangular solve (else per-block launches)
 };
 
 namespace bem {

@@ -138,6 +138,7 @@ int bem_ctx_create(int device, bem_ctx** out) {
   }
   ctx->stream = ctx->own_stream;
   if (const char* env = getenv("BEM_TF32_MMA_SYNC")) ctx->use_tcgen05 = env[0] != '1';
+  if (const char* env = getenv("BEM_TRSV_LEGACY")) ctx->use_trsv_coop = env[0] != '1';
   *out = ctx;
   return BEM_OK;
 }
@@ -162,6 +163,9 @@ int bem_ctx_destroy(bem_ctx* ctx) {
   cudaFree(L.cand);
   cudaFree(L.drow);
   cudaFree(L.barrier);
+  cudaFree(L.trsv_w);
+  cudaFree(L.trsv_ctr);
+  cudaFree(L.pstart);
   release_sweep(ctx);
   tc_release(ctx);
   for (cudaEvent_t e : ctx->prof.pool) cudaEventDestroy(e);

@@ -13,16 +13,17 @@
 // triangular-solve kernel.
 //
 // k_gemm_tc: persistent, one CTA per SM, 8 warps, one 64 x 128 complex tile
-// of C at a time.  Warp 0 issues TMA loads (no multicast): the C tile through
-// a 3-D map (floats of a column x columns x problems, so edges and padding
-// are clipped) into one of two shared-memory buffers, and the operands
-// (128-byte swizzle) into one stage.  Warp 1 allocates 512 TMEM columns and
-// one elected thread issues tcgen05.mma (M=128, N=128, K=8, kind::tf32) into
-// double-buffered accumulators.  Warps 4-7 read the accumulators with
-// tcgen05.ld, combine real and imaginary parts with one lane shuffle,
-// subtract into the shared C tile and write it back with one TMA store, so C
-// moves through HBM as 64 KB bulk copies in each direction.  Every mbarrier
-// wait is bounded; on timeout the kernel records ST_TIMEOUT and drains.
+// of C at a time.  Warp 0 issues TMA loads (128-byte swizzle, no multicast)
+// of the operands in 32-wide K chunks through a 3-stage ring, and L2
+// prefetches of the C tiles a few tiles ahead.  Warp 1 allocates 512 TMEM
+// columns and one elected thread issues tcgen05.mma (M=128, N=128, K=8,
+// kind::tf32) into double-buffered accumulators.  Warps 4-7 read the
+// accumulators with tcgen05.ld, combine real and imaginary parts with one
+// lane shuffle, stage -(L21 U12) in shared memory per 64-column half and
+// hand it to a TMA reduce-add (f32), so C is updated in L2 without ever
+// being loaded into the SM: C = C + (-D) rounds exactly like C - D.  Every
+// mbarrier wait is bounded; on timeout the kernel records ST_TIMEOUT and
+// drains.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -37,11 +38,13 @@ namespace {
 
 constexpr int kTcRows = 64;        // complex rows per tile (UMMA M = 128 real rows)
 constexpr int kTcCols = 128;       // columns per tile (UMMA N)
-constexpr uint32_t kBox = 128 * 128;  // one operand box: 128 rows x 32 floats = 16 KB
-constexpr uint32_t kStageBytes = 6 * kBox;  // Lhat, U_re, U_im, 2 K-halves each
-constexpr uint32_t kCBytes = 128 * 128 * 4;  // C tile: 64 complex rows x 128 columns
+constexpr uint32_t kChunk = 128 * 32 * 4;  // one operand box: 128 rows x 32 floats (K) = 16 KB
+constexpr uint32_t kStageBytes = 3 * kChunk;  // Lhat, U_re, U_im for 32 of K
+constexpr int kStages = 3;
+constexpr uint32_t kHalfBytes = 128 * 64 * 4;  // C staging: 64 complex rows x 64 columns = 32 KB
 constexpr uint32_t kTmemCols = 512;
-constexpr size_t kTcSmem = (size_t)kStageBytes + 2 * kCBytes + 1024;
+constexpr int kPrefetch = 3;  // C tiles prefetched into L2 ahead of the current one
+constexpr size_t kTcSmem = (size_t)kStages * kStageBytes + 2 * kHalfBytes + 1024;
 
 __device__ __forceinline__ uint32_t idesc_tf32_128x128() {
   // c_format F32 (bit 4), a/b format TF32 = 2 (bits 7, 10), K-major A and B,
@@ -68,20 +71,22 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
-          smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int x, int y, int z, const void* src) {
-  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(map), "r"(x),
-               "r"(y), "r"(z), "r"(smem_u32(src))
+// L2 prefetch of one C tile (no shared memory, no completion to wait for).
+__device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap* map, int x, int y, int z) {
+  asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(map), "r"(x), "r"(y),
+               "r"(z)
                : "memory");
+}
+// C += staged tile, the add done by the TMA unit at L2 (f32 add, the type of
+// the tensor map).
+__device__ __forceinline__ void tma_reduce_add_3d(const CUtensorMap* map, int x, int y, int z, const void* src) {
+  asm volatile(
+      "cp.reduce.async.bulk.tensor.3d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(map),
+      "r"(x), "r"(y), "r"(z), "r"(smem_u32(src))
+      : "memory");
   asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }
-__device__ __forceinline__ void tma_store_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void tma_wait_read_1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
 __device__ __forceinline__ void tma_store_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void epi_bar_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
@@ -140,20 +145,21 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
                                                     const __grid_constant__ CUtensorMap tm_c, TcArgs a) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  unsigned char* ops = smem;                     // one operand stage
-  float* cbuf = reinterpret_cast<float*>(smem + kStageBytes);  // 2 C tiles [col][128 floats]
-  __shared__ uint64_t op_full, op_empty, c_full[2], c_empty[2], t_full[2], t_empty[2];
+  unsigned char* ring = smem;                                              // kStages x (Lhat, U_re, U_im) chunks
+  float* stage_c = reinterpret_cast<float*>(smem + kStages * kStageBytes);  // 2 x [64 cols][128 floats]
+  __shared__ uint64_t full[kStages], empty[kStages], t_full[2], t_empty[2];
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int total = a.mtiles * a.ntiles * a.batch;
+  const int nchunks = (a.kw + 31) / 32;
 
   if (threadIdx.x == 0) {
-    mbar_init(&op_full, 1);
-    mbar_init(&op_empty, 1);
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
     for (int s = 0; s < 2; ++s) {
-      mbar_init(&c_full[s], 1);
-      mbar_init(&c_empty[s], 1);
       mbar_init(&t_full[s], 1);
       mbar_init(&t_empty[s], 4);
     }
@@ -169,98 +175,126 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s_tmem;
-  const int ksteps = (a.kw + 7) / 8;
-  const int boxes = (a.kw + 31) / 32;
   volatile int* abort_flag = &s_abort;
 
   if (warp == 0 && lane == 0) {
-    // ---- TMA producer: C tile (2 buffers) and operands (1 stage) ----
-    int it = 0;
-    for (int t = blockIdx.x; t < total; t += gridDim.x, ++it) {
+    // ---- TMA producer: operand K-chunks through a kStages ring; C tiles
+    //      kPrefetch ahead are prefetched into L2 for the reduce-adds ----
+    auto prefetch_c = [&](int t) {
+      if (t >= total) return;
+      const int b = t / (a.mtiles * a.ntiles);
+      const int rem = t % (a.mtiles * a.ntiles);
+      const int x = 2 * (a.r0 + (rem % a.mtiles) * kTcRows), y = a.c0 + (rem / a.mtiles) * kTcCols;
+      tma_prefetch_3d(&tm_c, x, y, b);
+      tma_prefetch_3d(&tm_c, x, y + 64, b);
+    };
+    for (int q = 0; q < kPrefetch; ++q) prefetch_c(blockIdx.x + q * gridDim.x);
+    int s = 0;
+    uint32_t ph = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+      prefetch_c(t + kPrefetch * gridDim.x);
       const int b = t / (a.mtiles * a.ntiles);
       const int rem = t % (a.mtiles * a.ntiles);
       const int tm = rem % a.mtiles, tn = rem / a.mtiles;
-      const int cb = it & 1;
-      if (!wait_or_abort(&c_empty[cb], ((uint32_t)(it >> 1) & 1u) ^ 1u, abort_flag, a.status)) break;
-      mbar_expect_tx(&c_full[cb], kCBytes);
-      tma_load_3d(cbuf + (size_t)cb * (kCBytes / 4), &tm_c, 2 * (a.r0 + tm * kTcRows), a.c0 + tn * kTcCols, b,
-                  &c_full[cb]);
-      if (!wait_or_abort(&op_empty, ((uint32_t)it & 1u) ^ 1u, abort_flag, a.status)) break;
-      mbar_expect_tx(&op_full, (uint32_t)boxes * 3u * kBox);
       const int ly = b * a.lrows + 2 * tm * kTcRows;
       const int uy = b * a.urows + tn * kTcCols;
-      for (int h = 0; h < boxes; ++h) {
-        tma_load_2d(ops + (0 + h) * kBox, &tm_l, 32 * h, ly, &op_full);
-        tma_load_2d(ops + (2 + h) * kBox, &tm_ure, 32 * h, uy, &op_full);
-        tma_load_2d(ops + (4 + h) * kBox, &tm_uim, 32 * h, uy, &op_full);
+      for (int h = 0; h < nchunks; ++h) {
+        if (!wait_or_abort(&empty[s], ph ^ 1u, abort_flag, a.status)) {
+          ok = false;
+          break;
+        }
+        unsigned char* st = ring + (size_t)s * kStageBytes;
+        mbar_expect_tx(&full[s], kStageBytes);
+        tma_load_2d(st, &tm_l, 32 * h, ly, &full[s]);
+        tma_load_2d(st + kChunk, &tm_ure, 32 * h, uy, &full[s]);
+        tma_load_2d(st + 2 * kChunk, &tm_uim, 32 * h, uy, &full[s]);
+        if (++s == kStages) {
+          s = 0;
+          ph ^= 1u;
+        }
       }
     }
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer ----
     const uint32_t idesc = idesc_tf32_128x128();
+    int s = 0;
+    uint32_t ph = 0;
     int it = 0;
-    for (int t = blockIdx.x; t < total; t += gridDim.x, ++it) {
+    bool ok = true;
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++it) {
       const int buf = it & 1;
       if (!wait_or_abort(&t_empty[buf], ((uint32_t)(it >> 1) & 1u) ^ 1u, abort_flag, a.status)) break;
       tc_fence_after();
-      if (!wait_or_abort(&op_full, (uint32_t)it & 1u, abort_flag, a.status)) break;
-      tc_fence_after();
-      const uint32_t sbase = smem_u32(ops);
       const uint32_t d1 = tmem + (uint32_t)buf * 256u, d2 = d1 + 128u;
-      for (int kk = 0; kk < ksteps; ++kk) {
-        const uint32_t off = (uint32_t)(kk >> 2) * kBox + (uint32_t)(kk & 3) * 32u;
-        const uint64_t da = sdesc(sbase + 0 * kBox + off);
-        const uint64_t dre = sdesc(sbase + 2 * kBox + off);
-        const uint64_t dim = sdesc(sbase + 4 * kBox + off);
-        umma_tf32(d1, da, dre, idesc, kk > 0 ? 1u : 0u);
-        umma_tf32(d2, da, dim, idesc, kk > 0 ? 1u : 0u);
+      for (int h = 0; h < nchunks; ++h) {
+        if (!wait_or_abort(&full[s], ph, abort_flag, a.status)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sbase = smem_u32(ring + (size_t)s * kStageBytes);
+        const int ks = min(4, (a.kw - 32 * h) / 8);
+        for (int kk = 0; kk < ks; ++kk) {
+          const uint32_t off = (uint32_t)kk * 32u;
+          const uint64_t da = sdesc(sbase + off);
+          const uint64_t dre = sdesc(sbase + kChunk + off);
+          const uint64_t dim = sdesc(sbase + 2 * kChunk + off);
+          const uint32_t acc = (h > 0 || kk > 0) ? 1u : 0u;
+          umma_tf32(d1, da, dre, idesc, acc);
+          umma_tf32(d2, da, dim, idesc, acc);
+        }
+        umma_commit(&empty[s]);
+        if (++s == kStages) {
+          s = 0;
+          ph ^= 1u;
+        }
       }
-      umma_commit(&op_empty);
-      umma_commit(&t_full[buf]);
+      if (ok) umma_commit(&t_full[buf]);
     }
   } else if (warp >= 4) {
-    // ---- epilogue: C tile in shared memory -= combined accumulators ----
+    // ---- epilogue: stage -(D) per 64-column half, reduce-add it into C ----
     const int e = warp - 4;
+    const int rho = 32 * e + lane;  // real row in the tile = float index in the C column
+    const int p = lane & 1;
+    const bool issuer = (e == 0 && lane == 0);
     int it = 0;
     for (int t = blockIdx.x; t < total; t += gridDim.x, ++it) {
-      const int buf = it & 1, cb = it & 1;
-      const uint32_t ph = (uint32_t)(it >> 1) & 1u;
-      // every lane observes both barriers, so the TMA-written C tile is visible to it
-      int ok = wait_or_abort(&t_full[buf], ph, abort_flag, a.status) &&
-               wait_or_abort(&c_full[cb], ph, abort_flag, a.status);
-      if (!__all_sync(0xffffffffu, ok)) break;
+      const int buf = it & 1;
+      if (!__all_sync(0xffffffffu, wait_or_abort(&t_full[buf], (uint32_t)(it >> 1) & 1u, abort_flag, a.status)))
+        break;
       tc_fence_after();
       const int b = t / (a.mtiles * a.ntiles);
       const int rem = t % (a.mtiles * a.ntiles);
       const int tm = rem % a.mtiles, tn = rem / a.mtiles;
-      const int rho = 32 * e + lane;  // real row in the tile = float index in the C column
-      const int p = lane & 1;
-      float* ct = cbuf + (size_t)cb * (kCBytes / 4);
       const uint32_t tbase = tmem + (uint32_t)buf * 256u + ((uint32_t)(32 * e) << 16);
-      for (int c = 0; c < kTcCols; c += 16) {
-        float v1[16], v2[16];
-        tmem_ld16(tbase + (uint32_t)c, v1);
-        tmem_ld16(tbase + 128u + (uint32_t)c, v2);
-        tmem_ld_wait();
+      for (int hc = 0; hc < 2; ++hc) {
+        float* ct = stage_c + (size_t)hc * (kHalfBytes / 4);
+        if (issuer) tma_wait_read_1();  // this half's previous reduce has left shared memory
+        epi_bar_sync();
+        for (int c = 0; c < 64; c += 16) {
+          float v1[16], v2[16];
+          tmem_ld16(tbase + (uint32_t)(64 * hc + c), v1);
+          tmem_ld16(tbase + 128u + (uint32_t)(64 * hc + c), v2);
+          tmem_ld_wait();
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const float x = __shfl_xor_sync(0xffffffffu, v2[i], 1);
-          const float val = p ? (v1[i] + x) : (v1[i] - x);
-          ct[(c + i) * 128 + rho] -= val;
+          for (int i = 0; i < 16; ++i) {
+            const float x = __shfl_xor_sync(0xffffffffu, v2[i], 1);
+            const float val = p ? (v1[i] + x) : (v1[i] - x);
+            ct[(c + i) * 128 + rho] = -val;
+          }
         }
-      }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&t_empty[buf]);
-      fence_proxy_async();
-      epi_bar_sync();
-      if (e == 0 && lane == 0) {
-        tma_store_3d(&tm_c, 2 * (a.r0 + tm * kTcRows), a.c0 + tn * kTcCols, b, ct);
-        tma_store_wait_read();
-        mbar_arrive(&c_empty[cb]);
+        if (hc == 1) {
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&t_empty[buf]);
+        }
+        fence_proxy_async();
+        epi_bar_sync();
+        if (issuer) tma_reduce_add_3d(&tm_c, 2 * (a.r0 + tm * kTcRows), a.c0 + tn * kTcCols + 64 * hc, b, ct);
       }
     }
-    if (e == 0 && lane == 0) tma_store_wait_all();
+    if (issuer) tma_store_wait_all();
   }
   __syncthreads();
   if (warp == 1) {
@@ -330,13 +364,14 @@ bool make_map(CUtensorMap* m, float* base, size_t rows) {
 }
 
 // 3-D map over the FP32 systems: floats of a column (2*nn, the rest of lda is
-// padding), nn+1 columns, batch problems; 128 x 128 boxes, no swizzle.
+// padding), nn+1 columns, batch problems; 128 x 64 boxes (64 complex rows x
+// 64 columns), no swizzle.
 bool make_cmap(CUtensorMap* m, float2* base, int nn, size_t lda, size_t bstride, int batch) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return false;
   cuuint64_t dims[3] = {(cuuint64_t)2 * nn, (cuuint64_t)nn + 1, (cuuint64_t)batch};
   cuuint64_t strides[2] = {(cuuint64_t)lda * sizeof(float2), (cuuint64_t)bstride * sizeof(float2)};
-  cuuint32_t box[3] = {128, 128, 1};
+  cuuint32_t box[3] = {128, 64, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,

@@ -205,6 +205,26 @@ __device__ __forceinline__ void local_argmax(const cpx<R>* col, int rcount, int 
 }
 
 // Scale column j and apply the rank-1 update to the panel columns right of j.
+// Rows [row0, row0 + rcount) x columns [col0, col0 + w) of A into s
+// (column-major, leading dimension rp) with one cp.async per element: every
+// copy is in flight before the single wait, so the slice costs one memory
+// round trip rather than one per loop iteration.
+template <typename R>
+__device__ __forceinline__ void load_slice_async(const typename Elt<R>::T* A, size_t lda, int row0, int col0,
+                                                 int rcount, int w, cpx<R>* s, int rp) {
+  constexpr int kBytes = (int)sizeof(typename Elt<R>::T);
+  for (int r = threadIdx.x; r < rcount; r += blockDim.x)
+    for (int c = 0; c < w; ++c) {
+      const unsigned dst = smem_u32(&s[(size_t)c * rp + r]);
+      const void* src = &A[(size_t)(col0 + c) * lda + row0 + r];
+      if constexpr (kBytes == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+      else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+    }
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 template <typename R>
 __device__ __forceinline__ void eliminate(cpx<R>* s_a, int rp, int rcount, int rbase, int gj, int j, int w,
                                           const cpx<R>* s_piv, int* status, bool report) {
@@ -263,10 +283,7 @@ __global__ void __launch_bounds__(NT, 1) k_panel_cluster(PanelArgs a) {
   const int rbase = k + (int)rank * rp;
   const int rcount = max(0, min(rp, a.nn - rbase));
 
-  for (int idx = tid; idx < w * rcount; idx += blockDim.x) {
-    const int c = idx / rcount, r = idx % rcount;
-    s_a[c * rp + r] = ldc<R>(&A[(size_t)(k + c) * a.lda + rbase + r]);
-  }
+  load_slice_async<R>(A, a.lda, rbase, k, rcount, w, s_a, rp);
   if (rank == 0 && tid < w) {
     s_pdst[tid] = k + tid;
     s_psrc[tid] = k + tid;
@@ -557,10 +574,7 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel_grid(PanelArgs a) {
   C* cand = static_cast<C*>(a.cand);
   C* drow = static_cast<C*>(a.drow);
 
-  for (int idx = tid; idx < w * rcount; idx += blockDim.x) {
-    const int c = idx / rcount, r = idx % rcount;
-    s_a[c * rp + r] = ldc<R>(&A[(size_t)(k + c) * a.lda + rbase + r]);
-  }
+  load_slice_async<R>(A, a.lda, rbase, k, rcount, w, s_a, rp);
   if (b == 0 && tid < w) {
     s_pdst[tid] = k + tid;
     s_psrc[tid] = k + tid;
@@ -654,57 +668,78 @@ __global__ void __launch_bounds__(256) k_laswp_trsm(void* Av, size_t lda, size_t
   C* s_L = reinterpret_cast<C*>(smem_raw);  // [NB][NB] column-major
   E* A = static_cast<E*>(Av) + (size_t)blockIdx.y * bstride;
   const int* pl = perm + (size_t)blockIdx.y * perm_stride;
-  for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
-    const int c = idx / w, r = idx % w;
-    s_L[c * NB + r] = ldc<R>(&A[(size_t)(k + c) * lda + k + r]);
-  }
+  load_slice_async<R>(A, lda, k, k, w, w, s_L, NB);
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int count = pl[0];
   pl += 1;
-  for (int col = c0 + blockIdx.x * 8 + warp; col < ncols; col += gridDim.x * 8) {
-    E* cp = A + (size_t)col * lda;
-    C v0 = lane < w ? ldc<R>(&cp[pl[2 * lane + 1]]) : C{R(0), R(0)};
-    C v1 = lane + 32 < w ? ldc<R>(&cp[pl[2 * (lane + 32) + 1]]) : C{R(0), R(0)};
-    C x[2];
-    int xd[2] = {-1, -1};
+  // The gather list is the same for every column: source rows of the panel
+  // rows lane, lane+32, and (destination, source) of the displaced rows.
+  const int s0 = lane < w ? pl[2 * lane + 1] : 0;
+  const int s1 = lane + 32 < w ? pl[2 * (lane + 32) + 1] : 0;
+  int xd[2], xs[2];
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int e = w + lane + 32 * q;
-      if (e < count) {
-        xd[q] = pl[2 * e];
-        x[q] = ldc<R>(&cp[pl[2 * e + 1]]);
-      }
+  for (int h = 0; h < 2; ++h) {
+    const int e = w + lane + 32 * h;
+    xd[h] = e < count ? pl[2 * e] : -1;
+    xs[h] = e < count ? pl[2 * e + 1] : 0;
+  }
+  constexpr int QC = 4;  // columns per warp, solved as interleaved chains
+  const int ncol = ncols - c0;
+  for (int cb = (blockIdx.x * 8 + warp) * QC; cb < ncol; cb += gridDim.x * 8 * QC) {
+    C v0[QC], v1[QC], x[QC][2];
+#pragma unroll
+    for (int q = 0; q < QC; ++q) {
+      const bool ok = cb + q < ncol;
+      const E* cp = A + (size_t)(c0 + cb + q) * lda;
+      v0[q] = ok && lane < w ? ldc<R>(&cp[s0]) : C{R(0), R(0)};
+      v1[q] = ok && lane + 32 < w ? ldc<R>(&cp[s1]) : C{R(0), R(0)};
+#pragma unroll
+      for (int h = 0; h < 2; ++h) x[q][h] = ok && xd[h] >= 0 ? ldc<R>(&cp[xs[h]]) : C{R(0), R(0)};
     }
     __syncwarp();
 #pragma unroll
-    for (int q = 0; q < 2; ++q)
-      if (xd[q] >= 0) stc<R>(&cp[xd[q]], x[q]);
+    for (int q = 0; q < QC; ++q) {
+      if (cb + q >= ncol) continue;
+      E* cp = A + (size_t)(c0 + cb + q) * lda;
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+        if (xd[h] >= 0) stc<R>(&cp[xd[h]], x[q][h]);
+    }
     // Forward substitution with the unit lower L11: rows lane and lane+32.
     for (int i = 0; i < w; ++i) {
-      const C src = (i < 32) ? v0 : v1;
-      C ui;
-      ui.re = __shfl_sync(0xffffffffu, src.re, i & 31);
-      ui.im = __shfl_sync(0xffffffffu, src.im, i & 31);
-      if (lane > i && lane < w) cfms(v0, s_L[i * NB + lane], ui);
-      if (lane + 32 > i && lane + 32 < w) cfms(v1, s_L[i * NB + lane + 32], ui);
+      const C l0 = s_L[i * NB + lane], l1 = s_L[i * NB + lane + 32];
+#pragma unroll
+      for (int q = 0; q < QC; ++q) {
+        const C src = (i < 32) ? v0[q] : v1[q];
+        C ui;
+        ui.re = __shfl_sync(0xffffffffu, src.re, i & 31);
+        ui.im = __shfl_sync(0xffffffffu, src.im, i & 31);
+        if (lane > i && lane < w) cfms(v0[q], l0, ui);
+        if (lane + 32 > i && lane + 32 < w) cfms(v1[q], l1, ui);
+      }
     }
-    if (lane < w) stc<R>(&cp[k + lane], v0);
-    if (lane + 32 < w) stc<R>(&cp[k + lane + 32], v1);
-    if (ure) {
-      // Packed K-major copies of U12 for the tensor-core update, rounded to TF32.
-      const size_t row = ((size_t)blockIdx.y * urows + (col - c0)) * 64;
-      const float r0 = lane < w ? (float)v0.re : 0.f, i0 = lane < w ? (float)v0.im : 0.f;
-      const float r1 = lane + 32 < w ? (float)v1.re : 0.f, i1 = lane + 32 < w ? (float)v1.im : 0.f;
-      unsigned t0, t1, t2, t3;
-      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t0) : "f"(r0));
-      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t1) : "f"(r1));
-      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t2) : "f"(i0));
-      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t3) : "f"(i1));
-      ure[row + lane] = __uint_as_float(t0);
-      ure[row + lane + 32] = __uint_as_float(t1);
-      uim[row + lane] = __uint_as_float(t2);
-      uim[row + lane + 32] = __uint_as_float(t3);
+#pragma unroll
+    for (int q = 0; q < QC; ++q) {
+      if (cb + q >= ncol) continue;
+      E* cp = A + (size_t)(c0 + cb + q) * lda;
+      if (lane < w) stc<R>(&cp[k + lane], v0[q]);
+      if (lane + 32 < w) stc<R>(&cp[k + lane + 32], v1[q]);
+      if (ure) {
+        // Packed K-major copies of U12 for the tensor-core update, rounded to TF32.
+        const size_t row = ((size_t)blockIdx.y * urows + (cb + q)) * 64;
+        const float r0 = lane < w ? (float)v0[q].re : 0.f, i0 = lane < w ? (float)v0[q].im : 0.f;
+        const float r1 = lane + 32 < w ? (float)v1[q].re : 0.f, i1 = lane + 32 < w ? (float)v1[q].im : 0.f;
+        unsigned t0, t1, t2, t3;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t0) : "f"(r0));
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t1) : "f"(r1));
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t2) : "f"(i0));
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t3) : "f"(i1));
+        ure[row + lane] = __uint_as_float(t0);
+        ure[row + lane + 32] = __uint_as_float(t1);
+        uim[row + lane] = __uint_as_float(t2);
+        uim[row + lane + 32] = __uint_as_float(t3);
+      }
     }
   }
 }
@@ -1032,6 +1067,227 @@ __global__ void __launch_bounds__(256) k_backsub(void* Av, size_t lda, size_t bs
 }
 
 // ---------------------------------------------------------------------------
+// k_trsv: the forward and back substitutions with the stored factors in ONE
+// cooperative launch.  The CTAs form one group per problem (`group` CTAs
+// each); a group walks the forward panels, then the backward 64-row blocks,
+// with one bounded group barrier per step.  In every step each CTA of the
+// group solves the step's small diagonal triangle redundantly in shared
+// memory (warp 0), then updates its share of the remaining rows, rebalanced
+// every step (64 rows x 4 column groups per pass).
+//
+// Forward (panel p, rows [k, k+w)): the panel's row interchanges are replayed
+// by gathering from buffer B[p%2] and every updated row is written to
+// B[(p+1)%2] (B0 = v, B1 = scratch), so gathers never race with updates.
+// The solved panel rows go to v, in a step that does not read v (odd p), or
+// one step later (even p).  Backward (U x = y, y in v): rows of the current
+// block are read and rows above it are updated in place; the solution
+// collects in a second scratch vector that is copied into v at the end.
+// ---------------------------------------------------------------------------
+struct TrsvArgs {
+  const void* A;
+  size_t lda, bstride;
+  int nn, batch, group, npanels, forward;
+  const int* pstart;  // [npanels + 1] first row of each forward panel, then nn
+  const int* perm;    // [panel][batch][kPermStride] gather lists
+  void* v;            // problem b at v + b * vstride: right-hand side in, solution out
+  size_t vstride;
+  void* w;            // scratch: [batch][2][nn]
+  unsigned* ctr;      // [batch] group barrier counters, zero at launch
+  int* status;
+};
+constexpr int kTrsvBlk = 64;
+
+// dst[r] = src[r] - sum_{c < w} M(r, c0 + c) x_c for rows [lo, hi).  256 threads:
+// 64 rows x 4 column groups per pass, partial sums combined in shared memory.
+template <typename R>
+__device__ __forceinline__ void trsv_rows(const typename Elt<R>::T* __restrict__ A, size_t lda, int c0, int w,
+                                          const cpx<R>* s_x, const typename Elt<R>::T* src,
+                                          typename Elt<R>::T* dst, int lo, int hi, cpx<R> (*s_part)[64]) {
+  using E = typename Elt<R>::T;
+  using C = cpx<R>;
+  const int rl = threadIdx.x & 63, cg = threadIdx.x >> 6;
+  const int cw = (w + 3) >> 2, cb = cg * cw, ce = min(w, cb + cw);
+  for (int base = lo; base < hi; base += 64) {
+    const int r = base + rl;
+    C part{R(0), R(0)};
+    C acc{R(0), R(0)};
+    if (r < hi) {
+      if (cg == 0) acc = ldc_cg<R>(&src[r]);
+      const E* col = A + (size_t)(c0 + cb) * lda + r;
+#pragma unroll 16
+      for (int c = cb; c < ce; ++c) {
+        const E t = __ldg(col);
+        col += lda;
+        const C xc = s_x[c];
+        part.re = fma(t.x, xc.re, fma(-t.y, xc.im, part.re));
+        part.im = fma(t.x, xc.im, fma(t.y, xc.re, part.im));
+      }
+    }
+    s_part[cg][rl] = part;
+    __syncthreads();
+    if (cg == 0 && r < hi) {
+      acc.re -= (s_part[0][rl].re + s_part[1][rl].re) + (s_part[2][rl].re + s_part[3][rl].re);
+      acc.im -= (s_part[0][rl].im + s_part[1][rl].im) + (s_part[2][rl].im + s_part[3][rl].im);
+      stc<R>(&dst[r], acc);
+    }
+    __syncthreads();
+  }
+}
+
+// The w x w block at (r0, c0) into s_T (column-major, ld 64): 256 threads as
+// 64 rows x 4 groups of 16 columns; all 16 loads of a thread are issued
+// before any shared-memory store, so the block costs one memory round trip.
+template <typename R>
+__device__ __forceinline__ void trsv_load_block(const typename Elt<R>::T* __restrict__ A, size_t lda, int r0, int c0,
+                                                int w, cpx<R>* s_T) {
+  using E = typename Elt<R>::T;
+  const int r = threadIdx.x & 63, cg = threadIdx.x >> 6;
+  E t[16];
+#pragma unroll
+  for (int u = 0; u < 16; ++u) {
+    const int c = cg * 16 + u;
+    if (r < w && c < w) t[u] = __ldg(&A[(size_t)(c0 + c) * lda + r0 + r]);
+  }
+#pragma unroll
+  for (int u = 0; u < 16; ++u) {
+    const int c = cg * 16 + u;
+    if (r < w && c < w) s_T[c * kTrsvBlk + r] = cpx<R>{t[u].x, t[u].y};
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_trsv(TrsvArgs a) {
+  using E = typename Elt<R>::T;
+  using C = cpx<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s_T = reinterpret_cast<C*>(smem_raw);  // [64][64] diagonal triangle, column-major
+  __shared__ C s_g[128];                    // gathered values / right-hand block
+  __shared__ C s_x[kTrsvBlk];
+  __shared__ C s_xprev[kTrsvBlk];
+  __shared__ C s_part[4][64];
+  const int prob = blockIdx.x / a.group, rank = blockIdx.x % a.group, G = a.group;
+  if (prob >= a.batch) return;
+  const E* A = static_cast<const E*>(a.A) + (size_t)prob * a.bstride;
+  E* v = static_cast<E*>(a.v) + (size_t)prob * a.vstride;
+  E* b1 = static_cast<E*>(a.w) + (size_t)prob * 2 * a.nn;
+  E* xo = b1 + a.nn;
+  const int nn = a.nn;
+  unsigned* ctr = a.ctr + prob;
+  unsigned epoch = 0;
+
+  if (a.forward) {
+    int kprev = 0, wprev = 0;
+    for (int p = 0; p < a.npanels; ++p) {
+      const int k = a.pstart[p], w = a.pstart[p + 1] - k;
+      E* cur = (p & 1) ? b1 : v;
+      E* nxt = (p & 1) ? v : b1;
+      const int* pl = a.perm + ((size_t)p * a.batch + prob) * kPermStride;
+      const int count = pl[0];
+      for (int e = threadIdx.x; e < count; e += blockDim.x) s_g[e] = ldc_cg<R>(&cur[pl[2 + 2 * e]]);
+      trsv_load_block<R>(A, a.lda, k, k, w, s_T);
+      __syncthreads();
+      if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        C v0 = lane < w ? s_g[lane] : C{R(0), R(0)};
+        C v1 = lane + 32 < w ? s_g[lane + 32] : C{R(0), R(0)};
+        for (int i = 0; i < w; ++i) {
+          const C src = (i < 32) ? v0 : v1;
+          C ui;
+          ui.re = __shfl_sync(0xffffffffu, src.re, i & 31);
+          ui.im = __shfl_sync(0xffffffffu, src.im, i & 31);
+          if (lane > i && lane < w) cfms(v0, s_T[i * kTrsvBlk + lane], ui);
+          if (lane + 32 > i && lane + 32 < w) cfms(v1, s_T[i * kTrsvBlk + lane + 32], ui);
+        }
+        if (lane < w) s_x[lane] = v0;
+        if (lane + 32 < w) s_x[lane + 32] = v1;
+      }
+      __syncthreads();
+      if (rank == 0 && (p & 1)) {  // v is not read in odd steps
+        for (int i = threadIdx.x; i < wprev; i += blockDim.x) stc<R>(&v[kprev + i], s_xprev[i]);
+        for (int i = threadIdx.x; i < w; i += blockDim.x) stc<R>(&v[k + i], s_x[i]);
+      }
+      const int r0 = k + w;
+      if (r0 < nn) {
+        const int per = (nn - r0 + G - 1) / G;
+        const int lo = min(nn, r0 + rank * per), hi = min(nn, lo + per);
+        trsv_rows<R>(A, a.lda, k, w, s_x, cur, nxt, lo, hi, s_part);
+        // rows that received a displaced panel row start from the gathered value
+        for (int e = w + threadIdx.x; e < count; e += blockDim.x) {
+          const int r = pl[1 + 2 * e];
+          if (r >= lo && r < hi) {
+            C acc = s_g[e];
+            const E* row = A + (size_t)k * a.lda + r;
+            for (int cb = 0; cb < w; cb += 16) {
+              E t[16];
+#pragma unroll
+              for (int u = 0; u < 16; ++u)
+                if (cb + u < w) t[u] = __ldg(row + (size_t)(cb + u) * a.lda);
+#pragma unroll
+              for (int u = 0; u < 16; ++u)
+                if (cb + u < w) cfms(acc, C{t[u].x, t[u].y}, s_x[cb + u]);
+            }
+            stc<R>(&nxt[r], acc);
+          }
+        }
+      }
+      if (p & 1) {
+        wprev = 0;
+      } else {
+        for (int i = threadIdx.x; i < w; i += blockDim.x) s_xprev[i] = s_x[i];
+        kprev = k;
+        wprev = w;
+      }
+      if (!grid_barrier(ctr, ++epoch, G, a.status)) return;
+    }
+    if (wprev > 0) {  // the last panel was even: its rows still go to v
+      if (rank == 0)
+        for (int i = threadIdx.x; i < wprev; i += blockDim.x) stc<R>(&v[kprev + i], s_xprev[i]);
+      if (!grid_barrier(ctr, ++epoch, G, a.status)) return;
+    }
+  }
+
+  const int nblk = (nn + kTrsvBlk - 1) / kTrsvBlk;
+  for (int sb = nblk - 1; sb >= 0; --sb) {
+    const int b0 = sb * kTrsvBlk, wb = min(kTrsvBlk, nn - b0);
+    for (int i = threadIdx.x; i < wb; i += blockDim.x) s_g[i] = ldc_cg<R>(&v[b0 + i]);
+    trsv_load_block<R>(A, a.lda, b0, b0, wb, s_T);
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      C v0 = lane < wb ? s_g[lane] : C{R(0), R(0)};
+      C v1 = lane + 32 < wb ? s_g[lane + 32] : C{R(0), R(0)};
+      for (int i = wb - 1; i >= 0; --i) {
+        const C src = (i < 32) ? v0 : v1;
+        C yi;
+        yi.re = __shfl_sync(0xffffffffu, src.re, i & 31);
+        yi.im = __shfl_sync(0xffffffffu, src.im, i & 31);
+        const C d = s_T[i * kTrsvBlk + i];
+        const R den = R(1) / fma(d.re, d.re, d.im * d.im);
+        const C xi{(yi.re * d.re + yi.im * d.im) * den, (yi.im * d.re - yi.re * d.im) * den};
+        if (lane == i) v0 = xi;
+        if (lane + 32 == i) v1 = xi;
+        if (lane < i) cfms(v0, s_T[i * kTrsvBlk + lane], xi);
+        if (lane + 32 < i) cfms(v1, s_T[i * kTrsvBlk + lane + 32], xi);
+      }
+      if (lane < wb) s_x[lane] = v0;
+      if (lane + 32 < wb) s_x[lane + 32] = v1;
+    }
+    __syncthreads();
+    if (rank == 0)
+      for (int i = threadIdx.x; i < wb; i += blockDim.x) stc<R>(&xo[b0 + i], s_x[i]);
+    if (b0 > 0) {
+      const int per = (b0 + G - 1) / G;
+      const int lo = min(b0, rank * per), hi = min(b0, lo + per);
+      trsv_rows<R>(A, a.lda, b0, wb, s_x, v, v, lo, hi, s_part);
+    }
+    if (!grid_barrier(ctr, ++epoch, G, a.status)) return;
+  }
+  const int per = (nn + G - 1) / G;
+  const int lo = min(nn, rank * per), hi = min(nn, lo + per);
+  for (int r = lo + threadIdx.x; r < hi; r += blockDim.x) v[r] = __ldcg(&xo[r]);
+}
+
+// ---------------------------------------------------------------------------
 // Host side.
 // ---------------------------------------------------------------------------
 int lu_ensure_workspace(bem_ctx* ctx, int nn, int batch) {
@@ -1149,6 +1405,78 @@ static int cluster_size(bem_ctx* ctx) {
   return cs;
 }
 
+// Uploads the panel starts of the factorisation just enqueued; only when they
+// differ from the last upload (the choice of widths depends on sizes only, so
+// repeated factorisations of one size upload once).
+static int trsv_upload_panels(bem_ctx* ctx, int nn) {
+  LuWork& L = ctx->lu;
+  std::vector<int> ps;
+  ps.reserve(L.panels.size() + 1);
+  for (const auto& pw : L.panels) ps.push_back(pw.first);
+  ps.push_back(nn);
+  if (ps == L.pstart_host && L.pstart) return BEM_OK;
+  if (L.pstart_cap < (int)ps.size()) {
+    cudaFree(L.pstart);
+    L.pstart = nullptr;
+    L.pstart_cap = 0;
+    BEM_CUDA(ctx, cudaMalloc(&L.pstart, ps.size() * sizeof(int)));
+    L.pstart_cap = (int)ps.size();
+  }
+  L.pstart_host = ps;
+  BEM_CUDA(ctx, cudaMemcpyAsync(L.pstart, L.pstart_host.data(), ps.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                ctx->stream));
+  return BEM_OK;
+}
+
+// One cooperative k_trsv launch over `batch` problems: forward (with the
+// interchanges of the last factorisation) and back substitution, or back
+// substitution only.
+template <typename R>
+static int trsv_coop(bem_ctx* ctx, const void* A, size_t lda, size_t bstride, int nn, int batch, void* v,
+                     size_t vstride, bool forward) {
+  using E = typename Elt<R>::T;
+  LuWork& L = ctx->lu;
+  const size_t wbytes = (size_t)2 * nn * batch * sizeof(E);
+  if (L.trsv_w_bytes < wbytes) {
+    cudaFree(L.trsv_w);
+    L.trsv_w = nullptr;
+    L.trsv_w_bytes = 0;
+    BEM_CUDA(ctx, cudaMalloc(&L.trsv_w, wbytes));
+    L.trsv_w_bytes = wbytes;
+  }
+  if (!L.trsv_ctr) BEM_CUDA(ctx, cudaMalloc(&L.trsv_ctr, kMaxBatch * sizeof(unsigned)));
+  if (batch < 1 || batch > kMaxBatch) return fail(ctx, BEM_ERR_ARG, "batch size out of range");
+  const size_t smem = (size_t)kTrsvBlk * kTrsvBlk * sizeof(cpx<R>);
+  BEM_CUDA(ctx, cudaFuncSetAttribute(k_trsv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0;
+  BEM_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trsv<R>, 256, smem));
+  int group = std::min(64, occ * ctx->num_sms / batch);
+  group = std::min(group, std::max(1, (nn + kTrsvBlk - 1) / kTrsvBlk));
+  if (group < 1) return fail(ctx, BEM_ERR_ARG, "cooperative solve does not fit the device");
+  TrsvArgs t{};
+  t.A = A;
+  t.lda = lda;
+  t.bstride = bstride;
+  t.nn = nn;
+  t.batch = batch;
+  t.group = group;
+  t.forward = forward ? 1 : 0;
+  t.npanels = forward ? (int)L.panels.size() : 0;
+  t.pstart = L.pstart;
+  t.perm = L.perm;
+  t.v = v;
+  t.vstride = vstride;
+  t.w = L.trsv_w;
+  t.ctr = L.trsv_ctr;
+  t.status = ctx->d_status;
+  BEM_CUDA(ctx, cudaMemsetAsync(L.trsv_ctr, 0, batch * sizeof(unsigned), ctx->stream));
+  void* args[] = {&t};
+  BEM_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)k_trsv<R>, dim3(group * batch), dim3(256), args, smem,
+                                            ctx->stream));
+  ctx->launches++;
+  return BEM_OK;
+}
+
 template <typename R>
 static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int batch) {
   LuWork& L = ctx->lu;
@@ -1234,7 +1562,7 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     const int c0 = k + w;
     if (c0 < ncols) {
       const int cols = ncols - c0;
-      const int blocks = std::max(1, std::min((cols + 7) / 8, (4 * ctx->num_sms + batch - 1) / batch));
+      const int blocks = std::max(1, std::min((cols + 31) / 32, (4 * ctx->num_sms + batch - 1) / batch));
       const bool tc = sizeof(R) == 4 && ctx->use_tcgen05;
       {
         ProfScope ps(ctx, 2, 0.0);
@@ -1265,8 +1593,14 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     L.panels.push_back({k, w});
     k += w;
   }
-  const int nblocks = (nn + 63) / 64;
+  int rc = trsv_upload_panels(ctx, nn);
+  if (rc) return rc;
   ProfScope ps(ctx, 4, 0.0);
+  if (ctx->use_trsv_coop) {
+    using E = typename Elt<R>::T;
+    return trsv_coop<R>(ctx, A, lda, bstride, nn, batch, static_cast<E*>(A) + (size_t)nn * lda, bstride, false);
+  }
+  const int nblocks = (nn + 63) / 64;
   for (int sblk = nblocks - 1; sblk >= 0; --sblk) {
     const int b0 = sblk * 64;
     k_backsub<R><<<dim3(1 + (b0 + 255) / 256, batch), 256, bsmem, ctx->stream>>>(A, lda, bstride, nn, sblk,
@@ -1347,6 +1681,7 @@ static int lu_solve_vec_t(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int
   BEM_CUDA(ctx, cudaFuncSetAttribute(k_fwd_panel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem));
   BEM_CUDA(ctx, cudaFuncSetAttribute(k_backsub<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem));
   ProfScope ps(ctx, 4, 0.0);
+  if (ctx->use_trsv_coop) return trsv_coop<R>(ctx, A, lda, bstride, nn, batch, v, vstride, true);
   for (size_t p = 0; p < L.panels.size(); ++p) {
     const int k = L.panels[p].first, w = L.panels[p].second;
     const int* perm_p = L.perm + p * (size_t)batch * kPermStride;

@@ -57,6 +57,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch", type=int, default=8, help="frequencies per lockstep batch")
     ap.add_argument("--refine", type=int, default=3, help="FP64 refinement steps (mixed form)")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run only warmup+steps headline sweep batches and print a launch count "
+                         "(a small, short command to run under ncu); no bench line")
     return ap.parse_args()
 
 
@@ -233,6 +236,15 @@ def run_ours(args):
             ctx.prof(False)
         ctx.sync()
         return out
+
+    if args.profile_case:
+        for i in range(args.warmup + args.steps):
+            sweep_step(i)
+        ctx.sync()
+        print(json.dumps({"profile_case": "mixed sweep", "batch": B, "batches": args.warmup + args.steps,
+                          "launches": ctx.launches}), flush=True)
+        ctx.close()
+        return
 
     # --- accuracy of the mixed form against the plain FP64 path (untimed) ---
     fr0 = batch_freqs(0)
