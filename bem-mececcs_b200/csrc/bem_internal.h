@@ -194,6 +194,7 @@ int lu_ensure_workspace(bem_ctx* ctx, int nn, int batch);
 int lu_factor_solve(bem_ctx* ctx);
 // Factor and solve `batch` problems A + b*bstride (elements of complex64 when
 // fp32, else complex128), each nn x (nn+1) with the right-hand side last.
+int lu_lockstep_capacity(bem_ctx* ctx, int nn, bool fp32);
 int lu_factor_solve_batch(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int batch, bool fp32);
 // Solves with the factors of the last lu_factor_solve_batch for right-hand
 // sides v + b*vstride (overwritten by the solutions).

@@ -451,6 +451,15 @@ int bem_sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const doub
   return BEM_OK;
 }
 
+int bem_sweep_batch_limit(bem_ctx* ctx, int form, int* limit) {
+  if (!ctx || !limit || (form != BEM_FORM_PLAIN && form != BEM_FORM_MIXED)) return BEM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!ctx->have_mesh) return fail(ctx, BEM_ERR_STATE, "bem_sweep_batch_limit needs the mesh");
+  cudaSetDevice(ctx->device);
+  *limit = lu_lockstep_capacity(ctx, 3 * ctx->mesh.nbe, form == BEM_FORM_MIXED);
+  return BEM_OK;
+}
+
 int bem_prof_enable(bem_ctx* ctx, int on) {
   if (!ctx) return BEM_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);

@@ -1139,7 +1139,7 @@ __device__ __forceinline__ void trsv_rows(const typename Elt<R>::T* __restrict__
 // before any shared-memory store, so the block costs one memory round trip.
 template <typename R>
 __device__ __forceinline__ void trsv_load_block(const typename Elt<R>::T* __restrict__ A, size_t lda, int r0, int c0,
-                                                int w, cpx<R>* s_T) {
+                                                int w, cpx<R>* s_T, cpx<R>* s_rdiag = nullptr) {
   using E = typename Elt<R>::T;
   const int r = threadIdx.x & 63, cg = threadIdx.x >> 6;
   E t[16];
@@ -1152,6 +1152,7 @@ __device__ __forceinline__ void trsv_load_block(const typename Elt<R>::T* __rest
   for (int u = 0; u < 16; ++u) {
     const int c = cg * 16 + u;
     if (r < w && c < w) s_T[c * kTrsvBlk + r] = cpx<R>{t[u].x, t[u].y};
+    if (s_rdiag && r < w && c == r) s_rdiag[r] = crcp(cpx<R>{t[u].x, t[u].y});
   }
 }
 
@@ -1165,6 +1166,7 @@ __global__ void __launch_bounds__(256) k_trsv(TrsvArgs a) {
   __shared__ C s_x[kTrsvBlk];
   __shared__ C s_xprev[kTrsvBlk];
   __shared__ C s_part[4][64];
+  __shared__ C s_rd[kTrsvBlk];  // reciprocals of the diagonal of U (backward)
   const int prob = blockIdx.x / a.group, rank = blockIdx.x % a.group, G = a.group;
   if (prob >= a.batch) return;
   const E* A = static_cast<const E*>(a.A) + (size_t)prob * a.bstride;
@@ -1250,7 +1252,7 @@ __global__ void __launch_bounds__(256) k_trsv(TrsvArgs a) {
   for (int sb = nblk - 1; sb >= 0; --sb) {
     const int b0 = sb * kTrsvBlk, wb = min(kTrsvBlk, nn - b0);
     for (int i = threadIdx.x; i < wb; i += blockDim.x) s_g[i] = ldc_cg<R>(&v[b0 + i]);
-    trsv_load_block<R>(A, a.lda, b0, b0, wb, s_T);
+    trsv_load_block<R>(A, a.lda, b0, b0, wb, s_T, s_rd);
     __syncthreads();
     if (threadIdx.x < 32) {
       const int lane = threadIdx.x;
@@ -1261,9 +1263,7 @@ __global__ void __launch_bounds__(256) k_trsv(TrsvArgs a) {
         C yi;
         yi.re = __shfl_sync(0xffffffffu, src.re, i & 31);
         yi.im = __shfl_sync(0xffffffffu, src.im, i & 31);
-        const C d = s_T[i * kTrsvBlk + i];
-        const R den = R(1) / fma(d.re, d.re, d.im * d.im);
-        const C xi{(yi.re * d.re + yi.im * d.im) * den, (yi.im * d.re - yi.re * d.im) * den};
+        const C xi = yi * s_rd[i];
         if (lane == i) v0 = xi;
         if (lane + 32 == i) v1 = xi;
         if (lane < i) cfms(v0, s_T[i * kTrsvBlk + lane], xi);
@@ -1403,6 +1403,54 @@ static int cluster_size(bem_ctx* ctx) {
   cudaGetLastError();
   ctx->lu.cluster_cs = cs;
   return cs;
+}
+
+// Clusters of the panel kernel that can be resident at once (0 if unknown).
+template <typename R, int NB, int NT>
+static int cluster_capacity(int cs, int rp) {
+  const size_t smem = ((size_t)NB * rp + 4 * NB + 2 * 8 * NB) * sizeof(cpx<R>);
+  auto kern = k_panel_cluster<R, NB, NT>;
+  int n = 0;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+      cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs, 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess) n = 0;
+  }
+  cudaGetLastError();
+  return n;
+}
+
+template <typename R>
+static int lockstep_capacity_t(bem_ctx* ctx, int nn) {
+  const int cs = cluster_size(ctx);
+  const int rp = (nn + cs - 1) / cs;
+  if (rp > 512) return kMaxBatch;  // grid-panel fallback: problems take turns anyway
+  const bool big = rp > 256;
+  for (int nb : {64, 32, 16}) {
+    if (!cluster_panel_fits_any<R>(nb, rp)) continue;
+    int n = 0;
+    if (nb == 64) n = big ? cluster_capacity<R, 64, 512>(cs, rp) : cluster_capacity<R, 64, 256>(cs, rp);
+    if (nb == 32) n = big ? cluster_capacity<R, 32, 512>(cs, rp) : cluster_capacity<R, 32, 256>(cs, rp);
+    if (nb == 16) n = big ? cluster_capacity<R, 16, 512>(cs, rp) : cluster_capacity<R, 16, 256>(cs, rp);
+    return n >= 1 ? std::min(n, kMaxBatch) : kMaxBatch;
+  }
+  return kMaxBatch;
+}
+
+// Problems whose panels run in one wave: the first (tallest) panel's cluster
+// kernel, as many clusters as can be resident at once.
+int lu_lockstep_capacity(bem_ctx* ctx, int nn, bool fp32) {
+  return fp32 ? lockstep_capacity_t<float>(ctx, nn) : lockstep_capacity_t<double>(ctx, nn);
 }
 
 // Uploads the panel starts of the factorisation just enqueued; only when they

@@ -153,6 +153,8 @@ int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double z
   if (!mixed && form != BEM_FORM_PLAIN) return fail(ctx, BEM_ERR_ARG, "unknown form");
   if (batch < 1 || batch > kMaxBatch || nfreq < 0 || iters < 0 || iters > kMaxRefine)
     return fail(ctx, BEM_ERR_ARG, "bem_sweep: batch, count or refinement steps out of range");
+  // No more problems in lockstep than the panel kernel keeps resident at once.
+  batch = std::min(batch, lu_lockstep_capacity(ctx, 3 * ctx->mesh.nbe, mixed));
   int rc = ensure_sweep(ctx, batch, mixed);
   if (rc) return rc;
   SweepBuf& S = ctx->sweep;

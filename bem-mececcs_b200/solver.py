@@ -15,6 +15,8 @@ BemError(BEM_ERR_SINGULAR) where the reference's lu_assert exits.
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 
 from . import host
@@ -112,6 +114,14 @@ class BemSolver:
             ptr(f64([zcp.real, zcp.imag])), ptr(f64(self.c)), ptr(freqs), nf, fm, batch, refine,
             ptr(x), ptr(corr)), "bem_sweep")
         return x, corr
+
+    def sweep_batch_limit(self, form: str = "mixed") -> int:
+        """Largest lockstep batch bem_sweep uses for this mesh and form."""
+        out = ctypes.c_int(0)
+        fm = BEM_FORM_MIXED if form == "mixed" else BEM_FORM_PLAIN
+        self.ctx.check(self.ctx.L.bem_sweep_batch_limit(self.ctx.h, fm, ctypes.byref(out)),
+                       "bem_sweep_batch_limit")
+        return int(out.value)
 
     def solve_frequency(self, fr: float):
         """GHMATECD + LINSOLVE + un-swap: boundary displacements and tractions."""

@@ -55,7 +55,9 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--batch", type=int, default=8, help="frequencies per lockstep batch")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="frequencies per lockstep batch (0: the library's limit for this mesh, "
+                         "bem_sweep_batch_limit)")
     ap.add_argument("--refine", type=int, default=3, help="FP64 refinement steps (mixed form)")
     ap.add_argument("--profile-case", action="store_true",
                     help="run only warmup+steps headline sweep batches and print a launch count "
@@ -178,11 +180,12 @@ def run_ours(args):
     from bem_mececcs_b200 import capi
     from bem_mececcs_b200.solver import BemSolver
 
-    B, R = args.batch, args.refine
     s, d = meshgen.config_mesh("c2_2160")
     freqs = meshgen.sweep_frequencies(128, seed=3)
     mine = freqs[rank::world]
     sol = BemSolver(s, device=local)
+    limit = sol.sweep_batch_limit("mixed")
+    B, R = (min(args.batch, limit) if args.batch > 0 else limit), args.refine
     sol.ghmatece(compute_gest=True)
     sol.set_bc(d.kode, d.bc.astype(np.complex128), d.dam, d.rho)
     ctx = sol.ctx

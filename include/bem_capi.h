@@ -197,7 +197,10 @@ int bem_linsolve_async(bem_ctx *ctx);
  * time in lockstep.  form BEM_FORM_PLAIN: FP64 assembly and FP64 LU.
  * form BEM_FORM_MIXED: FP64 assembly plus a complex64 copy, FP32 LU with
  * TF32 tensor-core updates, then `refine` (0..8) steps of FP64 iterative
- * refinement against the FP64 matrix.  x_out (nfreq x nn complex, may be
+ * refinement against the FP64 matrix.  `batch` is an upper bound: no more
+ * problems run in lockstep than bem_sweep_batch_limit reports, so that every
+ * problem's panel factorisation runs in the same wave (results do not depend
+ * on the grouping).  x_out (nfreq x nn complex, may be
  * NULL) receives the raw solutions (before the un-swap); corr_out (nfreq,
  * may be NULL) the relative size max|d|/max|x| of the last refinement
  * correction.  With both NULL the call only enqueues work on ctx's stream. */
@@ -207,6 +210,11 @@ int bem_sweep(bem_ctx *ctx, const double zge[2], const double zcs[2],
               const double zcp[2], const double c[4], const double *freqs,
               int nfreq, int form, int batch, int refine, double *x_out,
               double *corr_out);
+
+/* Largest lockstep batch bem_sweep uses for this mesh and form: the number
+ * of panel-factorisation thread-block clusters the device keeps resident at
+ * once (7 for n = 6480 on a 148-SM B200), capped at 16. */
+int bem_sweep_batch_limit(bem_ctx *ctx, int form, int *limit);
 
 /* Kernel-class timing with CUDA events on ctx's stream.  Classes:
  * 0 assembly, 1 LU panel, 2 row interchange + triangular solve,
