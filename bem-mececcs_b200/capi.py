@@ -84,6 +84,7 @@ def lib():
     L.bem_prof_reset.argtypes = [vp]
     L.bem_prof_read.argtypes = [vp, vp, vp, vp]
     L.bem_measure_fp64_peak.argtypes = [vp, vp]
+    L.bem_measure_peaks.argtypes = [vp, vp]
     L.bem_sweep.argtypes = [vp, vp, vp, vp, vp, vp, ip, ip, ip, ip, vp, vp]
     L.bem_sweep_batch_limit.argtypes = [vp, ip, P(ip)]
     _lib = L
@@ -155,6 +156,13 @@ class Context:
         out = np.zeros(1)
         self.check(self.L.bem_measure_fp64_peak(self.h, ptr(out)), "bem_measure_fp64_peak")
         return float(out[0])
+
+    def peaks(self) -> dict:
+        """bem_measure_peaks: measured arithmetic peaks, TFLOP/s."""
+        out = np.zeros(5)
+        self.check(self.L.bem_measure_peaks(self.h, ptr(out)), "bem_measure_peaks")
+        keys = ["fp64_fma", "fp32_fma", "fp64_dmma", "tf32_umma_n128", "tf32_umma_n256"]
+        return {k: round(float(v), 2) for k, v in zip(keys, out)}
 
     def sync(self):
         return self.check(self.L.bem_sync(self.h), "bem_sync")

@@ -211,6 +211,8 @@ int tc_ensure(bem_ctx* ctx, int nn, int batch);
 void tc_release(bem_ctx* ctx);
 int tc_trailing_update(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int k, int w, int batch);
 int measure_fp64_peak(bem_ctx* ctx, double* tflops);
+int measure_fma_peaks(bem_ctx* ctx, double* fp64_tflops, double* fp32_tflops);
+int measure_tf32_peak(bem_ctx* ctx, int n, double* tflops);
 
 int check_status(bem_ctx* ctx);
 

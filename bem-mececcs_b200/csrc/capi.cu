@@ -510,6 +510,18 @@ int bem_measure_fp64_peak(bem_ctx* ctx, double* tflops) {
   return measure_fp64_peak(ctx, tflops);
 }
 
+int bem_measure_peaks(bem_ctx* ctx, double* out) {
+  if (!ctx || !out) return BEM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  BEM_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->stream));
+  int rc = measure_fma_peaks(ctx, &out[0], &out[1]);
+  if (!rc) rc = measure_fp64_peak(ctx, &out[2]);
+  if (!rc) rc = measure_tf32_peak(ctx, 128, &out[3]);
+  if (!rc) rc = measure_tf32_peak(ctx, 256, &out[4]);
+  return rc;
+}
+
 int bem_unswap(bem_ctx* ctx, double* disp_out, double* trac_out) {
   if (!ctx || !disp_out || !trac_out) return BEM_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);

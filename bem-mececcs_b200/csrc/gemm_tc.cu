@@ -380,6 +380,69 @@ bool make_cmap(CUtensorMap* m, float2* base, int nn, size_t lda, size_t bstride,
 
 }  // namespace
 
+// tcgen05 kind::tf32 throughput: one elected thread per CTA issues `iters`
+// x 4 MMAs (M=128, N=n, K=8) from zeroed shared-memory operands into one
+// TMEM accumulator, then waits (bounded) for their completion.
+__global__ void __launch_bounds__(128, 1) k_umma_peak(int iters, int n, int* status) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const uint32_t abytes = kChunk, bbytes = (uint32_t)n * 128u;
+  for (uint32_t i = threadIdx.x; i < (abytes + bbytes) / 16; i += blockDim.x)
+    reinterpret_cast<uint4*>(smem)[i] = make_uint4(0, 0, 0, 0);
+  __shared__ uint64_t done;
+  __shared__ uint32_t s_tmem;
+  const int warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) mbar_init(&done, 1);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(256)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  if (threadIdx.x == 0) {
+    const uint32_t idesc =
+        (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    const uint32_t sa = smem_u32(smem), sb = sa + abytes;
+    for (int it = 0; it < iters; ++it)
+      for (int kk = 0; kk < 4; ++kk)
+        umma_tf32(tmem, sdesc(sa + 32u * kk), sdesc(sb + 32u * kk), idesc, (it | kk) ? 1u : 0u);
+    umma_commit(&done);
+    if (!mbar_wait(&done, 0)) atomicExch(&status[ST_TIMEOUT], 1);
+  }
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+  }
+}
+
+int measure_tf32_peak(bem_ctx* ctx, int n, double* tflops) {
+  if (n != 128 && n != 256) return fail(ctx, BEM_ERR_ARG, "UMMA peak probe: N must be 128 or 256");
+  const size_t smem = kChunk + (size_t)n * 128 + 1024;
+  BEM_CUDA(ctx, cudaFuncSetAttribute(k_umma_peak, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int iters = 2048;
+  cudaEvent_t e0, e1;
+  BEM_CUDA(ctx, cudaEventCreate(&e0));
+  BEM_CUDA(ctx, cudaEventCreate(&e1));
+  k_umma_peak<<<ctx->num_sms, 128, smem, ctx->stream>>>(iters / 8, n, ctx->d_status);  // warm-up
+  BEM_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
+  k_umma_peak<<<ctx->num_sms, 128, smem, ctx->stream>>>(iters, n, ctx->d_status);
+  BEM_CUDA(ctx, cudaEventRecord(e1, ctx->stream));
+  ctx->launches += 2;
+  BEM_CUDA(ctx, cudaEventSynchronize(e1));
+  float ms = 0.f;
+  BEM_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
+  *tflops = 2.0 * 128.0 * n * 8.0 * 4.0 * iters * ctx->num_sms / (ms * 1e-3) / 1e12;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return check_status(ctx);
+}
+
 int tc_ensure(bem_ctx* ctx, int nn, int batch) {
   TcWork& W = ctx->tc;
   if (W.nn == nn && W.batch >= batch && W.lhat) return BEM_OK;

@@ -1809,4 +1809,50 @@ int measure_fp64_peak(bem_ctx* ctx, double* tflops) {
   return BEM_OK;
 }
 
+// SIMT FMA throughput: 8 independent chains per thread, every result kept.
+template <typename T>
+__global__ void __launch_bounds__(256) k_fma_peak(T* out, int iters) {
+  T a[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) a[q] = T(1e-3) * T(threadIdx.x + q + 1);
+  const T b = T(0.999) + T(blockIdx.x & 7) * T(1e-6), c = T(1e-7);
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a[q] = fma(a[q], b, c);
+  }
+  T sum = T(0);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) sum += a[q];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = sum;
+}
+
+template <typename T>
+static int measure_fma_t(bem_ctx* ctx, int iters, double* tflops) {
+  const int blocks = ctx->num_sms * 8, threads = 256;
+  T* out = nullptr;
+  cudaEvent_t e0, e1;
+  BEM_CUDA(ctx, cudaMalloc(&out, (size_t)blocks * threads * sizeof(T)));
+  BEM_CUDA(ctx, cudaEventCreate(&e0));
+  BEM_CUDA(ctx, cudaEventCreate(&e1));
+  k_fma_peak<T><<<blocks, threads, 0, ctx->stream>>>(out, iters / 8);  // warm-up
+  BEM_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
+  k_fma_peak<T><<<blocks, threads, 0, ctx->stream>>>(out, iters);
+  BEM_CUDA(ctx, cudaEventRecord(e1, ctx->stream));
+  ctx->launches += 2;
+  BEM_CUDA(ctx, cudaEventSynchronize(e1));
+  float ms = 0.f;
+  BEM_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
+  *tflops = 2.0 * 8.0 * (double)blocks * threads * iters / (ms * 1e-3) / 1e12;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  return BEM_OK;
+}
+
+int measure_fma_peaks(bem_ctx* ctx, double* fp64_tflops, double* fp32_tflops) {
+  int rc = measure_fma_t<double>(ctx, 4096, fp64_tflops);
+  if (rc) return rc;
+  return measure_fma_t<float>(ctx, 16384, fp32_tflops);
+}
+
 }  // namespace bem

@@ -303,7 +303,7 @@ def run_ours(args):
     if not np.all(np.isfinite(x_pin)):
         raise RuntimeError("non-finite solution")
 
-    peak64 = ctx.fp64_peak_tflops()
+    mpeaks = ctx.peaks()
     value = world * args.steps * B / (ms_mix * 1e-3)
     value_plain = world * kp / (ms_plain * 1e-3)
     e2e_value = world * args.steps * B / (e2e_ms * 1e-3)
@@ -313,7 +313,7 @@ def run_ours(args):
     # Roofline of the dominant kernel of the headline form.
     peaks = _peaks()
     top = max(("assembly", "gemm", "panel", "residual"), key=lambda k: pm[k]["ms"])
-    roof = _roofline(top, pm[top], peaks, peak64)
+    roof = _roofline(top, pm[top], peaks, mpeaks)
     g64 = pp["gemm"]
     plain_gemm = g64["work"] / (g64["ms"] * 1e-3) / 1e12 if g64["ms"] > 0 else None
     line = {
@@ -343,6 +343,7 @@ def run_ours(args):
                        "kernel_share": {k: round(v["ms"] / t_plain["ms"], 4) for k, v in pp.items()}},
         "speedup_vs_plain_fp64": round(value / value_plain, 3),
         "roofline": roof,
+        "peaks_measured_tflops": mpeaks,
         "kernel_share": shares,
         "kernels": pm,
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT,
@@ -371,21 +372,31 @@ def _peaks():
         return {}
 
 
-def _roofline(name, k, peaks, peak64):
+def _roofline(name, k, peaks, mpeaks):
     """Roofline of one kernel class measured over the timed region."""
     secs = k["ms"] * 1e-3
     if name == "gemm":
-        bf16 = peaks.get("bf16_tflops")
-        peak = 0.5 * bf16 if bf16 else 0.5 * 1590.0
-        ach = k["work"] / secs / 1e12
+        # C -= L21 U12 with K = 64 (every FP32 panel at n = 6480 is 64 wide): 8*64 flops per
+        # complex element of C, whose 8 bytes are read and written once (TMA reduce-add), so
+        # the algorithmic traffic is flops / 32 bytes and the bound is HBM, not the tensor pipe.
+        hbm = peaks.get("hbm_gbs", 6650.0)
+        tf = k["work"] / secs / 1e12
+        gbs = k["work"] / 32.0 / secs / 1e9
         kern = ("k_gemm_tf32 (FP32 LU trailing update, TF32 mma.sync)"
                 if os.environ.get("BEM_TF32_MMA_SYNC") == "1" else
-                "k_pack_l21 + k_gemm_tc (FP32 LU trailing update, tcgen05 kind::tf32, TMEM accumulators)")
-        return {"bound": "tensor", "kernel": kern,
-                "achieved": round(ach, 3), "peak": round(peak, 1), "unit": "TFLOP/s",
-                "frac": round(ach / peak, 4), "traffic": None,
-                "peak_source": ("dense TF32 = half the measured dense BF16 cuBLAS figure of "
-                                "MEASURED_PEAKS.json" if bf16 else "half the fallback BF16 figure")}
+                "k_pack_l21 + k_gemm_tc (FP32 LU trailing update, tcgen05 kind::tf32, TMEM "
+                "accumulators, TMA reduce-add of C)")
+        return {"bound": "hbm", "kernel": kern,
+                "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(gbs / hbm, 4), "traffic": None,
+                "traffic_note": ("ncu, one launch of 2 problems: dram read+write = 1.15 x the "
+                                 "algorithmic C bytes (profiles/k_gemm_tc_2160.md)"),
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
+                "tensor": {"achieved_tflops": round(tf, 2),
+                           "peak_tflops": round(mpeaks["tf32_umma_n128"], 1),
+                           "frac": round(tf / mpeaks["tf32_umma_n128"], 4),
+                           "peak_source": "measured: tcgen05 kind::tf32 M=128 N=128 issue-rate "
+                                          "microbenchmark (bem_measure_peaks)"}}
     if name == "residual":
         hbm = peaks.get("hbm_gbs", 6650.0)
         nbytes = k["work"] / 8.0 * 16.0  # 8 n^2 flops <-> 16 n^2 bytes of the FP64 matrix

@@ -232,6 +232,12 @@ int bem_prof_read(bem_ctx *ctx, double *ms, long long *launches,
  * register-resident mma.sync loop; writes TFLOP/s. */
 int bem_measure_fp64_peak(bem_ctx *ctx, double *tflops);
 
+/* Microbenchmarks of the arithmetic peaks this library's rooflines use,
+ * TFLOP/s, in out[5]: FP64 FMA, FP32 FMA (SIMT, 8 independent chains per
+ * thread), FP64 DMMA m8n8k4, tcgen05 kind::tf32 with M=128 and N=128, and
+ * with N=256 (operands in shared memory, accumulator in TMEM). */
+int bem_measure_peaks(bem_ctx *ctx, double *out);
+
 #ifdef __cplusplus
 }
 #endif
