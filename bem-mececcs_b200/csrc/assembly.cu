@@ -577,7 +577,7 @@ int launch_static(bem_ctx* ctx, const double c[4], int compute_gest, double* hes
   return BEM_OK;
 }
 
-static StokesConsts<double> make_consts(const double zge_[2], const double zcs_[2],
+StokesConsts<double> make_consts(const double zge_[2], const double zcs_[2],
                                         const double zcp_[2], double fr) {
   // Solfund.for:29-35 in double on the host.
   auto mul = [](double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); };

@@ -164,6 +164,12 @@ struct bem_ctx {
   bem::Profiler prof;
   bem::SweepBuf sweep;
   bem::TcWork tc;
+  // interior-point workspace (interior.cu)
+  double4* int_pts = nullptr;
+  double2* int_ut = nullptr;    // [2][3nbe]: displacements, tractions
+  double2* int_part = nullptr;  // [l][chunks][12]
+  double2* int_out = nullptr;   // [l][12]
+  size_t int_cap_l = 0, int_cap_nn = 0;
   bool use_tcgen05 = true;  // FP32 trailing update on tcgen05 (else TF32 mma.sync)
   bool use_trsv_coop = true;  // one cooperative launch per triangular solve (else per-block launches)
 };
@@ -186,6 +192,13 @@ int launch_geometry(bem_ctx* ctx, const double* d_cx, const double* d_cy, const 
 int launch_static(bem_ctx* ctx, const double c[4], int compute_gest, double* hest_full);
 int launch_dynamic(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2],
                    const double c[4], double fr, int flags);
+// Solfund.for:29-35 constants of one frequency (assembly.cu).
+StokesConsts<double> make_consts(const double zge[2], const double zcs[2], const double zcp[2], double fr);
+// Interior displacements (and stresses when zssol is non-null) on the device (interior.cu).
+int interior_points(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], double rho,
+                    double fr, int l, const double* cxi, const double* cyi, const double* czi, const double* disp,
+                    const double* trac, double* zdsol, double* zssol);
+void release_interior(bem_ctx* ctx);
 int launch_dynamic_batch(bem_ctx* ctx, const DynBatch& b);
 int rhs_chunks(bem_ctx* ctx);
 

@@ -167,6 +167,7 @@ int bem_ctx_destroy(bem_ctx* ctx) {
   cudaFree(L.trsv_ctr);
   cudaFree(L.pstart);
   release_sweep(ctx);
+  release_interior(ctx);
   tc_release(ctx);
   for (cudaEvent_t e : ctx->prof.pool) cudaEventDestroy(e);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -510,6 +511,22 @@ int bem_measure_fp64_peak(bem_ctx* ctx, double* tflops) {
   return measure_fp64_peak(ctx, tflops);
 }
 
+int bem_interior(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], double rho, double fr,
+                 int l, const double* cxi, const double* cyi, const double* czi, const double* disp,
+                 const double* trac, double* zdsol, double* zssol) {
+  if (!ctx || !zge || !zcs || !zcp || l < 0 || (l > 0 && (!cxi || !cyi || !czi || !disp || !trac || !zdsol)))
+    return BEM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!ctx->have_mesh) return fail(ctx, BEM_ERR_STATE, "bem_interior needs the mesh");
+  if (ctx->mesh.ng * (int)sizeof(double4) > 1024 * 32) return fail(ctx, BEM_ERR_ARG, "Gauss rule too large");
+  cudaSetDevice(ctx->device);
+  BEM_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->stream));
+  int rc = interior_points(ctx, zge, zcs, zcp, rho, fr, l, cxi, cyi, czi, disp, trac, zdsol, zssol);
+  if (rc) return rc;
+  if (ctx->mesh_flag_bnd) return fail(ctx, BEM_ERR_DEGENERATE, "Jacobian below 1e-5 on a boundary element");
+  return BEM_OK;
+}
+
 int bem_measure_peaks(bem_ctx* ctx, double* out) {
   if (!ctx || !out) return BEM_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
@@ -627,6 +644,16 @@ void cuda_linsolve_(int* nn, int* n, double zh[], double zfi[]) {
     exit(1);
   }
   seam_check(rc, "cuda_linsolve");
+}
+
+void cuda_interec1_(int* n, int* nbe, int* npg, int* l, int* np, double cxi[], double cyi[], double czi[],
+                    double zge[2], double zcs[2], double zcp[2], double* c1, double* c2, double* c3, double* c4,
+                    double* fr, double zdfi[], double zfi[], double zdsol[], int* status) {
+  (void)n; (void)nbe; (void)npg; (void)np; (void)c1; (void)c2; (void)c3; (void)c4;
+  bem_ctx* ctx = seam_ctx();
+  int rc = bem_interior(ctx, zge, zcs, zcp, 0.0, *fr, *l, cxi, cyi, czi, zfi, zdfi, zdsol, nullptr);
+  seam_check(rc, "cuda_interec1");
+  *status = (rc == BEM_ERR_DEGENERATE) ? 1 : 0;
 }
 
 void deallocate_shared_gpu_data_(void) {

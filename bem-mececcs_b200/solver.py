@@ -66,6 +66,7 @@ class BemSolver:
         self.kode = i32(kode)
         self.zdfi = c128(zdfi)
         self.material = host.material(self.s.ge, self.s.rnu, dam, rho)
+        self.rho = float(rho)
         self.ctx.check(self.ctx.L.bem_dyn_upload(self.ctx.h, ptr(self.zdfi), ptr(self.kode)),
                        "bem_dyn_upload")
 
@@ -98,6 +99,24 @@ class BemSolver:
         trac = np.zeros(self.nn, dtype=np.complex128)
         self.ctx.check(self.ctx.L.bem_unswap(self.ctx.h, ptr(disp), ptr(trac)), "bem_unswap")
         return disp, trac
+
+    def interior(self, fr: float, disp, trac, cxi, cyi, czi, *, rho: float | None = None,
+                 stresses: bool = True):
+        """INTEREC's interior part on the device (bem_interior): displacements
+        zdsol (3L) and, with stresses, zssol (9L) at the points (cxi, cyi, czi)
+        from the boundary displacements and tractions of the un-swap."""
+        cxi, cyi, czi = f64(cxi), f64(cyi), f64(czi)
+        l = int(cxi.size)
+        zge, zcs, zcp = self.material
+        if rho is None:
+            rho = self.rho
+        zdsol = np.zeros(3 * l, dtype=np.complex128)
+        zssol = np.zeros(9 * l, dtype=np.complex128) if stresses else None
+        self.ctx.check(self.ctx.L.bem_interior(
+            self.ctx.h, ptr(f64([zge.real, zge.imag])), ptr(f64([zcs.real, zcs.imag])),
+            ptr(f64([zcp.real, zcp.imag])), float(rho), float(fr), l, ptr(cxi), ptr(cyi), ptr(czi),
+            ptr(c128(disp)), ptr(c128(trac)), ptr(zdsol), ptr(zssol)), "bem_interior")
+        return zdsol, zssol
 
     def sweep(self, freqs, *, form: str = "mixed", batch: int = 8, refine: int = 3,
               want_x: bool = True):

@@ -78,6 +78,18 @@ void cuda_ghmatecd_(int *nbe, int *npg, int *n, int *np, double zge[2],
  * matrix prints an error and exits, as the reference's lu_assert does. */
 void cuda_linsolve_(int *nn, int *n, double zh[], double zfi[]);
 
+/* Replaces cuda_interec1_, src/kernels/Interec1_cu.cu:44-237 (interface
+ * src/kernels/Interec1_cu.fd; caller src/Interec.for:142-164).  Displacements
+ * at the l interior points (cxi, cyi, czi) from the boundary displacements
+ * zfi and tractions zdfi (3*nbe complex each, after INTEREC's un-swap):
+ * zdsol (3*l complex).  c1..c4 are unused, as in the reference.
+ * *status = 1 on DET < 1e-5. */
+void cuda_interec1_(int *n, int *nbe, int *npg, int *l, int *np, double cxi[],
+                    double cyi[], double czi[], double zge[2], double zcs[2],
+                    double zcp[2], double *c1, double *c2, double *c3,
+                    double *c4, double *fr, double zdfi[], double zfi[],
+                    double zdsol[], int *status);
+
 /* Replaces deallocate_shared_gpu_data_, src/kernels/shared.cu:184-214. */
 void deallocate_shared_gpu_data_(void);
 
@@ -231,6 +243,20 @@ int bem_prof_read(bem_ctx *ctx, double *ms, long long *launches,
 /* Measures this GPU's FP64 tensor-core (DMMA) throughput with a
  * register-resident mma.sync loop; writes TFLOP/s. */
 int bem_measure_fp64_peak(bem_ctx *ctx, double *tflops);
+
+/* INTEREC's interior part on the device (src/Interec.for:81-285): for l
+ * interior points (cxi, cyi, czi), the displacements zdsol (3*l complex,
+ * NONSINGD as in src/Interec.for:111-133) and, when zssol is not NULL, the
+ * stresses zssol (9*l complex, SIGMAEC src/Sigmaec.for:9-212 contracted as in
+ * src/Interec.for:188-283; component (i, j) at 9k + i + 3j), from the
+ * boundary displacements `disp` and tractions `trac` (3*nbe complex each,
+ * after the un-swap, e.g. from bem_unswap).  rho is the density (stresses
+ * only).  Synchronous. */
+int bem_interior(bem_ctx *ctx, const double zge[2], const double zcs[2],
+                 const double zcp[2], double rho, double fr, int l,
+                 const double *cxi, const double *cyi, const double *czi,
+                 const double *disp, const double *trac, double *zdsol,
+                 double *zssol);
 
 /* Microbenchmarks of the arithmetic peaks this library's rooflines use,
  * TFLOP/s, in out[5]: FP64 FMA, FP32 FMA (SIMT, 8 independent chains per
