@@ -266,6 +266,7 @@ struct DynParams {
   float2* A32;      // optional complex64 copy (same layout)
   double2* zh_pre;  // optional, problem 0 only
   double2* zg_pre;  // optional, problem 0 only
+  double2* G;       // optional post-swap G (multiplies ZDFI), same layout as A
   double2* diag_h;  // [batch][nbe][9]
   double2* diag_g;
   double2* rhs_part;  // [batch][chunks][nn]
@@ -357,6 +358,7 @@ __global__ void __launch_bounds__(128) k_dyn_offdiag(DynParams p) {
   const StokesConsts<double>& kc = p.kb[prob];
   double2* A = p.A + (size_t)prob * p.a_stride;
   float2* A32 = p.A32 ? p.A32 + (size_t)prob * p.a_stride : nullptr;
+  double2* Gp = p.G ? p.G + (size_t)prob * p.a_stride : nullptr;
   const double2* diag_h = p.diag_h + (size_t)prob * p.nbe * 9;
   const double2* diag_g = p.diag_g + (size_t)prob * p.nbe * 9;
   const bool preswap = p.zh_pre && prob == 0;
@@ -469,6 +471,7 @@ __global__ void __launch_bounds__(128) k_dyn_offdiag(DynParams p) {
           }
           st(&A[(size_t)col * p.lda + row], h);
           if (A32) A32[(size_t)col * p.lda + row] = make_float2((float)h.re, (float)h.im);
+          if (Gp) st(&Gp[(size_t)col * p.lda + row], g);
           cfma(rhs[i], g, x);
         }
       }
@@ -638,6 +641,7 @@ int launch_dynamic_batch(bem_ctx* ctx, const DynBatch& b) {
   p.diag_h = b.diag_h;
   p.diag_g = b.diag_g;
   p.rhs_part = b.rhs_part;
+  p.G = b.G;
   p.status = ctx->d_status;
   for (int i = 0; i < b.batch; ++i) p.kb[i] = make_consts(b.zge, b.zcs, b.zcp, b.freqs[i]);
 

@@ -32,6 +32,7 @@ struct SweepBuf {
   double2 *diag_h = nullptr, *diag_g = nullptr;  // [batch][nbe][9]
   double2* rhs_part = nullptr;  // [batch][rhs_chunks][nn]
   unsigned long long* norm = nullptr;  // [kMaxRefine][batch][2] max|d|, max|x|
+  double2* G64 = nullptr;       // [batch] post-swap G (serving: right-hand-side reuse)
 };
 
 // One batched dynamic assembly: `batch` frequencies of the resident mesh.
@@ -45,6 +46,7 @@ struct DynBatch {
   double2 *zh_pre, *zg_pre;
   double2 *diag_h, *diag_g;  // [batch][nbe][9]
   double2* rhs_part;         // [batch][chunks][nn]
+  double2* G = nullptr;      // optional post-swap G, same layout as A
 };
 
 struct Mesh {
@@ -218,6 +220,15 @@ int lu_solve_vec(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int 
 int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], const double c[4],
           const double* freqs, int nfreq, int form, int batch, int iters, double* x_out, double* corr_out);
 void release_sweep(bem_ctx* ctx);
+// Serving (one problem per context): bytes a cached problem of size nn keeps
+// on the device; enqueue a full solve (assembly + LU (+ refinement), keeping
+// the post-swap G) or a right-hand-side-only solve with the cached factors,
+// asynchronously on ctx->stream; the raw solution's device address.
+size_t slot_footprint(int nn, int nbe, int ng, bool mixed);
+int slot_solve_full(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], const double c[4],
+                    double fr, bool mixed, int iters);
+int slot_solve_rhs(bem_ctx* ctx, bool mixed, int iters);
+const double2* slot_solution(bem_ctx* ctx, bool mixed, bool rhs_only);
 
 // Tensor-core FP32 trailing update (gemm_tc.cu).
 int tc_ensure(bem_ctx* ctx, int nn, int batch);

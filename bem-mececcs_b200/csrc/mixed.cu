@@ -69,6 +69,19 @@ __global__ void k_resid_final(const double2* __restrict__ A, size_t lda, size_t 
 }
 
 // x = (complex128) column nn of the FP32 system (the first, FP32, solution).
+// y = sum of the partials (y = A x), FP64.
+__global__ void k_gemv_final(const double2* __restrict__ part, int nn, int chunks, double2* y) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nn) return;
+  double re = 0.0, im = 0.0;
+  for (int c = 0; c < chunks; ++c) {
+    const double2 q = part[(size_t)c * nn + r];
+    re += q.x;
+    im += q.y;
+  }
+  y[r] = make_double2(re, im);
+}
+
 __global__ void k_x_init(const float2* __restrict__ A32, size_t lda, size_t a_stride, int nn, double2* x,
                          size_t x_stride) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -115,15 +128,17 @@ void free_sweep(SweepBuf& S) {
   cudaFree(S.diag_g);
   cudaFree(S.rhs_part);
   cudaFree(S.norm);
+  cudaFree(S.G64);
   S = SweepBuf{};
 }
 
-int ensure_sweep(bem_ctx* ctx, int batch, bool mixed) {
+int ensure_sweep(bem_ctx* ctx, int batch, bool mixed, bool keep_g = false) {
   SweepBuf& S = ctx->sweep;
   const int nn = 3 * ctx->mesh.nbe;
   const int nbe = ctx->mesh.nbe;
   const int chunks = rhs_chunks(ctx);
-  if (S.nn == nn && S.batch >= batch && (!mixed || S.A32) && S.rhs_chunks >= chunks) return BEM_OK;
+  if (S.nn == nn && S.batch >= batch && (!mixed || S.A32) && (!keep_g || S.G64) && S.rhs_chunks >= chunks)
+    return BEM_OK;
   free_sweep(S);
   S.nn = nn;
   S.batch = batch;
@@ -139,7 +154,32 @@ int ensure_sweep(bem_ctx* ctx, int batch, bool mixed) {
   BEM_CUDA(ctx, cudaMalloc(&S.diag_h, (size_t)nbe * 9 * batch * sizeof(double2)));
   BEM_CUDA(ctx, cudaMalloc(&S.diag_g, (size_t)nbe * 9 * batch * sizeof(double2)));
   BEM_CUDA(ctx, cudaMalloc(&S.rhs_part, (size_t)chunks * nn * batch * sizeof(double2)));
-  BEM_CUDA(ctx, cudaMalloc(&S.norm, (size_t)2 * batch * kMaxRefine * sizeof(unsigned long long)));
+  BEM_CUDA(ctx, cudaMalloc(&S.norm, (size_t)2 * batch * (kMaxRefine + 1) * sizeof(unsigned long long)));
+  if (keep_g) BEM_CUDA(ctx, cudaMalloc(&S.G64, S.a_stride * batch * sizeof(double2)));
+  return BEM_OK;
+}
+
+// `iters` refinement steps on the first `bsz` problems of S, the k-th step's
+// norms in slot it0 + k: r = b - A64 x (FP64, b = column nn), d = LU32^-1 r,
+// x += d.
+int refine_steps(bem_ctx* ctx, SweepBuf& S, int bsz, int iters, int it0) {
+  const int nn = S.nn;
+  const dim3 vgrid((nn + 255) / 256, bsz);
+  for (int it = 0; it < iters; ++it) {
+    {
+      ProfScope ps(ctx, 5, 8.0 * (double)nn * nn * bsz);
+      k_resid_partial<<<dim3((nn + kResidRows - 1) / kResidRows, S.resid_chunks, bsz), kResidRows, 0,
+                        ctx->stream>>>(S.A64, S.lda, S.a_stride, S.x64, nn, nn, S.resid_chunks, S.part);
+      k_resid_final<<<vgrid, 256, 0, ctx->stream>>>(S.A64, S.lda, S.a_stride, S.part, nn, S.resid_chunks, S.v32,
+                                                    nn);
+    }
+    ctx->launches += 2;
+    int rc = lu_solve_vec(ctx, S.A32, S.lda, S.a_stride, nn, bsz, S.v32, nn, true);
+    if (rc) return rc;
+    k_ir_update<<<vgrid, 256, 0, ctx->stream>>>(S.x64, nn, S.v32, nn, nn, S.norm + (size_t)2 * bsz * (it0 + it));
+    ctx->launches++;
+    BEM_CUDA(ctx, cudaGetLastError());
+  }
   return BEM_OK;
 }
 
@@ -188,21 +228,8 @@ int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double z
       ctx->launches++;
       BEM_CUDA(ctx, cudaMemsetAsync(S.norm, 0, (size_t)2 * bsz * kMaxRefine * sizeof(unsigned long long),
                                     ctx->stream));
-      for (int it = 0; it < iters; ++it) {
-        {
-          ProfScope ps(ctx, 5, 8.0 * (double)nn * nn * bsz);
-          k_resid_partial<<<dim3((nn + kResidRows - 1) / kResidRows, S.resid_chunks, bsz), kResidRows, 0,
-                            ctx->stream>>>(S.A64, S.lda, S.a_stride, S.x64, nn, nn, S.resid_chunks, S.part);
-          k_resid_final<<<vgrid, 256, 0, ctx->stream>>>(S.A64, S.lda, S.a_stride, S.part, nn, S.resid_chunks, S.v32,
-                                                        nn);
-        }
-        ctx->launches += 2;
-        rc = lu_solve_vec(ctx, S.A32, S.lda, S.a_stride, nn, bsz, S.v32, nn, true);
-        if (rc) return rc;
-        k_ir_update<<<vgrid, 256, 0, ctx->stream>>>(S.x64, nn, S.v32, nn, nn, S.norm + (size_t)2 * bsz * it);
-        ctx->launches++;
-        BEM_CUDA(ctx, cudaGetLastError());
-      }
+      rc = refine_steps(ctx, S, bsz, iters, 0);
+      if (rc) return rc;
     } else {
       rc = lu_factor_solve_batch(ctx, S.A64, S.lda, S.a_stride, nn, bsz, false);
       if (rc) return rc;
@@ -238,6 +265,91 @@ int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double z
   }
   if (x_out || corr_out) return check_status(ctx);
   return BEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Serving slots: one problem per context, kept on the device after its solve
+// (FP64 H, its factors and the post-swap G), so that a new right-hand side for
+// the same (mesh, material, omega, KODE) costs a GEMV and the refinement.
+// ---------------------------------------------------------------------------
+size_t slot_footprint(int nn, int nbe, int ng, bool mixed) {
+  const size_t lda = (size_t)((nn + 1) & ~1), a_stride = lda * (size_t)(nn + 1);
+  const int jc = std::max(1, std::min(64, 1024 / std::max(ng, 1)));
+  const size_t chunks = (size_t)(nbe + jc - 1) / jc;
+  const size_t resid_chunks = (size_t)(nn + kResidCols - 1) / kResidCols;
+  size_t b = a_stride * sizeof(double2) * 2;               // A64 and G64
+  if (mixed) b += a_stride * sizeof(float2);               // A32
+  b += (size_t)nn * (sizeof(double2) + sizeof(float2));   // x64, v32
+  b += resid_chunks * nn * sizeof(double2);                // residual partials
+  b += (size_t)nbe * 9 * 2 * sizeof(double2);              // diagonal blocks
+  b += chunks * nn * sizeof(double2);                      // RHS partials
+  b += (size_t)nn * (sizeof(int) + 2 * sizeof(double2));   // pivots, solve scratch
+  if (mixed) b += (size_t)(2 * nn + 2 * (nn + 1)) * 64 * sizeof(float);  // tensor-core operands
+  return b;
+}
+
+int slot_solve_full(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], const double c[4],
+                    double fr, bool mixed, int iters) {
+  if (iters < 0 || iters > kMaxRefine) return fail(ctx, BEM_ERR_ARG, "refinement steps out of range");
+  int rc = ensure_sweep(ctx, 1, mixed, true);
+  if (rc) return rc;
+  SweepBuf& S = ctx->sweep;
+  const int nn = S.nn;
+  BEM_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->stream));
+  DynBatch db{};
+  db.zge = zge;
+  db.zcs = zcs;
+  db.zcp = zcp;
+  db.c = c;
+  db.freqs = &fr;
+  db.batch = 1;
+  db.flags = BEM_FAST_SINGULAR;
+  db.A = S.A64;
+  db.lda = S.lda;
+  db.a_stride = S.a_stride;
+  db.A32 = mixed ? S.A32 : nullptr;
+  db.diag_h = S.diag_h;
+  db.diag_g = S.diag_g;
+  db.rhs_part = S.rhs_part;
+  db.G = S.G64;
+  rc = launch_dynamic_batch(ctx, db);
+  if (rc) return rc;
+  if (!mixed) return lu_factor_solve_batch(ctx, S.A64, S.lda, S.a_stride, nn, 1, false);
+  rc = lu_factor_solve_batch(ctx, S.A32, S.lda, S.a_stride, nn, 1, true);
+  if (rc) return rc;
+  k_x_init<<<(nn + 255) / 256, 256, 0, ctx->stream>>>(S.A32, S.lda, S.a_stride, nn, S.x64, nn);
+  ctx->launches++;
+  BEM_CUDA(ctx, cudaMemsetAsync(S.norm, 0, (size_t)2 * (kMaxRefine + 1) * sizeof(unsigned long long),
+                                ctx->stream));
+  return refine_steps(ctx, S, 1, iters, 0);
+}
+
+int slot_solve_rhs(bem_ctx* ctx, bool mixed, int iters) {
+  SweepBuf& S = ctx->sweep;
+  if (!S.G64 || !ctx->zdfi) return fail(ctx, BEM_ERR_STATE, "no cached problem on this context");
+  if (iters < 0 || iters > kMaxRefine) return fail(ctx, BEM_ERR_ARG, "refinement steps out of range");
+  const int nn = S.nn;
+  BEM_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->stream));
+  // b = G ZDFI (FP64): into column nn of A64 (the refinement's b), or into x64
+  // for the FP64 triangular solves.
+  k_resid_partial<<<dim3((nn + kResidRows - 1) / kResidRows, S.resid_chunks, 1), kResidRows, 0, ctx->stream>>>(
+      S.G64, S.lda, S.a_stride, ctx->zdfi, 0, nn, S.resid_chunks, S.part);
+  double2* b = mixed ? S.A64 + (size_t)nn * S.lda : S.x64;
+  k_gemv_final<<<(nn + 255) / 256, 256, 0, ctx->stream>>>(S.part, nn, S.resid_chunks, b);
+  ctx->launches += 2;
+  BEM_CUDA(ctx, cudaGetLastError());
+  if (!mixed) return lu_solve_vec(ctx, S.A64, S.lda, S.a_stride, nn, 1, S.x64, nn, false);
+  // x = 0, then one more step than requested: the first one is the FP32 solve.
+  BEM_CUDA(ctx, cudaMemsetAsync(S.x64, 0, (size_t)nn * sizeof(double2), ctx->stream));
+  BEM_CUDA(ctx, cudaMemsetAsync(S.norm, 0, (size_t)2 * (kMaxRefine + 1) * sizeof(unsigned long long),
+                                ctx->stream));
+  return refine_steps(ctx, S, 1, iters + 1, 0);
+}
+
+const double2* slot_solution(bem_ctx* ctx, bool mixed, bool rhs_only) {
+  SweepBuf& S = ctx->sweep;
+  if (mixed || rhs_only) return S.x64;
+  return S.A64 + (size_t)S.nn * S.lda;
 }
 
 }  // namespace bem

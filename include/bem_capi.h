@@ -258,6 +258,51 @@ int bem_interior(bem_ctx *ctx, const double zge[2], const double zcs[2],
                  const double *disp, const double *trac, double *zdsol,
                  double *zssol);
 
+/* ------------------------------------------------------------------------ */
+/* 3. Serving (no counterpart in the reference: its driver solves one mesh   */
+/*    at a time).                                                             */
+/* ------------------------------------------------------------------------ */
+
+/* A request loop on one GPU.  Requests (mesh, material, omega, boundary
+ * conditions) are solved as they arrive: a scheduler thread admits every
+ * request that fits `budget_bytes` of device memory into a slot (one problem
+ * with its own stream and workspaces) and enqueues it at once, so requests
+ * that arrive while others run overlap with them on the device.  A solved
+ * problem stays resident (H, its factors and the post-swap G): a later
+ * request with the same mesh, material, omega and KODE but a new right-hand
+ * side is solved with the cached factors (GEMV + solves).  Idle problems are
+ * evicted least-recently-used when a new one needs room.  form:
+ * BEM_FORM_PLAIN or BEM_FORM_MIXED (with `refine` refinement steps). */
+typedef struct bem_server bem_server;
+int bem_server_create(int device, double budget_bytes, int form, int refine,
+                      bem_server **out);
+int bem_server_destroy(bem_server *srv);
+/* Registers a mesh (the arrays of bem_mesh_upload, copied); returns its id. */
+int bem_server_add_mesh(bem_server *srv, int n, int nbe, int np, int npg,
+                        const int *cone, const double *cx, const double *cy,
+                        const double *cz, const double *cxm, const double *cym,
+                        const double *czm, const double *etas,
+                        const double *gi, const double *ome, int *mesh_id);
+/* material = {GE, nu, damping, density} (Inputecd.for:58-60); bc: 3*nbe
+ * complex (ZDFI), kode: 3*nbe.  Returns at once with a request id. */
+int bem_server_submit(bem_server *srv, int mesh_id, const double material[4],
+                      double fr, const double *bc, const int *kode,
+                      long long *req_id);
+/* Waits up to timeout_s for a request; on BEM_OK writes the boundary
+ * displacements and tractions (3*nbe complex each, after the un-swap) and
+ * info = {latency ms (submit to done), queueing ms (submit to start),
+ * 1 if solved with cached factors, device bytes of its slot}.  Returns the
+ * request's status (BEM_ERR_TIMEOUT if still running; the request then
+ * stays waitable).  A request is forgotten once waited for. */
+int bem_server_wait(bem_server *srv, long long req_id, double timeout_s,
+                    double *disp, double *trac, double *info);
+/* out[10] = {completed, p50 ms, p99 ms, solves/s (completed / time from the
+ * first submit to the last completion), cached-factor solves, evictions,
+ * peak admitted bytes, most slots busy at once, admitted bytes now,
+ * budget}. */
+int bem_server_stats(bem_server *srv, double *out);
+int bem_server_reset_stats(bem_server *srv);
+
 /* Microbenchmarks of the arithmetic peaks this library's rooflines use,
  * TFLOP/s, in out[5]: FP64 FMA, FP32 FMA (SIMT, 8 independent chains per
  * thread), FP64 DMMA m8n8k4, tcgen05 kind::tf32 with M=128 and N=128, and
