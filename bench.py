@@ -59,6 +59,10 @@ def parse_args():
                     help="frequencies per lockstep batch (0: the library's limit for this mesh, "
                          "bem_sweep_batch_limit)")
     ap.add_argument("--refine", type=int, default=3, help="FP64 refinement steps (mixed form)")
+    ap.add_argument("--serve-count", type=int, default=40,
+                    help="requests of the serving stream replayed in the served measurement "
+                         "(0 skips the stream; the 128-request served sweep always runs)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served measurements")
     ap.add_argument("--profile-case", action="store_true",
                     help="run only warmup+steps headline sweep batches and print a launch count "
                          "(a small, short command to run under ncu); no bench line")
@@ -358,10 +362,79 @@ def run_ours(args):
         line["cpu_baseline"] = {"value": round(1.0 / secs, 5), "unit": UNIT, "cores": threads,
                                 "kind": "port", "sample": sample}
     ctx.close()
+    if not args.no_serve:
+        line["served"] = run_served(args, s, d, mine, local)
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def _served_summary(st, wall_s):
+    return {"solves_per_s": round(st["solves_per_s"], 3), "p50_ms": round(st["p50_ms"], 2),
+            "p99_ms": round(st["p99_ms"], 2), "completed": int(st["completed"]),
+            "rhs_only": int(st["rhs_only"]), "evictions": int(st["evictions"]),
+            "max_busy": int(st["max_busy"]), "peak_gb": round(st["peak_bytes"] / 1e9, 2),
+            "wall_s": round(wall_s, 2)}
+
+
+def run_served(args, s, d, mine, device):
+    """The serving form (bem_server_*, one request per (mesh, omega, BCs)):
+    (1) this rank's share of the 128-frequency sweep on the 2160 mesh,
+    submitted as one burst of requests; (2) the first --serve-count requests
+    of the seeded serving stream (Poisson arrivals at 50/s, 240..12000
+    elements, 30% right-hand-side-only), replayed in real time.  Mixed and
+    plain FP64, HBM budget 160 GB.  Latency = submit to result on the host."""
+    from bem_mececcs_b200 import serve
+    mat = (s.ge, s.rnu, d.dam, d.rho)
+    bc = d.bc.astype(np.complex128)
+    out = {"budget_gb": 160.0}
+    sweep = {}
+    for form in ("mixed", "plain"):
+        srv = serve.Server(device=device, budget_bytes=160e9, form=form, refine=args.refine)
+        mid = srv.add_mesh(s)
+        srv.wait(srv.submit(mid, mat, 0.05, bc, d.kode))  # warm-up (an omega not in the sweep)
+        srv.reset_stats()
+        t0 = time.perf_counter()
+        ids = [srv.submit(mid, mat, float(f), bc, d.kode) for f in mine]
+        for i in ids:
+            srv.wait(i)
+        sweep[form] = _served_summary(srv.stats(), time.perf_counter() - t0)
+        srv.close()
+    sweep["speedup_mixed_vs_plain"] = round(sweep["mixed"]["solves_per_s"] /
+                                            max(sweep["plain"]["solves_per_s"], 1e-9), 3)
+    out["sweep_2160"] = sweep
+    if args.serve_count > 0:
+        reqs = serve.serving_workload(count=args.serve_count)
+        meshes, prepared = {}, []
+        for r in reqs:
+            if r.key not in meshes:
+                meshes[r.key] = serve.request_mesh(r)
+            prepared.append((r, *serve.request_bc(meshes[r.key], r)))
+        stream = {"requests": len(reqs), "arrival_rate_per_s": 50.0,
+                  "elements": [int(min(r.grid[0] * r.grid[1] for r in reqs)),
+                               int(max(r.grid[0] * r.grid[1] for r in reqs))]}
+        for form in ("mixed", "plain"):
+            srv = serve.Server(device=device, budget_bytes=160e9, form=form, refine=args.refine)
+            ids_mesh = {k: srv.add_mesh(m) for k, m in meshes.items()}
+            wm = serve.request_mesh(serve.Request(0.0, (12, 10), 1, 0.0, mat, (0, 0, 1)))
+            w = srv.add_mesh(wm)
+            srv.wait(srv.submit(w, mat, 1.0, *serve.request_bc(wm, serve.Request(
+                0.0, (12, 10), 1, 0.0, mat, (0.0, 0.0, 1.0)))))
+            srv.reset_stats()
+            t0 = time.perf_counter()
+            ids = []
+            for r, rbc, rk in prepared:
+                dt = r.t - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                ids.append(srv.submit(ids_mesh[r.key], r.material, r.fr, rbc, rk))
+            for i in ids:
+                srv.wait(i, timeout=1800.0)
+            stream[form] = _served_summary(srv.stats(), time.perf_counter() - t0)
+            srv.close()
+        out["stream"] = stream
+    return out
 
 
 def _peaks():
