@@ -699,6 +699,132 @@ int launch_dynamic(bem_ctx* ctx, const double zge[2], const double zcs[2], const
 }
 
 // ---------------------------------------------------------------------------
+// Static boundary system (an extension: the reference keeps only the static
+// diagonals).  H(3I+i, 3J+j): Kelvin T of element J seen from collocation
+// point I (SOLFUNE, Solfune.for:18-31, NPG^2 rule of Nonsinge.for), G: Kelvin
+// U (SOLFUNE_G, Singge.for:195-198, rule of NONSINGE_G); I == J blocks are
+// HESTdiag and GESTdiag.  Then the boundary-condition swap with the real GE
+// (as Ghmatecd.for:316-333); A receives H (imaginary parts 0), Gs the
+// post-swap G (real, nn x nn).  32 collocation rows per warp, one element
+// column per warp iteration (coalesced column-major stores).
+// ---------------------------------------------------------------------------
+struct StaticSysParams {
+  int nbe, nn, ng;
+  size_t lda;
+  double c1, c2, c3, c4, ge;
+  const double4* gq;
+  const double4* eta;
+  const double4* colloc;
+  const double* hestdiag;
+  const double* gestdiag;
+  const int* kode;
+  double2* A;
+  double* Gs;
+};
+
+__global__ void __launch_bounds__(128) k_static_system(StaticSysParams p) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int I = blockIdx.x * 32 + lane;
+  if (I >= p.nbe) return;
+  const double4 P = p.colloc[I];
+  for (int J = blockIdx.y * 4 + w; J < p.nbe; J += gridDim.y * 4) {
+    double T[3][3], U[3][3];
+    if (J != I) {
+      const double4 nv = p.eta[J];
+      const double n3[3] = {nv.x, nv.y, nv.z};
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) T[i][j] = U[i][j] = 0.0;
+      const double4* q = p.gq + (size_t)J * p.ng;
+      for (int g = 0; g < p.ng; ++g) {
+        const double4 qq = q[g];
+        const double r1 = qq.x - P.x, r2 = qq.y - P.y, r3 = qq.z - P.z;
+        const double r = sqrt(fma(r1, r1, fma(r2, r2, r3 * r3)));
+        const double ir = 1.0 / r;
+        const double rd[3] = {r1 * ir, r2 * ir, r3 * ir};
+        const double rdn = rd[0] * n3[0] + rd[1] * n3[1] + rd[2] * n3[2];
+        const double ct = p.c3 * ir * ir * qq.w, cu = p.c1 * ir * qq.w;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const double dij = (i == j) ? 1.0 : 0.0;
+            T[i][j] = fma(ct, rdn * (p.c4 * dij + 3.0 * rd[i] * rd[j]) + p.c4 * (rd[j] * n3[i] - rd[i] * n3[j]), T[i][j]);
+            U[i][j] = fma(cu, p.c2 * dij + rd[i] * rd[j], U[i][j]);
+          }
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          T[i][j] = p.hestdiag[(size_t)9 * J + 3 * j + i];
+          U[i][j] = p.gestdiag[(size_t)9 * J + 3 * j + i];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const int col = 3 * J + j;
+      const bool swap = p.kode[col] == 0;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const size_t row = (size_t)3 * I + i;
+        double h = T[i][j], g = U[i][j];
+        if (swap) {
+          const double hg = h * p.ge;
+          h = -g;
+          g = -hg;
+        }
+        p.A[(size_t)col * p.lda + row] = make_double2(h, 0.0);
+        p.Gs[(size_t)col * p.nn + row] = g;
+      }
+    }
+  }
+}
+
+// Right-hand side: column nn of A = Gs * dfi (one thread per row).
+__global__ void k_static_rhs(const double* __restrict__ Gs, int nn, const double* __restrict__ dfi, double2* A,
+                             size_t lda) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nn) return;
+  double acc = 0.0;
+  for (int c = 0; c < nn; ++c) acc = fma(Gs[(size_t)c * nn + r], dfi[c], acc);
+  A[(size_t)nn * lda + r] = make_double2(acc, 0.0);
+}
+
+int launch_static_system(bem_ctx* ctx, const double c[4], double ge, const int* d_kode, const double* d_dfi,
+                         double2* A, size_t lda, double* Gs) {
+  const Mesh& m = ctx->mesh;
+  StaticSysParams p{};
+  p.nbe = m.nbe;
+  p.nn = 3 * m.nbe;
+  p.ng = m.ng;
+  p.lda = lda;
+  p.c1 = c[0];
+  p.c2 = c[1];
+  p.c3 = c[2];
+  p.c4 = c[3];
+  p.ge = ge;
+  p.gq = m.gq;
+  p.eta = m.eta;
+  p.colloc = m.colloc;
+  p.hestdiag = ctx->hestdiag;
+  p.gestdiag = ctx->gestdiag;
+  p.kode = d_kode;
+  p.A = A;
+  p.Gs = Gs;
+  const int ycols = std::max(1, std::min((m.nbe + 3) / 4, 4 * ctx->num_sms * 4 / std::max(1, (m.nbe + 31) / 32)));
+  k_static_system<<<dim3((m.nbe + 31) / 32, ycols), 128, 0, ctx->stream>>>(p);
+  ctx->launches++;
+  BEM_CUDA(ctx, cudaGetLastError());
+  k_static_rhs<<<(p.nn + 127) / 128, 128, 0, ctx->stream>>>(Gs, p.nn, d_dfi, A, lda);
+  ctx->launches++;
+  BEM_CUDA(ctx, cudaGetLastError());
+  return BEM_OK;
+}
+
+// ---------------------------------------------------------------------------
 // GHMATECD without allocation (bem_ghmatecd_noalloc).
 //
 // The assembly needs two scratch buffers besides its inputs and outputs: the

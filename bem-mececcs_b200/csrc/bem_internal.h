@@ -201,6 +201,10 @@ int interior_points(bem_ctx* ctx, const double zge[2], const double zcs[2], cons
                     double fr, int l, const double* cxi, const double* cyi, const double* czi, const double* disp,
                     const double* trac, double* zdsol, double* zssol);
 void release_interior(bem_ctx* ctx);
+// Static boundary system (extension): swapped H into A (complex, imaginary
+// parts 0), post-swap G into Gs (nn x nn real), column nn of A = Gs dfi.
+int launch_static_system(bem_ctx* ctx, const double c[4], double ge, const int* d_kode, const double* d_dfi,
+                         double2* A, size_t lda, double* Gs);
 int launch_dynamic_batch(bem_ctx* ctx, const DynBatch& b);
 int rhs_chunks(bem_ctx* ctx);
 

@@ -428,6 +428,57 @@ int bem_solve_dense(bem_ctx* ctx, int nn, const double* a, const double* b, doub
   return check_status(ctx);
 }
 
+int bem_static_solve(bem_ctx* ctx, const double c[4], double ge, const int* kode, const double* dfi, double* disp,
+                     double* trac) {
+  if (!ctx || !c || !kode || !dfi || !disp || !trac) return BEM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!ctx->have_mesh || !ctx->have_hest || !ctx->have_gest)
+    return fail(ctx, BEM_ERR_STATE, "bem_static_solve needs the mesh, HESTdiag and GESTdiag");
+  cudaSetDevice(ctx->device);
+  const int nn = 3 * ctx->mesh.nbe;
+  int rc = ensure_system(ctx, nn, false);
+  if (rc) return rc;
+  System& s = ctx->sys;
+  double* Gs = nullptr;
+  double* d_dfi = nullptr;
+  int* d_kode = nullptr;
+  BEM_CUDA(ctx, cudaMalloc(&Gs, (size_t)nn * nn * sizeof(double)));
+  BEM_CUDA(ctx, cudaMalloc(&d_dfi, (size_t)nn * sizeof(double)));
+  BEM_CUDA(ctx, cudaMalloc(&d_kode, (size_t)nn * sizeof(int)));
+  BEM_CUDA(ctx, cudaMemcpyAsync(d_dfi, dfi, (size_t)nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  BEM_CUDA(ctx, cudaMemcpyAsync(d_kode, kode, (size_t)nn * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  BEM_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->stream));
+  rc = launch_static_system(ctx, c, ge, d_kode, d_dfi, s.A, s.lda, Gs);
+  s.assembled = true;
+  s.solved = false;
+  s.have_preswap = false;
+  if (!rc) rc = lu_factor_solve(ctx);
+  std::vector<double2> x((size_t)nn);
+  if (!rc) {
+    s.solved = true;
+    BEM_CUDA(ctx, cudaMemcpyAsync(x.data(), s.A + (size_t)nn * s.lda, (size_t)nn * sizeof(double2),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    rc = check_status(ctx);
+  }
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(Gs);
+  cudaFree(d_dfi);
+  cudaFree(d_kode);
+  if (rc) return rc;
+  // Interec.for:59-67 with the real GE.
+  for (int i = 0; i < nn; ++i) {
+    if (kode[i] == 0) {
+      disp[i] = dfi[i];
+      trac[i] = x[i].x * ge;
+    } else {
+      disp[i] = x[i].x;
+      trac[i] = dfi[i];
+    }
+  }
+  if (ctx->mesh_flag_bnd) return fail(ctx, BEM_ERR_DEGENERATE, "Jacobian below 1e-5 on a boundary element");
+  return BEM_OK;
+}
+
 int bem_linsolve_async(bem_ctx* ctx) {
   if (!ctx) return BEM_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);

@@ -59,6 +59,18 @@ class BemSolver:
                        "bem_static_h")
         return out
 
+    def static_solve(self, kode, dfi):
+        """Static boundary solve (bem_static_solve, an extension with no
+        reference counterpart): real boundary displacements and tractions.
+        Needs ghmatece() first."""
+        nn = self.nn
+        disp = np.zeros(nn)
+        trac = np.zeros(nn)
+        self.ctx.check(self.ctx.L.bem_static_solve(self.ctx.h, ptr(f64(self.c)), float(self.s.ge),
+                                                   ptr(i32(kode)), ptr(f64(dfi)), ptr(disp), ptr(trac)),
+                       "bem_static_solve")
+        return disp, trac
+
     def set_gestdiag(self, gd):
         self.ctx.check(self.ctx.L.bem_set_gestdiag(self.ctx.h, ptr(f64(gd))), "bem_set_gestdiag")
 

@@ -192,6 +192,18 @@ int bem_linsolve(bem_ctx *ctx, double *zfi_out);
 int bem_solve_dense(bem_ctx *ctx, int nn, const double *a, const double *b,
                     double *x);
 
+/* Static boundary solve.  No counterpart in the reference (it keeps only
+ * HESTdiag and GESTdiag of the static problem); an extension built from its
+ * static pieces: H = Kelvin T off the diagonal (NONSINGE) + HESTdiag, G =
+ * Kelvin U off the diagonal (NONSINGE_G / SOLFUNE_G, Singge.for:83-202) +
+ * GESTdiag, the boundary-condition swap with the real GE, G*dfi, the FP64 LU
+ * of bem_linsolve and the un-swap.  c = {C1..C4} of the static material
+ * (the ones bem_ghmatece was called with), kode/dfi: 3*nbe; disp/trac:
+ * 3*nbe real.  Replaces any assembled system of ctx. */
+int bem_static_solve(bem_ctx *ctx, const double c[4], double ge,
+                     const int *kode, const double *dfi, double *disp,
+                     double *trac);
+
 /* The Interec.for:59-67 un-swap of the last solution: boundary
  * displacements into disp_out and tractions into trac_out (nn complex). */
 int bem_unswap(bem_ctx *ctx, double *disp_out, double *trac_out);

@@ -792,3 +792,109 @@ int orc_interior_stress(int n, int nbe, int np, int npg, const int *cone,
     }
     return status;
 }
+
+/* EXTENSION (the reference never solves a static system: it only keeps
+ * HESTdiag and GESTdiag): the static boundary solve assembled from the
+ * reference's own static pieces.  H: off-diagonal 3x3 blocks NONSINGE
+ * (Kelvin T, Nonsinge.for:12-121), diagonal blocks HESTdiag (rigid body,
+ * Ghmatece.for:258-282).  G: off-diagonal blocks NONSINGE_G (Kelvin U,
+ * Singge.for:83-173 with SOLFUNE_G, Singge.for:195-198) over the element's
+ * own four corners, diagonal blocks GESTdiag (SINGGE, Singge.for:11-81).
+ * Rows and columns over the NBE boundary elements, as in GHMATECD; then the
+ * boundary-condition swap of Ghmatecd.for:316-333 with the real GE, the
+ * right-hand side G*DFI, the solve (ZGESV restated, imaginary parts zero)
+ * and the un-swap of Interec.for:59-67.  h_out / g_out (nn x nn, after the
+ * swap, column-major) may be NULL. */
+int orc_static_solve(int n, int nbe, int np, int npg, const int *cone,
+                     const double *cx, const double *cy, const double *cz,
+                     const double *cxm, const double *cym, const double *czm,
+                     const double *etas, const double *gi, const double *ome,
+                     double ge, double rnu, const int *kode, const double *dfi,
+                     double *disp, double *trac, double *h_out, double *g_out)
+{
+    const int nn = 3 * nbe;
+    double c[4];
+    orc_static_consts(ge, rnu, c);
+    double *hd = malloc((size_t)9 * nbe * sizeof(double));
+    double *gd = malloc((size_t)9 * nbe * sizeof(double));
+    double *h = malloc((size_t)nn * nn * sizeof(double));
+    double *g = malloc((size_t)nn * nn * sizeof(double));
+    double *a = malloc((size_t)2 * nn * nn * sizeof(double));
+    double *b = malloc((size_t)2 * nn * sizeof(double));
+    int *ipiv = malloc((size_t)nn * sizeof(int));
+    int status = -1;
+    if (!hd || !gd || !h || !g || !a || !b || !ipiv) goto out;
+    status = orc_ghmatece(n, nbe, np, npg, cone, cx, cy, cz, cxm, cym, czm, etas, gi, ome, ge,
+                          rnu, hd, gd, NULL);
+#pragma omp parallel for schedule(dynamic, 4) reduction(max : status)
+    for (int j = 0; j < nbe; ++j) {
+        double co[4][3];
+        load_co(n, j, cone, cx, cy, cz, co);
+        for (int i = 0; i < nbe; ++i) {
+            double he[3][3], gel[3][3];
+            if (i == j) {
+                memcpy(he, hd + 9 * j, sizeof he);
+                memcpy(gel, gd + 9 * j, sizeof gel);
+            } else {
+                int s = nonsinge(he, (const double (*)[3])co, cxm[i], cym[i], czm[i],
+                                 etas + 3 * j, npg, gi, ome, c[2], c[3]);
+                int s2 = nonsinge_g(gel, (const double (*)[3])co, cxm[i], cym[i], czm[i], npg,
+                                    gi, ome, c[0], c[1]);
+                if (s > status) status = s;
+                if (s2 > status) status = s2;
+            }
+            for (int jj = 0; jj < 3; ++jj)
+                for (int ii = 0; ii < 3; ++ii) {
+                    size_t k = (size_t)(3 * j + jj) * nn + 3 * i + ii;
+                    h[k] = he[jj][ii];
+                    g[k] = gel[jj][ii];
+                }
+        }
+    }
+    /* Ghmatecd.for:324-332 (effective semantics) with real GE. */
+    for (int col = 0; col < nn; ++col) {
+        if (kode[col] != 0) continue;
+        for (int i = 0; i < nn; ++i) {
+            size_t k = (size_t)col * nn + i;
+            double hg = h[k] * ge;
+            h[k] = -g[k];
+            g[k] = -hg;
+        }
+    }
+    for (int i = 0; i < nn; ++i) {
+        double acc = 0.0;
+        for (int col = 0; col < nn; ++col) acc += g[(size_t)col * nn + i] * dfi[col];
+        b[2 * i] = acc;
+        b[2 * i + 1] = 0.0;
+    }
+    for (size_t k = 0; k < (size_t)nn * nn; ++k) {
+        a[2 * k] = h[k];
+        a[2 * k + 1] = 0.0;
+    }
+    if (h_out) memcpy(h_out, h, (size_t)nn * nn * sizeof(double));
+    if (g_out) memcpy(g_out, g, (size_t)nn * nn * sizeof(double));
+    if (orc_zgesv(nn, a, ipiv, b) != 0) {
+        status = ORC_SINGULAR;
+        goto out;
+    }
+    /* Interec.for:59-67 with real GE. */
+    for (int i = 0; i < nn; ++i) {
+        if (kode[i] == 0) {
+            disp[i] = dfi[i];
+            trac[i] = b[2 * i] * ge;
+        } else {
+            disp[i] = b[2 * i];
+            trac[i] = dfi[i];
+        }
+    }
+out:
+    free(hd);
+    free(gd);
+    free(h);
+    free(g);
+    free(a);
+    free(b);
+    free(ipiv);
+    return status;
+}
+

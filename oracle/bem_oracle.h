@@ -88,6 +88,17 @@ int orc_zgesv(int nn, double *a, int *ipiv, double *b);
 void orc_unswap(int nn, const int *kode, const double *zge, double *zfi,
                 double *zdfi);
 
+/* EXTENSION, no reference counterpart: the static boundary solve from the
+ * reference's static pieces (H: NONSINGE + HESTdiag; G: NONSINGE_G +
+ * GESTdiag), the boundary-condition swap with real GE, G*DFI, ZGESV and the
+ * un-swap.  disp/trac: 3nbe real; h_out/g_out (nn x nn) may be NULL. */
+int orc_static_solve(int n, int nbe, int np, int npg, const int *cone,
+                     const double *cx, const double *cy, const double *cz,
+                     const double *cxm, const double *cym, const double *czm,
+                     const double *etas, const double *gi, const double *ome,
+                     double ge, double rnu, const int *kode, const double *dfi,
+                     double *disp, double *trac, double *h_out, double *g_out);
+
 /* Interec.for:81-139: interior displacements ZDSOL(3L). */
 int orc_interior_disp(int n, int nbe, int np, int npg, const int *cone,
                       const double *cx, const double *cy, const double *cz,

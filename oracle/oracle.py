@@ -61,6 +61,8 @@ def lib():
         L.orc_interior_stress.argtypes = geo + [_d, _d, _d, _int, _d, _d, _d, _d, _d,
                                                 _d, _dbl, _dbl, _c, _c, _c]
         L.orc_solfund.argtypes = [_d, _d, _d, _d, _d, _d, _dbl, _c, _c]
+        L.orc_static_solve.argtypes = geo + [_d, _d, _d, _d, _d, _d, _dbl, _dbl, _i, _d, _d, _d,
+                                             ctypes.c_void_p, ctypes.c_void_p]
         _LIB = L
     return _LIB
 
@@ -174,6 +176,26 @@ class OracleProblem:
         if st != 0:
             raise RuntimeError(f"GHMATECD status {st}")
         return zh, zg
+
+    def static_solve(self, want_matrices: bool = False):
+        """EXTENSION (no reference counterpart): the static boundary solve,
+        orc_static_solve.  Returns (disp, trac[, h, g]) with the real BC
+        values of the dynamic input (its real parts) and its KODE."""
+        s, nn = self.s, self.nn
+        kode = np.ascontiguousarray(self.d.kode, dtype=np.int32)
+        dfi = np.ascontiguousarray(np.real(self.d.bc), dtype=np.float64)
+        disp = np.zeros(nn)
+        trac = np.zeros(nn)
+        h = np.zeros(nn * nn) if want_matrices else None
+        g = np.zeros(nn * nn) if want_matrices else None
+        hp = h.ctypes.data_as(ctypes.c_void_p) if want_matrices else None
+        gp = g.ctypes.data_as(ctypes.c_void_p) if want_matrices else None
+        st = lib().orc_static_solve(*self._geo(), self.cxm, self.cym, self.czm, self.etas,
+                                    self.gi, self.ome, float(s.ge), float(s.rnu), kode, dfi,
+                                    disp, trac, hp, gp)
+        if st != 0:
+            raise RuntimeError(f"static solve status {st}")
+        return (disp, trac, h, g) if want_matrices else (disp, trac)
 
     def system(self, fr: float, zdfi=None):
         """ZH after the boundary-condition swap and ZFI = ZG * ZDFI

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import oracle
-from bem_mececcs_b200 import formats
+from bem_mececcs_b200 import formats, meshgen
 
 EPS = 1.0e-3  # src/dtester.c:24
 
@@ -83,3 +83,21 @@ def test_results_format_roundtrip(tmp_path, golden_dir):
     back = formats.parse_results(path)[0]
     err = formats.dtester_errors(back, gold)
     assert max(err.values()) == 0.0
+
+
+def test_oracle_static_solve_satisfies_its_system():
+    """The static extension's restatement: H x = G dfi after the swap, and
+    the prescribed values come back unchanged through the un-swap."""
+    s, d = meshgen.config_mesh("c1_240")
+    d.kode[::5] = 0
+    d.bc[::5] = 0.02
+    p = oracle.OracleProblem(s, d)
+    disp, trac, h, g = p.static_solve(want_matrices=True)
+    nn = 3 * s.nbe
+    H = h.reshape(nn, nn, order="F")
+    G = g.reshape(nn, nn, order="F")
+    dfi = np.real(d.bc)
+    x = np.where(d.kode == 0, trac / s.ge, disp)
+    assert np.linalg.norm(H @ x - G @ dfi) < 1e-12 * np.linalg.norm(G @ dfi)
+    k0 = d.kode == 0
+    assert np.array_equal(disp[k0], dfi[k0]) and np.array_equal(trac[~k0], dfi[~k0])
