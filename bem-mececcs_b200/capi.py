@@ -86,6 +86,7 @@ def lib():
     L.bem_measure_fp64_peak.argtypes = [vp, vp]
     L.bem_measure_peaks.argtypes = [vp, vp]
     L.bem_static_solve.argtypes = [vp, vp, dp, vp, vp, vp, vp]
+    L.bem_batch_solve.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, ip, ip, vp, vp]
     L.bem_interior.argtypes = [vp, vp, vp, vp, dp, dp, ip, vp, vp, vp, vp, vp, vp, vp]
     L.bem_sweep.argtypes = [vp, vp, vp, vp, vp, vp, ip, ip, ip, ip, vp, vp]
     L.bem_sweep_batch_limit.argtypes = [vp, ip, P(ip)]

@@ -33,6 +33,7 @@ struct SweepBuf {
   double2* rhs_part = nullptr;  // [batch][rhs_chunks][nn]
   unsigned long long* norm = nullptr;  // [kMaxRefine][batch][2] max|d|, max|x|
   double2* G64 = nullptr;       // [batch] post-swap G (serving: right-hand-side reuse)
+  size_t norm_cap = 0;          // problems the norm buffer holds (batched solves)
 };
 
 // One batched dynamic assembly: `batch` frequencies of the resident mesh.
@@ -100,7 +101,7 @@ constexpr int kMaxGrid = 160;
 
 // Packed operands of the tensor-core FP32 trailing update (gemm_tc.cu).
 struct TcWork {
-  int nn = 0, batch = 0;
+  size_t lrows_cap = 0, urows_cap = 0;  // rows the operand buffers hold
   float* lhat = nullptr;  // [batch][2nn][64]  re/im rows of L21, TF32
   float* ure = nullptr;   // [batch][nn+1][64] Re U12, K-major, TF32
   float* uim = nullptr;   // [batch][nn+1][64] Im U12
@@ -172,6 +173,7 @@ struct bem_ctx {
   double2* int_part = nullptr;  // [l][chunks][12]
   double2* int_out = nullptr;   // [l][12]
   size_t int_cap_l = 0, int_cap_nn = 0;
+  bem::SweepBuf bbuf;  // padded systems of bem_batch_solve
   bool use_tcgen05 = true;  // FP32 trailing update on tcgen05 (else TF32 mma.sync)
   bool use_trsv_coop = true;  // one cooperative launch per triangular solve (else per-block launches)
 };
@@ -224,6 +226,10 @@ int lu_solve_vec(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int 
 int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], const double c[4],
           const double* freqs, int nfreq, int form, int batch, int iters, double* x_out, double* corr_out);
 void release_sweep(bem_ctx* ctx);
+// Lockstep solve of problems of uneven size (bem_batch_solve).
+int batch_solve(bem_ctx* driver, int nprob, bem_ctx* const* probs, const double* freqs, const double* zge,
+                const double* zcs, const double* zcp, const double* c, int form, int iters, double* const* x_out,
+                double* corr_out);
 // Serving (one problem per context): bytes a cached problem of size nn keeps
 // on the device; enqueue a full solve (assembly + LU (+ refinement), keeping
 // the post-swap G) or a right-hand-side-only solve with the cached factors,

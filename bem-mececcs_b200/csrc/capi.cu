@@ -503,6 +503,23 @@ int bem_sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const doub
   return BEM_OK;
 }
 
+int bem_batch_solve(bem_ctx* driver, int nprob, bem_ctx* const* probs, const double* freqs, const double* zge,
+                    const double* zcs, const double* zcp, const double* c, int form, int refine,
+                    double* const* x_out, double* corr_out) {
+  if (!driver || nprob < 0 || (nprob > 0 && (!probs || !freqs || !zge || !zcs || !zcp || !c))) return BEM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(driver->mu);
+  for (int p = 0; p < nprob; ++p) {
+    bem_ctx* pc = probs[p];
+    if (!pc || pc == driver) return fail(driver, BEM_ERR_ARG, "bem_batch_solve: bad problem context");
+    if (pc->device != driver->device) return fail(driver, BEM_ERR_ARG, "bem_batch_solve: contexts on other devices");
+    if (!pc->have_mesh || !pc->have_dyn || !pc->have_hest || !pc->have_gest)
+      return fail(driver, BEM_ERR_STATE, "bem_batch_solve: a problem lacks mesh, BCs or static diagonals");
+    if (pc->mesh.ng * (int)sizeof(double4) > 1024 * 32) return fail(driver, BEM_ERR_ARG, "Gauss rule too large");
+  }
+  cudaSetDevice(driver->device);
+  return batch_solve(driver, nprob, probs, freqs, zge, zcs, zcp, c, form, refine, x_out, corr_out);
+}
+
 int bem_sweep_batch_limit(bem_ctx* ctx, int form, int* limit) {
   if (!ctx || !limit || (form != BEM_FORM_PLAIN && form != BEM_FORM_MIXED)) return BEM_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);

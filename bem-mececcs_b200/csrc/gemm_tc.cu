@@ -445,12 +445,9 @@ int measure_tf32_peak(bem_ctx* ctx, int n, double* tflops) {
 
 int tc_ensure(bem_ctx* ctx, int nn, int batch) {
   TcWork& W = ctx->tc;
-  if (W.nn == nn && W.batch >= batch && W.lhat) return BEM_OK;
-  cudaFree(W.lhat);
-  cudaFree(W.ure);
-  cudaFree(W.uim);
-  W = TcWork{};
   const size_t lrows = (size_t)2 * nn * batch, urows = (size_t)(nn + 1) * batch;
+  if (W.lhat && lrows <= W.lrows_cap && urows <= W.urows_cap) return BEM_OK;
+  tc_release(ctx);
   BEM_CUDA(ctx, cudaMalloc(&W.lhat, lrows * 64 * sizeof(float)));
   BEM_CUDA(ctx, cudaMalloc(&W.ure, urows * 64 * sizeof(float)));
   BEM_CUDA(ctx, cudaMalloc(&W.uim, urows * 64 * sizeof(float)));
@@ -461,8 +458,8 @@ int tc_ensure(bem_ctx* ctx, int nn, int batch) {
   CUtensorMap* maps = static_cast<CUtensorMap*>(W.maps);
   if (!make_map(&maps[0], W.lhat, lrows) || !make_map(&maps[1], W.ure, urows) || !make_map(&maps[2], W.uim, urows))
     return fail(ctx, BEM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-  W.nn = nn;
-  W.batch = batch;
+  W.lrows_cap = lrows;
+  W.urows_cap = urows;
   BEM_CUDA(ctx, cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
   return BEM_OK;
 }

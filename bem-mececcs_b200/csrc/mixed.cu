@@ -118,6 +118,32 @@ __global__ void k_ir_update(double2* x, size_t x_stride, const float2* __restric
   }
 }
 
+// Padded embedding of a problem of size n in an npad system (bem_batch_solve):
+// the right-hand side moves from column n to column npad, rows n..npad-1 of
+// it are zero.
+template <typename T>
+__global__ void k_pad_rhs(T* A, size_t lda, int n, int npad) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= npad) return;
+  T v;
+  v.x = 0;
+  v.y = 0;
+  if (r < n) v = A[(size_t)n * lda + r];
+  A[(size_t)npad * lda + r] = v;
+}
+// Then columns < n get zero rows n..npad-1 and columns n..npad-1 become the
+// identity, so the padding never pivots and stays untouched by the updates.
+template <typename T>
+__global__ void k_pad_rest(T* A, size_t lda, int n, int npad) {
+  const int col = blockIdx.y;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= npad || col >= npad) return;
+  T v;
+  v.x = (col >= n && r == col) ? 1 : 0;
+  v.y = 0;
+  if (col >= n || r >= n) A[(size_t)col * lda + r] = v;
+}
+
 void free_sweep(SweepBuf& S) {
   cudaFree(S.A64);
   cudaFree(S.A32);
@@ -185,7 +211,10 @@ int refine_steps(bem_ctx* ctx, SweepBuf& S, int bsz, int iters, int it0) {
 
 }  // namespace
 
-void release_sweep(bem_ctx* ctx) { free_sweep(ctx->sweep); }
+void release_sweep(bem_ctx* ctx) {
+  free_sweep(ctx->sweep);
+  free_sweep(ctx->bbuf);
+}
 
 int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], const double c[4],
           const double* freqs, int nfreq, int form, int batch, int iters, double* x_out, double* corr_out) {
@@ -265,6 +294,178 @@ int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double z
   }
   if (x_out || corr_out) return check_status(ctx);
   return BEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Problems of uneven size (bem_batch_solve): sorted by size and grouped into
+// classes whose largest member is at most 1.25 x the smallest and whose count
+// fits the lockstep limit; each class is embedded in one padded size (the
+// problem, then the identity) and runs through the lockstep LU of bem_sweep.
+// Every problem is assembled from its own context (mesh, static diagonals,
+// BCs) straight into its padded slot, on the driver's stream.
+// ---------------------------------------------------------------------------
+namespace {
+
+int ensure_batchbuf(bem_ctx* d, int npad, int batch, bool mixed, int max_nbe, int max_chunks) {
+  SweepBuf& S = d->bbuf;
+  const size_t lda = (size_t)((npad + 1) & ~1), a_stride = lda * (size_t)(npad + 1);
+  const int resid_chunks = (npad + kResidCols - 1) / kResidCols;
+  const bool fits = S.A64 && a_stride * batch <= S.a_stride * S.batch && (!mixed || S.A32) &&
+                    (size_t)npad * batch <= (size_t)S.nn * S.batch && S.rhs_chunks >= max_chunks * 3 * max_nbe &&
+                    S.resid_chunks >= resid_chunks * npad * batch && (int)S.norm_cap >= batch;
+  if (!fits) {
+    free_sweep(S);
+    BEM_CUDA(d, cudaMalloc(&S.A64, a_stride * batch * sizeof(double2)));
+    if (mixed) BEM_CUDA(d, cudaMalloc(&S.A32, a_stride * batch * sizeof(float2)));
+    BEM_CUDA(d, cudaMalloc(&S.x64, (size_t)npad * batch * sizeof(double2)));
+    BEM_CUDA(d, cudaMalloc(&S.v32, (size_t)npad * batch * sizeof(float2)));
+    BEM_CUDA(d, cudaMalloc(&S.part, (size_t)resid_chunks * npad * batch * sizeof(double2)));
+    BEM_CUDA(d, cudaMalloc(&S.diag_h, (size_t)max_nbe * 9 * sizeof(double2)));
+    BEM_CUDA(d, cudaMalloc(&S.diag_g, (size_t)max_nbe * 9 * sizeof(double2)));
+    BEM_CUDA(d, cudaMalloc(&S.rhs_part, (size_t)max_chunks * 3 * max_nbe * sizeof(double2)));
+    BEM_CUDA(d, cudaMalloc(&S.norm, (size_t)2 * batch * (kMaxRefine + 1) * sizeof(unsigned long long)));
+    // capacities (in the units the check above compares)
+    S.batch = batch;
+    S.nn = npad;
+    S.lda = lda;
+    S.a_stride = a_stride;
+    S.rhs_chunks = max_chunks * 3 * max_nbe;
+    S.resid_chunks = resid_chunks * npad * batch;
+    S.norm_cap = batch;
+  }
+  return BEM_OK;
+}
+
+}  // namespace
+
+int batch_solve(bem_ctx* d, int nprob, bem_ctx* const* probs, const double* freqs, const double* zge,
+                const double* zcs, const double* zcp, const double* c, int form, int iters, double* const* x_out,
+                double* corr_out) {
+  const bool mixed = form == BEM_FORM_MIXED;
+  if (!mixed && form != BEM_FORM_PLAIN) return fail(d, BEM_ERR_ARG, "unknown form");
+  if (iters < 0 || iters > kMaxRefine) return fail(d, BEM_ERR_ARG, "refinement steps out of range");
+  std::vector<int> order(nprob);
+  for (int i = 0; i < nprob; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](int a, int b) { return probs[a]->mesh.nbe < probs[b]->mesh.nbe; });
+  BEM_CUDA(d, cudaMemsetAsync(d->d_status, 0, ST_COUNT * sizeof(int), d->stream));
+  std::vector<unsigned long long> hnorm;
+  for (int g0 = 0; g0 < nprob;) {
+    // one size class
+    const int n0 = 3 * probs[order[g0]]->mesh.nbe;
+    int g1 = g0 + 1;
+    int npad = n0;
+    while (g1 < nprob) {
+      const int n1 = 3 * probs[order[g1]]->mesh.nbe;
+      if (n1 * 4 > n0 * 5) break;
+      if (g1 - g0 + 1 > std::min(kMaxBatch, lu_lockstep_capacity(d, n1, mixed))) break;
+      npad = n1;
+      ++g1;
+    }
+    const int B = g1 - g0;
+    int max_nbe = 0, max_chunks = 0;
+    for (int k = g0; k < g1; ++k) {
+      max_nbe = std::max(max_nbe, probs[order[k]]->mesh.nbe);
+      max_chunks = std::max(max_chunks, rhs_chunks(probs[order[k]]));
+    }
+    int rc = ensure_batchbuf(d, npad, B, mixed, max_nbe, max_chunks);
+    if (rc) return rc;
+    SweepBuf& S = d->bbuf;
+    const size_t lda = (size_t)((npad + 1) & ~1), a_stride = lda * (size_t)(npad + 1);
+    for (int k = g0; k < g1; ++k) {
+      const int p = order[k], slot = k - g0;
+      bem_ctx* pc = probs[p];
+      const int n = 3 * pc->mesh.nbe;
+      std::lock_guard<std::mutex> lk(pc->mu);
+      cudaStream_t keep = pc->stream;
+      pc->stream = d->stream;
+      DynBatch db{};
+      db.zge = zge + 2 * p;
+      db.zcs = zcs + 2 * p;
+      db.zcp = zcp + 2 * p;
+      db.c = c + 4 * p;
+      db.freqs = freqs + p;
+      db.batch = 1;
+      db.flags = BEM_FAST_SINGULAR;
+      db.A = S.A64 + (size_t)slot * a_stride;
+      db.lda = lda;
+      db.a_stride = 0;
+      db.A32 = mixed ? S.A32 + (size_t)slot * a_stride : nullptr;
+      db.diag_h = S.diag_h;
+      db.diag_g = S.diag_g;
+      db.rhs_part = S.rhs_part;
+      const long long l0 = pc->launches;
+      BEM_CUDA(pc, cudaMemsetAsync(pc->d_status, 0, ST_COUNT * sizeof(int), d->stream));
+      rc = launch_dynamic_batch(pc, db);
+      pc->stream = keep;
+      d->launches += pc->launches - l0;
+      if (rc) return fail(d, rc, std::string("assembly of a batched problem: ") + pc->last_error);
+      if (n < npad) {
+        const dim3 rg((npad + 255) / 256);
+        k_pad_rhs<<<rg, 256, 0, d->stream>>>(db.A, lda, n, npad);
+        k_pad_rest<<<dim3(rg.x, npad), 256, 0, d->stream>>>(db.A, lda, n, npad);
+        d->launches += 2;
+        if (mixed) {
+          k_pad_rhs<<<rg, 256, 0, d->stream>>>(db.A32, lda, n, npad);
+          k_pad_rest<<<dim3(rg.x, npad), 256, 0, d->stream>>>(db.A32, lda, n, npad);
+          d->launches += 2;
+        }
+        BEM_CUDA(d, cudaGetLastError());
+      }
+    }
+    // the padded class through the lockstep LU (+ refinement)
+    SweepBuf V = S;  // a view with this class's size for refine_steps
+    V.nn = npad;
+    V.lda = lda;
+    V.a_stride = a_stride;
+    V.resid_chunks = (npad + kResidCols - 1) / kResidCols;
+    if (mixed) {
+      rc = lu_factor_solve_batch(d, V.A32, lda, a_stride, npad, B, true);
+      if (rc) return rc;
+      k_x_init<<<dim3((npad + 255) / 256, B), 256, 0, d->stream>>>(V.A32, lda, a_stride, npad, V.x64, npad);
+      d->launches++;
+      BEM_CUDA(d, cudaMemsetAsync(V.norm, 0, (size_t)2 * B * (kMaxRefine + 1) * sizeof(unsigned long long),
+                                  d->stream));
+      rc = refine_steps(d, V, B, iters, 0);
+      if (rc) return rc;
+    } else {
+      rc = lu_factor_solve_batch(d, V.A64, lda, a_stride, npad, B, false);
+      if (rc) return rc;
+    }
+    for (int k = g0; k < g1; ++k) {
+      const int p = order[k], slot = k - g0;
+      const int n = 3 * probs[p]->mesh.nbe;
+      if (x_out && x_out[p]) {
+        const double2* src = mixed ? V.x64 + (size_t)slot * npad : V.A64 + (size_t)slot * a_stride + (size_t)npad * lda;
+        BEM_CUDA(d, cudaMemcpyAsync(x_out[p], src, (size_t)n * sizeof(double2), cudaMemcpyDeviceToHost, d->stream));
+      }
+    }
+    if (corr_out) {
+      if (mixed && iters > 0) {
+        hnorm.assign((size_t)2 * B * (kMaxRefine + 1), 0ull);
+        BEM_CUDA(d, cudaMemcpyAsync(hnorm.data(), V.norm, hnorm.size() * sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToHost, d->stream));
+        BEM_CUDA(d, cudaStreamSynchronize(d->stream));
+        const size_t last = (size_t)2 * B * (iters - 1);
+        for (int k = g0; k < g1; ++k) {
+          double dm, xm;
+          const unsigned long long du = hnorm[last + 2 * (k - g0)], xu = hnorm[last + 2 * (k - g0) + 1];
+          memcpy(&dm, &du, sizeof dm);
+          memcpy(&xm, &xu, sizeof xm);
+          corr_out[order[k]] = xm > 0 ? dm / xm : 0.0;
+        }
+      } else {
+        for (int k = g0; k < g1; ++k) corr_out[order[k]] = 0.0;
+      }
+    }
+    g0 = g1;
+  }
+  BEM_CUDA(d, cudaStreamSynchronize(d->stream));
+  for (int p = 0; p < nprob; ++p) {
+    int rc = check_status(probs[p]);
+    if (rc) return fail(d, rc, std::string("batched problem: ") + probs[p]->last_error);
+    if (probs[p]->mesh_flag_bnd) return fail(d, BEM_ERR_DEGENERATE, "Jacobian below 1e-5 on a boundary element");
+  }
+  return check_status(d);
 }
 
 // ---------------------------------------------------------------------------

@@ -161,6 +161,37 @@ class BemSolver:
         return self.interec()
 
 
+def batch_solve(driver: Context, problems, *, form: str = "mixed", refine: int = 3):
+    """bem_batch_solve: problems = [(BemSolver with ghmatece() and set_bc()
+    done, omega), ...] of uneven sizes, solved in padded lockstep classes on
+    the driver context.  Returns (list of raw solutions, corrections); the
+    un-swapped (disp, trac) of problem p follow from `unswap_host`."""
+    n = len(problems)
+    ctxs = (ctypes.c_void_p * n)(*[p[0].ctx.h.value for p in problems])
+    freqs = f64([p[1] for p in problems])
+    zge = f64([[p[0].material[0].real, p[0].material[0].imag] for p in problems])
+    zcs = f64([[p[0].material[1].real, p[0].material[1].imag] for p in problems])
+    zcp = f64([[p[0].material[2].real, p[0].material[2].imag] for p in problems])
+    c = f64([p[0].c for p in problems])
+    xs = [np.zeros(p[0].nn, dtype=np.complex128) for p in problems]
+    xptr = (ctypes.c_void_p * n)(*[x.ctypes.data for x in xs])
+    corr = np.zeros(n)
+    fm = BEM_FORM_MIXED if form == "mixed" else BEM_FORM_PLAIN
+    driver.check(driver.L.bem_batch_solve(driver.h, n, ctxs, ptr(freqs), ptr(zge), ptr(zcs), ptr(zcp),
+                                          ptr(c), fm, refine, xptr, ptr(corr)), "bem_batch_solve")
+    return xs, corr
+
+
+def unswap_host(x, kode, zdfi, zge):
+    """Interec.for:59-67 on the host: (boundary displacements, tractions)."""
+    x = np.asarray(x)
+    kode = np.asarray(kode)
+    zdfi = np.asarray(zdfi, dtype=np.complex128)
+    disp = np.where(kode == 0, zdfi, x)
+    trac = np.where(kode == 0, x * zge, zdfi)
+    return disp, trac
+
+
 def solve_dense(ctx: Context, a: np.ndarray, b: np.ndarray) -> np.ndarray:
     """ZGESV on the device for one right-hand side; a is (n, n)."""
     n = b.shape[0]

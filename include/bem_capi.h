@@ -235,6 +235,23 @@ int bem_sweep(bem_ctx *ctx, const double zge[2], const double zcs[2],
               int nfreq, int form, int batch, int refine, double *x_out,
               double *corr_out);
 
+/* Many problems of uneven size in lockstep (the batching form for small
+ * meshes).  probs[p] is a context holding problem p's mesh, static
+ * diagonals (bem_ghmatece) and BCs (bem_dyn_upload); p is solved at
+ * freqs[p] with material zge/zcs/zcp[2p..2p+1] and static constants
+ * c[4p..4p+3].  The problems are sorted by size and grouped into classes
+ * (largest <= 1.25 x smallest, at most bem_sweep_batch_limit problems); each
+ * class is assembled into one padded size (the problem, then the identity,
+ * which never pivots) and factored, solved and -- form BEM_FORM_MIXED --
+ * refined together, on the driver context's stream and workspaces.  x_out[p]
+ * (3 nbe_p complex, raw as bem_sweep's; NULL entries skipped) and corr_out[p]
+ * (may be NULL) receive the results.  Synchronous.  No counterpart in the
+ * reference (its driver solves one mesh at a time). */
+int bem_batch_solve(bem_ctx *driver, int nprob, bem_ctx *const *probs,
+                    const double *freqs, const double *zge, const double *zcs,
+                    const double *zcp, const double *c, int form, int refine,
+                    double *const *x_out, double *corr_out);
+
 /* Largest lockstep batch bem_sweep uses for this mesh and form: the number
  * of panel-factorisation thread-block clusters the device keeps resident at
  * once (7 for n = 6480 on a 148-SM B200), capped at 16. */
