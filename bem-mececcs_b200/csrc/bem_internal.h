@@ -92,9 +92,8 @@ struct LuWork {
   void* trsv_w = nullptr;       // [batch][2][nn] scratch vectors
   size_t trsv_w_bytes = 0;
   unsigned* trsv_ctr = nullptr;  // [kMaxBatch] group barrier counters
-  int* pstart = nullptr;         // device copy of pstart_host
-  int pstart_cap = 0;
-  std::vector<int> pstart_host;  // first row of each panel of the last factorisation, then nn
+  int* pstart = nullptr;         // first row of each panel of the last factorisation, then nn
+                                 // (written by the panel kernels)
 };
 
 constexpr int kMaxGrid = 160;
@@ -174,6 +173,9 @@ struct bem_ctx {
   double2* int_out = nullptr;   // [l][12]
   size_t int_cap_l = 0, int_cap_nn = 0;
   bem::SweepBuf bbuf;  // padded systems of bem_batch_solve
+  std::vector<bem_ctx*> workers;   // bem_batch_solve: contexts whose streams run classes concurrently
+  void* pinned = nullptr;          // bem_batch_solve: pinned staging of solutions and norms
+  size_t pinned_bytes = 0;
   bool use_tcgen05 = true;  // FP32 trailing update on tcgen05 (else TF32 mma.sync)
   bool use_trsv_coop = true;  // one cooperative launch per triangular solve (else per-block launches)
 };

@@ -166,6 +166,9 @@ int bem_ctx_destroy(bem_ctx* ctx) {
   cudaFree(L.trsv_w);
   cudaFree(L.trsv_ctr);
   cudaFree(L.pstart);
+  for (bem_ctx* w : ctx->workers) bem_ctx_destroy(w);
+  ctx->workers.clear();
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
   release_sweep(ctx);
   release_interior(ctx);
   tc_release(ctx);

@@ -129,6 +129,8 @@ struct PanelArgs {
   int* perm;       // [B][kPermStride]: count, then dst/src pairs
   int perm_stride;
   int* status;
+  int* pstart;     // panel starts for the later solves: [pidx] = k, [pidx + 1] = k + w
+  int pidx;
   // grid fallback only:
   void* slot_val;
   int* slot_row;
@@ -284,6 +286,10 @@ __global__ void __launch_bounds__(NT, 1) k_panel_cluster(PanelArgs a) {
   const int rcount = max(0, min(rp, a.nn - rbase));
 
   load_slice_async<R>(A, a.lda, rbase, k, rcount, w, s_a, rp);
+  if (rank == 0 && prob == 0 && tid == 0 && a.pstart) {
+    a.pstart[a.pidx] = k;
+    a.pstart[a.pidx + 1] = k + w;
+  }
   if (rank == 0 && tid < w) {
     s_pdst[tid] = k + tid;
     s_psrc[tid] = k + tid;
@@ -575,6 +581,10 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel_grid(PanelArgs a) {
   C* drow = static_cast<C*>(a.drow);
 
   load_slice_async<R>(A, a.lda, rbase, k, rcount, w, s_a, rp);
+  if (b == 0 && tid == 0 && a.pstart) {
+    a.pstart[a.pidx] = k;
+    a.pstart[a.pidx + 1] = k + w;
+  }
   if (b == 0 && tid < w) {
     s_pdst[tid] = k + tid;
     s_psrc[tid] = k + tid;
@@ -1300,6 +1310,9 @@ int lu_ensure_workspace(bem_ctx* ctx, int nn, int batch) {
   BEM_CUDA(ctx, cudaMalloc(&L.ipiv, (size_t)nn * batch * sizeof(int)));
   const int max_panels = (nn + 15) / 16 + 1;
   BEM_CUDA(ctx, cudaMalloc(&L.perm, (size_t)max_panels * kPermStride * batch * sizeof(int)));
+  cudaFree(L.pstart);
+  L.pstart = nullptr;
+  BEM_CUDA(ctx, cudaMalloc(&L.pstart, (size_t)(max_panels + 1) * sizeof(int)));
   L.cap_nn = nn;
   L.cap_batch = batch;
   if (!L.slot_val) {
@@ -1453,29 +1466,6 @@ int lu_lockstep_capacity(bem_ctx* ctx, int nn, bool fp32) {
   return fp32 ? lockstep_capacity_t<float>(ctx, nn) : lockstep_capacity_t<double>(ctx, nn);
 }
 
-// Uploads the panel starts of the factorisation just enqueued; only when they
-// differ from the last upload (the choice of widths depends on sizes only, so
-// repeated factorisations of one size upload once).
-static int trsv_upload_panels(bem_ctx* ctx, int nn) {
-  LuWork& L = ctx->lu;
-  std::vector<int> ps;
-  ps.reserve(L.panels.size() + 1);
-  for (const auto& pw : L.panels) ps.push_back(pw.first);
-  ps.push_back(nn);
-  if (ps == L.pstart_host && L.pstart) return BEM_OK;
-  if (L.pstart_cap < (int)ps.size()) {
-    cudaFree(L.pstart);
-    L.pstart = nullptr;
-    L.pstart_cap = 0;
-    BEM_CUDA(ctx, cudaMalloc(&L.pstart, ps.size() * sizeof(int)));
-    L.pstart_cap = (int)ps.size();
-  }
-  L.pstart_host = ps;
-  BEM_CUDA(ctx, cudaMemcpyAsync(L.pstart, L.pstart_host.data(), ps.size() * sizeof(int), cudaMemcpyHostToDevice,
-                                ctx->stream));
-  return BEM_OK;
-}
-
 // One cooperative k_trsv launch over `batch` problems: forward (with the
 // interchanges of the last factorisation) and back substitution, or back
 // substitution only.
@@ -1556,6 +1546,8 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     pa.perm = perm_p;
     pa.perm_stride = kPermStride;
     pa.status = ctx->d_status;
+    pa.pstart = L.pstart;
+    pa.pidx = (int)L.panels.size();
     // Panel width: the widest of 64/32/16 whose rows fit one cluster, at most
     // 512 rows per CTA (one row per thread).
     const int rp_c = (m + cs - 1) / cs;
@@ -1641,8 +1633,6 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     L.panels.push_back({k, w});
     k += w;
   }
-  int rc = trsv_upload_panels(ctx, nn);
-  if (rc) return rc;
   ProfScope ps(ctx, 4, 0.0);
   if (ctx->use_trsv_coop) {
     using E = typename Elt<R>::T;

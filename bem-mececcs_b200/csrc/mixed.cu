@@ -306,37 +306,50 @@ int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double z
 // ---------------------------------------------------------------------------
 namespace {
 
-int ensure_batchbuf(bem_ctx* d, int npad, int batch, bool mixed, int max_nbe, int max_chunks) {
-  SweepBuf& S = d->bbuf;
-  const size_t lda = (size_t)((npad + 1) & ~1), a_stride = lda * (size_t)(npad + 1);
-  const int resid_chunks = (npad + kResidCols - 1) / kResidCols;
-  const bool fits = S.A64 && a_stride * batch <= S.a_stride * S.batch && (!mixed || S.A32) &&
-                    (size_t)npad * batch <= (size_t)S.nn * S.batch && S.rhs_chunks >= max_chunks * 3 * max_nbe &&
-                    S.resid_chunks >= resid_chunks * npad * batch && (int)S.norm_cap >= batch;
-  if (!fits) {
-    free_sweep(S);
-    BEM_CUDA(d, cudaMalloc(&S.A64, a_stride * batch * sizeof(double2)));
-    if (mixed) BEM_CUDA(d, cudaMalloc(&S.A32, a_stride * batch * sizeof(float2)));
-    BEM_CUDA(d, cudaMalloc(&S.x64, (size_t)npad * batch * sizeof(double2)));
-    BEM_CUDA(d, cudaMalloc(&S.v32, (size_t)npad * batch * sizeof(float2)));
-    BEM_CUDA(d, cudaMalloc(&S.part, (size_t)resid_chunks * npad * batch * sizeof(double2)));
-    BEM_CUDA(d, cudaMalloc(&S.diag_h, (size_t)max_nbe * 9 * sizeof(double2)));
-    BEM_CUDA(d, cudaMalloc(&S.diag_g, (size_t)max_nbe * 9 * sizeof(double2)));
-    BEM_CUDA(d, cudaMalloc(&S.rhs_part, (size_t)max_chunks * 3 * max_nbe * sizeof(double2)));
-    BEM_CUDA(d, cudaMalloc(&S.norm, (size_t)2 * batch * (kMaxRefine + 1) * sizeof(unsigned long long)));
-    // capacities (in the units the check above compares)
-    S.batch = batch;
-    S.nn = npad;
-    S.lda = lda;
-    S.a_stride = a_stride;
-    S.rhs_chunks = max_chunks * 3 * max_nbe;
-    S.resid_chunks = resid_chunks * npad * batch;
-    S.norm_cap = batch;
+struct BatchNeed {
+  size_t a_elems = 0, vec_elems = 0, resid_elems = 0, rhs_elems = 0;
+  int max_nbe = 0, norm_batch = 0;
+  void add(int npad, int batch, int nbe, int chunks) {
+    const size_t lda = (size_t)((npad + 1) & ~1), a_stride = lda * (size_t)(npad + 1);
+    a_elems = std::max(a_elems, a_stride * batch);
+    vec_elems = std::max(vec_elems, (size_t)npad * batch);
+    resid_elems = std::max(resid_elems, (size_t)((npad + kResidCols - 1) / kResidCols) * npad * batch);
+    rhs_elems = std::max(rhs_elems, (size_t)chunks * 3 * nbe);
+    max_nbe = std::max(max_nbe, nbe);
+    norm_batch = std::max(norm_batch, batch);
   }
+};
+
+// Sizes a worker's padded-system buffers for every class it will run.
+int ensure_batchbuf(bem_ctx* d, const BatchNeed& q, bool mixed) {
+  SweepBuf& S = d->bbuf;
+  const bool fits = S.A64 && q.a_elems <= S.a_stride && (!mixed || S.A32) && q.vec_elems <= (size_t)S.nn &&
+                    q.resid_elems <= (size_t)S.resid_chunks && q.rhs_elems <= (size_t)S.rhs_chunks &&
+                    q.max_nbe <= S.batch && (size_t)q.norm_batch <= S.norm_cap;
+  if (fits) return BEM_OK;
+  free_sweep(S);
+  BEM_CUDA(d, cudaMalloc(&S.A64, q.a_elems * sizeof(double2)));
+  if (mixed) BEM_CUDA(d, cudaMalloc(&S.A32, q.a_elems * sizeof(float2)));
+  BEM_CUDA(d, cudaMalloc(&S.x64, q.vec_elems * sizeof(double2)));
+  BEM_CUDA(d, cudaMalloc(&S.v32, q.vec_elems * sizeof(float2)));
+  BEM_CUDA(d, cudaMalloc(&S.part, q.resid_elems * sizeof(double2)));
+  BEM_CUDA(d, cudaMalloc(&S.diag_h, (size_t)q.max_nbe * 9 * sizeof(double2)));
+  BEM_CUDA(d, cudaMalloc(&S.diag_g, (size_t)q.max_nbe * 9 * sizeof(double2)));
+  BEM_CUDA(d, cudaMalloc(&S.rhs_part, q.rhs_elems * sizeof(double2)));
+  BEM_CUDA(d, cudaMalloc(&S.norm, (size_t)2 * q.norm_batch * (kMaxRefine + 1) * sizeof(unsigned long long)));
+  // capacities, in elements (this buffer set is only read through views)
+  S.a_stride = q.a_elems;
+  S.nn = (int)q.vec_elems;
+  S.resid_chunks = (int)q.resid_elems;
+  S.rhs_chunks = (int)q.rhs_elems;
+  S.batch = q.max_nbe;
+  S.norm_cap = (size_t)q.norm_batch;
   return BEM_OK;
 }
 
 }  // namespace
+
+constexpr int kBatchWorkers = 8;
 
 int batch_solve(bem_ctx* d, int nprob, bem_ctx* const* probs, const double* freqs, const double* zge,
                 const double* zcs, const double* zcp, const double* c, int form, int iters, double* const* x_out,
@@ -347,13 +360,43 @@ int batch_solve(bem_ctx* d, int nprob, bem_ctx* const* probs, const double* freq
   std::vector<int> order(nprob);
   for (int i = 0; i < nprob; ++i) order[i] = i;
   std::sort(order.begin(), order.end(), [&](int a, int b) { return probs[a]->mesh.nbe < probs[b]->mesh.nbe; });
-  BEM_CUDA(d, cudaMemsetAsync(d->d_status, 0, ST_COUNT * sizeof(int), d->stream));
-  std::vector<unsigned long long> hnorm;
+  // Worker contexts: classes go round-robin to their streams and run concurrently.
+  while ((int)d->workers.size() < kBatchWorkers) {
+    bem_ctx* w = nullptr;
+    const int rc = bem_ctx_create(d->device, &w);
+    if (rc) return fail(d, rc, "bem_batch_solve: worker context");
+    d->workers.push_back(w);
+  }
+  // Pinned staging: solutions, then per-class refinement norms.
+  size_t xoff_total = 0;
+  std::vector<size_t> xoff(nprob);
+  for (int p = 0; p < nprob; ++p) {
+    xoff[p] = xoff_total;
+    xoff_total += (size_t)3 * probs[p]->mesh.nbe;
+  }
+  const size_t norm_words = (size_t)nprob * 2 * (kMaxRefine + 1);
+  const size_t need = xoff_total * sizeof(double2) + norm_words * sizeof(unsigned long long);
+  if (d->pinned_bytes < need) {
+    if (d->pinned) cudaFreeHost(d->pinned);
+    d->pinned = nullptr;
+    d->pinned_bytes = 0;
+    BEM_CUDA(d, cudaMallocHost(&d->pinned, need));
+    d->pinned_bytes = need;
+  }
+  double2* hx = static_cast<double2*>(d->pinned);
+  unsigned long long* hnorm = reinterpret_cast<unsigned long long*>(hx + xoff_total);
+  std::vector<int> class_of(nprob), slot_of(nprob);
+  // Plan: size classes in sorted order, round-robin over the workers, each
+  // worker's buffers sized once for all its classes (no allocation between
+  // launches).
+  struct Cls {
+    int g0, g1, npad;
+  };
+  std::vector<Cls> plan;
+  std::vector<BatchNeed> need_w(kBatchWorkers);
   for (int g0 = 0; g0 < nprob;) {
-    // one size class
     const int n0 = 3 * probs[order[g0]]->mesh.nbe;
-    int g1 = g0 + 1;
-    int npad = n0;
+    int g1 = g0 + 1, npad = n0;
     while (g1 < nprob) {
       const int n1 = 3 * probs[order[g1]]->mesh.nbe;
       if (n1 * 4 > n0 * 5) break;
@@ -361,23 +404,37 @@ int batch_solve(bem_ctx* d, int nprob, bem_ctx* const* probs, const double* freq
       npad = n1;
       ++g1;
     }
-    const int B = g1 - g0;
     int max_nbe = 0, max_chunks = 0;
     for (int k = g0; k < g1; ++k) {
       max_nbe = std::max(max_nbe, probs[order[k]]->mesh.nbe);
       max_chunks = std::max(max_chunks, rhs_chunks(probs[order[k]]));
     }
-    int rc = ensure_batchbuf(d, npad, B, mixed, max_nbe, max_chunks);
-    if (rc) return rc;
-    SweepBuf& S = d->bbuf;
+    need_w[plan.size() % kBatchWorkers].add(npad, g1 - g0, max_nbe, max_chunks);
+    plan.push_back({g0, g1, npad});
+    g0 = g1;
+  }
+  for (int w = 0; w < kBatchWorkers; ++w) {
+    if (need_w[w].a_elems == 0) continue;
+    const int rc = ensure_batchbuf(d->workers[w], need_w[w], mixed);
+    if (rc) return fail(d, rc, std::string("bem_batch_solve: ") + d->workers[w]->last_error);
+  }
+  for (bem_ctx* w : d->workers) BEM_CUDA(w, cudaMemsetAsync(w->d_status, 0, ST_COUNT * sizeof(int), w->stream));
+  for (int ncls = 0; ncls < (int)plan.size(); ++ncls) {
+    bem_ctx* wk = d->workers[ncls % kBatchWorkers];
+    const int g0 = plan[ncls].g0, g1 = plan[ncls].g1, npad = plan[ncls].npad;
+    const int B = g1 - g0;
+    int rc = BEM_OK;
+    SweepBuf& S = wk->bbuf;
     const size_t lda = (size_t)((npad + 1) & ~1), a_stride = lda * (size_t)(npad + 1);
     for (int k = g0; k < g1; ++k) {
       const int p = order[k], slot = k - g0;
+      class_of[p] = ncls;
+      slot_of[p] = slot;
       bem_ctx* pc = probs[p];
       const int n = 3 * pc->mesh.nbe;
       std::lock_guard<std::mutex> lk(pc->mu);
       cudaStream_t keep = pc->stream;
-      pc->stream = d->stream;
+      pc->stream = wk->stream;
       DynBatch db{};
       db.zge = zge + 2 * p;
       db.zcs = zcs + 2 * p;
@@ -394,19 +451,20 @@ int batch_solve(bem_ctx* d, int nprob, bem_ctx* const* probs, const double* freq
       db.diag_g = S.diag_g;
       db.rhs_part = S.rhs_part;
       const long long l0 = pc->launches;
-      BEM_CUDA(pc, cudaMemsetAsync(pc->d_status, 0, ST_COUNT * sizeof(int), d->stream));
-      rc = launch_dynamic_batch(pc, db);
+      rc = cudaMemsetAsync(pc->d_status, 0, ST_COUNT * sizeof(int), wk->stream) == cudaSuccess
+               ? launch_dynamic_batch(pc, db)
+               : BEM_ERR_CUDA;
       pc->stream = keep;
       d->launches += pc->launches - l0;
       if (rc) return fail(d, rc, std::string("assembly of a batched problem: ") + pc->last_error);
       if (n < npad) {
         const dim3 rg((npad + 255) / 256);
-        k_pad_rhs<<<rg, 256, 0, d->stream>>>(db.A, lda, n, npad);
-        k_pad_rest<<<dim3(rg.x, npad), 256, 0, d->stream>>>(db.A, lda, n, npad);
+        k_pad_rhs<<<rg, 256, 0, wk->stream>>>(db.A, lda, n, npad);
+        k_pad_rest<<<dim3(rg.x, npad), 256, 0, wk->stream>>>(db.A, lda, n, npad);
         d->launches += 2;
         if (mixed) {
-          k_pad_rhs<<<rg, 256, 0, d->stream>>>(db.A32, lda, n, npad);
-          k_pad_rest<<<dim3(rg.x, npad), 256, 0, d->stream>>>(db.A32, lda, n, npad);
+          k_pad_rhs<<<rg, 256, 0, wk->stream>>>(db.A32, lda, n, npad);
+          k_pad_rest<<<dim3(rg.x, npad), 256, 0, wk->stream>>>(db.A32, lda, n, npad);
           d->launches += 2;
         }
         BEM_CUDA(d, cudaGetLastError());
@@ -418,54 +476,64 @@ int batch_solve(bem_ctx* d, int nprob, bem_ctx* const* probs, const double* freq
     V.lda = lda;
     V.a_stride = a_stride;
     V.resid_chunks = (npad + kResidCols - 1) / kResidCols;
+    const long long l0 = wk->launches;
     if (mixed) {
-      rc = lu_factor_solve_batch(d, V.A32, lda, a_stride, npad, B, true);
-      if (rc) return rc;
-      k_x_init<<<dim3((npad + 255) / 256, B), 256, 0, d->stream>>>(V.A32, lda, a_stride, npad, V.x64, npad);
-      d->launches++;
-      BEM_CUDA(d, cudaMemsetAsync(V.norm, 0, (size_t)2 * B * (kMaxRefine + 1) * sizeof(unsigned long long),
-                                  d->stream));
-      rc = refine_steps(d, V, B, iters, 0);
-      if (rc) return rc;
+      rc = lu_factor_solve_batch(wk, V.A32, lda, a_stride, npad, B, true);
+      if (!rc) {
+        k_x_init<<<dim3((npad + 255) / 256, B), 256, 0, wk->stream>>>(V.A32, lda, a_stride, npad, V.x64, npad);
+        wk->launches++;
+        rc = cudaMemsetAsync(V.norm, 0, (size_t)2 * B * (kMaxRefine + 1) * sizeof(unsigned long long),
+                             wk->stream) == cudaSuccess
+                 ? refine_steps(wk, V, B, iters, 0)
+                 : BEM_ERR_CUDA;
+      }
     } else {
-      rc = lu_factor_solve_batch(d, V.A64, lda, a_stride, npad, B, false);
-      if (rc) return rc;
+      rc = lu_factor_solve_batch(wk, V.A64, lda, a_stride, npad, B, false);
     }
+    d->launches += wk->launches - l0;
+    if (rc) return fail(d, rc, std::string("bem_batch_solve: ") + wk->last_error);
     for (int k = g0; k < g1; ++k) {
       const int p = order[k], slot = k - g0;
       const int n = 3 * probs[p]->mesh.nbe;
-      if (x_out && x_out[p]) {
-        const double2* src = mixed ? V.x64 + (size_t)slot * npad : V.A64 + (size_t)slot * a_stride + (size_t)npad * lda;
-        BEM_CUDA(d, cudaMemcpyAsync(x_out[p], src, (size_t)n * sizeof(double2), cudaMemcpyDeviceToHost, d->stream));
-      }
+      const double2* src = mixed ? V.x64 + (size_t)slot * npad : V.A64 + (size_t)slot * a_stride + (size_t)npad * lda;
+      BEM_CUDA(d, cudaMemcpyAsync(hx + xoff[p], src, (size_t)n * sizeof(double2), cudaMemcpyDeviceToHost,
+                                  wk->stream));
     }
-    if (corr_out) {
-      if (mixed && iters > 0) {
-        hnorm.assign((size_t)2 * B * (kMaxRefine + 1), 0ull);
-        BEM_CUDA(d, cudaMemcpyAsync(hnorm.data(), V.norm, hnorm.size() * sizeof(unsigned long long),
-                                    cudaMemcpyDeviceToHost, d->stream));
-        BEM_CUDA(d, cudaStreamSynchronize(d->stream));
-        const size_t last = (size_t)2 * B * (iters - 1);
-        for (int k = g0; k < g1; ++k) {
-          double dm, xm;
-          const unsigned long long du = hnorm[last + 2 * (k - g0)], xu = hnorm[last + 2 * (k - g0) + 1];
-          memcpy(&dm, &du, sizeof dm);
-          memcpy(&xm, &xu, sizeof xm);
-          corr_out[order[k]] = xm > 0 ? dm / xm : 0.0;
-        }
-      } else {
-        for (int k = g0; k < g1; ++k) corr_out[order[k]] = 0.0;
-      }
-    }
-    g0 = g1;
+    if (mixed && iters > 0)
+      BEM_CUDA(d, cudaMemcpyAsync(hnorm + (size_t)2 * (kMaxRefine + 1) * g0, V.norm,
+                                  (size_t)2 * B * (kMaxRefine + 1) * sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, wk->stream));
   }
-  BEM_CUDA(d, cudaStreamSynchronize(d->stream));
+  for (bem_ctx* w : d->workers) {
+    BEM_CUDA(d, cudaStreamSynchronize(w->stream));
+    const int rc = check_status(w);
+    if (rc) return fail(d, rc, std::string("bem_batch_solve: ") + w->last_error);
+  }
   for (int p = 0; p < nprob; ++p) {
     int rc = check_status(probs[p]);
     if (rc) return fail(d, rc, std::string("batched problem: ") + probs[p]->last_error);
     if (probs[p]->mesh_flag_bnd) return fail(d, BEM_ERR_DEGENERATE, "Jacobian below 1e-5 on a boundary element");
+    if (x_out && x_out[p]) memcpy(x_out[p], hx + xoff[p], (size_t)3 * probs[p]->mesh.nbe * sizeof(double2));
   }
-  return check_status(d);
+  if (corr_out) {
+    // class norms were staged at the class's first sorted position
+    for (int k = 0, g0 = 0; k < nprob; ++k) {
+      const int p = order[k];
+      if (slot_of[p] == 0) g0 = k;
+      if (!(mixed && iters > 0)) {
+        corr_out[p] = 0.0;
+        continue;
+      }
+      int B = 0;
+      for (int q = g0; q < nprob && class_of[order[q]] == class_of[p]; ++q) ++B;
+      const unsigned long long* hn = hnorm + (size_t)2 * (kMaxRefine + 1) * g0 + (size_t)2 * B * (iters - 1);
+      double dm, xm;
+      memcpy(&dm, &hn[2 * slot_of[p]], sizeof dm);
+      memcpy(&xm, &hn[2 * slot_of[p] + 1], sizeof xm);
+      corr_out[p] = xm > 0 ? dm / xm : 0.0;
+    }
+  }
+  return BEM_OK;
 }
 
 // ---------------------------------------------------------------------------

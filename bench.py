@@ -63,6 +63,8 @@ def parse_args():
                     help="requests of the serving stream replayed in the served measurement "
                          "(0 skips the stream; the 128-request served sweep always runs)")
     ap.add_argument("--no-serve", action="store_true", help="skip the served measurements")
+    ap.add_argument("--small-count", type=int, default=512,
+                    help="small meshes (24..600 elements) of the batching measurement (0 skips it)")
     ap.add_argument("--profile-case", action="store_true",
                     help="run only warmup+steps headline sweep batches and print a launch count "
                          "(a small, short command to run under ncu); no bench line")
@@ -364,10 +366,63 @@ def run_ours(args):
     ctx.close()
     if not args.no_serve:
         line["served"] = run_served(args, s, d, mine, local)
+    if args.small_count > 0:
+        line["batched_small_meshes"] = run_small_batch(args, local)
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def run_small_batch(args, device):
+    """The batching form's small meshes: --small-count meshes of 24..600
+    elements (rectangular jittered grids, seeded), random Poisson ratio in
+    [0.15, 0.35] and damping in [0.005, 0.05], omega uniform in [0.1, 10].
+    bem_batch_solve (padded lockstep classes) in both forms against the same
+    problems solved one after another through bem_ghmatecd + bem_linsolve.
+    Per-mesh static work (upload, GHMATECE) is done before the clocks."""
+    import torch
+    from bem_mececcs_b200 import capi, serve
+    from bem_mececcs_b200.solver import BemSolver, batch_solve
+    rng = np.random.Generator(np.random.PCG64(5))
+    probs = []
+    for _ in range(args.small_count):
+        nx, ny = serve.grid_for(int(rng.integers(24, 601)))
+        nu = float(rng.uniform(0.15, 0.35))
+        dam = float(rng.uniform(0.005, 0.05))
+        m = meshgen.enclosed_grid(nx, ny, jitter=0.10, seed=int(rng.integers(1 << 30)), rnu=nu,
+                                  depth=2.5, layers=4)
+        dd = meshgen.traction_patch(m, dam=dam)
+        sol = BemSolver(m, device=device)
+        sol.ghmatece()
+        sol.set_bc(dd.kode, dd.bc, dam, 1.0)
+        probs.append((sol, float(rng.uniform(0.1, 10.0))))
+    nns = [p[0].nn for p in probs]
+    driver = capi.Context(device)
+    out = {"problems": len(probs), "n_range": [min(nns), max(nns)],
+           "flops_lu_total": float(sum(8.0 / 3.0 * n ** 3 for n in nns))}
+    for form in ("mixed", "plain"):
+        batch_solve(driver, probs[:8], form=form)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, corr = batch_solve(driver, probs, form=form)
+        dt = time.perf_counter() - t0
+        out[f"batch_{form}"] = {"solves_per_s": round(len(probs) / dt, 2), "wall_s": round(dt, 3),
+                                "max_last_correction": float(np.max(corr))}
+    t0 = time.perf_counter()
+    for sol, fr in probs:
+        sol.ghmatecd(fr)
+        sol.ctx.check(sol.ctx.L.bem_linsolve_async(sol.ctx.h), "bem_linsolve_async")
+    for sol, _ in probs:
+        sol.ctx.sync()
+    dt = time.perf_counter() - t0
+    out["one_by_one_plain"] = {"solves_per_s": round(len(probs) / dt, 2), "wall_s": round(dt, 3)}
+    out["speedup_batch_mixed_vs_one_by_one_plain"] = round(
+        out["batch_mixed"]["solves_per_s"] / out["one_by_one_plain"]["solves_per_s"], 2)
+    driver.close()
+    for sol, _ in probs:
+        sol.ctx.close()
+    return out
 
 
 def _served_summary(st, wall_s):
