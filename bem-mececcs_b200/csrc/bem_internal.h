@@ -177,7 +177,8 @@ struct bem_ctx {
   void* pinned = nullptr;          // bem_batch_solve: pinned staging of solutions and norms
   size_t pinned_bytes = 0;
   bool use_tcgen05 = true;  // FP32 trailing update on tcgen05 (else TF32 mma.sync)
-  bool use_trsv_coop = true;  // one cooperative launch per triangular solve (else per-block launches)
+  bool use_trsv_coop = true;
+  bool lu_pairs = true;       // FP32 tensor-core LU: two 64-column panels per trailing update (K = 128)  // one cooperative launch per triangular solve (else per-block launches)
 };
 
 namespace bem {
@@ -246,6 +247,11 @@ const double2* slot_solution(bem_ctx* ctx, bool mixed, bool rhs_only);
 int tc_ensure(bem_ctx* ctx, int nn, int batch);
 void tc_release(bem_ctx* ctx);
 int tc_trailing_update(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int k, int w, int batch);
+int tc_pack_l(bem_ctx* ctx, const float2* A, size_t lda, size_t bstride, int nn, int kcol, int kw, int r0, int koff,
+              int batch, const int* gperm, int gstride);
+int tc_gemm(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int r0, int c0, int cend, int kw,
+            int urow_off, int batch);
+constexpr int kTcKPitch = 128;  // floats per packed tensor-core operand row
 int measure_fp64_peak(bem_ctx* ctx, double* tflops);
 int measure_fma_peaks(bem_ctx* ctx, double* fp64_tflops, double* fp32_tflops);
 int measure_tf32_peak(bem_ctx* ctx, int n, double* tflops);

@@ -44,6 +44,7 @@ constexpr int kStages = 3;
 constexpr uint32_t kHalfBytes = 128 * 64 * 4;  // C staging: 64 complex rows x 64 columns = 32 KB
 constexpr uint32_t kTmemCols = 512;
 constexpr int kPrefetch = 3;  // C tiles prefetched into L2 ahead of the current one
+constexpr int kKPitch = 128;  // floats per packed operand row: K up to 128 (two 64-column panels)
 constexpr size_t kTcSmem = (size_t)kStages * kStageBytes + 2 * kHalfBytes + 1024;
 
 __device__ __forceinline__ uint32_t idesc_tf32_128x128() {
@@ -124,6 +125,8 @@ struct TcArgs {
   float2* A;        // the systems (complex64), problem b at A + b*bstride
   size_t lda, bstride;
   int nn, r0, c0, ncols, kw;
+  int cend;         // columns >= cend are left unchanged
+  int urow_off;     // packed U row of column c0
   int mtiles, ntiles, batch;
   int lrows;        // Lhat rows per problem (2*nn)
   int urows;        // U rows per problem (nn+1)
@@ -198,7 +201,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
       const int rem = t % (a.mtiles * a.ntiles);
       const int tm = rem % a.mtiles, tn = rem / a.mtiles;
       const int ly = b * a.lrows + 2 * tm * kTcRows;
-      const int uy = b * a.urows + tn * kTcCols;
+      const int uy = b * a.urows + a.urow_off + tn * kTcCols;
       for (int h = 0; h < nchunks; ++h) {
         if (!wait_or_abort(&empty[s], ph ^ 1u, abort_flag, a.status)) {
           ok = false;
@@ -277,11 +280,12 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
           tmem_ld16(tbase + (uint32_t)(64 * hc + c), v1);
           tmem_ld16(tbase + 128u + (uint32_t)(64 * hc + c), v2);
           tmem_ld_wait();
+          const int colbase = a.c0 + tn * kTcCols + 64 * hc + c;
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
             const float x = __shfl_xor_sync(0xffffffffu, v2[i], 1);
             const float val = p ? (v1[i] + x) : (v1[i] - x);
-            ct[(c + i) * 128 + rho] = -val;
+            ct[(c + i) * 128 + rho] = colbase + i < a.cend ? -val : 0.0f;
           }
         }
         if (hc == 1) {
@@ -304,33 +308,49 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
 }
 
 // Lhat: rows 2(r - r0) + p of problem b hold part p of L(r, k..k+kw-1),
-// rounded to TF32, zero-padded to 64 columns.  32 rows x 64 columns per CTA
-// through a shared transpose so reads and writes are both coalesced.
+// K-major at K slots koff..koff+kw-1 of a kKPitch-float row, rounded to TF32.
+// With a gather list (a later panel's interchanges: count, then dst/src
+// pairs), row r takes L from the row that the list moves to r, i.e. L in the
+// later panel's row order; A itself is not changed.
 __global__ void __launch_bounds__(256) k_pack_l21(const float2* __restrict__ A, size_t lda, size_t bstride, int nn,
-                                                  int k, int kw, int r0, float* lhat, int lrows) {
+                                                  int k, int kw, int r0, int koff, float* lhat, int lrows,
+                                                  const int* __restrict__ gperm, int gstride) {
   __shared__ float2 tile[64][33];
+  __shared__ int s_src[32];
   const int b = blockIdx.y;
   const float2* Ap = A + (size_t)b * bstride;
   const int rbase = r0 + blockIdx.x * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 8 x 32
+  if (threadIdx.x < 32) s_src[threadIdx.x] = rbase + threadIdx.x;
+  __syncthreads();
+  if (gperm) {
+    const int* pl = gperm + (size_t)b * gstride;
+    const int count = pl[0];
+    for (int e = threadIdx.x; e < count; e += blockDim.x) {
+      const int dst = pl[1 + 2 * e];
+      if (dst >= rbase && dst < rbase + 32) s_src[dst - rbase] = pl[2 + 2 * e];
+    }
+    __syncthreads();
+  }
+  const int src = s_src[tx];
   for (int c = ty; c < 64; c += 8) {
     const int r = rbase + tx;
     float2 v = make_float2(0.f, 0.f);
-    if (c < kw && r < nn) v = Ap[(size_t)(k + c) * lda + r];
+    if (c < kw && r < nn) v = Ap[(size_t)(k + c) * lda + src];
     tile[c][tx] = v;
   }
   __syncthreads();
-  float* out = lhat + (size_t)b * lrows * 64;
+  float* out = lhat + (size_t)b * lrows * kKPitch;
   for (int idx = threadIdx.x; idx < 32 * 2 * 64; idx += blockDim.x) {
     const int c = idx & 63, rr = idx >> 6;  // rr = 2*local_row + part
     const int lr = rr >> 1, p = rr & 1;
     const int r = rbase + lr;
-    if (r >= nn) continue;
+    if (r >= nn || c >= kw) continue;
     const float2 v = tile[c][lr];
     const float x = p ? v.y : v.x;
     unsigned t;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(x));
-    out[(size_t)(2 * (r - r0) + p) * 64 + c] = __uint_as_float(t);
+    out[(size_t)(2 * (r - r0) + p) * kKPitch + koff + c] = __uint_as_float(t);
   }
 }
 
@@ -354,8 +374,8 @@ EncodeTiledFn encode_fn() {
 bool make_map(CUtensorMap* m, float* base, size_t rows) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return false;
-  cuuint64_t dims[2] = {64, (cuuint64_t)rows};
-  cuuint64_t strides[1] = {64 * sizeof(float)};
+  cuuint64_t dims[2] = {kKPitch, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {kKPitch * sizeof(float)};
   cuuint32_t box[2] = {32, 128};
   cuuint32_t estr[2] = {1, 1};
   return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -448,12 +468,12 @@ int tc_ensure(bem_ctx* ctx, int nn, int batch) {
   const size_t lrows = (size_t)2 * nn * batch, urows = (size_t)(nn + 1) * batch;
   if (W.lhat && lrows <= W.lrows_cap && urows <= W.urows_cap) return BEM_OK;
   tc_release(ctx);
-  BEM_CUDA(ctx, cudaMalloc(&W.lhat, lrows * 64 * sizeof(float)));
-  BEM_CUDA(ctx, cudaMalloc(&W.ure, urows * 64 * sizeof(float)));
-  BEM_CUDA(ctx, cudaMalloc(&W.uim, urows * 64 * sizeof(float)));
-  BEM_CUDA(ctx, cudaMemset(W.lhat, 0, lrows * 64 * sizeof(float)));
-  BEM_CUDA(ctx, cudaMemset(W.ure, 0, urows * 64 * sizeof(float)));
-  BEM_CUDA(ctx, cudaMemset(W.uim, 0, urows * 64 * sizeof(float)));
+  BEM_CUDA(ctx, cudaMalloc(&W.lhat, lrows * kKPitch * sizeof(float)));
+  BEM_CUDA(ctx, cudaMalloc(&W.ure, urows * kKPitch * sizeof(float)));
+  BEM_CUDA(ctx, cudaMalloc(&W.uim, urows * kKPitch * sizeof(float)));
+  BEM_CUDA(ctx, cudaMemset(W.lhat, 0, lrows * kKPitch * sizeof(float)));
+  BEM_CUDA(ctx, cudaMemset(W.ure, 0, urows * kKPitch * sizeof(float)));
+  BEM_CUDA(ctx, cudaMemset(W.uim, 0, urows * kKPitch * sizeof(float)));
   W.maps = new CUtensorMap[4];
   CUtensorMap* maps = static_cast<CUtensorMap*>(W.maps);
   if (!make_map(&maps[0], W.lhat, lrows) || !make_map(&maps[1], W.ure, urows) || !make_map(&maps[2], W.uim, urows))
@@ -473,12 +493,25 @@ void tc_release(bem_ctx* ctx) {
   W = TcWork{};
 }
 
-// C -= L21 U12 for rows [r0, nn) and columns [c0, ncols) of `batch` FP32
-// systems; U_re/U_im must already hold the step's U12 (rows c - c0).
-int tc_trailing_update(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int k, int w, int batch) {
-  TcWork& W = ctx->tc;
-  const int r0 = k + w, c0 = k + w, ncols = nn + 1;
+// Packs L (columns kcol..kcol+kw-1, rows r0..nn-1) into K slots
+// koff..koff+kw-1 of Lhat, optionally through a gather list.
+int tc_pack_l(bem_ctx* ctx, const float2* A, size_t lda, size_t bstride, int nn, int kcol, int kw, int r0, int koff,
+              int batch, const int* gperm, int gstride) {
   if (r0 >= nn) return BEM_OK;
+  k_pack_l21<<<dim3((nn - r0 + 31) / 32, batch), 256, 0, ctx->stream>>>(A, lda, bstride, nn, kcol, kw, r0, koff,
+                                                                        ctx->tc.lhat, 2 * nn, gperm, gstride);
+  ctx->launches++;
+  BEM_CUDA(ctx, cudaGetLastError());
+  return BEM_OK;
+}
+
+// C -= Lhat U for rows [r0, nn) and columns [c0, cend) of `batch` FP32
+// systems, K = kw (packed Lhat and U_re/U_im; U row urow_off + (c - c0)).
+int tc_gemm(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int r0, int c0, int cend, int kw,
+            int urow_off, int batch) {
+  TcWork& W = ctx->tc;
+  const int ncols = nn + 1;
+  if (r0 >= nn || c0 >= cend) return BEM_OK;
   CUtensorMap* maps = static_cast<CUtensorMap*>(W.maps);
   if (W.cbase != A || W.clda != lda || W.cbstride != bstride || W.cbatch != batch) {
     if ((lda % 2) != 0 || (bstride % 2) != 0 || !make_cmap(&maps[3], A, nn, lda, bstride, batch))
@@ -488,9 +521,6 @@ int tc_trailing_update(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int 
     W.cbstride = bstride;
     W.cbatch = batch;
   }
-  k_pack_l21<<<dim3((nn - r0 + 31) / 32, batch), 256, 0, ctx->stream>>>(A, lda, bstride, nn, k, w, r0, W.lhat,
-                                                                        2 * nn);
-  ctx->launches++;
   TcArgs t{};
   t.A = A;
   t.lda = lda;
@@ -499,9 +529,11 @@ int tc_trailing_update(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int 
   t.r0 = r0;
   t.c0 = c0;
   t.ncols = ncols;
-  t.kw = w;
+  t.kw = kw;
+  t.cend = cend;
+  t.urow_off = urow_off;
   t.mtiles = (nn - r0 + kTcRows - 1) / kTcRows;
-  t.ntiles = (ncols - c0 + kTcCols - 1) / kTcCols;
+  t.ntiles = (cend - c0 + kTcCols - 1) / kTcCols;
   t.batch = batch;
   t.lrows = 2 * nn;
   t.urows = nn + 1;
@@ -512,6 +544,15 @@ int tc_trailing_update(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int 
   ctx->launches++;
   BEM_CUDA(ctx, cudaGetLastError());
   return BEM_OK;
+}
+
+// One panel step: C -= L21 U12 for rows and columns from k + w on.
+int tc_trailing_update(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int k, int w, int batch) {
+  const int r0 = k + w;
+  if (r0 >= nn) return BEM_OK;
+  int rc = tc_pack_l(ctx, A, lda, bstride, nn, k, w, r0, 0, batch, nullptr, 0);
+  if (rc) return rc;
+  return tc_gemm(ctx, A, lda, bstride, nn, r0, r0, nn + 1, w, 0, batch);
 }
 
 }  // namespace bem

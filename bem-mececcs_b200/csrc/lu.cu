@@ -667,22 +667,38 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel_grid(PanelArgs a) {
 
 // Row interchanges of one panel applied to columns [c0, ncols) as a gather,
 // then U12 = L11^-1 A12 (unit lower).  One warp per column; problem = blockIdx.y.
-template <typename R>
+template <typename R, bool PRE>
 __global__ void __launch_bounds__(256) k_laswp_trsm(void* Av, size_t lda, size_t bstride, int k, int w, int c0,
                                                     int ncols, const int* __restrict__ perm, int perm_stride,
-                                                    float* ure, float* uim, int urows) {
+                                                    float* ure, float* uim, int urows, int ubase, int koff,
+                                                    int kprev) {
   using E = typename Elt<R>::T;
   using C = cpx<R>;
   constexpr int NB = 64;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s_L = reinterpret_cast<C*>(smem_raw);  // [NB][NB] column-major
+  C* s_Lb = s_L + NB * NB;                  // PRE: the previous panel's L rows k..k+w-1 in this panel's order
   E* A = static_cast<E*>(Av) + (size_t)blockIdx.y * bstride;
   const int* pl = perm + (size_t)blockIdx.y * perm_stride;
   load_slice_async<R>(A, lda, k, k, w, w, s_L, NB);
-  __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int count = pl[0];
   pl += 1;
+  if (PRE) {
+    // s_Lb[j][i] = L(src(k + i), kprev + j): row k + i after this panel's
+    // interchanges holds the old row src(k + i).  64 rows x 4 groups of 16
+    // columns, all loads of a thread issued before its stores.
+    const int i = threadIdx.x & 63, jg = threadIdx.x >> 6;
+    if (i < w) {
+      const int src = pl[2 * i + 1];
+      E t[16];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) t[u] = A[(size_t)(kprev + jg * 16 + u) * lda + src];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) s_Lb[(jg * 16 + u) * NB + i] = C{t[u].x, t[u].y};
+    }
+  }
+  __syncthreads();
   // The gather list is the same for every column: source rows of the panel
   // rows lane, lane+32, and (destination, source) of the displaced rows.
   const int s0 = lane < w ? pl[2 * lane + 1] : 0;
@@ -697,7 +713,7 @@ __global__ void __launch_bounds__(256) k_laswp_trsm(void* Av, size_t lda, size_t
   constexpr int QC = 4;  // columns per warp, solved as interleaved chains
   const int ncol = ncols - c0;
   for (int cb = (blockIdx.x * 8 + warp) * QC; cb < ncol; cb += gridDim.x * 8 * QC) {
-    C v0[QC], v1[QC], x[QC][2];
+    C v0[QC], v1[QC], x[QC][2], u0[QC], u1[QC];
 #pragma unroll
     for (int q = 0; q < QC; ++q) {
       const bool ok = cb + q < ncol;
@@ -706,6 +722,10 @@ __global__ void __launch_bounds__(256) k_laswp_trsm(void* Av, size_t lda, size_t
       v1[q] = ok && lane + 32 < w ? ldc<R>(&cp[s1]) : C{R(0), R(0)};
 #pragma unroll
       for (int h = 0; h < 2; ++h) x[q][h] = ok && xd[h] >= 0 ? ldc<R>(&cp[xs[h]]) : C{R(0), R(0)};
+      if (PRE) {
+        u0[q] = ok ? ldc<R>(&cp[kprev + lane]) : C{R(0), R(0)};
+        u1[q] = ok ? ldc<R>(&cp[kprev + lane + 32]) : C{R(0), R(0)};
+      }
     }
     __syncwarp();
 #pragma unroll
@@ -715,6 +735,22 @@ __global__ void __launch_bounds__(256) k_laswp_trsm(void* Av, size_t lda, size_t
 #pragma unroll
       for (int h = 0; h < 2; ++h)
         if (xd[h] >= 0) stc<R>(&cp[xd[h]], x[q][h]);
+    }
+    if (PRE) {
+      // The previous panel's deferred update of this panel's rows:
+      // v -= L(rows, kprev..kprev+63) U(kprev..kprev+63, col).
+      for (int j = 0; j < NB; ++j) {
+        const C l0 = s_Lb[j * NB + lane], l1 = s_Lb[j * NB + lane + 32];
+#pragma unroll
+        for (int q = 0; q < QC; ++q) {
+          const C src = (j < 32) ? u0[q] : u1[q];
+          C uj;
+          uj.re = __shfl_sync(0xffffffffu, src.re, j & 31);
+          uj.im = __shfl_sync(0xffffffffu, src.im, j & 31);
+          if (lane < w) cfms(v0[q], l0, uj);
+          if (lane + 32 < w) cfms(v1[q], l1, uj);
+        }
+      }
     }
     // Forward substitution with the unit lower L11: rows lane and lane+32.
     for (int i = 0; i < w; ++i) {
@@ -737,7 +773,7 @@ __global__ void __launch_bounds__(256) k_laswp_trsm(void* Av, size_t lda, size_t
       if (lane + 32 < w) stc<R>(&cp[k + lane + 32], v1[q]);
       if (ure) {
         // Packed K-major copies of U12 for the tensor-core update, rounded to TF32.
-        const size_t row = ((size_t)blockIdx.y * urows + (cb + q)) * 64;
+        const size_t row = ((size_t)blockIdx.y * urows + (c0 + cb + q - ubase)) * kTcKPitch + koff;
         const float r0 = lane < w ? (float)v0[q].re : 0.f, i0 = lane < w ? (float)v0[q].im : 0.f;
         const float r1 = lane + 32 < w ? (float)v1[q].re : 0.f, i1 = lane + 32 < w ? (float)v1[q].im : 0.f;
         unsigned t0, t1, t2, t3;
@@ -1523,7 +1559,10 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
   const int cs = cluster_size(ctx);
   const size_t lsmem = 64 * 64 * es;
   const size_t bsmem = 64 * 64 * es;
-  BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_trsm<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem));
+  BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_trsm<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)lsmem));
+  BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_trsm<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(2 * lsmem)));
   BEM_CUDA(ctx, cudaFuncSetAttribute(k_backsub<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem));
   BEM_CUDA(ctx, cudaFuncSetAttribute(k_gemm_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
   BEM_CUDA(ctx, cudaFuncSetAttribute(k_gemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmTf32Smem));
@@ -1532,9 +1571,21 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     if (rc) return rc;
   }
   L.panels.clear();
-  for (int k = 0; k < nn;) {
+  const bool tc = sizeof(R) == 4 && ctx->use_tcgen05;
+  // Panel width for m remaining rows: the widest of 64/32/16 whose rows fit
+  // one cluster, at most 512 rows per CTA (one row per thread); 0 when the
+  // panel needs the cooperative-grid kernel.
+  auto panel_nb = [&](int m) {
+    const int rp_c = (m + cs - 1) / cs;
+    if (rp_c <= 512)
+      for (int cand : {64, 32, 16})
+        if (cluster_panel_fits_any<R>(cand, rp_c)) return cand;
+    return 0;
+  };
+  // Factors the panel starting at column k; returns its width and gather lists.
+  auto run_panel = [&](int k, int& w, int*& perm_p) -> int {
     const int m = nn - k;
-    int* perm_p = L.perm + L.panels.size() * (size_t)batch * kPermStride;  // this panel's lists
+    perm_p = L.perm + L.panels.size() * (size_t)batch * kPermStride;  // this panel's lists
     PanelArgs pa{};
     pa.A = A;
     pa.lda = lda;
@@ -1548,89 +1599,127 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     pa.status = ctx->d_status;
     pa.pstart = L.pstart;
     pa.pidx = (int)L.panels.size();
-    // Panel width: the widest of 64/32/16 whose rows fit one cluster, at most
-    // 512 rows per CTA (one row per thread).
-    const int rp_c = (m + cs - 1) / cs;
-    int nb = 0;
-    if (rp_c <= 512)
-      for (int cand : {64, 32, 16})
-        if (cluster_panel_fits_any<R>(cand, rp_c)) {
-          nb = cand;
-          break;
-        }
-    int w;
-    {
-      ProfScope ps(ctx, 1, 0.0);
-      if (nb) {
-        w = std::min(nb, m);
-        pa.w = w;
-        pa.rp = rp_c;
-        pa.cs = cs;  // CTAs past the last row own no rows but join every barrier
-        int rc = launch_cluster_panel_any<R>(ctx, pa, batch, nb);
+    const int nb = panel_nb(m);
+    ProfScope ps(ctx, 1, 0.0);
+    if (nb) {
+      w = std::min(nb, m);
+      pa.w = w;
+      pa.rp = (m + cs - 1) / cs;
+      pa.cs = cs;  // CTAs past the last row own no rows but join every barrier
+      int rc = launch_cluster_panel_any<R>(ctx, pa, batch, nb);
+      if (rc) return rc;
+      ctx->launches++;
+    } else {
+      // Panel taller than one cluster holds: cooperative grid, one problem at a time.
+      int G = std::min({ctx->num_sms, kMaxGrid, (m + 15) / 16});
+      const int rp = (m + G - 1) / G;
+      int nbg = 64;
+      if ((size_t)rp * 64 * es > kPanelSmemBudget) nbg = 32;
+      if ((size_t)rp * nbg * es > kPanelSmemBudget) return fail(ctx, BEM_ERR_ARG, "matrix too large for the panel kernels");
+      w = std::min(nbg, m);
+      G = (m + rp - 1) / rp;
+      pa.w = w;
+      pa.rp = rp;
+      pa.cs = G;
+      pa.slot_val = L.slot_val;
+      pa.slot_row = L.slot_row;
+      pa.cand = L.cand;
+      pa.drow = L.drow;
+      pa.bar = L.barrier;
+      for (int b = 0; b < batch; ++b) {
+        PanelArgs pb = pa;
+        pb.A = static_cast<char*>(A) + (size_t)b * bstride * es;
+        pb.ipiv = L.ipiv + (size_t)b * nn;
+        pb.perm = perm_p + (size_t)b * kPermStride;
+        int rc = (nbg == 64) ? launch_grid_panel<R, 64>(ctx, pb) : launch_grid_panel<R, 32>(ctx, pb);
         if (rc) return rc;
         ctx->launches++;
-      } else {
-        // Panel taller than one cluster holds: cooperative grid, one problem at a time.
-        int G = std::min({ctx->num_sms, kMaxGrid, (m + 15) / 16});
-        const int rp = (m + G - 1) / G;
-        int nbg = 64;
-        if ((size_t)rp * 64 * es > kPanelSmemBudget) nbg = 32;
-        if ((size_t)rp * nbg * es > kPanelSmemBudget)
-          return fail(ctx, BEM_ERR_ARG, "matrix too large for the panel kernels");
-        w = std::min(nbg, m);
-        G = (m + rp - 1) / rp;
-        pa.w = w;
-        pa.rp = rp;
-        pa.cs = G;
-        pa.slot_val = L.slot_val;
-        pa.slot_row = L.slot_row;
-        pa.cand = L.cand;
-        pa.drow = L.drow;
-        pa.bar = L.barrier;
-        for (int b = 0; b < batch; ++b) {
-          PanelArgs pb = pa;
-          pb.A = static_cast<char*>(A) + (size_t)b * bstride * es;
-          pb.ipiv = L.ipiv + (size_t)b * nn;
-          pb.perm = perm_p + (size_t)b * kPermStride;
-          int rc = (nbg == 64) ? launch_grid_panel<R, 64>(ctx, pb) : launch_grid_panel<R, 32>(ctx, pb);
-          if (rc) return rc;
-          ctx->launches++;
-        }
       }
     }
     BEM_CUDA(ctx, cudaGetLastError());
+    L.panels.push_back({k, w});
+    return BEM_OK;
+  };
+  auto laswp = [&](bool pre, int k, int w, int c0, const int* perm_p, int ubase, int koff, int kprev) -> int {
+    const int cols = ncols - c0;
+    if (cols <= 0) return BEM_OK;
+    const int blocks = std::max(1, std::min((cols + 31) / 32, (4 * ctx->num_sms + batch - 1) / batch));
+    ProfScope ps(ctx, 2, 0.0);
+    float* ure = tc ? ctx->tc.ure : nullptr;
+    float* uim = tc ? ctx->tc.uim : nullptr;
+    if (pre)
+      k_laswp_trsm<R, true><<<dim3(blocks, batch), 256, 2 * lsmem, ctx->stream>>>(
+          A, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kprev);
+    else
+      k_laswp_trsm<R, false><<<dim3(blocks, batch), 256, lsmem, ctx->stream>>>(
+          A, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kprev);
+    ctx->launches++;
+    BEM_CUDA(ctx, cudaGetLastError());
+    return BEM_OK;
+  };
+  for (int k = 0; k < nn;) {
+    const int m = nn - k;
+    // Two 64-column panels per trailing update (K = 128) on the tensor-core
+    // path: panel 1's update reaches only the next 64 columns (panel 2) at
+    // once; for the columns right of both it is deferred and applied with
+    // panel 2's in one GEMM, with panel 1's L rows taken in panel 2's row
+    // order (its gather list) and panel 2's U rows finished by the deferred
+    // update of their own rows (k_laswp_trsm<PRE>).  A keeps the factors of
+    // the one-panel-at-a-time LU, so the solves are unchanged.
+    if (tc && ctx->lu_pairs && m > 128 && panel_nb(m) == 64 && panel_nb(m - 64) == 64) {
+      int w1 = 0, w2 = 0, *p1 = nullptr, *p2 = nullptr;
+      int rc = run_panel(k, w1, p1);
+      if (rc) return rc;
+      const int c0 = k + 64, c1 = k + 128;
+      rc = laswp(false, k, 64, c0, p1, c0, 0, 0);
+      if (rc) return rc;
+      {
+        ProfScope ps(ctx, 3, 8.0 * (double)(nn - c0) * 64.0 * 64.0 * batch);
+        rc = tc_pack_l(ctx, static_cast<float2*>(A), lda, bstride, nn, k, 64, c0, 0, batch, nullptr, 0);
+        if (!rc) rc = tc_gemm(ctx, static_cast<float2*>(A), lda, bstride, nn, c0, c0, c1, 64, 0, batch);
+        if (rc) return rc;
+      }
+      rc = run_panel(c0, w2, p2);
+      if (rc) return rc;
+      rc = laswp(true, c0, 64, c1, p2, c0, 64, k);
+      if (rc) return rc;
+      if (c1 < nn) {
+        ProfScope ps(ctx, 3, 8.0 * (double)(nn - c1) * (double)(ncols - c1) * 128.0 * batch);
+        rc = tc_pack_l(ctx, static_cast<float2*>(A), lda, bstride, nn, k, 64, c1, 0, batch, p2, kPermStride);
+        if (!rc) rc = tc_pack_l(ctx, static_cast<float2*>(A), lda, bstride, nn, c0, 64, c1, 64, batch, nullptr, 0);
+        if (!rc) rc = tc_gemm(ctx, static_cast<float2*>(A), lda, bstride, nn, c1, c1, ncols, 128, 64, batch);
+        if (rc) return rc;
+      }
+      k = c1;
+      continue;
+    }
+    int w = 0, *perm_p = nullptr;
+    int rc = run_panel(k, w, perm_p);
+    if (rc) return rc;
     const int c0 = k + w;
     if (c0 < ncols) {
       const int cols = ncols - c0;
-      const int blocks = std::max(1, std::min((cols + 31) / 32, (4 * ctx->num_sms + batch - 1) / batch));
-      const bool tc = sizeof(R) == 4 && ctx->use_tcgen05;
-      {
-        ProfScope ps(ctx, 2, 0.0);
-        k_laswp_trsm<R><<<dim3(blocks, batch), 256, lsmem, ctx->stream>>>(
-            A, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, tc ? ctx->tc.ure : nullptr,
-            tc ? ctx->tc.uim : nullptr, nn + 1);
-      }
-      ctx->launches++;
-      BEM_CUDA(ctx, cudaGetLastError());
+      rc = laswp(false, k, w, c0, perm_p, c0, 0, 0);
+      if (rc) return rc;
       if (c0 < nn) {
         ProfScope ps(ctx, 3, 8.0 * (double)(nn - c0) * (double)cols * (double)w * batch);
         if (tc) {
-          int rc = tc_trailing_update(ctx, static_cast<float2*>(A), lda, bstride, nn, k, w, batch);
+          rc = tc_trailing_update(ctx, static_cast<float2*>(A), lda, bstride, nn, k, w, batch);
           if (rc) return rc;
         } else if (sizeof(R) == 8) {
           dim3 grid((nn - c0 + GBM - 1) / GBM, (cols + GBN - 1) / GBN, batch);
           k_gemm_f64<<<grid, 256, kGemmSmem, ctx->stream>>>(static_cast<double2*>(A), lda, bstride, nn, k, w, c0, c0,
                                                            ncols);
+          ctx->launches++;
         } else {
           dim3 grid((nn - c0 + TBM - 1) / TBM, (cols + TBN - 1) / TBN, batch);
           k_gemm_tf32<<<grid, 256, kGemmTf32Smem, ctx->stream>>>(static_cast<float2*>(A), lda, bstride, nn, k, w, c0,
                                                                 c0, ncols);
+          ctx->launches++;
         }
-        ctx->launches++;
         BEM_CUDA(ctx, cudaGetLastError());
       }
     }
-    L.panels.push_back({k, w});
     k += w;
   }
   ProfScope ps(ctx, 4, 0.0);
