@@ -83,6 +83,7 @@ def lib():
     L.bem_prof_enable.argtypes = [vp, ip]
     L.bem_prof_reset.argtypes = [vp]
     L.bem_prof_read.argtypes = [vp, vp, vp, vp]
+    L.bem_prof_bytes.argtypes = [vp, vp]
     L.bem_measure_fp64_peak.argtypes = [vp, vp]
     L.bem_measure_peaks.argtypes = [vp, vp]
     L.bem_static_solve.argtypes = [vp, vp, dp, vp, vp, vp, vp]
@@ -152,7 +153,10 @@ class Context:
         n = np.zeros(nc, dtype=np.int64)
         work = np.zeros(nc)
         self.check(self.L.bem_prof_read(self.h, ptr(ms), ptr(n), ptr(work)), "bem_prof_read")
-        return {k: {"ms": float(ms[i]), "launches": int(n[i]), "work": float(work[i])}
+        nbytes = np.zeros(nc)
+        self.check(self.L.bem_prof_bytes(self.h, ptr(nbytes)), "bem_prof_bytes")
+        return {k: {"ms": float(ms[i]), "launches": int(n[i]), "work": float(work[i]),
+                    "bytes": float(nbytes[i])}
                 for i, k in enumerate(PROF_CLASSES)}
 
     def fp64_peak_tflops(self) -> float:

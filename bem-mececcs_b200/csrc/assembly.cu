@@ -645,7 +645,9 @@ int launch_dynamic_batch(bem_ctx* ctx, const DynBatch& b) {
   p.status = ctx->d_status;
   for (int i = 0; i < b.batch; ++i) p.kb[i] = make_consts(b.zge, b.zcs, b.zcp, b.freqs[i]);
 
-  ProfScope ps(ctx, 0, (double)m.nbe * (double)m.nbe * (double)m.ng * b.batch);
+  // work: Stokes evaluations; bytes: the FP64 system (and its complex64 copy) written once
+  ProfScope ps(ctx, 0, (double)m.nbe * (double)m.nbe * (double)m.ng * b.batch,
+               (double)(3 * m.nbe) * (3 * m.nbe + 1) * (16.0 + (b.A32 ? 8.0 : 0.0)) * b.batch);
   k_dyn_diag<<<dim3((m.nbe + 127) / 128, 1, b.batch), 128, 0, ctx->stream>>>(p);
   ctx->launches++;
   BEM_CUDA(ctx, cudaGetLastError());

@@ -123,6 +123,7 @@ struct Profiler {
   double ms[BEM_PROF_CLASSES] = {0};
   long long launches[BEM_PROF_CLASSES] = {0};
   double work[BEM_PROF_CLASSES] = {0};
+  double bytes[BEM_PROF_CLASSES] = {0};  // algorithmic device-memory bytes
 };
 
 // Brackets one launch of class `cls` with events when profiling is on.
@@ -130,7 +131,7 @@ struct ProfScope {
   bem_ctx* ctx;
   int cls;
   cudaEvent_t b = nullptr;
-  ProfScope(bem_ctx* c, int k, double work);
+  ProfScope(bem_ctx* c, int k, double work, double bytes = 0.0);
   ~ProfScope();
 };
 

@@ -80,11 +80,12 @@ static cudaEvent_t prof_event(bem_ctx* ctx) {
   return P.pool[P.used++];
 }
 
-ProfScope::ProfScope(bem_ctx* c, int k, double work) : ctx(c), cls(k) {
+ProfScope::ProfScope(bem_ctx* c, int k, double work, double bytes) : ctx(c), cls(k) {
   Profiler& P = ctx->prof;
   if (!P.on) return;
   P.launches[k]++;
   P.work[k] += work;
+  P.bytes[k] += bytes;
   cudaEvent_t a = prof_event(ctx);
   b = prof_event(ctx);
   cudaEventRecord(a, ctx->stream);
@@ -552,7 +553,15 @@ int bem_prof_reset(bem_ctx* ctx) {
     P.ms[c] = 0.0;
     P.launches[c] = 0;
     P.work[c] = 0.0;
+    P.bytes[c] = 0.0;
   }
+  return BEM_OK;
+}
+
+int bem_prof_bytes(bem_ctx* ctx, double* bytes) {
+  if (!ctx || !bytes) return BEM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  for (int c = 0; c < BEM_PROF_CLASSES; ++c) bytes[c] = ctx->prof.bytes[c];
   return BEM_OK;
 }
 

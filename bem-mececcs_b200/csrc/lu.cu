@@ -1600,7 +1600,7 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     pa.pstart = L.pstart;
     pa.pidx = (int)L.panels.size();
     const int nb = panel_nb(m);
-    ProfScope ps(ctx, 1, 0.0);
+    ProfScope ps(ctx, 1, 0.0, 2.0 * (double)m * std::min(nb ? nb : 64, m) * es * batch);
     if (nb) {
       w = std::min(nb, m);
       pa.w = w;
@@ -1644,7 +1644,8 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     const int cols = ncols - c0;
     if (cols <= 0) return BEM_OK;
     const int blocks = std::max(1, std::min((cols + 31) / 32, (4 * ctx->num_sms + batch - 1) / batch));
-    ProfScope ps(ctx, 2, 0.0);
+    // rows k..k+w-1 (and the displaced rows) of every column read and written once
+    ProfScope ps(ctx, 2, 0.0, 2.0 * (double)cols * (2 * w) * es * batch);
     float* ure = tc ? ctx->tc.ure : nullptr;
     float* uim = tc ? ctx->tc.uim : nullptr;
     if (pre)
@@ -1674,7 +1675,8 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
       rc = laswp(false, k, 64, c0, p1, c0, 0, 0);
       if (rc) return rc;
       {
-        ProfScope ps(ctx, 3, 8.0 * (double)(nn - c0) * 64.0 * 64.0 * batch);
+        ProfScope ps(ctx, 3, 8.0 * (double)(nn - c0) * 64.0 * 64.0 * batch,
+                     2.0 * (double)(nn - c0) * 64.0 * es * batch);
         rc = tc_pack_l(ctx, static_cast<float2*>(A), lda, bstride, nn, k, 64, c0, 0, batch, nullptr, 0);
         if (!rc) rc = tc_gemm(ctx, static_cast<float2*>(A), lda, bstride, nn, c0, c0, c1, 64, 0, batch);
         if (rc) return rc;
@@ -1684,7 +1686,8 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
       rc = laswp(true, c0, 64, c1, p2, c0, 64, k);
       if (rc) return rc;
       if (c1 < nn) {
-        ProfScope ps(ctx, 3, 8.0 * (double)(nn - c1) * (double)(ncols - c1) * 128.0 * batch);
+        ProfScope ps(ctx, 3, 8.0 * (double)(nn - c1) * (double)(ncols - c1) * 128.0 * batch,
+                     2.0 * (double)(nn - c1) * (double)(ncols - c1) * es * batch);
         rc = tc_pack_l(ctx, static_cast<float2*>(A), lda, bstride, nn, k, 64, c1, 0, batch, p2, kPermStride);
         if (!rc) rc = tc_pack_l(ctx, static_cast<float2*>(A), lda, bstride, nn, c0, 64, c1, 64, batch, nullptr, 0);
         if (!rc) rc = tc_gemm(ctx, static_cast<float2*>(A), lda, bstride, nn, c1, c1, ncols, 128, 64, batch);
@@ -1702,7 +1705,8 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
       rc = laswp(false, k, w, c0, perm_p, c0, 0, 0);
       if (rc) return rc;
       if (c0 < nn) {
-        ProfScope ps(ctx, 3, 8.0 * (double)(nn - c0) * (double)cols * (double)w * batch);
+        ProfScope ps(ctx, 3, 8.0 * (double)(nn - c0) * (double)cols * (double)w * batch,
+                     2.0 * (double)(nn - c0) * (double)cols * es * batch);
         if (tc) {
           rc = tc_trailing_update(ctx, static_cast<float2*>(A), lda, bstride, nn, k, w, batch);
           if (rc) return rc;
@@ -1722,7 +1726,7 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     }
     k += w;
   }
-  ProfScope ps(ctx, 4, 0.0);
+  ProfScope ps(ctx, 4, 4.0 * (double)nn * nn * batch, 0.5 * (double)nn * nn * es * batch);
   if (ctx->use_trsv_coop) {
     using E = typename Elt<R>::T;
     return trsv_coop<R>(ctx, A, lda, bstride, nn, batch, static_cast<E*>(A) + (size_t)nn * lda, bstride, false);
@@ -1807,7 +1811,7 @@ static int lu_solve_vec_t(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int
   const size_t lsmem = 64 * 64 * es;
   BEM_CUDA(ctx, cudaFuncSetAttribute(k_fwd_panel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem));
   BEM_CUDA(ctx, cudaFuncSetAttribute(k_backsub<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem));
-  ProfScope ps(ctx, 4, 0.0);
+  ProfScope ps(ctx, 4, 8.0 * (double)nn * nn * batch, (double)nn * nn * sizeof(cpx<R>) * batch);
   if (ctx->use_trsv_coop) return trsv_coop<R>(ctx, A, lda, bstride, nn, batch, v, vstride, true);
   for (size_t p = 0; p < L.panels.size(); ++p) {
     const int k = L.panels[p].first, w = L.panels[p].second;

@@ -193,7 +193,7 @@ int refine_steps(bem_ctx* ctx, SweepBuf& S, int bsz, int iters, int it0) {
   const dim3 vgrid((nn + 255) / 256, bsz);
   for (int it = 0; it < iters; ++it) {
     {
-      ProfScope ps(ctx, 5, 8.0 * (double)nn * nn * bsz);
+      ProfScope ps(ctx, 5, 8.0 * (double)nn * nn * bsz, 16.0 * (double)nn * nn * bsz);
       k_resid_partial<<<dim3((nn + kResidRows - 1) / kResidRows, S.resid_chunks, bsz), kResidRows, 0,
                         ctx->stream>>>(S.A64, S.lda, S.a_stride, S.x64, nn, nn, S.resid_chunks, S.part);
       k_resid_final<<<vgrid, 256, 0, ctx->stream>>>(S.A64, S.lda, S.a_stride, S.part, nn, S.resid_chunks, S.v32,

@@ -318,8 +318,9 @@ def run_ours(args):
     shares = {k: round(v["ms"] / t_mix["ms"], 4) for k, v in pm.items()}
     # Roofline of the dominant kernel of the headline form.
     peaks = _peaks()
-    top = max(("assembly", "gemm", "panel", "residual"), key=lambda k: pm[k]["ms"])
+    top = max(pm, key=lambda k: pm[k]["ms"])
     roof = _roofline(top, pm[top], peaks, mpeaks)
+    roof_all = {k: _roofline(k, v, peaks, mpeaks) for k, v in pm.items() if v["ms"] > 0}
     g64 = pp["gemm"]
     plain_gemm = g64["work"] / (g64["ms"] * 1e-3) / 1e12 if g64["ms"] > 0 else None
     line = {
@@ -349,6 +350,9 @@ def run_ours(args):
                        "kernel_share": {k: round(v["ms"] / t_plain["ms"], 4) for k, v in pp.items()}},
         "speedup_vs_plain_fp64": round(value / value_plain, 3),
         "roofline": roof,
+        "rooflines_all": {k: {kk: v[kk] for kk in ("achieved", "frac", "ms") if kk in v} |
+                          ({"tensor_frac": v["tensor"]["frac"]} if "tensor" in v else {})
+                          for k, v in roof_all.items()},
         "peaks_measured_tflops": mpeaks,
         "kernel_share": shares,
         "kernels": pm,
@@ -500,49 +504,47 @@ def _peaks():
         return {}
 
 
+KERNELS = {
+    "assembly": "k_dyn_diag + k_dyn_offdiag + k_rhs_reduce (FP64 Stokes assembly, BC swap, RHS)",
+    "panel": "k_panel_cluster (LU panel, one 16-CTA cluster per problem, DSMEM pivoting)",
+    "laswp_trsm": "k_laswp_trsm (row interchanges + U12 triangular solve, FP32)",
+    "gemm": "k_pack_l21 + k_gemm_tc (FP32 LU trailing update, tcgen05 kind::tf32, K = 128, TMA reduce-add)",
+    "solves": "k_trsv (cooperative forward + back substitution)",
+    "residual": "k_resid_partial + k_resid_final (FP64 refinement residual)",
+}
+NOTES = {
+    "panel": "latency bound: a CTA barrier, a cluster barrier and one DSMEM round per column",
+    "solves": "latency bound: one group barrier per 64-row step",
+    "laswp_trsm": "FP32 SIMT issue bound (the 64-step substitution per column)",
+    "assembly": "FP64-pipe bound (two complex exponentials per Gauss point); bytes are the systems written",
+}
+
+
 def _roofline(name, k, peaks, mpeaks):
-    """Roofline of one kernel class measured over the timed region."""
+    """Roofline of one kernel class over the timed region: achieved
+    algorithmic bytes (bem_prof_bytes) per second against the measured HBM
+    copy bandwidth; the trailing update also against the tcgen05 TF32 peak."""
     secs = k["ms"] * 1e-3
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    gbs = k.get("bytes", 0.0) / secs / 1e9 if secs > 0 else 0.0
+    out = {"bound": "hbm", "kernel": KERNELS.get(name, name), "achieved": round(gbs, 1), "peak": hbm,
+           "unit": "GB/s", "frac": round(gbs / hbm, 4), "traffic": None,
+           "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
+           "ms": round(k["ms"], 3), "launches": k["launches"]}
+    if name in NOTES:
+        out["note"] = NOTES[name]
     if name == "gemm":
-        # C -= L21 U12 with K = 64 (every FP32 panel at n = 6480 is 64 wide): 8*64 flops per
-        # complex element of C, whose 8 bytes are read and written once (TMA reduce-add), so
-        # the algorithmic traffic is flops / 32 bytes and the bound is HBM, not the tensor pipe.
-        hbm = peaks.get("hbm_gbs", 6650.0)
         tf = k["work"] / secs / 1e12
-        gbs = k["work"] / 32.0 / secs / 1e9
-        kern = ("k_gemm_tf32 (FP32 LU trailing update, TF32 mma.sync)"
-                if os.environ.get("BEM_TF32_MMA_SYNC") == "1" else
-                "k_pack_l21 + k_gemm_tc (FP32 LU trailing update, tcgen05 kind::tf32, TMEM "
-                "accumulators, TMA reduce-add of C)")
-        return {"bound": "hbm", "kernel": kern,
-                "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s",
-                "frac": round(gbs / hbm, 4), "traffic": None,
-                "traffic_note": ("ncu, one launch of 2 problems: dram read+write = 1.15 x the "
-                                 "algorithmic C bytes (profiles/k_gemm_tc_2160.md)"),
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
-                "tensor": {"achieved_tflops": round(tf, 2),
-                           "peak_tflops": round(mpeaks["tf32_umma_n128"], 1),
-                           "frac": round(tf / mpeaks["tf32_umma_n128"], 4),
-                           "peak_source": "measured: tcgen05 kind::tf32 M=128 N=128 issue-rate "
-                                          "microbenchmark (bem_measure_peaks)"}}
-    if name == "residual":
-        hbm = peaks.get("hbm_gbs", 6650.0)
-        nbytes = k["work"] / 8.0 * 16.0  # 8 n^2 flops <-> 16 n^2 bytes of the FP64 matrix
-        ach = nbytes / secs / 1e9
-        return {"bound": "hbm", "kernel": "k_resid_partial (FP64 refinement residual)",
-                "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s", "frac": round(ach / hbm, 4),
-                "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"}
+        peak = mpeaks["tf32_umma_n128"]
+        out["traffic_note"] = ("ncu, one K = 64 launch of 2 problems: dram read+write = 1.15 x the algorithmic "
+                               "C bytes (profiles/k_gemm_tc_2160.md)")
+        out["tensor"] = {"achieved_tflops": round(tf, 2), "peak_tflops": round(peak, 1),
+                         "frac": round(tf / peak, 4),
+                         "peak_source": "measured: tcgen05 kind::tf32 M=128 N=128 issue-rate "
+                                        "microbenchmark (bem_measure_peaks)"}
     if name == "assembly":
-        # Work = Stokes evaluations; the bound is the FP64 pipe: report
-        # evaluations/s against the FP64 tensor-probe peak converted at the
-        # instruction count of k_dyn_offdiag measured by ncu (see profiles/).
-        ach = k["work"] / secs / 1e9
-        return {"bound": "fp64-pipe", "kernel": "k_dyn_offdiag (FP64 Stokes assembly)",
-                "achieved": round(ach, 2), "peak": None, "unit": "G Stokes evaluations/s",
-                "frac": None, "traffic": None}
-    return {"bound": "latency", "kernel": "k_panel_cluster (LU panel, one cluster per problem)",
-            "achieved": None, "peak": None, "unit": None, "frac": None, "traffic": None,
-            "ms": round(k["ms"], 3), "launches": k["launches"]}
+        out["stokes_evals_per_s"] = round(k["work"] / secs, 1)
+    return out
 
 
 def run_reference(args):

@@ -268,6 +268,12 @@ int bem_prof_enable(bem_ctx *ctx, int on);
 int bem_prof_reset(bem_ctx *ctx);
 int bem_prof_read(bem_ctx *ctx, double *ms, long long *launches,
                   double *work);
+/* Algorithmic device-memory bytes per class since the last reset (data each
+ * class must read or write at least once: the panel slices, the rows
+ * interchanged and solved, C read and written once per trailing update, the
+ * factors read once per solve, the FP64 matrix once per residual, the
+ * systems written by the assembly). */
+int bem_prof_bytes(bem_ctx *ctx, double *bytes);
 
 /* Measures this GPU's FP64 tensor-core (DMMA) throughput with a
  * register-resident mma.sync loop; writes TFLOP/s. */
