@@ -179,6 +179,7 @@ struct bem_ctx {
   size_t pinned_bytes = 0;
   bool use_tcgen05 = true;  // FP32 trailing update on tcgen05 (else TF32 mma.sync)
   bool use_trsv_coop = true;
+  bool panel_calu = false;    // FP32 LU panels: tournament pivoting per 8-column sub-panel
   bool lu_pairs = true;       // FP32 tensor-core LU: two 64-column panels per trailing update (K = 128)  // one cooperative launch per triangular solve (else per-block launches)
 };
 

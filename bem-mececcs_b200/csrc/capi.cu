@@ -141,6 +141,7 @@ int bem_ctx_create(int device, bem_ctx** out) {
   if (const char* env = getenv("BEM_TF32_MMA_SYNC")) ctx->use_tcgen05 = env[0] != '1';
   if (const char* env = getenv("BEM_TRSV_LEGACY")) ctx->use_trsv_coop = env[0] != '1';
   if (const char* env = getenv("BEM_LU_PAIRS")) ctx->lu_pairs = env[0] != '0';
+  if (const char* env = getenv("BEM_PANEL_CALU")) ctx->panel_calu = env[0] == '1';
   *out = ctx;
   return BEM_OK;
 }

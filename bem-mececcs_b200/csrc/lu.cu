@@ -525,12 +525,19 @@ __global__ void __launch_bounds__(NT, 1) k_panel_cluster(PanelArgs a) {
       const int gr = grow[q];
       const int lr = gr - rbase;
       if (gr != INT_MAX && gr >= k + s0 + sw) {
-        for (int c = s0 + sw; c < w; ++c) {
-          C x = s_a[c * rp + lr];
+        // Four columns per iteration as independent chains (the remaining
+        // width is a multiple of 8).
+        for (int c = s0 + sw; c < w; c += 4) {
+          C x[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) x[u] = s_a[(c + u) * rp + lr];
 #pragma unroll
           for (int t = 0; t < SW; ++t)
-            if (t < sw) cfms(x, v[q][t], s_u[t][c]);
-          s_a[c * rp + lr] = x;
+            if (t < sw)
+#pragma unroll
+              for (int u = 0; u < 4; ++u) cfms(x[u], v[q][t], s_u[t][c + u]);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) s_a[(c + u) * rp + lr] = x[u];
         }
       } else if (gr != INT_MAX && gr >= k + s0) {
         const int i = gr - k - s0;
@@ -548,6 +555,411 @@ __global__ void __launch_bounds__(NT, 1) k_panel_cluster(PanelArgs a) {
     if (tid < w) ipiv[k + tid] = s_ipiv[tid];
     if (tid == 0) perm[0] = s_pcount;
     for (int e = tid; e < s_pcount; e += blockDim.x) {
+      perm[1 + 2 * e] = s_pdst[e];
+      perm[2 + 2 * e] = s_psrc[e];
+    }
+  }
+  cluster_sync();  // no CTA leaves while others may still read its shared memory
+}
+
+// ---------------------------------------------------------------------------
+// Panel with tournament pivoting (FP32: the mixed form's factorisation, which
+// only has to precondition the FP64 refinement).  Pivots are chosen per
+// 8-column sub-panel instead of per column: every CTA picks 8 candidate rows
+// of its own by partial pivoting on a copy of its rows (no cluster traffic),
+// then every CTA gathers the cluster's candidates (cs x 8 rows) over
+// distributed shared memory and runs the same partial pivoting on them, which
+// yields the 8 pivot rows and the sub-panel's 8 x 8 L\U block in every CTA
+// at once.  The 8 interchanges, applied in order as LAPACK would, move at
+// most 16 rows; those rows are published and pulled in one more exchange, and
+// every other row gets its L entries by a triangular solve against the U
+// block.  Two cluster barriers per sub-panel instead of one per column.  The
+// gather lists, pivot indices and the right-of-block update are those of
+// k_panel_cluster, so the later kernels are unchanged.
+// ---------------------------------------------------------------------------
+constexpr int kCaluSW = 8;
+constexpr int kCaluCand = 16 * kCaluSW;  // candidate rows of a 16-CTA cluster
+constexpr int kCaluMoves = 2 * kCaluSW;  // rows that move (or pivot) per sub-panel
+
+// CTA-wide argmax in the better() order; every thread returns with the
+// result.  One __syncthreads inside; s_rv/s_rr may be rewritten only after
+// the caller's next barrier.
+__device__ __forceinline__ void cta_argmax(float& v, int& r, float* s_rv, int* s_rr) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, v, off);
+    const int orr = __shfl_xor_sync(0xffffffffu, r, off);
+    if (better(ov, orr, v, r)) {
+      v = ov;
+      r = orr;
+    }
+  }
+  if (lane == 0) {
+    s_rv[warp] = v;
+    s_rr[warp] = r;
+  }
+  __syncthreads();
+  v = lane < nw ? s_rv[lane] : -1.f;
+  r = lane < nw ? s_rr[lane] : INT_MAX;
+#pragma unroll
+  for (int off = 8; off > 0; off >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, v, off);
+    const int orr = __shfl_xor_sync(0xffffffffu, r, off);
+    if (better(ov, orr, v, r)) {
+      v = ov;
+      r = orr;
+    }
+  }
+  v = __shfl_sync(0xffffffffu, v, 0);
+  r = __shfl_sync(0xffffffffu, r, 0);
+}
+
+template <int N>
+__device__ __forceinline__ zf sel(const zf (&x)[N], int j) {
+  zf r = x[0];
+#pragma unroll
+  for (int c = 1; c < N; ++c)
+    if (c == j) r = x[c];
+  return r;
+}
+
+template <int NB, int NT>
+__global__ void __launch_bounds__(NT, 1) k_panel_calu(PanelArgs a) {
+  using C = zf;
+  constexpr int SW = kCaluSW;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s_a = reinterpret_cast<C*>(smem_raw);  // [NB][rp] panel rows, column-major
+  C* s_x = s_a + (size_t)NB * a.rp;          // [kCaluCand][SW] gathered candidates, then
+                                             // [kCaluMoves][NB] published rows
+  __shared__ C s_u[SW][NB];                  // pivot rows: L\U in the block, A then U right of it
+  __shared__ C s_lu[SW][SW];                 // the sub-panel's pivot block, L\U
+  __shared__ C s_lv[SW][SW];                 // this CTA's candidates (values at the sub-panel start)
+  __shared__ int s_lid[SW];                  // their positions (-1: none)
+  __shared__ int s_cid[kCaluCand];
+  __shared__ int s_pid[SW];                  // pivot rows (positions at the sub-panel start), in order
+  __shared__ C s_tw[SW];
+  __shared__ float s_rv[NT / 32];
+  __shared__ int s_rr[NT / 32];
+  __shared__ int s_mdst[kCaluMoves], s_msrc[kCaluMoves], s_mcnt;
+  __shared__ int s_ppos[kCaluMoves], s_pcnt;
+  __shared__ int s_pdst[2 * NB], s_psrc[2 * NB];
+  __shared__ int s_pcount;
+  __shared__ int s_ipiv[NB];
+
+  const unsigned rank = cluster_rank();
+  const int prob = blockIdx.y, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  float2* A = static_cast<float2*>(a.A) + (size_t)prob * a.bstride;
+  int* ipiv = a.ipiv + (size_t)prob * a.ipiv_stride;
+  int* perm = a.perm + (size_t)prob * a.perm_stride;
+  const int rp = a.rp, w = a.w, k = a.k, cs = a.cs;
+  const int rbase = k + (int)rank * rp;
+  const int rcount = max(0, min(rp, a.nn - rbase));
+
+  load_slice_async<float>(A, a.lda, rbase, k, rcount, w, s_a, rp);
+  if (rank == 0 && prob == 0 && tid == 0 && a.pstart) {
+    a.pstart[a.pidx] = k;
+    a.pstart[a.pidx + 1] = k + w;
+  }
+  if (rank == 0 && tid < w) {
+    s_pdst[tid] = k + tid;
+    s_psrc[tid] = k + tid;
+  }
+  if (rank == 0 && tid == 0) s_pcount = w;
+  __syncthreads();
+
+  const int lr = tid;
+  const int grow = lr < rcount ? rbase + lr : INT_MAX;
+  C v[SW];
+  auto zero = [] { return C{0.f, 0.f}; };
+
+  for (int s0 = 0; s0 < w; s0 += SW) {
+    const int sw = min(SW, w - s0);
+    const int g0 = k + s0;
+#pragma unroll
+    for (int c = 0; c < SW; ++c) v[c] = (grow != INT_MAX && c < sw) ? s_a[(s0 + c) * rp + lr] : zero();
+    const bool elig = grow != INT_MAX && grow >= g0;
+
+    // 1. This CTA's candidates: partial pivoting on a copy of its rows.
+    {
+      C t[SW];
+#pragma unroll
+      for (int c = 0; c < SW; ++c) t[c] = v[c];
+      bool chosen = false;
+      for (int jj = 0; jj < sw; ++jj) {
+        float bv = -1.f;
+        int br = INT_MAX;
+        if (elig && !chosen) {
+          bv = cabs1(sel(t, jj));
+          if (!(bv >= 0.f)) bv = 0.f;  // a NaN still takes part, so a candidate always exists
+          br = grow;
+        }
+        cta_argmax(bv, br, s_rv, s_rr);
+        if (br != INT_MAX && grow == br) {
+          chosen = true;
+#pragma unroll
+          for (int c = 0; c < SW; ++c) {
+            s_tw[c] = t[c];
+            s_lv[jj][c] = v[c];
+          }
+          s_lid[jj] = br;
+        }
+        if (tid == 0 && br == INT_MAX) s_lid[jj] = -1;
+        __syncthreads();
+        if (br != INT_MAX && elig && !chosen) {
+          const C p = s_tw[jj];
+          const C l = (p.re == 0.f && p.im == 0.f) ? zero() : sel(t, jj) * crcp(p);
+#pragma unroll
+          for (int c = 0; c < SW; ++c)
+            if (c > jj) cfms(t[c], l, s_tw[c]);
+        }
+      }
+    }
+    cluster_sync();  // A: every CTA's candidates are published
+
+    // 2. The cluster's candidates, the same partial pivoting in every CTA.
+    C* s_cv = s_x;
+    for (int i = tid; i < cs * SW; i += NT) s_cid[i] = i / SW < cs ? dsm_ld(&s_lid[i % SW], (unsigned)(i / SW)) : -1;
+    for (int i = tid; i < cs * SW * SW; i += NT) {
+      const int cand = i / SW, c = i % SW;
+      s_cv[i] = dsm_ld(&s_lv[cand % SW][c], (unsigned)(cand / SW));
+    }
+    __syncthreads();
+    if (warp == 0) {
+      C T[4][SW];
+      int id[4];
+      bool ch[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int cand = lane + 32 * q;
+        id[q] = (cand < cs * SW && (cand % SW) < sw) ? s_cid[cand] : -1;
+        ch[q] = false;
+#pragma unroll
+        for (int c = 0; c < SW; ++c) T[q][c] = id[q] >= 0 ? s_cv[cand * SW + c] : zero();
+      }
+      for (int jj = 0; jj < sw; ++jj) {
+        float bv = -1.f;
+        int bid = INT_MAX, bq = 0, bl = lane;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (id[q] >= 0 && !ch[q]) {
+            float val = cabs1(sel(T[q], jj));
+            if (!(val >= 0.f)) val = 0.f;
+            if (better(val, id[q], bv, bid)) {
+              bv = val;
+              bid = id[q];
+              bq = q;
+            }
+          }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          const float ov = __shfl_xor_sync(0xffffffffu, bv, off);
+          const int oid = __shfl_xor_sync(0xffffffffu, bid, off);
+          const int oq = __shfl_xor_sync(0xffffffffu, bq, off);
+          const int ol = __shfl_xor_sync(0xffffffffu, bl, off);
+          if (better(ov, oid, bv, bid)) {
+            bv = ov;
+            bid = oid;
+            bq = oq;
+            bl = ol;
+          }
+        }
+        C tw[SW];
+#pragma unroll
+        for (int c = 0; c < SW; ++c) {
+          C mine = T[0][c];
+#pragma unroll
+          for (int q = 1; q < 4; ++q)
+            if (q == bq) mine = T[q][c];
+          tw[c].re = __shfl_sync(0xffffffffu, mine.re, bl);
+          tw[c].im = __shfl_sync(0xffffffffu, mine.im, bl);
+        }
+        if (lane == bl) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (q == bq) ch[q] = true;
+        }
+        if (lane == 0) {
+          s_pid[jj] = bid;
+#pragma unroll
+          for (int c = 0; c < SW; ++c) s_lu[jj][c] = tw[c];
+        }
+        const C piv = sel(tw, jj);
+        const bool zp = piv.re == 0.f && piv.im == 0.f;
+        if (zp && rank == 0 && lane == 0) atomicCAS(&a.status[ST_SINGULAR], 0, g0 + jj + 1);
+        const C rpv = zp ? zero() : crcp(piv);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (id[q] >= 0 && !ch[q]) {
+            const C l = sel(T[q], jj) * rpv;
+#pragma unroll
+            for (int c = 0; c < SW; ++c) {
+              if (c == jj) T[q][c] = l;
+              if (c > jj) cfms(T[q][c], l, tw[c]);
+            }
+          }
+      }
+    }
+    __syncthreads();
+
+    // 3. The interchanges in order (position of the pivot row swapped with
+    //    position g0 + j), as position moves dst <- src (sub-panel start values).
+    if (tid == 0) {
+      int cur[SW], pos[kCaluMoves], lab[kCaluMoves], n = 0;
+      for (int j = 0; j < sw; ++j) cur[j] = s_pid[j];
+      for (int j = 0; j < sw; ++j) {
+        const int tp = g0 + j, p = cur[j];
+        if (rank == 0) {
+          s_ipiv[s0 + j] = p + 1;
+          perm_swap(s_pdst, s_psrc, s_pcount, k, w, s0 + j, p);
+        }
+        if (p != tp) {
+          int it = -1, ip = -1;
+          for (int i = 0; i < n; ++i) {
+            if (pos[i] == tp) it = i;
+            if (pos[i] == p) ip = i;
+          }
+          if (it < 0) {
+            it = n++;
+            pos[it] = tp;
+            lab[it] = tp;
+          }
+          if (ip < 0) {
+            ip = n++;
+            pos[ip] = p;
+            lab[ip] = p;
+          }
+          const int tl = lab[it];
+          lab[it] = lab[ip];
+          lab[ip] = tl;
+          for (int i = j + 1; i < sw; ++i)
+            if (cur[i] == tp) cur[i] = p;
+        }
+      }
+      int m = 0;
+      for (int i = 0; i < n; ++i)
+        if (lab[i] != pos[i]) {
+          s_mdst[m] = pos[i];
+          s_msrc[m] = lab[i];
+          ++m;
+        }
+      s_mcnt = m;
+      int np = 0;
+      for (int j = 0; j < sw + m; ++j) {
+        const int y = j < sw ? s_pid[j] : s_msrc[j - sw];
+        bool seen = false;
+        for (int i = 0; i < np; ++i) seen |= s_ppos[i] == y;
+        if (!seen) s_ppos[np++] = y;
+      }
+      s_pcnt = np;
+    }
+    __syncthreads();
+
+    // 4. Publish the rows that move or pivot, then pull the moved rows.
+    C* s_pub = s_x;
+    const int npub = s_pcnt, nmov = s_mcnt;
+    for (int i = 0; i < npub; ++i) {
+      const int y = s_ppos[i];
+      if (y >= rbase && y < rbase + rcount) {
+        const int ly = y - rbase;
+        for (int c = tid; c < w; c += NT)
+          if (c < s0 || c >= s0 + sw) s_pub[i * NB + c] = s_a[c * rp + ly];
+        if (tid == ly)
+#pragma unroll
+          for (int c = 0; c < SW; ++c)
+            if (c < sw) s_pub[i * NB + s0 + c] = v[c];
+      }
+    }
+    cluster_sync();  // B: published rows visible
+    auto pub_index = [&](int y) {
+      int r = 0;
+      for (int i = 0; i < npub; ++i)
+        if (s_ppos[i] == y) r = i;
+      return r;
+    };
+    for (int mv = 0; mv < nmov; ++mv) {
+      const int x = s_mdst[mv];
+      if (x >= rbase && x < rbase + rcount) {
+        const int y = s_msrc[mv], pi = pub_index(y), lx = x - rbase;
+        const unsigned owner = (unsigned)((y - k) / rp);
+        for (int c = tid; c < w; c += NT)
+          if (c < s0 || c >= s0 + sw) s_a[c * rp + lx] = dsm_ld(&s_pub[pi * NB + c], owner);
+        if (tid == lx)
+#pragma unroll
+          for (int c = 0; c < SW; ++c)
+            if (c < sw) v[c] = dsm_ld(&s_pub[pi * NB + s0 + c], owner);
+      }
+    }
+    for (int idx = tid; idx < sw * w; idx += NT) {
+      const int j = idx / w, c = idx % w;
+      if (c >= s0 + sw) {
+        const int y = s_pid[j];
+        s_u[j][c] = dsm_ld(&s_pub[pub_index(y) * NB + c], (unsigned)((y - k) / rp));
+      } else if (c >= s0) {
+        s_u[j][c] = s_lu[j][c - s0];
+      }
+    }
+
+    // 5. The sub-panel's L (and the pivot block) for my row.
+    if (grow != INT_MAX && grow >= g0) {
+      if (grow < g0 + sw) {
+        const int j = grow - g0;
+#pragma unroll
+        for (int c = 0; c < SW; ++c) v[c] = s_lu[j][c];
+      } else {
+#pragma unroll
+        for (int jj = 0; jj < SW; ++jj) {
+          if (jj >= sw) break;
+          C x = v[jj];
+#pragma unroll
+          for (int i = 0; i < jj; ++i) cfms(x, v[i], s_lu[i][jj]);
+          const C d = s_lu[jj][jj];
+          v[jj] = (d.re == 0.f && d.im == 0.f) ? zero() : x * crcp(d);
+        }
+      }
+    }
+    // End of the sub-panel: registers back to shared memory.
+    if (grow != INT_MAX)
+#pragma unroll
+      for (int c = 0; c < SW; ++c)
+        if (c < sw) s_a[(s0 + c) * rp + lr] = v[c];
+    __syncthreads();
+    if (s0 + sw >= w) break;
+    // U of the pivot rows right of the block:
+    // U(i,c) = A(i,c) - sum_{t<i} L(i,t) U(t,c).
+    for (int c = s0 + sw + tid; c < w; c += NT)
+      for (int i = 1; i < sw; ++i) {
+        C x = s_u[i][c];
+        for (int t = 0; t < i; ++t) cfms(x, s_u[i][s0 + t], s_u[t][c]);
+        s_u[i][c] = x;
+      }
+    __syncthreads();
+    if (grow != INT_MAX && grow >= g0 + sw) {
+      for (int c = s0 + sw; c < w; c += 4) {
+        C x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = s_a[(c + u) * rp + lr];
+#pragma unroll
+        for (int t = 0; t < SW; ++t)
+          if (t < sw)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) cfms(x[u], v[t], s_u[t][c + u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) s_a[(c + u) * rp + lr] = x[u];
+      }
+    } else if (grow != INT_MAX && grow >= g0) {
+      const int i = grow - g0;
+      for (int c = s0 + sw; c < w; ++c) s_a[c * rp + lr] = s_u[i][c];
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  for (int r = tid; r < rcount; r += NT)
+    for (int c = 0; c < w; ++c) stc<float>(&A[(size_t)(k + c) * a.lda + rbase + r], s_a[c * rp + r]);
+  if (rank == 0) {
+    if (tid < w) ipiv[k + tid] = s_ipiv[tid];
+    if (tid == 0) perm[0] = s_pcount;
+    for (int e = tid; e < s_pcount; e += NT) {
       perm[1 + 2 * e] = s_pdst[e];
       perm[2 + 2 * e] = s_psrc[e];
     }
@@ -1406,6 +1818,59 @@ static bool cluster_panel_fits_any(int nb, int rp) {
   return false;
 }
 
+template <int NB>
+static size_t calu_dyn_smem(int rp) {
+  return ((size_t)NB * rp + (size_t)std::max(kCaluCand * kCaluSW, kCaluMoves * NB)) * sizeof(zf);
+}
+
+template <int NB, int NT>
+static bool calu_panel_fits(int rp) {
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, k_panel_calu<NB, NT>) != cudaSuccess) return false;
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return calu_dyn_smem<NB>(rp) + fa.sharedSizeBytes + 1024 <= (size_t)optin;
+}
+
+static bool calu_panel_fits_any(int nb, int rp) {
+  const bool big = rp > 256;
+  if (nb == 64) return big ? calu_panel_fits<64, 512>(rp) : calu_panel_fits<64, 256>(rp);
+  if (nb == 32) return big ? calu_panel_fits<32, 512>(rp) : calu_panel_fits<32, 256>(rp);
+  if (nb == 16) return big ? calu_panel_fits<16, 512>(rp) : calu_panel_fits<16, 256>(rp);
+  return false;
+}
+
+template <int NB, int NT>
+static int launch_calu_panel(bem_ctx* ctx, const PanelArgs& pa, int batch) {
+  const size_t smem = calu_dyn_smem<NB>(pa.rp);
+  auto kern = k_panel_calu<NB, NT>;
+  BEM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  BEM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(pa.cs, batch, 1);
+  cfg.blockDim = dim3(NT, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = pa.cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  BEM_CUDA(ctx, cudaLaunchKernelEx(&cfg, kern, pa));
+  return BEM_OK;
+}
+
+static int launch_calu_panel_any(bem_ctx* ctx, const PanelArgs& pa, int batch, int nb) {
+  const bool big = pa.rp > 256;
+  if (nb == 64) return big ? launch_calu_panel<64, 512>(ctx, pa, batch) : launch_calu_panel<64, 256>(ctx, pa, batch);
+  if (nb == 32) return big ? launch_calu_panel<32, 512>(ctx, pa, batch) : launch_calu_panel<32, 256>(ctx, pa, batch);
+  if (nb == 16) return big ? launch_calu_panel<16, 512>(ctx, pa, batch) : launch_calu_panel<16, 256>(ctx, pa, batch);
+  return fail(ctx, BEM_ERR_ARG, "no tournament panel variant for this size");
+}
+
 // Dispatch on (panel width, threads = rows per CTA rounded up to 256 or 512).
 template <typename R>
 static int launch_cluster_panel_any(bem_ctx* ctx, const PanelArgs& pa, int batch, int nb) {
@@ -1575,11 +2040,13 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
   // Panel width for m remaining rows: the widest of 64/32/16 whose rows fit
   // one cluster, at most 512 rows per CTA (one row per thread); 0 when the
   // panel needs the cooperative-grid kernel.
+  // FP32 (the mixed form) pivots by tournament per 8-column sub-panel.
+  const bool calu = sizeof(R) == 4 && ctx->panel_calu;
   auto panel_nb = [&](int m) {
     const int rp_c = (m + cs - 1) / cs;
     if (rp_c <= 512)
       for (int cand : {64, 32, 16})
-        if (cluster_panel_fits_any<R>(cand, rp_c)) return cand;
+        if (calu ? calu_panel_fits_any(cand, rp_c) : cluster_panel_fits_any<R>(cand, rp_c)) return cand;
     return 0;
   };
   // Factors the panel starting at column k; returns its width and gather lists.
@@ -1606,7 +2073,7 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
       pa.w = w;
       pa.rp = (m + cs - 1) / cs;
       pa.cs = cs;  // CTAs past the last row own no rows but join every barrier
-      int rc = launch_cluster_panel_any<R>(ctx, pa, batch, nb);
+      int rc = calu ? launch_calu_panel_any(ctx, pa, batch, nb) : launch_cluster_panel_any<R>(ctx, pa, batch, nb);
       if (rc) return rc;
       ctx->launches++;
     } else {
