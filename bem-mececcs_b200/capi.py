@@ -63,6 +63,8 @@ def lib():
     L.bem_status_string.restype = ctypes.c_char_p
     L.bem_last_error.argtypes = [vp]
     L.bem_last_error.restype = ctypes.c_char_p
+    L.bem_ctx_set_option.argtypes = [vp, ctypes.c_char_p, ip]
+    L.bem_ctx_get_option.argtypes = [vp, ctypes.c_char_p, P(ip)]
     L.bem_ctx_launch_count.argtypes = [vp]
     L.bem_ctx_launch_count.restype = ctypes.c_longlong
     L.bem_mesh_upload.argtypes = [vp, ip, ip, ip, ip] + [vp] * 10
@@ -136,6 +138,15 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def set_option(self, name: str, value) -> None:
+        """bem_ctx_set_option: tcgen05, trsv_coop, lu_pairs, panel_calu, graphs."""
+        self.check(self.L.bem_ctx_set_option(self.h, name.encode(), int(bool(value))), "bem_ctx_set_option")
+
+    def get_option(self, name: str) -> bool:
+        out = ctypes.c_int(0)
+        self.check(self.L.bem_ctx_get_option(self.h, name.encode(), ctypes.byref(out)), "bem_ctx_get_option")
+        return bool(out.value)
 
     @property
     def launches(self) -> int:

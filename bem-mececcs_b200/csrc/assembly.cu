@@ -608,11 +608,10 @@ StokesConsts<double> make_consts(const double zge_[2], const double zcs_[2],
   return k;
 }
 
-int launch_dynamic_batch(bem_ctx* ctx, const DynBatch& b) {
+static DynParams dyn_params(bem_ctx* ctx, const DynBatch& b) {
   Mesh& m = ctx->mesh;
   const int jc = jc_for(m.ng);
   const int chunks = (m.nbe + jc - 1) / jc;
-  if (b.batch < 1 || b.batch > kMaxBatch) return fail(ctx, BEM_ERR_ARG, "batch size out of range");
   DynParams p{};
   p.nbe = m.nbe;
   p.nn = 3 * m.nbe;
@@ -644,6 +643,50 @@ int launch_dynamic_batch(bem_ctx* ctx, const DynBatch& b) {
   p.G = b.G;
   p.status = ctx->d_status;
   for (int i = 0; i < b.batch; ++i) p.kb[i] = make_consts(b.zge, b.zcs, b.zcp, b.freqs[i]);
+  return p;
+}
+
+// The per-frequency constants of a captured step: every k_dyn_diag and
+// k_dyn_offdiag node of `exec` (listed in `nodes`) gets the parameters
+// launch_dynamic_batch would pass for `b`; grids and shared memory stay.
+int dyn_graph_update(bem_ctx* ctx, cudaGraphExec_t exec, const std::vector<cudaGraphNode_t>& nodes,
+                     const DynBatch& b) {
+  DynParams p = dyn_params(ctx, b);
+  void* args[] = {&p};
+  for (cudaGraphNode_t n : nodes) {
+    cudaKernelNodeParams kp{};
+    BEM_CUDA(ctx, cudaGraphKernelNodeGetParams(n, &kp));
+    kp.kernelParams = args;
+    kp.extra = nullptr;
+    BEM_CUDA(ctx, cudaGraphExecKernelNodeSetParams(exec, n, &kp));
+  }
+  return BEM_OK;
+}
+
+// The dynamic-assembly kernel nodes of a captured graph.
+int dyn_graph_nodes(bem_ctx* ctx, cudaGraph_t g, std::vector<cudaGraphNode_t>& out) {
+  size_t n = 0;
+  BEM_CUDA(ctx, cudaGraphGetNodes(g, nullptr, &n));
+  std::vector<cudaGraphNode_t> all(n);
+  BEM_CUDA(ctx, cudaGraphGetNodes(g, all.data(), &n));
+  out.clear();
+  for (cudaGraphNode_t node : all) {
+    cudaGraphNodeType t;
+    BEM_CUDA(ctx, cudaGraphNodeGetType(node, &t));
+    if (t != cudaGraphNodeTypeKernel) continue;
+    cudaKernelNodeParams kp{};
+    BEM_CUDA(ctx, cudaGraphKernelNodeGetParams(node, &kp));
+    if (kp.func == (void*)k_dyn_diag || kp.func == (void*)k_dyn_offdiag) out.push_back(node);
+  }
+  return BEM_OK;
+}
+
+int launch_dynamic_batch(bem_ctx* ctx, const DynBatch& b) {
+  Mesh& m = ctx->mesh;
+  const int jc = jc_for(m.ng);
+  const int chunks = (m.nbe + jc - 1) / jc;
+  if (b.batch < 1 || b.batch > kMaxBatch) return fail(ctx, BEM_ERR_ARG, "batch size out of range");
+  DynParams p = dyn_params(ctx, b);
 
   // work: Stokes evaluations; bytes: the FP64 system (and its complex64 copy) written once
   ProfScope ps(ctx, 0, (double)m.nbe * (double)m.nbe * (double)m.ng * b.batch,

@@ -179,6 +179,14 @@ struct bem_ctx {
   size_t pinned_bytes = 0;
   bool use_tcgen05 = true;  // FP32 trailing update on tcgen05 (else TF32 mma.sync)
   bool use_trsv_coop = true;
+  bool use_graphs = true;     // bem_sweep replays a captured batch step
+  // the captured step of bem_sweep
+  cudaGraph_t sweep_graph = nullptr;
+  cudaGraphExec_t sweep_exec = nullptr;
+  std::vector<cudaGraphNode_t> sweep_dyn_nodes;
+  int sg_nn = 0, sg_bsz = 0, sg_mixed = 0, sg_iters = 0;
+  long long sg_launches = 0;
+  int sw_nn = 0, sw_bsz = 0, sw_mixed = 0, sw_iters = 0;  // shape of the last directly enqueued step
   bool panel_calu = false;    // FP32 LU panels: tournament pivoting per 8-column sub-panel
   bool lu_pairs = true;       // FP32 tensor-core LU: two 64-column panels per trailing update (K = 128)  // one cooperative launch per triangular solve (else per-block launches)
 };
@@ -212,6 +220,9 @@ void release_interior(bem_ctx* ctx);
 // parts 0), post-swap G into Gs (nn x nn real), column nn of A = Gs dfi.
 int launch_static_system(bem_ctx* ctx, const double c[4], double ge, const int* d_kode, const double* d_dfi,
                          double2* A, size_t lda, double* Gs);
+int dyn_graph_update(bem_ctx* ctx, cudaGraphExec_t exec, const std::vector<cudaGraphNode_t>& nodes,
+                     const DynBatch& b);
+int dyn_graph_nodes(bem_ctx* ctx, cudaGraph_t g, std::vector<cudaGraphNode_t>& out);
 int launch_dynamic_batch(bem_ctx* ctx, const DynBatch& b);
 int rhs_chunks(bem_ctx* ctx);
 
@@ -231,6 +242,7 @@ int lu_solve_vec(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int 
 int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], const double c[4],
           const double* freqs, int nfreq, int form, int batch, int iters, double* x_out, double* corr_out);
 void release_sweep(bem_ctx* ctx);
+void release_sweep_graph(bem_ctx* ctx);
 // Lockstep solve of problems of uneven size (bem_batch_solve).
 int batch_solve(bem_ctx* driver, int nprob, bem_ctx* const* probs, const double* freqs, const double* zge,
                 const double* zcs, const double* zcp, const double* c, int form, int iters, double* const* x_out,

@@ -141,6 +141,7 @@ int bem_ctx_create(int device, bem_ctx** out) {
   if (const char* env = getenv("BEM_TF32_MMA_SYNC")) ctx->use_tcgen05 = env[0] != '1';
   if (const char* env = getenv("BEM_TRSV_LEGACY")) ctx->use_trsv_coop = env[0] != '1';
   if (const char* env = getenv("BEM_LU_PAIRS")) ctx->lu_pairs = env[0] != '0';
+  if (const char* env = getenv("BEM_GRAPHS")) ctx->use_graphs = env[0] != '0';
   if (const char* env = getenv("BEM_PANEL_CALU")) ctx->panel_calu = env[0] == '1';
   *out = ctx;
   return BEM_OK;
@@ -524,6 +525,37 @@ int bem_batch_solve(bem_ctx* driver, int nprob, bem_ctx* const* probs, const dou
   }
   cudaSetDevice(driver->device);
   return batch_solve(driver, nprob, probs, freqs, zge, zcs, zcp, c, form, refine, x_out, corr_out);
+}
+
+static bool* option_slot(bem_ctx* ctx, const char* name) {
+  if (!strcmp(name, "tcgen05")) return &ctx->use_tcgen05;
+  if (!strcmp(name, "trsv_coop")) return &ctx->use_trsv_coop;
+  if (!strcmp(name, "lu_pairs")) return &ctx->lu_pairs;
+  if (!strcmp(name, "panel_calu")) return &ctx->panel_calu;
+  if (!strcmp(name, "graphs")) return &ctx->use_graphs;
+  return nullptr;
+}
+
+int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
+  if (!ctx || !name) return BEM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  bool* slot = option_slot(ctx, name);
+  if (!slot) return fail(ctx, BEM_ERR_ARG, std::string("unknown option ") + name);
+  if (*slot != (value != 0)) {
+    *slot = value != 0;
+    cudaSetDevice(ctx->device);
+    release_sweep_graph(ctx);  // a captured step may embody the old choice
+  }
+  return BEM_OK;
+}
+
+int bem_ctx_get_option(bem_ctx* ctx, const char* name, int* value) {
+  if (!ctx || !name || !value) return BEM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  bool* slot = option_slot(ctx, name);
+  if (!slot) return fail(ctx, BEM_ERR_ARG, std::string("unknown option ") + name);
+  *value = *slot ? 1 : 0;
+  return BEM_OK;
 }
 
 int bem_sweep_batch_limit(bem_ctx* ctx, int form, int* limit) {

@@ -211,7 +211,22 @@ int refine_steps(bem_ctx* ctx, SweepBuf& S, int bsz, int iters, int it0) {
 
 }  // namespace
 
+static void drop_sweep_graph(bem_ctx* ctx) {
+  if (ctx->sweep_exec) cudaGraphExecDestroy(ctx->sweep_exec);
+  if (ctx->sweep_graph) cudaGraphDestroy(ctx->sweep_graph);
+  ctx->sweep_exec = nullptr;
+  ctx->sweep_graph = nullptr;
+  ctx->sweep_dyn_nodes.clear();
+}
+
+void release_sweep_graph(bem_ctx* ctx) {
+  drop_sweep_graph(ctx);
+  ctx->sw_nn = 0;
+}
+
 void release_sweep(bem_ctx* ctx) {
+  drop_sweep_graph(ctx);
+  ctx->sw_nn = 0;
   free_sweep(ctx->sweep);
   free_sweep(ctx->bbuf);
 }
@@ -230,6 +245,22 @@ int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double z
   const int nn = S.nn;
   BEM_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->stream));
   std::vector<unsigned long long> hnorm;
+  // One lockstep step: assembly, LU (+ refinement) of `bsz` problems.
+  auto enqueue = [&](const DynBatch& db, int bsz) -> int {
+    int r = launch_dynamic_batch(ctx, db);
+    if (r) return r;
+    const dim3 vgrid((nn + 255) / 256, bsz);
+    if (mixed) {
+      r = lu_factor_solve_batch(ctx, S.A32, S.lda, S.a_stride, nn, bsz, true);
+      if (r) return r;
+      k_x_init<<<vgrid, 256, 0, ctx->stream>>>(S.A32, S.lda, S.a_stride, nn, S.x64, nn);
+      ctx->launches++;
+      BEM_CUDA(ctx, cudaMemsetAsync(S.norm, 0, (size_t)2 * bsz * kMaxRefine * sizeof(unsigned long long),
+                                    ctx->stream));
+      return refine_steps(ctx, S, bsz, iters, 0);
+    }
+    return lu_factor_solve_batch(ctx, S.A64, S.lda, S.a_stride, nn, bsz, false);
+  };
   for (int f0 = 0; f0 < nfreq; f0 += batch) {
     const int bsz = std::min(batch, nfreq - f0);
     DynBatch db{};
@@ -247,21 +278,57 @@ int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double z
     db.diag_h = S.diag_h;
     db.diag_g = S.diag_g;
     db.rhs_part = S.rhs_part;
-    rc = launch_dynamic_batch(ctx, db);
-    if (rc) return rc;
-    const dim3 vgrid((nn + 255) / 256, bsz);
-    if (mixed) {
-      rc = lu_factor_solve_batch(ctx, S.A32, S.lda, S.a_stride, nn, bsz, true);
+    // Steps after the first (which allocates and warms everything) run as one
+    // CUDA graph: captured once per (size, batch, form), then replayed with
+    // the new frequencies written into its assembly nodes.
+    const bool warm = ctx->sw_nn == nn && ctx->sw_bsz == bsz && ctx->sw_mixed == (int)mixed &&
+                      ctx->sw_iters == iters;  // a step of this shape already ran directly
+    const bool graph = ctx->use_graphs && !ctx->prof.on && warm && bsz == batch;
+    const bool have = ctx->sweep_exec && ctx->sg_nn == nn && ctx->sg_bsz == bsz &&
+                      ctx->sg_mixed == (int)mixed && ctx->sg_iters == iters;
+    if (graph && have) {
+      rc = dyn_graph_update(ctx, ctx->sweep_exec, ctx->sweep_dyn_nodes, db);
       if (rc) return rc;
-      k_x_init<<<vgrid, 256, 0, ctx->stream>>>(S.A32, S.lda, S.a_stride, nn, S.x64, nn);
-      ctx->launches++;
-      BEM_CUDA(ctx, cudaMemsetAsync(S.norm, 0, (size_t)2 * bsz * kMaxRefine * sizeof(unsigned long long),
-                                    ctx->stream));
-      rc = refine_steps(ctx, S, bsz, iters, 0);
-      if (rc) return rc;
+      BEM_CUDA(ctx, cudaGraphLaunch(ctx->sweep_exec, ctx->stream));
+      ctx->launches += ctx->sg_launches;
+    } else if (graph) {
+      drop_sweep_graph(ctx);
+      const long long l0 = ctx->launches;
+      BEM_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      const int erc = enqueue(db, bsz);
+      cudaGraph_t g = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+      cudaGraphExec_t ex = nullptr;
+      bool ok = erc == BEM_OK && ce == cudaSuccess && g &&
+                cudaGraphInstantiate(&ex, g, 0) == cudaSuccess &&
+                dyn_graph_nodes(ctx, g, ctx->sweep_dyn_nodes) == BEM_OK;
+      cudaGetLastError();
+      if (ok) {
+        ctx->sweep_graph = g;
+        ctx->sweep_exec = ex;
+        ctx->sg_nn = nn;
+        ctx->sg_bsz = bsz;
+        ctx->sg_mixed = (int)mixed;
+        ctx->sg_iters = iters;
+        ctx->sg_launches = ctx->launches - l0;
+        BEM_CUDA(ctx, cudaGraphLaunch(ex, ctx->stream));
+      } else {
+        // The stream cannot be captured here: run the step directly from now on.
+        if (ex) cudaGraphExecDestroy(ex);
+        if (g) cudaGraphDestroy(g);
+        ctx->sweep_dyn_nodes.clear();
+        ctx->use_graphs = false;
+        ctx->launches = l0;
+        rc = enqueue(db, bsz);
+        if (rc) return rc;
+      }
     } else {
-      rc = lu_factor_solve_batch(ctx, S.A64, S.lda, S.a_stride, nn, bsz, false);
+      rc = enqueue(db, bsz);
       if (rc) return rc;
+      ctx->sw_nn = nn;
+      ctx->sw_bsz = bsz;
+      ctx->sw_mixed = (int)mixed;
+      ctx->sw_iters = iters;
     }
     if (x_out) {
       double* dst = x_out + (size_t)2 * nn * f0;

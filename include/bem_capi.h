@@ -119,6 +119,14 @@ int bem_ctx_destroy(bem_ctx *ctx);
 /* Runs every kernel of ctx on `stream` (a cudaStream_t); NULL restores the
  * context's own stream. */
 int bem_ctx_set_stream(bem_ctx *ctx, void *stream);
+/* Algorithm switches of a context (1 on, 0 off), for comparison and for the
+ * autotuner: "tcgen05" (FP32 trailing update on tcgen05, else TF32
+ * mma.sync), "trsv_coop" (one cooperative launch per triangular solve),
+ * "lu_pairs" (two 64-column panels per FP32 trailing update, K = 128),
+ * "panel_calu" (FP32 panels with tournament pivoting), "graphs" (bem_sweep
+ * replays a captured step).  Defaults: on, on, on, off, on. */
+int bem_ctx_set_option(bem_ctx *ctx, const char *name, int value);
+int bem_ctx_get_option(bem_ctx *ctx, const char *name, int *value);
 const char *bem_status_string(int status);
 const char *bem_last_error(bem_ctx *ctx);
 /* Number of kernels this library launched on ctx since creation. */
