@@ -65,6 +65,9 @@ def parse_args():
     ap.add_argument("--no-serve", action="store_true", help="skip the served measurements")
     ap.add_argument("--small-count", type=int, default=512,
                     help="small meshes (24..600 elements) of the batching measurement (0 skips it)")
+    ap.add_argument("--autotune", metavar="CACHE", default=None,
+                    help="tune the headline sweep's switches and lockstep batch on this GPU, store the "
+                         "result in the JSON file CACHE and print it (no bench line)")
     ap.add_argument("--profile-case", action="store_true",
                     help="run only warmup+steps headline sweep batches and print a launch count "
                          "(a small, short command to run under ncu); no bench line")
@@ -245,6 +248,13 @@ def run_ours(args):
             ctx.prof(False)
         ctx.sync()
         return out
+
+    if args.autotune:
+        from bem_mececcs_b200 import autotune
+        best = autotune.tune_sweep(sol, mine, form="mixed", refine=R, steps=3, cache_path=args.autotune)
+        print(json.dumps({"autotune": "2160-element sweep", "n": nn, **best}), flush=True)
+        ctx.close()
+        return
 
     if args.profile_case:
         for i in range(args.warmup + args.steps):
