@@ -117,6 +117,20 @@ __device__ __forceinline__ zf dsm_ld(const zf* p, unsigned rank) {
   return v;
 }
 
+// Four consecutive complex values of a shared-memory row (16-byte aligned
+// for float: two 16-byte broadcast loads instead of four 8-byte ones).
+__device__ __forceinline__ void ld4(const zf* p, zf (&o)[4]) {
+  const float4 a = reinterpret_cast<const float4*>(p)[0], b = reinterpret_cast<const float4*>(p)[1];
+  o[0] = zf{a.x, a.y};
+  o[1] = zf{a.z, a.w};
+  o[2] = zf{b.x, b.y};
+  o[3] = zf{b.z, b.w};
+}
+__device__ __forceinline__ void ld4(const zd* p, zd (&o)[4]) {
+#pragma unroll
+  for (int u = 0; u < 4; ++u) o[u] = p[u];
+}
+
 // Shared state of one problem's panel step.
 struct PanelArgs {
   void* A;
@@ -265,7 +279,7 @@ __global__ void __launch_bounds__(NT, 1) k_panel_cluster(PanelArgs a) {
   C* s_a = reinterpret_cast<C*>(smem_raw);  // [NB][rp] panel rows, column-major
   C* s_pub = s_a + (size_t)NB * a.rp;       // [2][2][NB]: candidate row, row gj
   C* s_blk = s_pub + 4 * NB;                // [2][SW][NB]: a sub-panel's pivot rows
-  __shared__ C s_u[SW][NB];                 // U of the sub-panel's pivot rows
+  __shared__ __align__(16) C s_u[SW][NB];   // U of the sub-panel's pivot rows (16-byte rows for ld4)
   __shared__ R s_pval[2];
   __shared__ int s_prow[2];
   __shared__ R s_rv[NT / 32];
@@ -533,9 +547,12 @@ __global__ void __launch_bounds__(NT, 1) k_panel_cluster(PanelArgs a) {
           for (int u = 0; u < 4; ++u) x[u] = s_a[(c + u) * rp + lr];
 #pragma unroll
           for (int t = 0; t < SW; ++t)
-            if (t < sw)
+            if (t < sw) {
+              C uu[4];
+              ld4(&s_u[t][c], uu);
 #pragma unroll
-              for (int u = 0; u < 4; ++u) cfms(x[u], v[q][t], s_u[t][c + u]);
+              for (int u = 0; u < 4; ++u) cfms(x[u], v[q][t], uu[u]);
+            }
 #pragma unroll
           for (int u = 0; u < 4; ++u) s_a[(c + u) * rp + lr] = x[u];
         }
@@ -632,7 +649,7 @@ __global__ void __launch_bounds__(NT, 1) k_panel_calu(PanelArgs a) {
   C* s_a = reinterpret_cast<C*>(smem_raw);  // [NB][rp] panel rows, column-major
   C* s_x = s_a + (size_t)NB * a.rp;          // [kCaluCand][SW] gathered candidates, then
                                              // [kCaluMoves][NB] published rows
-  __shared__ C s_u[SW][NB];                  // pivot rows: L\U in the block, A then U right of it
+  __shared__ __align__(16) C s_u[SW][NB];    // pivot rows: L\U in the block, A then U right of it
   __shared__ C s_lu[SW][SW];                 // the sub-panel's pivot block, L\U
   __shared__ C s_lv[SW][SW];                 // this CTA's candidates (values at the sub-panel start)
   __shared__ int s_lid[SW];                  // their positions (-1: none)
@@ -941,9 +958,12 @@ __global__ void __launch_bounds__(NT, 1) k_panel_calu(PanelArgs a) {
         for (int u = 0; u < 4; ++u) x[u] = s_a[(c + u) * rp + lr];
 #pragma unroll
         for (int t = 0; t < SW; ++t)
-          if (t < sw)
+          if (t < sw) {
+            C uu[4];
+            ld4(&s_u[t][c], uu);
 #pragma unroll
-            for (int u = 0; u < 4; ++u) cfms(x[u], v[t], s_u[t][c + u]);
+            for (int u = 0; u < 4; ++u) cfms(x[u], v[t], uu[u]);
+          }
 #pragma unroll
         for (int u = 0; u < 4; ++u) s_a[(c + u) * rp + lr] = x[u];
       }
