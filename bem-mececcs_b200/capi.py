@@ -139,14 +139,18 @@ class Context:
         except Exception:
             pass
 
-    def set_option(self, name: str, value) -> None:
-        """bem_ctx_set_option: tcgen05, trsv_coop, lu_pairs, panel_calu, graphs."""
-        self.check(self.L.bem_ctx_set_option(self.h, name.encode(), int(bool(value))), "bem_ctx_set_option")
+    INT_OPTIONS = ("gemm_ctas", "trsv_ctas")
 
-    def get_option(self, name: str) -> bool:
+    def set_option(self, name: str, value) -> None:
+        """bem_ctx_set_option: switches tcgen05, trsv_coop, lu_pairs,
+        panel_calu, graphs; CTA budgets gemm_ctas, trsv_ctas (0 = device)."""
+        v = int(value) if name in self.INT_OPTIONS else int(bool(value))
+        self.check(self.L.bem_ctx_set_option(self.h, name.encode(), v), "bem_ctx_set_option")
+
+    def get_option(self, name: str):
         out = ctypes.c_int(0)
         self.check(self.L.bem_ctx_get_option(self.h, name.encode(), ctypes.byref(out)), "bem_ctx_get_option")
-        return bool(out.value)
+        return out.value if name in self.INT_OPTIONS else bool(out.value)
 
     @property
     def launches(self) -> int:

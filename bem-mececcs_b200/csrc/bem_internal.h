@@ -188,7 +188,11 @@ struct bem_ctx {
   long long sg_launches = 0;
   int sw_nn = 0, sw_bsz = 0, sw_mixed = 0, sw_iters = 0;  // shape of the last directly enqueued step
   bool panel_calu = false;    // FP32 LU panels: tournament pivoting per 8-column sub-panel
-  bool lu_pairs = true;       // FP32 tensor-core LU: two 64-column panels per trailing update (K = 128)  // one cooperative launch per triangular solve (else per-block launches)
+  bool panel_push = true;     // cluster panels exchange pivots by remote stores before the barrier
+  bool lu_pairs = true;       // FP32 tensor-core LU: two 64-column panels per trailing update (K = 128)
+  // SM shares for contexts that run concurrently on one GPU (0: the whole device)
+  int gemm_ctas = 0;          // CTAs of the persistent tensor-core trailing update
+  int trsv_ctas = 0;          // CTAs of one cooperative triangular solve (all problems together)
 };
 
 namespace bem {

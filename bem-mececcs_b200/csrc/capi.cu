@@ -143,6 +143,7 @@ int bem_ctx_create(int device, bem_ctx** out) {
   if (const char* env = getenv("BEM_LU_PAIRS")) ctx->lu_pairs = env[0] != '0';
   if (const char* env = getenv("BEM_GRAPHS")) ctx->use_graphs = env[0] != '0';
   if (const char* env = getenv("BEM_PANEL_CALU")) ctx->panel_calu = env[0] == '1';
+  if (const char* env = getenv("BEM_PANEL_PUSH")) ctx->panel_push = env[0] != '0';
   *out = ctx;
   return BEM_OK;
 }
@@ -532,7 +533,16 @@ static bool* option_slot(bem_ctx* ctx, const char* name) {
   if (!strcmp(name, "trsv_coop")) return &ctx->use_trsv_coop;
   if (!strcmp(name, "lu_pairs")) return &ctx->lu_pairs;
   if (!strcmp(name, "panel_calu")) return &ctx->panel_calu;
+  if (!strcmp(name, "panel_push")) return &ctx->panel_push;
   if (!strcmp(name, "graphs")) return &ctx->use_graphs;
+  return nullptr;
+}
+
+// Integer options: CTA budgets for a context that shares its GPU with
+// another one running at the same time (0 = the whole device).
+static int* int_option_slot(bem_ctx* ctx, const char* name) {
+  if (!strcmp(name, "gemm_ctas")) return &ctx->gemm_ctas;
+  if (!strcmp(name, "trsv_ctas")) return &ctx->trsv_ctas;
   return nullptr;
 }
 
@@ -540,9 +550,13 @@ int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
   if (!ctx || !name) return BEM_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
   bool* slot = option_slot(ctx, name);
-  if (!slot) return fail(ctx, BEM_ERR_ARG, std::string("unknown option ") + name);
-  if (*slot != (value != 0)) {
-    *slot = value != 0;
+  int* islot = slot ? nullptr : int_option_slot(ctx, name);
+  if (!slot && !islot) return fail(ctx, BEM_ERR_ARG, std::string("unknown option ") + name);
+  if (islot && value < 0) return fail(ctx, BEM_ERR_ARG, std::string("negative value for ") + name);
+  const bool changed = slot ? *slot != (value != 0) : *islot != value;
+  if (changed) {
+    if (slot) *slot = value != 0;
+    else *islot = value;
     cudaSetDevice(ctx->device);
     release_sweep_graph(ctx);  // a captured step may embody the old choice
   }
@@ -552,10 +566,15 @@ int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
 int bem_ctx_get_option(bem_ctx* ctx, const char* name, int* value) {
   if (!ctx || !name || !value) return BEM_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
-  bool* slot = option_slot(ctx, name);
-  if (!slot) return fail(ctx, BEM_ERR_ARG, std::string("unknown option ") + name);
-  *value = *slot ? 1 : 0;
-  return BEM_OK;
+  if (bool* slot = option_slot(ctx, name)) {
+    *value = *slot ? 1 : 0;
+    return BEM_OK;
+  }
+  if (int* islot = int_option_slot(ctx, name)) {
+    *value = *islot;
+    return BEM_OK;
+  }
+  return fail(ctx, BEM_ERR_ARG, std::string("unknown option ") + name);
 }
 
 int bem_sweep_batch_limit(bem_ctx* ctx, int form, int* limit) {

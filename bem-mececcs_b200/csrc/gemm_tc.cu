@@ -539,7 +539,8 @@ int tc_gemm(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int r0,
   t.urows = nn + 1;
   t.status = ctx->d_status;
   const int total = t.mtiles * t.ntiles * batch;
-  const int grid = std::min(total, ctx->num_sms);
+  const int ctas = ctx->gemm_ctas > 0 ? std::min(ctx->gemm_ctas, ctx->num_sms) : ctx->num_sms;
+  const int grid = std::min(total, ctas);
   k_gemm_tc<<<grid, 256, kTcSmem, ctx->stream>>>(maps[0], maps[1], maps[2], maps[3], t);
   ctx->launches++;
   BEM_CUDA(ctx, cudaGetLastError());

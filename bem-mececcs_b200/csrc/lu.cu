@@ -598,47 +598,525 @@ constexpr int kCaluSW = 8;
 constexpr int kCaluCand = 16 * kCaluSW;  // candidate rows of a 16-CTA cluster
 constexpr int kCaluMoves = 2 * kCaluSW;  // rows that move (or pivot) per sub-panel
 
-// CTA-wide argmax in the better() order; every thread returns with the
-// result.  One __syncthreads inside; s_rv/s_rr may be rewritten only after
-// the caller's next barrier.
-__device__ __forceinline__ void cta_argmax(float& v, int& r, float* s_rv, int* s_rr) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    const float ov = __shfl_xor_sync(0xffffffffu, v, off);
-    const int orr = __shfl_xor_sync(0xffffffffu, r, off);
-    if (better(ov, orr, v, r)) {
-      v = ov;
-      r = orr;
-    }
-  }
-  if (lane == 0) {
-    s_rv[warp] = v;
-    s_rr[warp] = r;
-  }
-  __syncthreads();
-  v = lane < nw ? s_rv[lane] : -1.f;
-  r = lane < nw ? s_rr[lane] : INT_MAX;
-#pragma unroll
-  for (int off = 8; off > 0; off >>= 1) {
-    const float ov = __shfl_xor_sync(0xffffffffu, v, off);
-    const int orr = __shfl_xor_sync(0xffffffffu, r, off);
-    if (better(ov, orr, v, r)) {
-      v = ov;
-      r = orr;
-    }
-  }
-  v = __shfl_sync(0xffffffffu, v, 0);
-  r = __shfl_sync(0xffffffffu, r, 0);
-}
-
-template <int N>
-__device__ __forceinline__ zf sel(const zf (&x)[N], int j) {
-  zf r = x[0];
+template <typename T, int N>
+__device__ __forceinline__ T sel(const T (&x)[N], int j) {
+  T r = x[0];
 #pragma unroll
   for (int c = 1; c < N; ++c)
     if (c == j) r = x[c];
   return r;
+}
+
+// ---------------------------------------------------------------------------
+// Panel factorisation in one thread-block cluster per problem, push form
+// (the default).  Same partition as k_panel_cluster: CTA `rank` owns panel
+// rows [k + rank*rp, ...) in shared memory, one row per thread, and the
+// panel advances in 8-column sub-panels held in registers.  Every transfer
+// of a column step is a remote STORE issued before the cluster barrier:
+// each CTA pushes its candidate (|re| + |im|, row, and the row's 8 sub-panel
+// values) into its mailbox slot in every CTA of the cluster, and the owner of
+// row gj pushes that row's 8 sub-panel values the same way.  After the
+// barrier every warp picks the winner from its own CTA's mailboxes, so a
+// column costs one CTA barrier, one cluster barrier and no remote load.  The
+// interchange acts at once on the sub-panel values in registers; the rest of
+// the two rows (columns left and right of the sub-panel) moves once per
+// sub-panel, as a list of row moves pulled over distributed shared memory
+// after the sub-panel's own cluster barrier.  Pivot choice (LAPACK partial
+// pivoting by |re| + |im|, first row on ties) and arithmetic are those of
+// k_panel_cluster, so the factors are the same.
+// ---------------------------------------------------------------------------
+constexpr int kPushMoves = 16;  // positions that a sub-panel's 8 interchanges can touch
+
+__device__ __forceinline__ void dsm_st4(const void* p, unsigned rank, uint4 v) {
+  asm volatile("st.shared::cluster.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(map_rank(p, rank)), "r"(v.x), "r"(v.y),
+               "r"(v.z), "r"(v.w)
+               : "memory");
+}
+
+// 8 sub-panel values of one row as 16-byte words (2 complex64 or 1 complex128
+// per word), and a candidate's (value, row) word.
+template <typename R>
+struct RowWords {
+  static constexpr int kN = sizeof(R) == 4 ? 4 : 8;
+};
+template <typename R>
+__device__ __forceinline__ uint4 row_word(const cpx<R> (&x)[8], int q) {
+  if constexpr (sizeof(R) == 4) {
+    return make_uint4(__float_as_uint(x[2 * q].re), __float_as_uint(x[2 * q].im), __float_as_uint(x[2 * q + 1].re),
+                      __float_as_uint(x[2 * q + 1].im));
+  } else {
+    const unsigned long long a = __double_as_longlong(x[q].re), b = __double_as_longlong(x[q].im);
+    return make_uint4((unsigned)a, (unsigned)(a >> 32), (unsigned)b, (unsigned)(b >> 32));
+  }
+}
+template <typename R>
+__device__ __forceinline__ void row_unword(const uint4* wd, cpx<R> (&x)[8]) {
+  if constexpr (sizeof(R) == 4) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint4 t = wd[q];
+      x[2 * q] = cpx<R>{__uint_as_float(t.x), __uint_as_float(t.y)};
+      x[2 * q + 1] = cpx<R>{__uint_as_float(t.z), __uint_as_float(t.w)};
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const uint4 t = wd[q];
+      x[q] = cpx<R>{__longlong_as_double((long long)(((unsigned long long)t.y << 32) | t.x)),
+                    __longlong_as_double((long long)(((unsigned long long)t.w << 32) | t.z))};
+    }
+  }
+}
+template <typename R>
+__device__ __forceinline__ uint4 cand_word(R v, int r) {
+  if constexpr (sizeof(R) == 4) {
+    return make_uint4(__float_as_uint(v), 0u, (unsigned)r, 0u);
+  } else {
+    const unsigned long long a = __double_as_longlong(v);
+    return make_uint4((unsigned)a, (unsigned)(a >> 32), (unsigned)r, 0u);
+  }
+}
+template <typename R>
+__device__ __forceinline__ R cand_val(uint4 t) {
+  if constexpr (sizeof(R) == 4)
+    return __uint_as_float(t.x);
+  else
+    return __longlong_as_double((long long)(((unsigned long long)t.y << 32) | t.x));
+}
+
+template <typename R, int NB, int NT>
+__global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
+  using E = typename Elt<R>::T;
+  using C = cpx<R>;
+  constexpr int SW = 8, NW = NT / 32, KW = RowWords<R>::kN;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s_a = reinterpret_cast<C*>(smem_raw);  // [NB][rp] panel rows, column-major
+  C* s_pub = s_a + (size_t)NB * a.rp;       // [kPushMoves][NB] published rows (sub-panel start values)
+  __shared__ uint4 s_box[2][16][1 + KW];    // [column parity][CTA]: candidate word, then its 8 values
+  __shared__ uint4 s_dbox[2][KW];           // [column parity]: row gj's 8 values
+  __shared__ __align__(16) C s_u[SW][NB];   // the sub-panel's pivot rows: L\U in the sub-panel, then U
+  __shared__ R s_rv[2][NW];                 // per-warp candidates: value (FP64) or key (FP32), row
+  __shared__ unsigned s_rk[2][NW];
+  __shared__ int s_rr[2][NW];
+  __shared__ int s_mdst[kPushMoves], s_msrc[kPushMoves], s_ment[kPushMoves], s_mcnt;
+  __shared__ int s_ppos[kPushMoves], s_pcnt;  // published rows (positions)
+  __shared__ int s_pent[SW];                  // published row holding each pivot row's right part
+  __shared__ int s_pdst[2 * NB], s_psrc[2 * NB];
+  __shared__ int s_pcount;
+  __shared__ int s_ipiv[NB];
+
+  const unsigned rank = cluster_rank();
+  const int prob = blockIdx.y, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  E* A = static_cast<E*>(a.A) + (size_t)prob * a.bstride;
+  int* ipiv = a.ipiv + (size_t)prob * a.ipiv_stride;
+  int* perm = a.perm + (size_t)prob * a.perm_stride;
+  const int rp = a.rp, w = a.w, k = a.k, cs = a.cs;
+  const int rbase = k + (int)rank * rp;
+  const int rcount = max(0, min(rp, a.nn - rbase));
+
+  load_slice_async<R>(A, a.lda, rbase, k, rcount, w, s_a, rp);
+  if (rank == 0 && prob == 0 && tid == 0 && a.pstart) {
+    a.pstart[a.pidx] = k;
+    a.pstart[a.pidx + 1] = k + w;
+  }
+  if (rank == 0 && tid < w) {
+    s_pdst[tid] = k + tid;
+    s_psrc[tid] = k + tid;
+  }
+  if (rank == 0 && tid == 0) s_pcount = w;
+  __syncthreads();
+
+  const int grow = tid < rcount ? rbase + tid : INT_MAX;  // my row (position)
+  const C czero{R(0), R(0)};
+  C v[SW];
+  int swp[SW];  // pivot position chosen for each column of the sub-panel
+
+  for (int s0 = 0; s0 < w; s0 += SW) {
+    const int sw = min(SW, w - s0), g0 = k + s0;
+    const bool last = s0 + sw >= w;
+#pragma unroll
+    for (int c = 0; c < SW; ++c) v[c] = (grow != INT_MAX && c < sw) ? s_a[(s0 + c) * rp + tid] : czero;
+
+    for (int jj = 0; jj < sw; ++jj) {
+      const int j = s0 + jj, gj = k + j, par = j & 1;
+      const int owner = j / rp;
+      // 1. This CTA's candidate (a NaN counts as 0, so every column has a
+      //    pivot: row gj itself is always eligible).
+      const bool elig = grow != INT_MAX && grow >= gj;
+      R bv = R(-1);
+      if (elig) {
+        bv = cabs1(sel(v, jj));
+        if (!(bv >= R(0))) bv = R(0);
+      }
+      int cr;
+      uint4 cword;  // the candidate's mailbox word
+      if constexpr (sizeof(R) == 4) {
+        // |re| + |im| >= 0, so its bits + 1 order as the value does (0: not
+        // eligible) and the lowest lane, warp or CTA with the largest key
+        // holds the first such row: one redux per level.
+        const unsigned key = elig ? __float_as_uint(bv) + 1u : 0u;
+        const unsigned mk = __reduce_max_sync(FULL, key);
+        const int wl = __ffs(__ballot_sync(FULL, key == mk)) - 1;
+        if (lane == 0) {
+          s_rk[par][warp] = mk;
+          s_rr[par][warp] = rbase + warp * 32 + wl;
+        }
+        __syncthreads();
+        const unsigned ck = lane < NW ? s_rk[par][lane] : 0u;
+        const unsigned mck = __reduce_max_sync(FULL, ck);
+        const int ww = __ffs(__ballot_sync(FULL, lane < NW && ck == mck)) - 1;
+        cr = mck ? s_rr[par][ww] : INT_MAX;
+        cword = make_uint4(mck, 0u, (unsigned)cr, 0u);
+      } else {
+        int br = elig ? grow : INT_MAX;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          const R ov = __shfl_xor_sync(FULL, bv, off);
+          const int orr = __shfl_xor_sync(FULL, br, off);
+          if (better(ov, orr, bv, br)) {
+            bv = ov;
+            br = orr;
+          }
+        }
+        if (lane == 0) {
+          s_rv[par][warp] = bv;
+          s_rr[par][warp] = br;
+        }
+        __syncthreads();
+        R cv = lane < NW ? s_rv[par][lane] : R(-1);
+        cr = lane < NW ? s_rr[par][lane] : INT_MAX;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          if (off >= NW) continue;
+          const R ov = __shfl_xor_sync(FULL, cv, off);
+          const int orr = __shfl_xor_sync(FULL, cr, off);
+          if (better(ov, orr, cv, cr)) {
+            cv = ov;
+            cr = orr;
+          }
+        }
+        cv = __shfl_sync(FULL, cv, 0);
+        cr = __shfl_sync(FULL, cr, 0);
+        cword = cand_word<R>(cv, cr);
+      }
+      // 2. Push the candidate into slot [par][rank] of every CTA, and row
+      //    gj's values from its owner.
+      if (cr != INT_MAX) {
+        const int t = cr - rbase;
+        if (warp == (t >> 5)) {
+          C x[SW];
+#pragma unroll
+          for (int c = 0; c < SW; ++c) {
+            x[c].re = __shfl_sync(FULL, v[c].re, t & 31);
+            x[c].im = __shfl_sync(FULL, v[c].im, t & 31);
+          }
+          if (lane < cs) {
+            const uint4* slot = &s_box[par][rank][0];
+            dsm_st4(slot, lane, cword);
+#pragma unroll
+            for (int q = 0; q < KW; ++q) dsm_st4(slot + 1 + q, lane, row_word<R>(x, q));
+          }
+        }
+      } else if (warp == 0 && lane < cs) {
+        dsm_st4(&s_box[par][rank][0], lane, cword);
+      }
+      if ((int)rank == owner) {
+        const int t = gj - rbase;
+        if (warp == (t >> 5)) {
+          C x[SW];
+#pragma unroll
+          for (int c = 0; c < SW; ++c) {
+            x[c].re = __shfl_sync(FULL, v[c].re, t & 31);
+            x[c].im = __shfl_sync(FULL, v[c].im, t & 31);
+          }
+          if (lane < cs)
+#pragma unroll
+            for (int q = 0; q < KW; ++q) dsm_st4(&s_dbox[par][q], lane, row_word<R>(x, q));
+        }
+      }
+      cluster_sync();
+      // 3. The winner, by every warp from its own CTA's mailboxes.
+      int prow, wsrc;
+      if constexpr (sizeof(R) == 4) {
+        const unsigned key = lane < cs ? s_box[par][lane][0].x : 0u;
+        const unsigned mk = __reduce_max_sync(FULL, key);
+        wsrc = __ffs(__ballot_sync(FULL, lane < cs && key == mk)) - 1;
+        prow = (int)s_box[par][wsrc][0].z;
+      } else {
+        R wv = R(-1);
+        int wr = INT_MAX, wk = lane;
+        if (lane < cs) {
+          const uint4 t0 = s_box[par][lane][0];
+          wv = cand_val<R>(t0);
+          wr = (int)t0.z;
+        }
+#pragma unroll
+        for (int off = 8; off > 0; off >>= 1) {
+          const R ov = __shfl_xor_sync(FULL, wv, off);
+          const int orr = __shfl_xor_sync(FULL, wr, off);
+          const int ok = __shfl_xor_sync(FULL, wk, off);
+          if (better(ov, orr, wv, wr)) {
+            wv = ov;
+            wr = orr;
+            wk = ok;
+          }
+        }
+        prow = __shfl_sync(FULL, wr, 0);
+        wsrc = __shfl_sync(FULL, wk, 0);
+      }
+      if (prow == INT_MAX || prow < gj) prow = gj;  // unreachable: row gj always takes part
+      C piv[SW];
+      row_unword<R>(&s_box[par][wsrc][1], piv);
+      // 4. The interchange, on the sub-panel values in registers.
+      if (prow != gj) {
+        if (grow == prow) {
+          row_unword<R>(&s_dbox[par][0], v);
+        } else if (grow == gj) {
+#pragma unroll
+          for (int c = 0; c < SW; ++c) v[c] = piv[c];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < SW; ++c)
+        if (c == jj) swp[c] = prow;
+      if (tid < sw) s_u[jj][s0 + tid] = sel(piv, tid);  // the pivot row's L\U in the sub-panel
+      // 5. Multipliers and the rank-1 update of the sub-panel, in registers.
+      const C pj = sel(piv, jj);
+      const bool zero = pj.re == R(0) && pj.im == R(0);
+      if (zero && rank == 0 && tid == 0) atomicCAS(&a.status[ST_SINGULAR], 0, gj + 1);
+      const C rpv = zero ? czero : crcp(pj);
+      if (grow != INT_MAX && grow > gj) {
+        const C l = sel(v, jj) * rpv;
+#pragma unroll
+        for (int c = 0; c < SW; ++c) {
+          if (c == jj) v[c] = l;
+          if (c > jj) cfms(v[c], l, piv[c]);
+        }
+      }
+    }
+    // End of the sub-panel: registers back to shared memory.
+    if (grow != INT_MAX)
+#pragma unroll
+      for (int c = 0; c < SW; ++c)
+        if (c < sw) s_a[(s0 + c) * rp + tid] = v[c];
+    // The sub-panel's interchanges as whole-row moves (position dst <- the
+    // row at position src when the sub-panel started), by warp 0 of every
+    // CTA: lane i holds touched position i and the start position of the row
+    // now there.  Rank 0 also replays them on the panel's gather list.
+    if (warp == 1 && rank == 0) {  // the gather list, beside warp 0's moves
+      for (int jj = 0; jj < sw; ++jj) {
+        const int j = s0 + jj, p = sel(swp, jj);
+        {
+          int ip = -1;
+          if (p < k + w) {
+            ip = p - k;
+          } else {
+            const int pc = s_pcount;
+            for (int base = w; base < pc && ip < 0; base += 32) {
+              const int e = base + lane;
+              const unsigned m = __ballot_sync(FULL, e < pc && s_pdst[e] == p);
+              if (m) ip = base + __ffs(m) - 1;
+            }
+            if (ip < 0) {
+              ip = pc;
+              if (lane == 0) {
+                s_pdst[ip] = p;
+                s_psrc[ip] = p;
+                s_pcount = pc + 1;
+              }
+            }
+            __syncwarp();
+          }
+          if (lane == 0) {
+            s_ipiv[j] = p + 1;
+            const int t = s_psrc[j];
+            s_psrc[j] = s_psrc[ip];
+            s_psrc[ip] = t;
+          }
+          __syncwarp();
+        }
+      }
+    }
+    if (warp == 0) {
+      int pos = -1, lab = -1, n = 0;
+      for (int jj = 0; jj < sw; ++jj) {
+        const int tp = g0 + jj, p = sel(swp, jj);
+        if (p != tp) {
+          const unsigned mt = __ballot_sync(FULL, lane < n && pos == tp);
+          int it = mt ? __ffs(mt) - 1 : -1;
+          if (it < 0) {
+            it = n++;
+            if (lane == it) {
+              pos = tp;
+              lab = tp;
+            }
+          }
+          const unsigned mp = __ballot_sync(FULL, lane < n && pos == p);
+          int ipp = mp ? __ffs(mp) - 1 : -1;
+          if (ipp < 0) {
+            ipp = n++;
+            if (lane == ipp) {
+              pos = p;
+              lab = p;
+            }
+          }
+          const int lt = __shfl_sync(FULL, lab, it), lp = __shfl_sync(FULL, lab, ipp);
+          if (lane == it) lab = lp;
+          if (lane == ipp) lab = lt;
+        }
+      }
+      // moves: touched positions whose row changed
+      const bool mv = lane < n && lab != pos;
+      const unsigned mm = __ballot_sync(FULL, mv);
+      const int m = __popc(mm);
+      int mslot = -1;
+      if (mv) mslot = __popc(mm & ((1u << lane) - 1));
+      // published rows: the move sources, then the pivot positions that keep
+      // their row (their part right of the sub-panel is read from there)
+      int pmove = -1;  // lane < sw: the move that fills pivot position g0 + lane
+      {
+        const unsigned md = __ballot_sync(FULL, mv && pos >= g0 && pos < g0 + sw);
+        for (unsigned bits = md; bits; bits &= bits - 1) {
+          const int l = __ffs(bits) - 1;
+          const int d = __shfl_sync(FULL, pos, l), sl = __shfl_sync(FULL, mslot, l);
+          if (lane == d - g0) pmove = sl;
+        }
+      }
+      // move sources occupy entries 0..m-1 in move order
+      const unsigned keep_piv = __ballot_sync(FULL, lane < sw && pmove < 0);
+      if (mv) {
+        s_mdst[mslot] = pos;
+        s_msrc[mslot] = lab;
+        s_ment[mslot] = mslot;
+        s_ppos[mslot] = lab;
+      }
+      if (lane < sw) {
+        if (pmove >= 0) {
+          s_pent[lane] = pmove;
+        } else {
+          const int e = m + __popc(keep_piv & ((1u << lane) - 1));
+          s_ppos[e] = g0 + lane;
+          s_pent[lane] = e;
+        }
+      }
+      if (lane == 0) {
+        s_mcnt = m;
+        s_pcnt = m + __popc(keep_piv);
+      }
+    }
+    __syncthreads();
+    // Publish: the part outside the sub-panel of every published row, as it
+    // was when the sub-panel started (those columns have not changed since).
+    const int npub = s_pcnt, nmov = s_mcnt;
+    constexpr int PU = (kPushMoves * NB + NT - 1) / NT;
+    {
+      C t[PU];
+      int off[PU];
+#pragma unroll
+      for (int u = 0; u < PU; ++u) {
+        off[u] = -1;
+        const int idx = tid + u * NT;
+        if (idx < npub * w) {
+          const int e = idx / w, c = idx % w, y = s_ppos[e];
+          if (y >= rbase && y < rbase + rcount && (c < s0 || c >= s0 + sw)) {
+            t[u] = s_a[(size_t)c * rp + (y - rbase)];
+            off[u] = e * NB + c;
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < PU; ++u)
+        if (off[u] >= 0) s_pub[off[u]] = t[u];
+    }
+    cluster_sync();
+    // Pull: rows of mine that receive another row, and (unless this is the
+    // last sub-panel) the pivot rows' part right of the sub-panel; all remote
+    // loads before the stores.
+    {
+      constexpr int UU = (SW * NB + NT - 1) / NT;
+      C t[PU], tu[UU];
+      int off[PU], offu[UU];
+#pragma unroll
+      for (int u = 0; u < PU; ++u) {
+        off[u] = -1;
+        const int idx = tid + u * NT;
+        if (idx < nmov * w) {
+          const int mi = idx / w, c = idx % w, x = s_mdst[mi];
+          if (x >= rbase && x < rbase + rcount && (c < s0 || c >= s0 + sw)) {
+            const int ys = s_msrc[mi];
+            t[u] = dsm_ld(&s_pub[(size_t)s_ment[mi] * NB + c], (unsigned)((ys - k) / rp));
+            off[u] = c * rp + (x - rbase);
+          }
+        }
+      }
+      const int wr = last ? 0 : w - s0 - sw;
+#pragma unroll
+      for (int u = 0; u < UU; ++u) {
+        offu[u] = -1;
+        const int idx = tid + u * NT;
+        if (idx < sw * wr) {
+          const int i = idx / wr, c = s0 + sw + idx % wr;
+          const int e = s_pent[i], ys = s_ppos[e];
+          tu[u] = dsm_ld(&s_pub[(size_t)e * NB + c], (unsigned)((ys - k) / rp));
+          offu[u] = i * NB + c;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < PU; ++u)
+        if (off[u] >= 0) s_a[off[u]] = t[u];
+#pragma unroll
+      for (int u = 0; u < UU; ++u)
+        if (offu[u] >= 0) (&s_u[0][0])[offu[u]] = tu[u];
+    }
+    __syncthreads();
+    if (last) break;
+    // U of the pivot rows right of the sub-panel:
+    // U(i,c) = A(i,c) - sum_{t<i} L(i,t) U(t,c), L = the sub-panel's unit lower.
+    for (int c = s0 + sw + tid; c < w; c += NT)
+      for (int i = 1; i < sw; ++i) {
+        C x = s_u[i][c];
+        for (int t = 0; t < i; ++t) cfms(x, s_u[i][s0 + t], s_u[t][c]);
+        s_u[i][c] = x;
+      }
+    __syncthreads();
+    // Rank-sw update of my row right of the sub-panel; the pivot rows take
+    // their U values.
+    if (grow != INT_MAX && grow >= g0 + sw) {
+      for (int c = s0 + sw; c < w; c += 4) {  // the remaining width is a multiple of 8
+        C x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = s_a[(c + u) * rp + tid];
+#pragma unroll
+        for (int t = 0; t < SW; ++t)
+          if (t < sw) {
+            C uu[4];
+            ld4(&s_u[t][c], uu);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) cfms(x[u], v[t], uu[u]);
+          }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) s_a[(c + u) * rp + tid] = x[u];
+      }
+    } else if (grow != INT_MAX && grow >= g0) {
+      const int i = grow - g0;
+      for (int c = s0 + sw; c < w; ++c) s_a[c * rp + tid] = s_u[i][c];
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < w * rcount; idx += blockDim.x) {
+    const int c = idx / rcount, r = idx % rcount;
+    stc<R>(&A[(size_t)(k + c) * a.lda + rbase + r], s_a[c * rp + r]);
+  }
+  if (rank == 0) {
+    if (tid < w) ipiv[k + tid] = s_ipiv[tid];
+    if (tid == 0) perm[0] = s_pcount;
+    for (int e = tid; e < s_pcount; e += blockDim.x) {
+      perm[1 + 2 * e] = s_pdst[e];
+      perm[2 + 2 * e] = s_psrc[e];
+    }
+  }
+  cluster_sync();  // no CTA leaves while others may still read its shared memory
 }
 
 template <int NB, int NT>
@@ -655,9 +1133,10 @@ __global__ void __launch_bounds__(NT, 1) k_panel_calu(PanelArgs a) {
   __shared__ int s_lid[SW];                  // their positions (-1: none)
   __shared__ int s_cid[kCaluCand];
   __shared__ int s_pid[SW];                  // pivot rows (positions at the sub-panel start), in order
-  __shared__ C s_tw[SW];
-  __shared__ float s_rv[NT / 32];
-  __shared__ int s_rr[NT / 32];
+  __shared__ float s_rv[2][NT / 32];         // per-warp winners, double-buffered by step parity
+  __shared__ int s_rr[2][NT / 32];
+  __shared__ C s_wt[2][NT / 32][SW];         // ... and their current rows
+  __shared__ C s_rcp[SW];                    // reciprocals of the pivot block's diagonal
   __shared__ int s_mdst[kCaluMoves], s_msrc[kCaluMoves], s_mcnt;
   __shared__ int s_ppos[kCaluMoves], s_pcnt;
   __shared__ int s_pdst[2 * NB], s_psrc[2 * NB];
@@ -697,13 +1176,16 @@ __global__ void __launch_bounds__(NT, 1) k_panel_calu(PanelArgs a) {
     for (int c = 0; c < SW; ++c) v[c] = (grow != INT_MAX && c < sw) ? s_a[(s0 + c) * rp + lr] : zero();
     const bool elig = grow != INT_MAX && grow >= g0;
 
-    // 1. This CTA's candidates: partial pivoting on a copy of its rows.
+    // 1. This CTA's candidates: partial pivoting on a copy of its rows, one
+    //    barrier per column (each warp's winner stages its row before it).
     {
+      constexpr int NW = NT / 32;
       C t[SW];
 #pragma unroll
       for (int c = 0; c < SW; ++c) t[c] = v[c];
       bool chosen = false;
       for (int jj = 0; jj < sw; ++jj) {
+        const int buf = jj & 1;
         float bv = -1.f;
         int br = INT_MAX;
         if (elig && !chosen) {
@@ -711,164 +1193,234 @@ __global__ void __launch_bounds__(NT, 1) k_panel_calu(PanelArgs a) {
           if (!(bv >= 0.f)) bv = 0.f;  // a NaN still takes part, so a candidate always exists
           br = grow;
         }
-        cta_argmax(bv, br, s_rv, s_rr);
-        if (br != INT_MAX && grow == br) {
+        int bl = lane;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          const float ov = __shfl_xor_sync(0xffffffffu, bv, off);
+          const int orr = __shfl_xor_sync(0xffffffffu, br, off);
+          const int ol = __shfl_xor_sync(0xffffffffu, bl, off);
+          if (better(ov, orr, bv, br)) {
+            bv = ov;
+            br = orr;
+            bl = ol;
+          }
+        }
+        if (br != INT_MAX && lane == bl) {
+#pragma unroll
+          for (int c = 0; c < SW; ++c) s_wt[buf][warp][c] = t[c];
+        }
+        if (lane == 0) {
+          s_rv[buf][warp] = bv;
+          s_rr[buf][warp] = br;
+        }
+        __syncthreads();
+        float cv = lane < NW ? s_rv[buf][lane] : -1.f;
+        int cr = lane < NW ? s_rr[buf][lane] : INT_MAX;
+        int cw = lane;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          if (off >= NW) continue;
+          const float ov = __shfl_xor_sync(0xffffffffu, cv, off);
+          const int orr = __shfl_xor_sync(0xffffffffu, cr, off);
+          const int ow = __shfl_xor_sync(0xffffffffu, cw, off);
+          if (better(ov, orr, cv, cr)) {
+            cv = ov;
+            cr = orr;
+            cw = ow;
+          }
+        }
+        cr = __shfl_sync(0xffffffffu, cr, 0);
+        cw = __shfl_sync(0xffffffffu, cw, 0);
+        if (cr == INT_MAX) {
+          if (tid == 0) s_lid[jj] = -1;
+          continue;
+        }
+        if (grow == cr) {
           chosen = true;
 #pragma unroll
-          for (int c = 0; c < SW; ++c) {
-            s_tw[c] = t[c];
-            s_lv[jj][c] = v[c];
-          }
-          s_lid[jj] = br;
-        }
-        if (tid == 0 && br == INT_MAX) s_lid[jj] = -1;
-        __syncthreads();
-        if (br != INT_MAX && elig && !chosen) {
-          const C p = s_tw[jj];
+          for (int c = 0; c < SW; ++c) s_lv[jj][c] = v[c];
+          s_lid[jj] = cr;
+        } else if (elig && !chosen) {
+          const C* tw = s_wt[buf][cw];
+          const C p = tw[jj];
           const C l = (p.re == 0.f && p.im == 0.f) ? zero() : sel(t, jj) * crcp(p);
 #pragma unroll
           for (int c = 0; c < SW; ++c)
-            if (c > jj) cfms(t[c], l, s_tw[c]);
+            if (c > jj) cfms(t[c], l, tw[c]);
         }
       }
     }
     cluster_sync();  // A: every CTA's candidates are published
 
-    // 2. The cluster's candidates, the same partial pivoting in every CTA.
+    // 2. The cluster's candidates, the same partial pivoting in every CTA:
+    //    4 warps, one candidate per thread, one named barrier per column.
     C* s_cv = s_x;
-    for (int i = tid; i < cs * SW; i += NT) s_cid[i] = i / SW < cs ? dsm_ld(&s_lid[i % SW], (unsigned)(i / SW)) : -1;
+    for (int i = tid; i < cs * SW; i += NT) s_cid[i] = dsm_ld(&s_lid[i % SW], (unsigned)(i / SW));
     for (int i = tid; i < cs * SW * SW; i += NT) {
       const int cand = i / SW, c = i % SW;
       s_cv[i] = dsm_ld(&s_lv[cand % SW][c], (unsigned)(cand / SW));
     }
     __syncthreads();
-    if (warp == 0) {
-      C T[4][SW];
-      int id[4];
-      bool ch[4];
+    if (tid < kCaluCand) {
+      const int cand = tid;
+      const int id = (cand < cs * SW && (cand % SW) < sw) ? s_cid[cand] : -1;
+      bool ch = false;
+      C T[SW];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int cand = lane + 32 * q;
-        id[q] = (cand < cs * SW && (cand % SW) < sw) ? s_cid[cand] : -1;
-        ch[q] = false;
-#pragma unroll
-        for (int c = 0; c < SW; ++c) T[q][c] = id[q] >= 0 ? s_cv[cand * SW + c] : zero();
-      }
+      for (int c = 0; c < SW; ++c) T[c] = id >= 0 ? s_cv[cand * SW + c] : zero();
       for (int jj = 0; jj < sw; ++jj) {
+        const int buf = jj & 1;
         float bv = -1.f;
-        int bid = INT_MAX, bq = 0, bl = lane;
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-          if (id[q] >= 0 && !ch[q]) {
-            float val = cabs1(sel(T[q], jj));
-            if (!(val >= 0.f)) val = 0.f;
-            if (better(val, id[q], bv, bid)) {
-              bv = val;
-              bid = id[q];
-              bq = q;
-            }
-          }
+        int bid = INT_MAX;
+        if (id >= 0 && !ch) {
+          bv = cabs1(sel(T, jj));
+          if (!(bv >= 0.f)) bv = 0.f;
+          bid = id;
+        }
+        int bl = lane;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
           const float ov = __shfl_xor_sync(0xffffffffu, bv, off);
           const int oid = __shfl_xor_sync(0xffffffffu, bid, off);
-          const int oq = __shfl_xor_sync(0xffffffffu, bq, off);
           const int ol = __shfl_xor_sync(0xffffffffu, bl, off);
           if (better(ov, oid, bv, bid)) {
             bv = ov;
             bid = oid;
-            bq = oq;
             bl = ol;
           }
         }
-        C tw[SW];
+        if (bid != INT_MAX && lane == bl) {
 #pragma unroll
-        for (int c = 0; c < SW; ++c) {
-          C mine = T[0][c];
-#pragma unroll
-          for (int q = 1; q < 4; ++q)
-            if (q == bq) mine = T[q][c];
-          tw[c].re = __shfl_sync(0xffffffffu, mine.re, bl);
-          tw[c].im = __shfl_sync(0xffffffffu, mine.im, bl);
-        }
-        if (lane == bl) {
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-            if (q == bq) ch[q] = true;
+          for (int c = 0; c < SW; ++c) s_wt[buf][warp][c] = T[c];
         }
         if (lane == 0) {
-          s_pid[jj] = bid;
+          s_rv[buf][warp] = bv;
+          s_rr[buf][warp] = bid;
+        }
+        asm volatile("bar.sync 1, %0;" ::"n"(kCaluCand) : "memory");
+        float fv = s_rv[buf][0];
+        int fid = s_rr[buf][0], fw = 0;
+#pragma unroll
+        for (int q = 1; q < kCaluCand / 32; ++q)
+          if (better(s_rv[buf][q], s_rr[buf][q], fv, fid)) {
+            fv = s_rv[buf][q];
+            fid = s_rr[buf][q];
+            fw = q;
+          }
+        const C* tw = s_wt[buf][fw];
+        if (id == fid) ch = true;
+        if (tid == 0) {
+          s_pid[jj] = fid;
 #pragma unroll
           for (int c = 0; c < SW; ++c) s_lu[jj][c] = tw[c];
         }
-        const C piv = sel(tw, jj);
+        const C piv = tw[jj];
         const bool zp = piv.re == 0.f && piv.im == 0.f;
-        if (zp && rank == 0 && lane == 0) atomicCAS(&a.status[ST_SINGULAR], 0, g0 + jj + 1);
-        const C rpv = zp ? zero() : crcp(piv);
+        if (zp && rank == 0 && tid == 0) atomicCAS(&a.status[ST_SINGULAR], 0, g0 + jj + 1);
+        if (id >= 0 && !ch) {
+          const C l = zp ? zero() : sel(T, jj) * crcp(piv);
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-          if (id[q] >= 0 && !ch[q]) {
-            const C l = sel(T[q], jj) * rpv;
-#pragma unroll
-            for (int c = 0; c < SW; ++c) {
-              if (c == jj) T[q][c] = l;
-              if (c > jj) cfms(T[q][c], l, tw[c]);
-            }
+          for (int c = 0; c < SW; ++c) {
+            if (c == jj) T[c] = l;
+            if (c > jj) cfms(T[c], l, tw[c]);
           }
+        }
       }
     }
     __syncthreads();
 
     // 3. The interchanges in order (position of the pivot row swapped with
-    //    position g0 + j), as position moves dst <- src (sub-panel start values).
-    if (tid == 0) {
-      int cur[SW], pos[kCaluMoves], lab[kCaluMoves], n = 0;
-      for (int j = 0; j < sw; ++j) cur[j] = s_pid[j];
+    //    position g0 + j), as position moves dst <- src (sub-panel start
+    //    values), by warp 0: lane i holds touched position i and the start
+    //    position of the row now there; the panel's gather list is updated
+    //    the same way (rank 0).
+    if (warp == 0) {
+      int cur = lane < sw ? s_pid[lane] : -1;  // current position of pivot row `lane`
+      int pos = -1, lab = -1, n = 0;
       for (int j = 0; j < sw; ++j) {
-        const int tp = g0 + j, p = cur[j];
+        const int tp = g0 + j, p = __shfl_sync(0xffffffffu, cur, j);
         if (rank == 0) {
-          s_ipiv[s0 + j] = p + 1;
-          perm_swap(s_pdst, s_psrc, s_pcount, k, w, s0 + j, p);
+          // the gather list: psrc[j'] <-> psrc[entry of position p]
+          int ip = -1;
+          if (p < k + w) {
+            ip = p - k;
+          } else {
+            const int pc = s_pcount;
+            for (int base = w; base < pc && ip < 0; base += 32) {
+              const int e = base + lane;
+              const unsigned m = __ballot_sync(0xffffffffu, e < pc && s_pdst[e] == p);
+              if (m) ip = base + __ffs(m) - 1;
+            }
+            if (ip < 0) {
+              ip = pc;
+              if (lane == 0) {
+                s_pdst[ip] = p;
+                s_psrc[ip] = p;
+                s_pcount = pc + 1;
+              }
+            }
+            __syncwarp();
+          }
+          if (lane == 0) {
+            s_ipiv[s0 + j] = p + 1;
+            const int tmp = s_psrc[s0 + j];
+            s_psrc[s0 + j] = s_psrc[ip];
+            s_psrc[ip] = tmp;
+          }
+          __syncwarp();
         }
         if (p != tp) {
-          int it = -1, ip = -1;
-          for (int i = 0; i < n; ++i) {
-            if (pos[i] == tp) it = i;
-            if (pos[i] == p) ip = i;
-          }
+          unsigned mt = __ballot_sync(0xffffffffu, lane < n && pos == tp);
+          int it = mt ? __ffs(mt) - 1 : -1;
           if (it < 0) {
             it = n++;
-            pos[it] = tp;
-            lab[it] = tp;
+            if (lane == it) {
+              pos = tp;
+              lab = tp;
+            }
           }
-          if (ip < 0) {
-            ip = n++;
-            pos[ip] = p;
-            lab[ip] = p;
+          unsigned mp = __ballot_sync(0xffffffffu, lane < n && pos == p);
+          int ipp = mp ? __ffs(mp) - 1 : -1;
+          if (ipp < 0) {
+            ipp = n++;
+            if (lane == ipp) {
+              pos = p;
+              lab = p;
+            }
           }
-          const int tl = lab[it];
-          lab[it] = lab[ip];
-          lab[ip] = tl;
-          for (int i = j + 1; i < sw; ++i)
-            if (cur[i] == tp) cur[i] = p;
+          const int lt = __shfl_sync(0xffffffffu, lab, it), lp = __shfl_sync(0xffffffffu, lab, ipp);
+          if (lane == it) lab = lp;
+          if (lane == ipp) lab = lt;
+          if (lane > j && lane < sw && cur == tp) cur = p;
         }
       }
-      int m = 0;
-      for (int i = 0; i < n; ++i)
-        if (lab[i] != pos[i]) {
-          s_mdst[m] = pos[i];
-          s_msrc[m] = lab[i];
-          ++m;
-        }
-      s_mcnt = m;
-      int np = 0;
-      for (int j = 0; j < sw + m; ++j) {
-        const int y = j < sw ? s_pid[j] : s_msrc[j - sw];
-        bool seen = false;
-        for (int i = 0; i < np; ++i) seen |= s_ppos[i] == y;
-        if (!seen) s_ppos[np++] = y;
+      // moves: touched positions whose row changed
+      const bool mv = lane < n && lab != pos;
+      const unsigned mm = __ballot_sync(0xffffffffu, mv);
+      if (mv) {
+        const int slot = __popc(mm & ((1u << lane) - 1));
+        s_mdst[slot] = pos;
+        s_msrc[slot] = lab;
       }
-      s_pcnt = np;
+      const int m = __popc(mm);
+      // rows to publish: the pivot rows, then move sources not among them
+      __syncwarp();
+      const int cand_y = lane < sw ? s_pid[lane] : (lane < sw + m ? s_msrc[lane - sw] : -1);
+      bool keep = cand_y >= 0;
+      for (int i = 0; i < sw + m; ++i) {
+        const int other = __shfl_sync(0xffffffffu, cand_y, i);
+        if (i < lane && other == cand_y) keep = false;
+      }
+      const unsigned km = __ballot_sync(0xffffffffu, keep);
+      if (keep) s_ppos[__popc(km & ((1u << lane) - 1))] = cand_y;
+      if (lane == 0) {
+        s_mcnt = m;
+        s_pcnt = __popc(km);
+      }
+      if (lane < sw) {
+        const C d = s_lu[lane][lane];
+        s_rcp[lane] = (d.re == 0.f && d.im == 0.f) ? zero() : crcp(d);
+      }
     }
     __syncthreads();
 
@@ -930,8 +1482,7 @@ __global__ void __launch_bounds__(NT, 1) k_panel_calu(PanelArgs a) {
           C x = v[jj];
 #pragma unroll
           for (int i = 0; i < jj; ++i) cfms(x, v[i], s_lu[i][jj]);
-          const C d = s_lu[jj][jj];
-          v[jj] = (d.re == 0.f && d.im == 0.f) ? zero() : x * crcp(d);
+          v[jj] = x * s_rcp[jj];
         }
       }
     }
@@ -1795,10 +2346,16 @@ int lu_ensure_workspace(bem_ctx* ctx, int nn, int batch) {
 
 constexpr size_t kPanelSmemBudget = 220 * 1024;
 
+template <typename R, int NB>
+static size_t push_panel_smem(int rp) {
+  return ((size_t)NB * rp + (size_t)kPushMoves * NB) * sizeof(cpx<R>);
+}
+
 template <typename R, int NB, int NT>
 static int launch_cluster_panel(bem_ctx* ctx, const PanelArgs& pa, int batch) {
-  const size_t smem = ((size_t)NB * pa.rp + 4 * NB + 2 * 8 * NB) * sizeof(cpx<R>);
-  auto kern = k_panel_cluster<R, NB, NT>;
+  const bool push = ctx->panel_push;
+  const size_t smem = push ? push_panel_smem<R, NB>(pa.rp) : ((size_t)NB * pa.rp + 4 * NB + 2 * 8 * NB) * sizeof(cpx<R>);
+  auto kern = push ? k_panel_push<R, NB, NT> : k_panel_cluster<R, NB, NT>;
   BEM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   BEM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   cudaLaunchConfig_t cfg = {};
@@ -1820,13 +2377,16 @@ static int launch_cluster_panel(bem_ctx* ctx, const PanelArgs& pa, int batch) {
 // Does a panel of width NB with rp rows per CTA fit one CTA's shared memory?
 template <typename R, int NB, int NT>
 static bool cluster_panel_fits(int rp) {
-  cudaFuncAttributes fa{};
+  // both forms (pull and push) must fit, so that either can run any panel
+  cudaFuncAttributes fa{}, fp{};
   if (cudaFuncGetAttributes(&fa, k_panel_cluster<R, NB, NT>) != cudaSuccess) return false;
+  if (cudaFuncGetAttributes(&fp, k_panel_push<R, NB, NT>) != cudaSuccess) return false;
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   const size_t dyn = ((size_t)NB * rp + 4 * NB + 2 * 8 * NB) * sizeof(cpx<R>);
-  return dyn + fa.sharedSizeBytes + 1024 <= (size_t)optin;
+  return dyn + fa.sharedSizeBytes + 1024 <= (size_t)optin &&
+         push_panel_smem<R, NB>(rp) + fp.sharedSizeBytes + 1024 <= (size_t)optin;
 }
 
 template <typename R>
@@ -2009,7 +2569,9 @@ static int trsv_coop(bem_ctx* ctx, const void* A, size_t lda, size_t bstride, in
   BEM_CUDA(ctx, cudaFuncSetAttribute(k_trsv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
   BEM_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trsv<R>, 256, smem));
-  int group = std::min(64, occ * ctx->num_sms / batch);
+  int slots = occ * ctx->num_sms;
+  if (ctx->trsv_ctas > 0) slots = std::min(slots, ctx->trsv_ctas);
+  int group = std::min(64, slots / batch);
   group = std::min(group, std::max(1, (nn + kTrsvBlk - 1) / kTrsvBlk));
   if (group < 1) return fail(ctx, BEM_ERR_ARG, "cooperative solve does not fit the device");
   TrsvArgs t{};

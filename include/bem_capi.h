@@ -124,7 +124,11 @@ int bem_ctx_set_stream(bem_ctx *ctx, void *stream);
  * mma.sync), "trsv_coop" (one cooperative launch per triangular solve),
  * "lu_pairs" (two 64-column panels per FP32 trailing update, K = 128),
  * "panel_calu" (FP32 panels with tournament pivoting), "graphs" (bem_sweep
- * replays a captured step).  Defaults: on, on, on, off, on. */
+ * replays a captured step).  Defaults: on, on, on, off, on.
+ * Integer budgets for a context that shares the GPU with another one running
+ * at the same time (0, the default, means the whole device): "gemm_ctas"
+ * (CTAs of the persistent FP32 trailing update) and "trsv_ctas" (CTAs of one
+ * cooperative triangular solve, over all problems of the batch). */
 int bem_ctx_set_option(bem_ctx *ctx, const char *name, int value);
 int bem_ctx_get_option(bem_ctx *ctx, const char *name, int *value);
 const char *bem_status_string(int status);

@@ -25,7 +25,8 @@ def test_options_give_the_same_solutions():
     # graphs: the second and later batches (and calls) replay a captured step
     again, _ = sol.sweep(freqs, form="mixed", batch=7, refine=3)
     assert np.array_equal(again, ref)
-    for opt, val in (("graphs", False), ("lu_pairs", False), ("panel_calu", True), ("trsv_coop", False)):
+    for opt, val in (("graphs", False), ("lu_pairs", False), ("panel_calu", True), ("trsv_coop", False),
+                     ("panel_push", False)):
         sol.ctx.set_option(opt, val)
         assert sol.ctx.get_option(opt) == val
         x, _ = sol.sweep(freqs, form="mixed", batch=7, refine=3)
