@@ -731,6 +731,33 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
   const C czero{R(0), R(0)};
   C v[SW];
   int swp[SW];  // pivot position chosen for each column of the sub-panel
+  // Rank-sw update of my row over columns [c0, c1) by the sub-panel whose
+  // pivot rows start at position ug0 (L of my row in lv, U in s_u); the
+  // pivot rows themselves take their U values.  Column groups of 4 (a group
+  // may run past w, into columns that are never stored).
+  auto rank_update = [&](const C(&lv)[SW], int ug0, int usw, int c0, int c1) {
+    if (grow == INT_MAX || grow < ug0) return;
+    if (grow >= ug0 + usw) {
+      for (int c = c0; c < c1; c += 4) {
+        C x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = s_a[(c + u) * rp + tid];
+#pragma unroll
+        for (int t = 0; t < SW; ++t)
+          if (t < usw) {
+            C uu[4];
+            ld4(&s_u[t][c], uu);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) cfms(x[u], lv[t], uu[u]);
+          }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) s_a[(c + u) * rp + tid] = x[u];
+      }
+    } else {
+      const int i = grow - ug0;
+      for (int c = c0; c < c1; ++c) s_a[c * rp + tid] = s_u[i][c];
+    }
+  };
 
   for (int s0 = 0; s0 < w; s0 += SW) {
     const int sw = min(SW, w - s0), g0 = k + s0;
@@ -738,7 +765,9 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
 #pragma unroll
     for (int c = 0; c < SW; ++c) v[c] = (grow != INT_MAX && c < sw) ? s_a[(s0 + c) * rp + tid] : czero;
 
-    for (int jj = 0; jj < sw; ++jj) {
+#pragma unroll
+    for (int jj = 0; jj < SW; ++jj) {  // unrolled: the register arrays are indexed statically
+      if (jj >= sw) break;
       const int j = s0 + jj, gj = k + j, par = j & 1;
       const int owner = j / rp;
       // 1. This CTA's candidate (a NaN counts as 0, so every column has a
@@ -1080,28 +1109,7 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
         s_u[i][c] = x;
       }
     __syncthreads();
-    // Rank-sw update of my row right of the sub-panel; the pivot rows take
-    // their U values.
-    if (grow != INT_MAX && grow >= g0 + sw) {
-      for (int c = s0 + sw; c < w; c += 4) {  // the remaining width is a multiple of 8
-        C x[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) x[u] = s_a[(c + u) * rp + tid];
-#pragma unroll
-        for (int t = 0; t < SW; ++t)
-          if (t < sw) {
-            C uu[4];
-            ld4(&s_u[t][c], uu);
-#pragma unroll
-            for (int u = 0; u < 4; ++u) cfms(x[u], v[t], uu[u]);
-          }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) s_a[(c + u) * rp + tid] = x[u];
-      }
-    } else if (grow != INT_MAX && grow >= g0) {
-      const int i = grow - g0;
-      for (int c = s0 + sw; c < w; ++c) s_a[c * rp + tid] = s_u[i][c];
-    }
+    rank_update(v, g0, sw, s0 + sw, w);
     __syncthreads();
   }
   for (int idx = tid; idx < w * rcount; idx += blockDim.x) {
