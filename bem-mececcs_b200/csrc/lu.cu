@@ -625,6 +625,21 @@ __device__ __forceinline__ T sel(const T (&x)[N], int j) {
 // pivoting by |re| + |im|, first row on ties) and arithmetic are those of
 // k_panel_cluster, so the factors are the same.
 // ---------------------------------------------------------------------------
+// TF32 tensor-core product of m16n8k8 fragments (FP32 accumulation); operands
+// rounded to TF32 (round to nearest, ties away) first.
+__device__ __forceinline__ unsigned to_tf32(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
 constexpr int kPushMoves = 16;  // positions that a sub-panel's 8 interchanges can touch
 
 __device__ __forceinline__ void dsm_st4(const void* p, unsigned rank, uint4 v) {
@@ -695,6 +710,8 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
   C* s_pub = s_a + (size_t)NB * a.rp;       // [kPushMoves][NB] published rows (sub-panel start values)
   __shared__ uint4 s_box[2][16][1 + KW];    // [column parity][CTA]: candidate word, then its 8 values
   __shared__ uint4 s_dbox[2][KW];           // [column parity]: row gj's 8 values
+  __shared__ uint4 s_wt[2][NW][KW];         // staged best row of every warp
+  __shared__ uint4 s_gw[2][KW];             // staged row gj (its owner CTA)
   __shared__ __align__(16) C s_u[SW][NB];   // the sub-panel's pivot rows: L\U in the sub-panel, then U
   __shared__ R s_rv[2][NW];                 // per-warp candidates: value (FP64) or key (FP32), row
   __shared__ unsigned s_rk[2][NW];
@@ -770,16 +787,16 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
       if (jj >= sw) break;
       const int j = s0 + jj, gj = k + j, par = j & 1;
       const int owner = j / rp;
-      // 1. This CTA's candidate (a NaN counts as 0, so every column has a
-      //    pivot: row gj itself is always eligible).
+      // 1. Candidates: the best row of every warp stages its 8 values (and
+      //    the thread holding row gj stages that row) before the CTA barrier.
+      //    A NaN counts as 0, so every column has a pivot: row gj itself is
+      //    always eligible.
       const bool elig = grow != INT_MAX && grow >= gj;
       R bv = R(-1);
       if (elig) {
-        bv = cabs1(sel(v, jj));
+        bv = cabs1(v[jj]);
         if (!(bv >= R(0))) bv = R(0);
       }
-      int cr;
-      uint4 cword;  // the candidate's mailbox word
       if constexpr (sizeof(R) == 4) {
         // |re| + |im| >= 0, so its bits + 1 order as the value does (0: not
         // eligible) and the lowest lane, warp or CTA with the largest key
@@ -787,82 +804,82 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
         const unsigned key = elig ? __float_as_uint(bv) + 1u : 0u;
         const unsigned mk = __reduce_max_sync(FULL, key);
         const int wl = __ffs(__ballot_sync(FULL, key == mk)) - 1;
+        if (lane == wl && mk != 0u)
+#pragma unroll
+          for (int q = 0; q < KW; ++q) s_wt[par][warp][q] = row_word<R>(v, q);
         if (lane == 0) {
           s_rk[par][warp] = mk;
           s_rr[par][warp] = rbase + warp * 32 + wl;
         }
-        __syncthreads();
-        const unsigned ck = lane < NW ? s_rk[par][lane] : 0u;
-        const unsigned mck = __reduce_max_sync(FULL, ck);
-        const int ww = __ffs(__ballot_sync(FULL, lane < NW && ck == mck)) - 1;
-        cr = mck ? s_rr[par][ww] : INT_MAX;
-        cword = make_uint4(mck, 0u, (unsigned)cr, 0u);
       } else {
-        int br = elig ? grow : INT_MAX;
+        int br = elig ? grow : INT_MAX, bl = lane;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
           const R ov = __shfl_xor_sync(FULL, bv, off);
           const int orr = __shfl_xor_sync(FULL, br, off);
+          const int ol = __shfl_xor_sync(FULL, bl, off);
           if (better(ov, orr, bv, br)) {
             bv = ov;
             br = orr;
+            bl = ol;
           }
         }
+        if (lane == bl && br != INT_MAX)
+#pragma unroll
+          for (int q = 0; q < KW; ++q) s_wt[par][warp][q] = row_word<R>(v, q);
         if (lane == 0) {
           s_rv[par][warp] = bv;
           s_rr[par][warp] = br;
         }
-        __syncthreads();
-        R cv = lane < NW ? s_rv[par][lane] : R(-1);
-        cr = lane < NW ? s_rr[par][lane] : INT_MAX;
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-          if (off >= NW) continue;
-          const R ov = __shfl_xor_sync(FULL, cv, off);
-          const int orr = __shfl_xor_sync(FULL, cr, off);
-          if (better(ov, orr, cv, cr)) {
-            cv = ov;
-            cr = orr;
-          }
-        }
-        cv = __shfl_sync(FULL, cv, 0);
-        cr = __shfl_sync(FULL, cr, 0);
-        cword = cand_word<R>(cv, cr);
       }
-      // 2. Push the candidate into slot [par][rank] of every CTA, and row
-      //    gj's values from its owner.
-      if (cr != INT_MAX) {
-        const int t = cr - rbase;
-        if (warp == (t >> 5)) {
-          C x[SW];
+      if (grow == gj)
 #pragma unroll
-          for (int c = 0; c < SW; ++c) {
-            x[c].re = __shfl_sync(FULL, v[c].re, t & 31);
-            x[c].im = __shfl_sync(FULL, v[c].im, t & 31);
-          }
-          if (lane < cs) {
-            const uint4* slot = &s_box[par][rank][0];
-            dsm_st4(slot, lane, cword);
+        for (int q = 0; q < KW; ++q) s_gw[par][q] = row_word<R>(v, q);
+      __syncthreads();
+      // 2. The pushes, one 16-byte word per warp: word 0 is the candidate's
+      //    (key or value, row), words 1..KW its values, the next KW row gj's
+      //    (from its owner); every pushing warp finds this CTA's candidate.
+      constexpr int NWORD = 1 + 2 * KW;
+      if (warp < NWORD) {
+        int cr, ww;
+        uint4 cword;
+        if constexpr (sizeof(R) == 4) {
+          const unsigned ck = lane < NW ? s_rk[par][lane] : 0u;
+          const unsigned mck = __reduce_max_sync(FULL, ck);
+          ww = __ffs(__ballot_sync(FULL, lane < NW && ck == mck)) - 1;
+          cr = mck ? s_rr[par][ww] : INT_MAX;
+          cword = make_uint4(mck, 0u, (unsigned)cr, 0u);
+        } else {
+          R cv = lane < NW ? s_rv[par][lane] : R(-1);
+          cr = lane < NW ? s_rr[par][lane] : INT_MAX;
+          ww = lane;
 #pragma unroll
-            for (int q = 0; q < KW; ++q) dsm_st4(slot + 1 + q, lane, row_word<R>(x, q));
+          for (int off = 16; off > 0; off >>= 1) {
+            if (off >= NW) continue;
+            const R ov = __shfl_xor_sync(FULL, cv, off);
+            const int orr = __shfl_xor_sync(FULL, cr, off);
+            const int ow = __shfl_xor_sync(FULL, ww, off);
+            if (better(ov, orr, cv, cr)) {
+              cv = ov;
+              cr = orr;
+              ww = ow;
+            }
           }
+          cv = __shfl_sync(FULL, cv, 0);
+          cr = __shfl_sync(FULL, cr, 0);
+          ww = __shfl_sync(FULL, ww, 0);
+          cword = cand_word<R>(cv, cr);
         }
-      } else if (warp == 0 && lane < cs) {
-        dsm_st4(&s_box[par][rank][0], lane, cword);
-      }
-      if ((int)rank == owner) {
-        const int t = gj - rbase;
-        if (warp == (t >> 5)) {
-          C x[SW];
-#pragma unroll
-          for (int c = 0; c < SW; ++c) {
-            x[c].re = __shfl_sync(FULL, v[c].re, t & 31);
-            x[c].im = __shfl_sync(FULL, v[c].im, t & 31);
+        if (lane < cs)
+          for (int wi = warp; wi < NWORD; wi += NW) {
+            if (wi == 0)
+              dsm_st4(&s_box[par][rank][0], lane, cword);
+            else if (wi <= KW) {
+              if (cr != INT_MAX) dsm_st4(&s_box[par][rank][wi], lane, s_wt[par][ww][wi - 1]);
+            } else if ((int)rank == owner) {
+              dsm_st4(&s_dbox[par][wi - 1 - KW], lane, s_gw[par][wi - 1 - KW]);
+            }
           }
-          if (lane < cs)
-#pragma unroll
-            for (int q = 0; q < KW; ++q) dsm_st4(&s_dbox[par][q], lane, row_word<R>(x, q));
-        }
       }
       cluster_sync();
       // 3. The winner, by every warp from its own CTA's mailboxes.
@@ -911,12 +928,12 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
         if (c == jj) swp[c] = prow;
       if (tid < sw) s_u[jj][s0 + tid] = sel(piv, tid);  // the pivot row's L\U in the sub-panel
       // 5. Multipliers and the rank-1 update of the sub-panel, in registers.
-      const C pj = sel(piv, jj);
+      const C pj = piv[jj];
       const bool zero = pj.re == R(0) && pj.im == R(0);
       if (zero && rank == 0 && tid == 0) atomicCAS(&a.status[ST_SINGULAR], 0, gj + 1);
       const C rpv = zero ? czero : crcp(pj);
       if (grow != INT_MAX && grow > gj) {
-        const C l = sel(v, jj) * rpv;
+        const C l = v[jj] * rpv;
 #pragma unroll
         for (int c = 0; c < SW; ++c) {
           if (c == jj) v[c] = l;
@@ -1109,7 +1126,51 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
         s_u[i][c] = x;
       }
     __syncthreads();
-    rank_update(v, g0, sw, s0 + sw, w);
+    if constexpr (sizeof(R) == 4) {
+      // FP32 (the mixed form): the rank-8 product of the rows below the
+      // pivot block on the tensor cores, as in the trailing update (TF32
+      // operands, FP32 accumulation, subtracted in FP32): 16-row by 8-column
+      // tiles, row tiles dealt round-robin to the warps.
+      const int lo = max(0, g0 + sw - rbase);  // first local row to update
+      const int mlo = lo & ~15;
+      const int mtiles = rcount > lo ? (rcount - mlo + 15) / 16 : 0;
+      const int c0 = s0 + sw, ntiles = (w - c0 + 7) / 8;
+      const int g = lane >> 2, t4 = lane & 3;
+      for (int mt = warp; mt < mtiles; mt += NW) {
+        const int rb = mlo + mt * 16;
+        const C x0 = s_a[(s0 + t4) * rp + rb + g], x1 = s_a[(s0 + t4) * rp + rb + g + 8];
+        const C x2 = s_a[(s0 + t4 + 4) * rp + rb + g], x3 = s_a[(s0 + t4 + 4) * rp + rb + g + 8];
+        const unsigned ar[4] = {to_tf32(x0.re), to_tf32(x1.re), to_tf32(x2.re), to_tf32(x3.re)};
+        const unsigned ai[4] = {to_tf32(x0.im), to_tf32(x1.im), to_tf32(x2.im), to_tf32(x3.im)};
+        const unsigned an[4] = {ai[0] ^ 0x80000000u, ai[1] ^ 0x80000000u, ai[2] ^ 0x80000000u,
+                                ai[3] ^ 0x80000000u};
+        for (int nt = 0; nt < ntiles; ++nt) {
+          const int cb = c0 + nt * 8;
+          const C y0 = s_u[t4][cb + g], y1 = s_u[t4 + 4][cb + g];
+          const unsigned br[2] = {to_tf32(y0.re), to_tf32(y1.re)}, bi[2] = {to_tf32(y0.im), to_tf32(y1.im)};
+          float pr[4] = {0.f, 0.f, 0.f, 0.f}, pi[4] = {0.f, 0.f, 0.f, 0.f};
+          mma_tf32(pr, ar, br);
+          mma_tf32(pr, an, bi);
+          mma_tf32(pi, ar, bi);
+          mma_tf32(pi, ai, br);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int lr = rb + g + ((e >> 1) << 3), c = cb + 2 * t4 + (e & 1);
+            if (lr >= lo && lr < rcount) {
+              C& z = s_a[c * rp + lr];
+              z.re -= pr[e];
+              z.im -= pi[e];
+            }
+          }
+        }
+      }
+      if (grow != INT_MAX && grow >= g0 && grow < g0 + sw) {  // the pivot rows take their U
+        const int i = grow - g0;
+        for (int c = s0 + sw; c < w; ++c) s_a[c * rp + tid] = s_u[i][c];
+      }
+    } else {
+      rank_update(v, g0, sw, s0 + sw, w);
+    }
     __syncthreads();
   }
   for (int idx = tid; idx < w * rcount; idx += blockDim.x) {
@@ -1909,18 +1970,6 @@ constexpr int TAS = TBM + 8;   // float2 units
 constexpr int TBS = TBK + 4;
 constexpr size_t kGemmTf32Smem = (size_t)2 * (TBK * TAS + TBN * TBS) * sizeof(float2);
 
-__device__ __forceinline__ unsigned to_tf32(float x) {
-  unsigned r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
-}
-__device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
 
 __global__ void __launch_bounds__(256) k_gemm_tf32(float2* Abase, size_t lda, size_t bstride, int nn, int k, int w,
                                                    int r0, int c0, int ncols) {
