@@ -300,8 +300,8 @@ __global__ void __launch_bounds__(128) k_dyn_diag(DynParams p) {
   for (int g = 0; g < p.ng; ++g) {
     const double4 qq = q[g];
     double r1 = qq.x - P.x, r2 = qq.y - P.y, r3 = qq.z - P.z;
-    double r = sqrt(r1 * r1 + r2 * r2 + r3 * r3);
-    double ir = 1.0 / r;
+    const double ir = rsqrt(fma(r1, r1, fma(r2, r2, r3 * r3)));  // r and 1/r from one rsqrt
+    const double r = fma(r1, r1, fma(r2, r2, r3 * r3)) * ir;
     double drn = (r1 * rn0 + r2 * rn1 + r3 * rn2) * ir;
     const double rd[3] = {r1 * ir, r2 * ir, r3 * ir};
     const double rn[3] = {rn0, rn1, rn2};
@@ -397,8 +397,9 @@ __global__ void __launch_bounds__(128) k_dyn_offdiag(DynParams p) {
       for (int g = 0; g < p.ng; ++g) {
         const double4 qq = q[g];
         const double r1 = qq.x - P.x, r2 = qq.y - P.y, r3 = qq.z - P.z;
-        const double r = sqrt(fma(r1, r1, fma(r2, r2, r3 * r3)));
-        const double ir = 1.0 / r;
+        const double rr = fma(r1, r1, fma(r2, r2, r3 * r3));
+        const double ir = rsqrt(rr);  // r and 1/r from one rsqrt
+        const double r = rr * ir;
         const double d0 = r1 * ir, d1 = r2 * ir, d2 = r3 * ir;
         const double drn = (r1 * n3[0] + r2 * n3[1] + r3 * n3[2]) * ir;
         const StokesRadial<double> s = stokes_radial(kc, r, ir);
@@ -605,6 +606,9 @@ StokesConsts<double> make_consts(const double zge_[2], const double zcs_[2],
   k.zc1m2 = zd{c1.x - 2.0, c1.y};
   k.zc0 = zd{c0.x, c0.y};
   k.inv4pi = 1.0 / (4.0 * pi);
+  const double2 ikp = div(make_double2(1.0, 0.0), kp), iks = div(make_double2(1.0, 0.0), ks);
+  k.izkp = zd{ikp.x, ikp.y};
+  k.izks = zd{iks.x, iks.y};
   return k;
 }
 
@@ -785,8 +789,8 @@ __global__ void __launch_bounds__(128) k_static_system(StaticSysParams p) {
       for (int g = 0; g < p.ng; ++g) {
         const double4 qq = q[g];
         const double r1 = qq.x - P.x, r2 = qq.y - P.y, r3 = qq.z - P.z;
-        const double r = sqrt(fma(r1, r1, fma(r2, r2, r3 * r3)));
-        const double ir = 1.0 / r;
+        const double rr = fma(r1, r1, fma(r2, r2, r3 * r3));
+        const double ir = rsqrt(rr);
         const double rd[3] = {r1 * ir, r2 * ir, r3 * ir};
         const double rdn = rd[0] * n3[0] + rd[1] * n3[1] + rd[2] * n3[2];
         const double ct = p.c3 * ir * ir * qq.w, cu = p.c1 * ir * qq.w;

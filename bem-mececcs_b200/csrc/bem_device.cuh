@@ -91,6 +91,7 @@ struct StokesConsts {
   cpx<R> zc1m2;      // (cp/cs)^2 - 2
   cpx<R> zc0;        // 1 / (4 pi zge)
   R inv4pi;
+  cpx<R> izkp, izks; // 1 / zkp, 1 / zks: 1 / (zk r) = (1 / zk) (1 / r), no division per point
 };
 
 // The radial functions of the Stokes solution at distance r (inverse ir),
@@ -105,7 +106,7 @@ __device__ __forceinline__ StokesRadial<R> stokes_radial(const StokesConsts<R>& 
   cpx<R> zzs = k.zks * r, zzp = k.zkp * r;
   cpx<R> es = cexp_scaled(zzs, ir);           // exp(zzs) / r
   cpx<R> ep = cexp_scaled(zzp, ir) * k.zc2;   // zc2 exp(zzp) / r
-  cpx<R> izs = crcp(zzs), izp = crcp(zzp);
+  cpx<R> izs = k.izks * ir, izp = k.izkp * ir;
   cpx<R> izs2 = izs * izs, izp2 = izp * izp;
   const R one = R(1), two = R(2), three = R(3), four = R(4), nine = R(9);
   StokesRadial<R> s;

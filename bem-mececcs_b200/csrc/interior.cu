@@ -84,8 +84,9 @@ __global__ void __launch_bounds__(kIntThreads) k_interior(InteriorParams p) {
     for (int g = 0; g < p.ng; ++g) {
       const double4 qq = q[g];
       const double r1 = qq.x - P.x, r2 = qq.y - P.y, r3 = qq.z - P.z;
-      const double r = sqrt(fma(r1, r1, fma(r2, r2, r3 * r3)));
-      const double ir = 1.0 / r;
+      const double rr = fma(r1, r1, fma(r2, r2, r3 * r3));
+      const double ir = rsqrt(rr);  // r and 1/r from one rsqrt
+      const double r = rr * ir;
       const double rd[3] = {r1 * ir, r2 * ir, r3 * ir};
       const double drn = rd[0] * n[0] + rd[1] * n[1] + rd[2] * n[2];
       const double wt = qq.w;
@@ -94,7 +95,7 @@ __global__ void __launch_bounds__(kIntThreads) k_interior(InteriorParams p) {
       const zd zzs = kc.zks * r, zzp = kc.zkp * r;
       const zd es = cexp_scaled(zzs, ir);           // exp(zzs) / r
       const zd ep = cexp_scaled(zzp, ir) * kc.zc2;  // (cs/cp)^2 exp(zzp) / r
-      const zd izs = crcp(zzs), izp = crcp(zzp);
+      const zd izs = kc.izks * ir, izp = kc.izkp * ir;
       const zd izs2 = izs * izs, izp2 = izp * izp;
       const zd fhi = (1.0 + izs2 - izs) * es - (izp2 - izp) * ep;
       const zd cappa = (1.0 + 3.0 * izs2 - 3.0 * izs) * es - (1.0 + 3.0 * izp2 - 3.0 * izp) * ep;
