@@ -94,6 +94,9 @@ struct LuWork {
   unsigned* trsv_ctr = nullptr;  // [kMaxBatch] group barrier counters
   int* pstart = nullptr;         // first row of each panel of the last factorisation, then nn
                                  // (written by the panel kernels)
+  float2* tinv = nullptr;        // FP32 solves: inverted diagonal blocks of the last factors
+  size_t tinv_bytes = 0;
+  bool tinv_valid = false;
 };
 
 constexpr int kMaxGrid = 160;
@@ -179,6 +182,7 @@ struct bem_ctx {
   size_t pinned_bytes = 0;
   bool use_tcgen05 = true;  // FP32 trailing update on tcgen05 (else TF32 mma.sync)
   bool use_trsv_coop = true;
+  bool trsv_inv = true;        // FP32 cooperative solves apply inverted diagonal blocks (k_trsv_f32)
   bool use_graphs = true;     // bem_sweep replays a captured batch step
   // the captured step of bem_sweep
   cudaGraph_t sweep_graph = nullptr;

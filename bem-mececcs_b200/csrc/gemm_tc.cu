@@ -400,6 +400,22 @@ bool make_cmap(CUtensorMap* m, float2* base, int nn, size_t lda, size_t bstride,
 
 }  // namespace
 
+// 3-D map over the FP32 systems as 8-byte (complex) elements: nn rows, nn+1
+// columns, batch problems; box_rows x 64 column boxes, no swizzle (the
+// row shares of the triangular solves; rows past nn read as zero).
+bool make_rows_map(CUtensorMap* m, const void* base, int nn, size_t lda, size_t bstride, int batch, int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)nn, (cuuint64_t)nn + 1, (cuuint64_t)batch};
+  cuuint64_t strides[2] = {(cuuint64_t)lda * sizeof(float2), (cuuint64_t)bstride * sizeof(float2)};
+  cuuint32_t box[3] = {(cuuint32_t)box_rows, 64, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+
 // tcgen05 kind::tf32 throughput: one elected thread per CTA issues `iters`
 // x 4 MMAs (M=128, N=n, K=8) from zeroed shared-memory operands into one
 // TMEM accumulator, then waits (bounded) for their completion.

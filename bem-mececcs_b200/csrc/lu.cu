@@ -26,6 +26,7 @@
 // Row interchanges are never applied to columns left of a panel; each panel's
 // interchanges are kept (ipiv and a dst/src gather list) so that later solves
 // can replay them in panel order.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -2374,6 +2375,323 @@ __global__ void __launch_bounds__(256) k_trsv(TrsvArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// FP32 solves (the mixed form's refinement) with inverted diagonal blocks.
+// k_tri_inv inverts, once per factorisation, every diagonal block the solves
+// step through: blocks [0, npanels) are the unit-lower L11 of the forward
+// panels (w x w at (k, k)), blocks [npanels, npanels + nblk) the upper
+// triangles of the 64-row backward blocks.  Thread j solves T x = e_j; the
+// inverse is stored row-major [64][64], zero outside the block.  The factors
+// come from partial pivoting (|L| <= 1), and the FP32 solves only
+// precondition the FP64 refinement, so explicit block inverses are accurate
+// enough there; the FP64 solves keep the substitution of k_trsv.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(64) k_tri_inv(const float2* __restrict__ Abase, size_t lda, size_t bstride, int nn,
+                                                int npanels, const int* __restrict__ pstart, float2* inv) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto s_T = reinterpret_cast<zf(*)[65]>(smem_raw);  // [64][65]: [column][row]
+  auto s_X = s_T + 64;                                // [64][65]: [column j of the inverse][row]
+  const int b = blockIdx.x, prob = blockIdx.y, j = threadIdx.x;
+  const int nblk = (nn + kTrsvBlk - 1) / kTrsvBlk;
+  const float2* A = Abase + (size_t)prob * bstride;
+  float2* out = inv + ((size_t)prob * (npanels + nblk) + b) * kTrsvBlk * kTrsvBlk;
+  const bool lower = b < npanels;
+  const int k0 = lower ? pstart[b] : (b - npanels) * kTrsvBlk;
+  const int w = lower ? pstart[b + 1] - k0 : min(kTrsvBlk, nn - k0);
+  for (int c = 0; c < w; ++c)
+    if (j < w) {
+      const float2 t = A[(size_t)(k0 + c) * lda + k0 + j];
+      s_T[c][j] = zf{t.x, t.y};
+    }
+  __syncthreads();
+  if (j < w) {
+    if (lower) {  // x_i = [i == j] - sum_{j <= k < i} L(i,k) x_k
+      for (int i = 0; i < j; ++i) s_X[j][i] = zf{0.f, 0.f};
+      s_X[j][j] = zf{1.f, 0.f};
+      for (int i = j + 1; i < w; ++i) {
+        zf acc{0.f, 0.f};
+        for (int kk = j; kk < i; ++kk) cfms(acc, s_T[kk][i], s_X[j][kk]);
+        s_X[j][i] = acc;
+      }
+    } else {  // x_i = ([i == j] - sum_{i < k <= j} U(i,k) x_k) / U(i,i)
+      for (int i = j + 1; i < w; ++i) s_X[j][i] = zf{0.f, 0.f};
+      for (int i = j; i >= 0; --i) {
+        zf acc{i == j ? 1.f : 0.f, 0.f};
+        for (int kk = i + 1; kk <= j; ++kk) cfms(acc, s_T[kk][i], s_X[j][kk]);
+        const zf d = s_T[i][i];
+        s_X[j][i] = (d.re == 0.f && d.im == 0.f) ? zf{0.f, 0.f} : acc * crcp(d);
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = 0; i < kTrsvBlk; ++i) {
+    const zf x = (i < w && j < w) ? s_X[j][i] : zf{0.f, 0.f};
+    out[(size_t)i * kTrsvBlk + j] = make_float2(x.re, x.im);
+  }
+}
+
+__device__ __forceinline__ void bulk_prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void tma_rows_load(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_rows_prefetch(const CUtensorMap* map, int x, int y, int z) {
+  asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(map), "r"(x), "r"(y),
+               "r"(z)
+               : "memory");
+}
+
+// k_trsv with the FP32 factors, same group structure, gathers and buffers
+// (see k_trsv), three changes per step: (1) the step's diagonal triangle is
+// applied as its precomputed inverse (a 64 x 64 product over 256 threads
+// instead of a 64-step warp solve); (2) this CTA's share of the step's L (or
+// U) rows is brought into shared memory by one TMA box load issued when the
+// step starts, before the gather and the product it does not depend on; (3)
+// the next step's rows and inverse are prefetched into L2 meanwhile.  A box
+// is `ldl` rows (even, <= 256) by 64 columns of the rows map `tm` (8-byte
+// elements; rows past nn read as zero); 1, 2 or 4 threads per row for the
+// row updates.
+__global__ void __launch_bounds__(256) k_trsv_f32(const __grid_constant__ CUtensorMap tm, TrsvArgs a,
+                                                  const float2* __restrict__ tinv, int ldl, int ninv_l) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // [64][ldl] this CTA's rows of the step's columns: a TMA tile destination,
+  // so 128-byte aligned (the launch adds 128 bytes for the rounding)
+  float2* s_L = reinterpret_cast<float2*>(smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u));
+  int* s_ovr = reinterpret_cast<int*>(s_L + (size_t)kTrsvBlk * ldl);  // [ldl] gather entry of a displaced row, or -1
+  __shared__ zf s_g[128];
+  __shared__ zf s_x[kTrsvBlk];
+  __shared__ zf s_xprev[kTrsvBlk];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ int s_pl[kPermStride];  // the step's gather list: count, then dst/src pairs
+  __shared__ int s_ok;
+  const int prob = blockIdx.x / a.group, rank = blockIdx.x % a.group, G = a.group;
+  if (prob >= a.batch) return;
+  float2* v = static_cast<float2*>(a.v) + (size_t)prob * a.vstride;
+  float2* b1 = static_cast<float2*>(a.w) + (size_t)prob * 2 * a.nn;
+  float2* xo = b1 + a.nn;
+  const int nn = a.nn, tid = threadIdx.x;
+  const int nblk = (nn + kTrsvBlk - 1) / kTrsvBlk;
+  // inverses of this problem: ninv_l forward panels (of the factorisation), then nblk blocks
+  const float2* inv = tinv + (size_t)prob * (ninv_l + nblk) * kTrsvBlk * kTrsvBlk;
+  unsigned* ctr = a.ctr + prob;
+  unsigned epoch = 0, phase = 0;
+  if (tid == 0) mbar_init(&s_bar, 1);
+  for (int i = tid; i < ldl; i += blockDim.x) s_ovr[i] = -1;
+  __syncthreads();
+
+  // This CTA's rows of a step whose updated rows are [r0, r1): [lo, hi).
+  auto share = [&](int r0, int r1, int& lo, int& hi) {
+    const int per = (r1 - r0 + G - 1) / G;
+    lo = min(r1, r0 + rank * per);
+    hi = min(r1, lo + per);
+  };
+  // Rows [lo, hi) of columns [c0, c0 + 64) into s_L as one box starting
+  // at the even row below lo (16-byte aligned), or its L2 prefetch.
+  auto fetch = [&](int c0, int lo, int hi, bool prefetch) {
+    if (prefetch) {
+      if (hi > lo) tma_rows_prefetch(&tm, lo & ~1, c0, prob);
+      return;
+    }
+    mbar_expect_tx(&s_bar, hi > lo ? (unsigned)ldl * kTrsvBlk * 8u : 0u);
+    if (hi > lo) tma_rows_load(s_L, &tm, lo & ~1, c0, prob, &s_bar);
+  };
+  // dst[r] = base[r] - sum_{c < w} s_L[c][r - la] x_c for rows [lo, hi),
+  // base = the gathered value of a displaced row (s_ovr) or src[r]; tpr
+  // threads per row (consecutive lanes) combine their columns by shuffles.
+  auto update_rows = [&](int lo, int hi, int w, const float2* src, float2* dst) {
+    const int rows = hi - lo, la = lo & ~1;
+    const int tpr = rows <= 64 ? 4 : (rows <= 128 ? 2 : 1), rpp = 256 / tpr;
+    const int sub = tid & (tpr - 1), rl = tid / tpr;
+    const int passes = (rows + rpp - 1) / rpp;
+    for (int ps = 0; ps < passes; ++ps) {
+      const int r = lo + ps * rpp + rl;
+      const bool act = r < hi;
+      // the base value first: its load overlaps the products below
+      const int e = act && sub == 0 ? s_ovr[r - lo] : -1;
+      zf base{0.f, 0.f};
+      if (act && sub == 0) base = e >= 0 ? s_g[e] : ldc_cg<float>(&src[r]);
+      zf acc{0.f, 0.f}, acc2{0.f, 0.f};
+      if (act) {
+        const float2* col = s_L + (r - la);
+        for (int c = sub; c < w; c += 2 * tpr) {
+          const float2 t0 = col[(size_t)c * ldl];
+          cfms(acc, zf{t0.x, t0.y}, s_x[c]);
+          if (c + tpr < w) {
+            const float2 t1 = col[(size_t)(c + tpr) * ldl];
+            cfms(acc2, zf{t1.x, t1.y}, s_x[c + tpr]);
+          }
+        }
+      }
+      acc.re += acc2.re;
+      acc.im += acc2.im;
+      for (int off = 1; off < tpr; off <<= 1) {
+        acc.re += __shfl_xor_sync(0xffffffffu, acc.re, off);
+        acc.im += __shfl_xor_sync(0xffffffffu, acc.im, off);
+      }
+      if (act && sub == 0) {
+        if (e >= 0) s_ovr[r - lo] = -1;
+        stc<float>(&dst[r], zf{base.re + acc.re, base.im + acc.im});
+      }
+    }
+  };
+  // x = inv(block) g for the step's w values: 4 threads per row, 16 columns
+  // each; the thread's 16 inverse entries are loaded first (load_inv, at the
+  // start of the step: they do not depend on g).
+  float4 tv[8];
+  auto load_inv = [&](const float2* blk) {
+    const float4* row = reinterpret_cast<const float4*>(blk + (size_t)(tid >> 2) * kTrsvBlk + 16 * (tid & 3));
+#pragma unroll
+    for (int u = 0; u < 8; ++u) tv[u] = __ldg(row + u);
+  };
+  auto apply_inv = [&](int w) {
+    const int i = tid >> 2, q = tid & 3;
+    zf acc{0.f, 0.f};
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const float4 t = tv[u];
+      const int jj = 16 * q + 2 * u;
+      if (jj < w) cfms(acc, zf{-t.x, -t.y}, s_g[jj]);
+      if (jj + 1 < w) cfms(acc, zf{-t.z, -t.w}, s_g[jj + 1]);
+    }
+#pragma unroll
+    for (int off = 1; off < 4; off <<= 1) {
+      acc.re += __shfl_xor_sync(0xffffffffu, acc.re, off);
+      acc.im += __shfl_xor_sync(0xffffffffu, acc.im, off);
+    }
+    if (q == 0 && i < w) s_x[i] = acc;
+  };
+
+  // The steps: forward panels s < nf, then backward blocks.  Step s works
+  // on columns [c0, c0 + w) (inverse block ib) and updates rows [r0, r1).
+  const int nf = a.forward ? a.npanels : 0, nsteps = nf + nblk;
+  auto desc = [&](int st, int& c0, int& w, int& r0, int& r1, int& ib) {
+    if (st < nf) {
+      c0 = __ldg(&a.pstart[st]);
+      w = __ldg(&a.pstart[st + 1]) - c0;
+      r0 = c0 + w;
+      r1 = nn;
+      ib = st;
+    } else {
+      const int sb = nblk - 1 - (st - nf);
+      c0 = sb * kTrsvBlk;
+      w = min(kTrsvBlk, nn - c0);
+      r0 = 0;
+      r1 = c0;
+      ib = ninv_l + sb;
+    }
+  };
+  // The loads of step st that do not depend on the previous step's values:
+  // this CTA's rows (TMA box), its inverse entries (registers), the panel's
+  // gather list (shared memory), and the L2 prefetch of step st + 1.
+  auto issue = [&](int st) {
+    int c0, w, r0, r1, ib, lo, hi;
+    desc(st, c0, w, r0, r1, ib);
+    share(r0, r1, lo, hi);
+    if (tid == 0) {
+      fetch(c0, lo, hi, false);
+      if (st + 1 < nsteps) {
+        int c1, w1, q0, q1, ib1, lo1, hi1;
+        desc(st + 1, c1, w1, q0, q1, ib1);
+        share(q0, q1, lo1, hi1);
+        fetch(c1, lo1, hi1, true);
+        bulk_prefetch_l2(inv + (size_t)ib1 * kTrsvBlk * kTrsvBlk, kTrsvBlk * kTrsvBlk * 8u);
+      }
+    }
+    load_inv(inv + (size_t)ib * kTrsvBlk * kTrsvBlk);
+    if (st < nf) {
+      const int* pl = a.perm + ((size_t)st * a.batch + prob) * kPermStride;
+      for (int i = tid; i < kPermStride; i += blockDim.x) s_pl[i] = __ldg(&pl[i]);
+    }
+  };
+
+  int kprev = 0, wprev = 0;
+  issue(0);
+  __syncthreads();
+  for (int st = 0; st < nsteps; ++st) {
+    int c0, w, r0, r1, ib, lo, hi;
+    desc(st, c0, w, r0, r1, ib);
+    share(r0, r1, lo, hi);
+    const bool fwd = st < nf, odd = st & 1;
+    float2* cur = fwd ? (odd ? b1 : v) : v;
+    float2* nxt = fwd ? (odd ? v : b1) : v;
+    if (fwd) {  // the panel's interchanges, replayed as a gather
+      const int count = s_pl[0];
+      for (int e = tid; e < count; e += blockDim.x) {
+        s_g[e] = ldc_cg<float>(&cur[s_pl[2 + 2 * e]]);
+        const int r = s_pl[1 + 2 * e];
+        if (e >= w && r >= lo && r < hi) s_ovr[r - lo] = e;
+      }
+    } else {
+      for (int i = tid; i < w; i += blockDim.x) s_g[i] = ldc_cg<float>(&v[c0 + i]);
+    }
+    __syncthreads();
+    apply_inv(w);  // s_x = L11^-1 (gathered panel rows) or U_bb^-1 y_b
+    __syncthreads();
+    if (fwd && rank == 0 && odd) {  // v is not read in odd forward steps
+      for (int i = tid; i < wprev; i += blockDim.x) stc<float>(&v[kprev + i], s_xprev[i]);
+      for (int i = tid; i < w; i += blockDim.x) stc<float>(&v[c0 + i], s_x[i]);
+    }
+    if (!fwd && rank == 0)
+      for (int i = tid; i < w; i += blockDim.x) stc<float>(&xo[c0 + i], s_x[i]);
+    if (!mbar_wait(&s_bar, phase)) {
+      atomicExch(&a.status[ST_TIMEOUT], 1);
+      return;
+    }
+    phase ^= 1u;
+    // rows [lo, hi): nxt = cur - L x (a row that received a displaced panel
+    // row starts from the gathered value), or v -= U x in place
+    update_rows(lo, hi, w, cur, nxt);
+    if (fwd) {
+      if (odd) {
+        wprev = 0;
+      } else {
+        for (int i = tid; i < w; i += blockDim.x) s_xprev[i] = s_x[i];
+        kprev = c0;
+        wprev = w;
+      }
+    }
+    // Group barrier, split: arrive, issue the next step's loads, then wait.
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      red_release_gpu_add(ctr, 1u);
+    }
+    ++epoch;
+    if (st + 1 < nsteps) issue(st + 1);
+    if (tid == 0) {
+      const unsigned target = epoch * (unsigned)G;
+      const unsigned long long t0 = globaltimer_ns();
+      int ok = 1;
+      unsigned spins = 0;
+      while (ld_acquire_gpu(ctr) < target) {
+        if ((++spins & 255u) == 0) {
+          if (*(volatile int*)&a.status[ST_TIMEOUT] != 0 || globaltimer_ns() - t0 > kWaitLimitNs) {
+            atomicExch(&a.status[ST_TIMEOUT], 1);
+            ok = 0;
+            break;
+          }
+        }
+      }
+      s_ok = ok;
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    if (st == nf - 1 && wprev > 0) {  // the last panel was even: its rows still go to v
+      if (rank == 0)
+        for (int i = tid; i < wprev; i += blockDim.x) stc<float>(&v[kprev + i], s_xprev[i]);
+      if (!grid_barrier(ctr, ++epoch, G, a.status)) return;
+    }
+  }
+  int lo, hi;
+  share(0, nn, lo, hi);
+  for (int r = lo + tid; r < hi; r += blockDim.x) v[r] = __ldcg(&xo[r]);
+}
+
+// ---------------------------------------------------------------------------
 // Host side.
 // ---------------------------------------------------------------------------
 int lu_ensure_workspace(bem_ctx* ctx, int nn, int batch) {
@@ -2607,6 +2925,86 @@ int lu_lockstep_capacity(bem_ctx* ctx, int nn, bool fp32) {
 // One cooperative k_trsv launch over `batch` problems: forward (with the
 // interchanges of the last factorisation) and back substitution, or back
 // substitution only.
+bool make_rows_map(CUtensorMap* m, const void* base, int nn, size_t lda, size_t bstride, int batch, int box_rows);
+
+// The FP32 solves with inverted diagonal blocks (k_tri_inv once per
+// factorisation, then k_trsv_f32); done = false when the group's shared
+// memory would not fit, and k_trsv runs instead.
+constexpr size_t kTrsvF32SmemMax = 200 * 1024;
+
+static int trsv_f32(bem_ctx* ctx, const void* A, size_t lda, size_t bstride, int nn, int batch, void* v,
+                    size_t vstride, bool forward, bool& done) {
+  LuWork& L = ctx->lu;
+  done = false;
+  const int npan = (int)L.panels.size(), nblk = (nn + kTrsvBlk - 1) / kTrsvBlk;
+  // the largest group (at most 64 CTAs per problem) whose CTAs are all resident
+  int group = 0, ldl = 0;
+  size_t smem = 0;
+  for (int g = std::min(64, std::max(1, nblk)); g >= 1; --g) {
+    const int per = (nn + g - 1) / g;
+    const int l = (per + 3) & ~1;  // rows of a share rounded out to even ends
+    const size_t sm = (size_t)kTrsvBlk * l * sizeof(float2) + (size_t)l * sizeof(int) + 128;
+    if (sm > kTrsvF32SmemMax || l > 256) break;  // smaller groups only need more; TMA boxes <= 256 rows
+    BEM_CUDA(ctx, cudaFuncSetAttribute(k_trsv_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int occ = 0;
+    BEM_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trsv_f32, 256, sm));
+    int slots = occ * ctx->num_sms;
+    if (ctx->trsv_ctas > 0) slots = std::min(slots, ctx->trsv_ctas);
+    if (g * batch <= slots) {
+      group = g;
+      ldl = l;
+      smem = sm;
+      break;
+    }
+  }
+  if (!group) return BEM_OK;
+  if (!L.tinv_valid) {
+    const size_t bytes = (size_t)batch * (npan + nblk) * kTrsvBlk * kTrsvBlk * sizeof(float2);
+    if (L.tinv_bytes < bytes) {
+      cudaFree(L.tinv);
+      L.tinv = nullptr;
+      L.tinv_bytes = 0;
+      BEM_CUDA(ctx, cudaMalloc(&L.tinv, bytes));
+      L.tinv_bytes = bytes;
+    }
+    ProfScope ps(ctx, 4, 8.0 * (double)(npan + nblk) * kTrsvBlk * kTrsvBlk * kTrsvBlk / 3.0 * batch,
+                 2.0 * (double)(npan + nblk) * kTrsvBlk * kTrsvBlk * sizeof(float2) * batch);
+    constexpr size_t kInvSmem = (size_t)2 * 64 * 65 * sizeof(float2);
+    BEM_CUDA(ctx, cudaFuncSetAttribute(k_tri_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
+    k_tri_inv<<<dim3(npan + nblk, batch), 64, kInvSmem, ctx->stream>>>(static_cast<const float2*>(A), lda, bstride,
+                                                                       nn, npan, L.pstart, L.tinv);
+    ctx->launches++;
+    BEM_CUDA(ctx, cudaGetLastError());
+    L.tinv_valid = true;
+  }
+  TrsvArgs t{};
+  t.A = A;
+  t.lda = lda;
+  t.bstride = bstride;
+  t.nn = nn;
+  t.batch = batch;
+  t.group = group;
+  t.forward = forward ? 1 : 0;
+  t.npanels = forward ? npan : 0;
+  t.pstart = L.pstart;
+  t.perm = L.perm;
+  t.v = v;
+  t.vstride = vstride;
+  t.w = L.trsv_w;
+  t.ctr = L.trsv_ctr;
+  t.status = ctx->d_status;
+  const float2* tinv = L.tinv;
+  CUtensorMap tm;
+  if (!make_rows_map(&tm, A, nn, lda, bstride, batch, ldl)) return BEM_OK;  // k_trsv instead
+  BEM_CUDA(ctx, cudaMemsetAsync(L.trsv_ctr, 0, batch * sizeof(unsigned), ctx->stream));
+  void* args[] = {&tm, &t, &tinv, &ldl, const_cast<int*>(&npan)};
+  BEM_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)k_trsv_f32, dim3(group * batch), dim3(256), args, smem,
+                                            ctx->stream));
+  ctx->launches++;
+  done = true;
+  return BEM_OK;
+}
+
 template <typename R>
 static int trsv_coop(bem_ctx* ctx, const void* A, size_t lda, size_t bstride, int nn, int batch, void* v,
                      size_t vstride, bool forward) {
@@ -2622,6 +3020,13 @@ static int trsv_coop(bem_ctx* ctx, const void* A, size_t lda, size_t bstride, in
   }
   if (!L.trsv_ctr) BEM_CUDA(ctx, cudaMalloc(&L.trsv_ctr, kMaxBatch * sizeof(unsigned)));
   if (batch < 1 || batch > kMaxBatch) return fail(ctx, BEM_ERR_ARG, "batch size out of range");
+  if constexpr (sizeof(R) == 4) {
+    if (ctx->trsv_inv) {
+      bool done = false;
+      const int rc = trsv_f32(ctx, A, lda, bstride, nn, batch, v, vstride, forward, done);
+      if (rc || done) return rc;
+    }
+  }
   const size_t smem = (size_t)kTrsvBlk * kTrsvBlk * sizeof(cpx<R>);
   BEM_CUDA(ctx, cudaFuncSetAttribute(k_trsv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
@@ -2675,6 +3080,7 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     if (rc) return rc;
   }
   L.panels.clear();
+  L.tinv_valid = false;  // the solves' block inverses belong to the previous factors
   const bool tc = sizeof(R) == 4 && ctx->use_tcgen05;
   // Panel width for m remaining rows: the widest of 64/32/16 whose rows fit
   // one cluster, at most 512 rows per CTA (one row per thread); 0 when the
