@@ -183,6 +183,7 @@ struct bem_ctx {
   bool use_tcgen05 = true;  // FP32 trailing update on tcgen05 (else TF32 mma.sync)
   bool use_trsv_coop = true;
   bool trsv_inv = true;        // FP32 cooperative solves apply inverted diagonal blocks (k_trsv_f32)
+  bool laswp_tc = true;        // FP32 row interchange + U12 solve on the tensor cores (k_laswp_tc)
   bool use_graphs = true;     // bem_sweep replays a captured batch step
   // the captured step of bem_sweep
   cudaGraph_t sweep_graph = nullptr;

@@ -145,6 +145,7 @@ int bem_ctx_create(int device, bem_ctx** out) {
   if (const char* env = getenv("BEM_PANEL_CALU")) ctx->panel_calu = env[0] == '1';
   if (const char* env = getenv("BEM_PANEL_PUSH")) ctx->panel_push = env[0] != '0';
   if (const char* env = getenv("BEM_TRSV_INV")) ctx->trsv_inv = env[0] != '0';
+  if (const char* env = getenv("BEM_LASWP_TC")) ctx->laswp_tc = env[0] != '0';
   *out = ctx;
   return BEM_OK;
 }
@@ -534,6 +535,7 @@ static bool* option_slot(bem_ctx* ctx, const char* name) {
   if (!strcmp(name, "tcgen05")) return &ctx->use_tcgen05;
   if (!strcmp(name, "trsv_coop")) return &ctx->use_trsv_coop;
   if (!strcmp(name, "trsv_inv")) return &ctx->trsv_inv;
+  if (!strcmp(name, "laswp_tc")) return &ctx->laswp_tc;
   if (!strcmp(name, "lu_pairs")) return &ctx->lu_pairs;
   if (!strcmp(name, "panel_calu")) return &ctx->panel_calu;
   if (!strcmp(name, "panel_push")) return &ctx->panel_push;

@@ -1844,9 +1844,15 @@ __global__ void __launch_bounds__(256) k_laswp_trsm(void* Av, size_t lda, size_t
 }
 
 // ---------------------------------------------------------------------------
-// Trailing update C -= L21 U12 on the tensor cores, complex as 4 real products.
-// C: rows [r0, nn), cols [c0, ncols) of problem blockIdx.z; L21 = columns
-// k..k+w-1 of the same rows; U12 = rows k..k+w-1 of the same columns.
+// k_laswp_tc: k_laswp_trsm for the FP32 factors on the tensor cores.  Each
+// CTA first inverts the panel's unit-lower L11 in shared memory (by 16 x 16
+// blocks), then loops over 64-column tiles of [c0, ncols): the tile's
+// panel rows are gathered (the panel's interchanges), the displaced rows are
+// copied down, PRE subtracts the previous panel's deferred product Lb Uprev,
+// and U12 = L11^-1 B; both products as TF32 mma.sync (FP32 accumulation,
+// complex as four real products): the deferred product in the accuracy class
+// of the trailing update, U12 with split operands (3 x TF32, about FP32).  U12 goes back to A and, packed and rounded to
+// TF32, to the tensor-core operand rows (ure/uim, when given).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
   const unsigned s = smem_u32(smem);
@@ -1864,6 +1870,248 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+constexpr int kLtLd = 68;  // complex pitch of the 64 x 64 shared tiles (conflict-free fragment loads)
+constexpr size_t kLtTile = (size_t)64 * kLtLd * sizeof(float2);
+
+template <bool PRE>
+__global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, size_t bstride, int k, int w, int c0,
+                                                     int ncols, const int* __restrict__ perm, int perm_stride,
+                                                     float* ure, float* uim, int urows, int ubase, int koff,
+                                                     int kprev) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* s_inv = reinterpret_cast<float2*>(smem_raw);  // [64][kLtLd] L11^-1, row-major
+  float2* s_bb = s_inv + 64 * kLtLd;                     // [2][64][kLtLd] tiles (panel rows x columns), two stages
+  float2* s_lb = s_bb + 2 * 64 * kLtLd;                  // PRE: previous panel's L at this panel's rows
+  float2* s_upb = s_lb + 64 * kLtLd;                     // PRE: [2][64][kLtLd] previous panel's U rows of the tiles
+  float2* s_b = s_bb;                                    // L11 while inverting
+  __shared__ int s_src[64];                              // source row of panel row i
+  __shared__ int s_xd[64], s_xs[64];                     // displaced rows: dst <- src
+  __shared__ int s_nx;
+  const int prob = blockIdx.y, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  float2* A = Abase + (size_t)prob * bstride;
+  const int* pl = perm + (size_t)prob * perm_stride;
+  const int count = pl[0];
+  if (tid < 64) s_src[tid] = tid < w ? pl[2 + 2 * tid] : 0;
+  if (tid < 64) {
+    const int e = w + tid;
+    s_xd[tid] = e < count ? pl[1 + 2 * e] : -1;
+    s_xs[tid] = e < count ? pl[2 + 2 * e] : 0;
+  }
+  if (tid == 0) s_nx = max(0, count - w);
+  // L11 (unit lower, w x w at (k, k)) into s_b, row-major; s_inv = I.
+  for (int idx = tid; idx < 64 * 64; idx += blockDim.x) {
+    const int i = idx & 63, c = idx >> 6;
+    s_b[i * kLtLd + c] = (i < w && c < w) ? A[(size_t)(k + c) * lda + k + i] : make_float2(0.f, 0.f);
+    s_inv[i * kLtLd + c] = make_float2(i == c ? 1.f : 0.f, 0.f);
+  }
+  __syncthreads();
+  // X = L11^-1 by blocks: the four 16 x 16 diagonal blocks (a warp each,
+  // lane = column), then [[X11, 0], [X21, X22]] with X21 = -X22 L21 X11 at
+  // 16 and at 32; the zero block above the diagonal (rows 0-31, columns
+  // 32-63 of s_inv) holds the intermediate L21 X11.
+  auto at = [&](float2* M, int i, int j) -> float2& { return M[i * kLtLd + j]; };
+  if (warp < 4 && lane < 16) {
+    const int b0 = 16 * warp, c = lane;
+    zf x[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) x[i] = zf{i == c ? 1.f : 0.f, 0.f};
+#pragma unroll
+    for (int i = 1; i < 16; ++i) {
+      zf acc{0.f, 0.f};
+#pragma unroll
+      for (int t = 0; t < i; ++t) {  // x_t = 0 for t < c
+        const float2 l = at(s_b, b0 + i, b0 + t);
+        cfms(acc, zf{l.x, l.y}, x[t]);
+      }
+      if (i > c) x[i] = acc;
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) at(s_inv, b0 + i, b0 + c) = make_float2(x[i].re, x[i].im);
+  }
+  __syncthreads();
+  // X21 = -X22 (L21 X11) for two 16-blocks (h = 16) and then one 32-block (h = 32)
+  for (int h = 16; h <= 32; h *= 2) {
+    const int npair = 64 / (2 * h), outs = npair * h * h;
+    for (int idx = tid; idx < outs; idx += blockDim.x) {  // T = L21 X11 into the scratch block
+      const int pp = idx / (h * h), i = (idx / h) % h, j = idx % h, o = pp * 2 * h;
+      zf acc{0.f, 0.f};
+      for (int t = 0; t < h; ++t) {
+        const float2 l = at(s_b, o + h + i, o + t), x = at(s_inv, o + t, o + j);
+        cfms(acc, zf{l.x, l.y}, zf{x.x, x.y});
+      }
+      at(s_inv, pp * h + i, 32 + j) = make_float2(-acc.re, -acc.im);  // acc = -T
+    }
+    __syncthreads();
+    for (int idx = tid; idx < outs; idx += blockDim.x) {  // X21 = -X22 T
+      const int pp = idx / (h * h), i = (idx / h) % h, j = idx % h, o = pp * 2 * h;
+      zf acc{0.f, 0.f};
+      for (int t = 0; t < h; ++t) {
+        const float2 x = at(s_inv, o + h + i, o + h + t), tt = at(s_inv, pp * h + t, 32 + j);
+        cfms(acc, zf{x.x, x.y}, zf{tt.x, tt.y});
+      }
+      at(s_inv, o + h + i, o + j) = make_float2(acc.re, acc.im);  // acc = -X22 T
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < 32 * 32; idx += blockDim.x) at(s_inv, idx >> 5, 32 + (idx & 31)) = make_float2(0.f, 0.f);
+  if (PRE) {  // Lb(i, t) = L(src(k + i), kprev + t)
+    for (int idx = tid; idx < 64 * 64; idx += blockDim.x) {
+      const int i = idx & 63, t = idx >> 6;
+      s_lb[i * kLtLd + t] = i < w ? A[(size_t)(kprev + t) * lda + s_src[i]] : make_float2(0.f, 0.f);
+    }
+  }
+  __syncthreads();
+
+  // warp tile: rows [16 * (warp & 3), +16) x columns [32 * (warp >> 2), +32)
+  const int g = lane >> 2, t4 = lane & 3, mrow = 16 * (warp & 3), ncol = 32 * (warp >> 2);
+  // acc = M B for this warp's tile, M (64 x 64) and B (64 x 64) complex in
+  // shared memory; split: each operand as a TF32 pair hi + lo and three
+  // products per real product (hi hi + hi lo + lo hi), about FP32 accuracy.
+  auto cproduct = [&](const float2* M, const float2* Bm, float (&pr)[4][4], float (&pi)[4][4], bool split) {
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) pr[nt][e] = pi[nt][e] = 0.f;
+#pragma unroll 2
+    for (int ks = 0; ks < 8; ++ks) {
+      const int kc = ks * 8 + t4;
+      const float2 x0 = M[(mrow + g) * kLtLd + kc], x1 = M[(mrow + g + 8) * kLtLd + kc];
+      const float2 x2 = M[(mrow + g) * kLtLd + kc + 4], x3 = M[(mrow + g + 8) * kLtLd + kc + 4];
+      const unsigned ar[4] = {to_tf32(x0.x), to_tf32(x1.x), to_tf32(x2.x), to_tf32(x3.x)};
+      const unsigned ai[4] = {to_tf32(x0.y), to_tf32(x1.y), to_tf32(x2.y), to_tf32(x3.y)};
+      const unsigned an[4] = {ai[0] ^ 0x80000000u, ai[1] ^ 0x80000000u, ai[2] ^ 0x80000000u, ai[3] ^ 0x80000000u};
+      unsigned arl[4], ail[4], anl[4];  // low parts (split)
+      if (split) {
+        const float xr[4] = {x0.x, x1.x, x2.x, x3.x}, xi[4] = {x0.y, x1.y, x2.y, x3.y};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          arl[e] = to_tf32(xr[e] - __uint_as_float(ar[e]));
+          ail[e] = to_tf32(xi[e] - __uint_as_float(ai[e]));
+          anl[e] = ail[e] ^ 0x80000000u;
+        }
+      }
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int cb = ncol + nt * 8 + g;
+        const float2 y0 = Bm[kc * kLtLd + cb], y1 = Bm[(kc + 4) * kLtLd + cb];
+        const unsigned br[2] = {to_tf32(y0.x), to_tf32(y1.x)}, bi[2] = {to_tf32(y0.y), to_tf32(y1.y)};
+        mma_tf32(pr[nt], ar, br);
+        mma_tf32(pr[nt], an, bi);
+        mma_tf32(pi[nt], ar, bi);
+        mma_tf32(pi[nt], ai, br);
+        if (split) {
+          const unsigned brl[2] = {to_tf32(y0.x - __uint_as_float(br[0])), to_tf32(y1.x - __uint_as_float(br[1]))};
+          const unsigned bil[2] = {to_tf32(y0.y - __uint_as_float(bi[0])), to_tf32(y1.y - __uint_as_float(bi[1]))};
+          mma_tf32(pr[nt], ar, brl);
+          mma_tf32(pr[nt], an, bil);
+          mma_tf32(pi[nt], ar, bil);
+          mma_tf32(pi[nt], ai, brl);
+          mma_tf32(pr[nt], arl, br);
+          mma_tf32(pr[nt], anl, bi);
+          mma_tf32(pi[nt], arl, bi);
+          mma_tf32(pi[nt], ail, br);
+        }
+      }
+    }
+  };
+
+  const int ntiles = (ncols - c0 + 63) / 64;
+  // A tile's inputs into stage st by cp.async (8-byte elements, zero-filled
+  // outside the panel rows and past the last column): one commit group.
+  auto issue = [&](int tile, int st) {
+    if (tile < ntiles) {
+      const int cbase = c0 + tile * 64, tw = min(64, ncols - cbase);
+      float2* b = s_bb + (size_t)st * 64 * kLtLd;
+      float2* up = s_upb + (size_t)st * 64 * kLtLd;
+      const int i = tid & 63, cg = tid >> 6;
+#pragma unroll
+      for (int u = 0; u < 16; ++u) {
+        const int c = cg + 4 * u;
+        const bool ok = c < tw && i < w;
+        cp_async8(&b[i * kLtLd + c], ok ? &A[(size_t)(cbase + c) * lda + s_src[i]] : A, ok);
+        if (PRE) cp_async8(&up[i * kLtLd + c], c < tw ? &A[(size_t)(cbase + c) * lda + kprev + i] : A, c < tw);
+      }
+    }
+    cp_async_commit();
+  };
+  issue(blockIdx.x, 0);
+  for (int it = 0;; ++it) {
+    const int tile = blockIdx.x + it * gridDim.x;
+    if (tile >= ntiles) break;
+    const int st = it & 1;
+    const int cbase = c0 + tile * 64, tw = min(64, ncols - cbase);
+    float2* sb = s_bb + (size_t)st * 64 * kLtLd;
+    float2* sup = s_upb + (size_t)st * 64 * kLtLd;
+    issue(tile + gridDim.x, st ^ 1);  // the next tile streams in meanwhile
+    cp_async_wait<1>();
+    __syncthreads();
+    // displaced rows: their sources, loaded now and stored after the products
+    float2 xv[16];
+    const int nx = s_nx;
+    {
+      const int i = tid & 63, cg = tid >> 6;
+#pragma unroll
+      for (int u = 0; u < 16; ++u) {
+        const int c = cg + 4 * u;
+        xv[u] = (i < nx && c < tw) ? A[(size_t)(cbase + c) * lda + s_xs[i]] : make_float2(0.f, 0.f);
+      }
+    }
+    float pr[4][4], pi[4][4];
+    if (PRE) {  // B -= Lb Uprev
+      cproduct(s_lb, sup, pr, pi, false);
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int r = mrow + g + ((e >> 1) << 3), c = ncol + nt * 8 + 2 * t4 + (e & 1);
+          float2& z = sb[r * kLtLd + c];
+          z.x -= pr[nt][e];
+          z.y -= pi[nt][e];
+        }
+      __syncthreads();
+    }
+    cproduct(s_inv, sb, pr, pi, true);  // U12 = L11^-1 B
+    __syncthreads();                     // every warp has read the tile
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int r = mrow + g + ((e >> 1) << 3), c = ncol + nt * 8 + 2 * t4 + (e & 1);
+        sb[r * kLtLd + c] = make_float2(pr[nt][e], pi[nt][e]);
+      }
+    {  // displaced rows get the rows they replaced (all reads of them came first)
+      const int i = tid & 63, cg = tid >> 6;
+#pragma unroll
+      for (int u = 0; u < 16; ++u) {
+        const int c = cg + 4 * u;
+        if (i < nx && c < tw) A[(size_t)(cbase + c) * lda + s_xd[i]] = xv[u];
+      }
+    }
+    __syncthreads();
+    {  // U12 to A (rows k..k+w-1) and packed K-major TF32 rows
+      const int i = tid & 63, cg = tid >> 6;
+#pragma unroll 4
+      for (int u = 0; u < 16; ++u) {
+        const int c = cg + 4 * u;
+        if (c >= tw) continue;
+        const float2 z = sb[i * kLtLd + c];
+        if (i < w) A[(size_t)(cbase + c) * lda + k + i] = z;
+        if (ure) {
+          const size_t row = ((size_t)prob * urows + (cbase + c - ubase)) * kTcKPitch + koff;
+          ure[row + i] = __uint_as_float(to_tf32(i < w ? z.x : 0.f));
+          uim[row + i] = __uint_as_float(to_tf32(i < w ? z.y : 0.f));
+        }
+      }
+    }
+    __syncthreads();  // this stage is refilled two tiles on
+  }
+  cp_async_wait<0>();
+}
+// ---------------------------------------------------------------------------
+// Trailing update C -= L21 U12 on the tensor cores, complex as 4 real products.
+// C: rows [r0, nn), cols [c0, ncols) of problem blockIdx.z; L21 = columns
+// k..k+w-1 of the same rows; U12 = rows k..k+w-1 of the same columns.
+// ---------------------------------------------------------------------------
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                : "+d"(d0), "+d"(d1)
@@ -3160,6 +3408,26 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     ProfScope ps(ctx, 2, 0.0, 2.0 * (double)cols * (2 * w) * es * batch);
     float* ure = tc ? ctx->tc.ure : nullptr;
     float* uim = tc ? ctx->tc.uim : nullptr;
+    if (sizeof(R) == 4 && ctx->laswp_tc) {
+      // one CTA per SM (registers; shared memory for three or six 64 x 64 tiles)
+      const int ntiles = (cols + 63) / 64;
+      const int per = std::max(1, ctx->num_sms / batch);
+      const int tb = std::min(ntiles, per);
+      const size_t sm = (pre ? 6 : 3) * kLtTile;
+      float2* A2 = static_cast<float2*>(A);
+      if (pre) {
+        BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_laswp_tc<true><<<dim3(tb, batch), 256, sm, ctx->stream>>>(A2, lda, bstride, k, w, c0, ncols, perm_p,
+                                                                     kPermStride, ure, uim, nn + 1, ubase, koff, kprev);
+      } else {
+        BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_laswp_tc<false><<<dim3(tb, batch), 256, sm, ctx->stream>>>(A2, lda, bstride, k, w, c0, ncols, perm_p,
+                                                                      kPermStride, ure, uim, nn + 1, ubase, koff, kprev);
+      }
+      ctx->launches++;
+      BEM_CUDA(ctx, cudaGetLastError());
+      return BEM_OK;
+    }
     if (pre)
       k_laswp_trsm<R, true><<<dim3(blocks, batch), 256, 2 * lsmem, ctx->stream>>>(
           A, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kprev);
