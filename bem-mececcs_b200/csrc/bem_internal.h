@@ -94,6 +94,8 @@ struct LuWork {
   unsigned* trsv_ctr = nullptr;  // [kMaxBatch] group barrier counters
   int* pstart = nullptr;         // first row of each panel of the last factorisation, then nn
                                  // (written by the panel kernels)
+  float2* linv = nullptr;        // [batch][64][64] L11^-1 of the current FP32 panel (k_laswp_tc)
+  size_t linv_bytes = 0;
   float2* tinv = nullptr;        // FP32 solves: inverted diagonal blocks of the last factors
   size_t tinv_bytes = 0;
   bool tinv_valid = false;

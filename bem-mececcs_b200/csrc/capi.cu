@@ -172,6 +172,7 @@ int bem_ctx_destroy(bem_ctx* ctx) {
   cudaFree(L.barrier);
   cudaFree(L.trsv_w);
   cudaFree(L.tinv);
+  cudaFree(L.linv);
   cudaFree(L.trsv_ctr);
   cudaFree(L.pstart);
   for (bem_ctx* w : ctx->workers) bem_ctx_destroy(w);

@@ -1845,8 +1845,8 @@ __global__ void __launch_bounds__(256) k_laswp_trsm(void* Av, size_t lda, size_t
 
 // ---------------------------------------------------------------------------
 // k_laswp_tc: k_laswp_trsm for the FP32 factors on the tensor cores.  Each
-// CTA first inverts the panel's unit-lower L11 in shared memory (by 16 x 16
-// blocks), then loops over 64-column tiles of [c0, ncols): the tile's
+// CTA first loads L11^-1 (k_l11_inv, once per panel), then loops over
+// 64-column tiles of [c0, ncols): the tile's
 // panel rows are gathered (the panel's interchanges), the displaced rows are
 // copied down, PRE subtracts the previous panel's deferred product Lb Uprev,
 // and U12 = L11^-1 B; both products as TF32 mma.sync (FP32 accumulation,
@@ -1873,31 +1873,19 @@ __device__ __forceinline__ void cp_async_wait() {
 constexpr int kLtLd = 68;  // complex pitch of the 64 x 64 shared tiles (conflict-free fragment loads)
 constexpr size_t kLtTile = (size_t)64 * kLtLd * sizeof(float2);
 
-template <bool PRE>
-__global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, size_t bstride, int k, int w, int c0,
-                                                     int ncols, const int* __restrict__ perm, int perm_stride,
-                                                     float* ure, float* uim, int urows, int ubase, int koff,
-                                                     int kprev) {
+// L11^-1 of the panel at (k, k) (unit lower, w x w, zero-padded to 64 x 64)
+// for k_laswp_tc, once per panel and problem (one CTA each): by 16 x 16
+// diagonal blocks (a warp each, lane = column), then [[X11, 0], [X21, X22]]
+// with X21 = -X22 L21 X11 at 16 and at 32; the zero block above the diagonal
+// (rows 0-31, columns 32-63) holds the intermediate L21 X11.  Row-major
+// [64][64] per problem.
+__global__ void __launch_bounds__(256) k_l11_inv(const float2* __restrict__ Abase, size_t lda, size_t bstride, int k,
+                                                 int w, float2* out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* s_inv = reinterpret_cast<float2*>(smem_raw);  // [64][kLtLd] L11^-1, row-major
-  float2* s_bb = s_inv + 64 * kLtLd;                     // [2][64][kLtLd] tiles (panel rows x columns), two stages
-  float2* s_lb = s_bb + 2 * 64 * kLtLd;                  // PRE: previous panel's L at this panel's rows
-  float2* s_upb = s_lb + 64 * kLtLd;                     // PRE: [2][64][kLtLd] previous panel's U rows of the tiles
-  float2* s_b = s_bb;                                    // L11 while inverting
-  __shared__ int s_src[64];                              // source row of panel row i
-  __shared__ int s_xd[64], s_xs[64];                     // displaced rows: dst <- src
-  __shared__ int s_nx;
-  const int prob = blockIdx.y, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  float2* A = Abase + (size_t)prob * bstride;
-  const int* pl = perm + (size_t)prob * perm_stride;
-  const int count = pl[0];
-  if (tid < 64) s_src[tid] = tid < w ? pl[2 + 2 * tid] : 0;
-  if (tid < 64) {
-    const int e = w + tid;
-    s_xd[tid] = e < count ? pl[1 + 2 * e] : -1;
-    s_xs[tid] = e < count ? pl[2 + 2 * e] : 0;
-  }
-  if (tid == 0) s_nx = max(0, count - w);
+  float2* s_inv = reinterpret_cast<float2*>(smem_raw);  // [64][kLtLd]
+  float2* s_b = s_inv + 64 * kLtLd;                      // [64][kLtLd] L11
+  const int prob = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const float2* A = Abase + (size_t)prob * bstride;
   // L11 (unit lower, w x w at (k, k)) into s_b, row-major; s_inv = I.
   for (int idx = tid; idx < 64 * 64; idx += blockDim.x) {
     const int i = idx & 63, c = idx >> 6;
@@ -1954,13 +1942,50 @@ __global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, 
     __syncthreads();
   }
   for (int idx = tid; idx < 32 * 32; idx += blockDim.x) at(s_inv, idx >> 5, 32 + (idx & 31)) = make_float2(0.f, 0.f);
+  __syncthreads();
+  float2* o = out + (size_t)prob * 64 * 64;
+  for (int idx = tid; idx < 64 * 64; idx += blockDim.x) o[idx] = s_inv[(idx >> 6) * kLtLd + (idx & 63)];
+}
+
+template <bool PRE>
+__global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, size_t bstride, int k, int w, int c0,
+                                                     int ncols, const int* __restrict__ perm, int perm_stride,
+                                                     float* ure, float* uim, int urows, int ubase, int koff,
+                                                     int kprev, const float2* __restrict__ linv) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* s_inv = reinterpret_cast<float2*>(smem_raw);  // [64][kLtLd] L11^-1, row-major
+  float2* s_bb = s_inv + 64 * kLtLd;                     // [2][64][kLtLd] tiles (panel rows x columns), two stages
+  float2* s_lb = s_bb + 2 * 64 * kLtLd;                  // PRE: previous panel's L at this panel's rows
+  float2* s_upb = s_lb + 64 * kLtLd;                     // PRE: [2][64][kLtLd] previous panel's U rows of the tiles
+  __shared__ int s_src[64];                              // source row of panel row i
+  __shared__ int s_xd[64], s_xs[64];                     // displaced rows: dst <- src
+  __shared__ int s_nx;
+  const int prob = blockIdx.y, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  float2* A = Abase + (size_t)prob * bstride;
+  const int* pl = perm + (size_t)prob * perm_stride;
+  const int count = pl[0];
+  if (tid < 64) s_src[tid] = tid < w ? pl[2 + 2 * tid] : 0;
+  if (tid < 64) {
+    const int e = w + tid;
+    s_xd[tid] = e < count ? pl[1 + 2 * e] : -1;
+    s_xs[tid] = e < count ? pl[2 + 2 * e] : 0;
+  }
+  if (tid == 0) s_nx = max(0, count - w);
+  // L11^-1 (k_l11_inv) into s_inv by cp.async
+  {
+    const float2* li = linv + (size_t)prob * 64 * 64;
+    for (int idx = tid; idx < 64 * 64; idx += blockDim.x)
+      cp_async8(&s_inv[(idx >> 6) * kLtLd + (idx & 63)], &li[idx], true);
+    cp_async_commit();
+  }
+  __syncthreads();  // s_src
   if (PRE) {  // Lb(i, t) = L(src(k + i), kprev + t)
     for (int idx = tid; idx < 64 * 64; idx += blockDim.x) {
       const int i = idx & 63, t = idx >> 6;
-      s_lb[i * kLtLd + t] = i < w ? A[(size_t)(kprev + t) * lda + s_src[i]] : make_float2(0.f, 0.f);
+      cp_async8(&s_lb[i * kLtLd + t], i < w ? &A[(size_t)(kprev + t) * lda + s_src[i]] : A, i < w);
     }
   }
-  __syncthreads();
+  cp_async_commit();
 
   // warp tile: rows [16 * (warp & 3), +16) x columns [32 * (warp >> 2), +32)
   const int g = lane >> 2, t4 = lane & 3, mrow = 16 * (warp & 3), ncol = 32 * (warp >> 2);
@@ -3415,14 +3440,26 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
       const int tb = std::min(ntiles, per);
       const size_t sm = (pre ? 6 : 3) * kLtTile;
       float2* A2 = static_cast<float2*>(A);
+      LuWork& LW = ctx->lu;
+      const size_t lbytes = (size_t)batch * 64 * 64 * sizeof(float2);
+      if (LW.linv_bytes < lbytes) {
+        cudaFree(LW.linv);
+        LW.linv = nullptr;
+        LW.linv_bytes = 0;
+        BEM_CUDA(ctx, cudaMalloc(&LW.linv, lbytes));
+        LW.linv_bytes = lbytes;
+      }
+      BEM_CUDA(ctx, cudaFuncSetAttribute(k_l11_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * kLtTile)));
+      k_l11_inv<<<batch, 256, 2 * kLtTile, ctx->stream>>>(A2, lda, bstride, k, w, LW.linv);
+      ctx->launches++;
       if (pre) {
         BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_laswp_tc<true><<<dim3(tb, batch), 256, sm, ctx->stream>>>(A2, lda, bstride, k, w, c0, ncols, perm_p,
-                                                                     kPermStride, ure, uim, nn + 1, ubase, koff, kprev);
+        k_laswp_tc<true><<<dim3(tb, batch), 256, sm, ctx->stream>>>(
+            A2, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kprev, LW.linv);
       } else {
         BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_laswp_tc<false><<<dim3(tb, batch), 256, sm, ctx->stream>>>(A2, lda, bstride, k, w, c0, ncols, perm_p,
-                                                                      kPermStride, ure, uim, nn + 1, ubase, koff, kprev);
+        k_laswp_tc<false><<<dim3(tb, batch), 256, sm, ctx->stream>>>(
+            A2, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kprev, LW.linv);
       }
       ctx->launches++;
       BEM_CUDA(ctx, cudaGetLastError());
