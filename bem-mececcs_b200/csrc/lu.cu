@@ -1876,10 +1876,10 @@ constexpr size_t kLtTile = (size_t)64 * kLtLd * sizeof(float2);
 // L11^-1 of the panel at (k, k) (unit lower, w x w, zero-padded to 64 x 64)
 // for k_laswp_tc, once per panel and problem (one CTA each): by 16 x 16
 // diagonal blocks (a warp each, lane = column), then [[X11, 0], [X21, X22]]
-// with X21 = -X22 L21 X11 at 16 and at 32; the zero block above the diagonal
-// (rows 0-31, columns 32-63) holds the intermediate L21 X11.  Row-major
-// [64][64] per problem.
-__global__ void __launch_bounds__(256) k_l11_inv(const float2* __restrict__ Abase, size_t lda, size_t bstride, int k,
+// with X21 = -X22 L21 X11 at 16 and at 32 (one output per thread of 1024);
+// the zero block above the diagonal (rows 0-31, columns 32-63) holds the
+// intermediate L21 X11.  Row-major [64][64] per problem.
+__global__ void __launch_bounds__(1024) k_l11_inv(const float2* __restrict__ Abase, size_t lda, size_t bstride, int k,
                                                  int w, float2* out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* s_inv = reinterpret_cast<float2*>(smem_raw);  // [64][kLtLd]
@@ -3450,7 +3450,7 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
         LW.linv_bytes = lbytes;
       }
       BEM_CUDA(ctx, cudaFuncSetAttribute(k_l11_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * kLtTile)));
-      k_l11_inv<<<batch, 256, 2 * kLtTile, ctx->stream>>>(A2, lda, bstride, k, w, LW.linv);
+      k_l11_inv<<<batch, 1024, 2 * kLtTile, ctx->stream>>>(A2, lda, bstride, k, w, LW.linv);
       ctx->launches++;
       if (pre) {
         BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));

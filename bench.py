@@ -521,16 +521,17 @@ def _peaks():
 
 KERNELS = {
     "assembly": "k_dyn_diag + k_dyn_offdiag + k_rhs_reduce (FP64 Stokes assembly, BC swap, RHS)",
-    "panel": "k_panel_cluster (LU panel, one 16-CTA cluster per problem, DSMEM pivoting)",
-    "laswp_trsm": "k_laswp_trsm (row interchanges + U12 triangular solve, FP32)",
+    "panel": "k_panel_push (LU panel, one 16-CTA cluster per problem; pivot candidates pushed by remote "
+             "stores before one cluster barrier per column)",
+    "laswp_trsm": "k_l11_inv + k_laswp_tc (row interchanges + U12 = L11^-1 A12 on TF32 tensor cores, FP32)",
     "gemm": "k_pack_l21 + k_gemm_tc (FP32 LU trailing update, tcgen05 kind::tf32, K = 128, TMA reduce-add)",
-    "solves": "k_trsv (cooperative forward + back substitution)",
+    "solves": "k_tri_inv + k_trsv_f32 (cooperative forward + back substitution with inverted diagonal blocks)",
     "residual": "k_resid_partial + k_resid_final (FP64 refinement residual)",
 }
 NOTES = {
-    "panel": "latency bound: a CTA barrier, a cluster barrier and one DSMEM round per column",
-    "solves": "latency bound: one group barrier per 64-row step",
-    "laswp_trsm": "FP32 SIMT issue bound (the 64-step substitution per column)",
+    "panel": "latency bound: a CTA barrier and a cluster barrier (remote-store mailboxes) per column",
+    "solves": "latency bound: one split group barrier per 64-row step, the next step's rows loading meanwhile",
+    "laswp_trsm": "latency bound: per 64-column tile a gather, two tensor-core products and the stores",
     "assembly": "FP64-pipe bound (two complex exponentials per Gauss point); bytes are the systems written",
 }
 
@@ -551,7 +552,7 @@ def _roofline(name, k, peaks, mpeaks):
     if name == "gemm":
         tf = k["work"] / secs / 1e12
         peak = mpeaks["tf32_umma_n128"]
-        out["traffic_note"] = ("ncu, one K = 64 launch of 2 problems: dram read+write = 1.15 x the algorithmic "
+        out["traffic_note"] = ("ncu, one K = 128 launch of 2 problems: dram read+write = 1.03 x the algorithmic "
                                "C bytes (profiles/k_gemm_tc_2160.md)")
         out["tensor"] = {"achieved_tflops": round(tf, 2), "peak_tflops": round(peak, 1),
                          "frac": round(tf / peak, 4),
