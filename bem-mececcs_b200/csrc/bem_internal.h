@@ -96,12 +96,15 @@ struct LuWork {
                                  // (written by the panel kernels)
   float2* linv = nullptr;        // [batch][64][64] L11^-1 of the current FP32 panel (k_laswp_tc)
   size_t linv_bytes = 0;
+  int* gmap = nullptr;           // [batch][kGroupMaps][nn] row maps of a panel group (k_l11_inv)
+  size_t gmap_bytes = 0;
   float2* tinv = nullptr;        // FP32 solves: inverted diagonal blocks of the last factors
   size_t tinv_bytes = 0;
   bool tinv_valid = false;
 };
 
 constexpr int kMaxGrid = 160;
+constexpr int kGroupMaps = 3;  // row maps of the first three panels of a four-panel group
 
 // Packed operands of the tensor-core FP32 trailing update (gemm_tc.cu).
 struct TcWork {
@@ -197,6 +200,7 @@ struct bem_ctx {
   bool panel_calu = false;    // FP32 LU panels: tournament pivoting per 8-column sub-panel
   bool panel_push = true;     // cluster panels exchange pivots by remote stores before the barrier
   bool lu_pairs = true;       // FP32 tensor-core LU: two 64-column panels per trailing update (K = 128)
+  bool lu_quads = true;       // ... four (K = 256) where four 64-column panels fit
   // SM shares for contexts that run concurrently on one GPU (0: the whole device)
   int gemm_ctas = 0;          // CTAs of the persistent tensor-core trailing update
   int trsv_ctas = 0;          // CTAs of one cooperative triangular solve (all problems together)
@@ -273,10 +277,10 @@ int tc_ensure(bem_ctx* ctx, int nn, int batch);
 void tc_release(bem_ctx* ctx);
 int tc_trailing_update(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int k, int w, int batch);
 int tc_pack_l(bem_ctx* ctx, const float2* A, size_t lda, size_t bstride, int nn, int kcol, int kw, int r0, int koff,
-              int batch, const int* gperm, int gstride);
+              int batch, const int* gmap, size_t gstride);
 int tc_gemm(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int r0, int c0, int cend, int kw,
-            int urow_off, int batch);
-constexpr int kTcKPitch = 128;  // floats per packed tensor-core operand row
+            int urow_off, int batch, int kbase);
+constexpr int kTcKPitch = 256;  // floats per packed tensor-core operand row
 int measure_fp64_peak(bem_ctx* ctx, double* tflops);
 int measure_fma_peaks(bem_ctx* ctx, double* fp64_tflops, double* fp32_tflops);
 int measure_tf32_peak(bem_ctx* ctx, int n, double* tflops);

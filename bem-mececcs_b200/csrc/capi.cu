@@ -146,6 +146,7 @@ int bem_ctx_create(int device, bem_ctx** out) {
   if (const char* env = getenv("BEM_PANEL_PUSH")) ctx->panel_push = env[0] != '0';
   if (const char* env = getenv("BEM_TRSV_INV")) ctx->trsv_inv = env[0] != '0';
   if (const char* env = getenv("BEM_LASWP_TC")) ctx->laswp_tc = env[0] != '0';
+  if (const char* env = getenv("BEM_LU_QUADS")) ctx->lu_quads = env[0] != '0';
   *out = ctx;
   return BEM_OK;
 }
@@ -173,6 +174,7 @@ int bem_ctx_destroy(bem_ctx* ctx) {
   cudaFree(L.trsv_w);
   cudaFree(L.tinv);
   cudaFree(L.linv);
+  cudaFree(L.gmap);
   cudaFree(L.trsv_ctr);
   cudaFree(L.pstart);
   for (bem_ctx* w : ctx->workers) bem_ctx_destroy(w);
@@ -538,6 +540,7 @@ static bool* option_slot(bem_ctx* ctx, const char* name) {
   if (!strcmp(name, "trsv_inv")) return &ctx->trsv_inv;
   if (!strcmp(name, "laswp_tc")) return &ctx->laswp_tc;
   if (!strcmp(name, "lu_pairs")) return &ctx->lu_pairs;
+  if (!strcmp(name, "lu_quads")) return &ctx->lu_quads;
   if (!strcmp(name, "panel_calu")) return &ctx->panel_calu;
   if (!strcmp(name, "panel_push")) return &ctx->panel_push;
   if (!strcmp(name, "graphs")) return &ctx->use_graphs;

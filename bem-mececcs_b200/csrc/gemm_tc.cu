@@ -44,7 +44,7 @@ constexpr int kStages = 3;
 constexpr uint32_t kHalfBytes = 128 * 64 * 4;  // C staging: 64 complex rows x 64 columns = 32 KB
 constexpr uint32_t kTmemCols = 512;
 constexpr int kPrefetch = 3;  // C tiles prefetched into L2 ahead of the current one
-constexpr int kKPitch = 128;  // floats per packed operand row: K up to 128 (two 64-column panels)
+constexpr int kKPitch = 256;  // floats per packed operand row: K up to 256 (four 64-column panels)
 constexpr size_t kTcSmem = (size_t)kStages * kStageBytes + 2 * kHalfBytes + 1024;
 
 __device__ __forceinline__ uint32_t idesc_tf32_128x128() {
@@ -125,6 +125,7 @@ struct TcArgs {
   float2* A;        // the systems (complex64), problem b at A + b*bstride
   size_t lda, bstride;
   int nn, r0, c0, ncols, kw;
+  int kbase;  // first K slot of the packed operands (a panel's own slot for a narrow update)
   int cend;         // columns >= cend are left unchanged
   int urow_off;     // packed U row of column c0
   int mtiles, ntiles, batch;
@@ -209,9 +210,9 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
         }
         unsigned char* st = ring + (size_t)s * kStageBytes;
         mbar_expect_tx(&full[s], kStageBytes);
-        tma_load_2d(st, &tm_l, 32 * h, ly, &full[s]);
-        tma_load_2d(st + kChunk, &tm_ure, 32 * h, uy, &full[s]);
-        tma_load_2d(st + 2 * kChunk, &tm_uim, 32 * h, uy, &full[s]);
+        tma_load_2d(st, &tm_l, a.kbase + 32 * h, ly, &full[s]);
+        tma_load_2d(st + kChunk, &tm_ure, a.kbase + 32 * h, uy, &full[s]);
+        tma_load_2d(st + 2 * kChunk, &tm_uim, a.kbase + 32 * h, uy, &full[s]);
         if (++s == kStages) {
           s = 0;
           ph ^= 1u;
@@ -314,24 +315,19 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
 // later panel's row order; A itself is not changed.
 __global__ void __launch_bounds__(256) k_pack_l21(const float2* __restrict__ A, size_t lda, size_t bstride, int nn,
                                                   int k, int kw, int r0, int koff, float* lhat, int lrows,
-                                                  const int* __restrict__ gperm, int gstride) {
+                                                  const int* __restrict__ gmap, size_t gstride) {
   __shared__ float2 tile[64][33];
   __shared__ int s_src[32];
   const int b = blockIdx.y;
   const float2* Ap = A + (size_t)b * bstride;
   const int rbase = r0 + blockIdx.x * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 8 x 32
-  if (threadIdx.x < 32) s_src[threadIdx.x] = rbase + threadIdx.x;
-  __syncthreads();
-  if (gperm) {
-    const int* pl = gperm + (size_t)b * gstride;
-    const int count = pl[0];
-    for (int e = threadIdx.x; e < count; e += blockDim.x) {
-      const int dst = pl[1 + 2 * e];
-      if (dst >= rbase && dst < rbase + 32) s_src[dst - rbase] = pl[2 + 2 * e];
-    }
-    __syncthreads();
+  if (threadIdx.x < 32) {
+    const int r = rbase + threadIdx.x;
+    // the row of L's storage that is row r now (a row map of a panel group), or r
+    s_src[threadIdx.x] = (gmap && r < nn) ? gmap[(size_t)b * gstride + r] : r;
   }
+  __syncthreads();
   const int src = s_src[tx];
   for (int c = ty; c < 64; c += 8) {
     const int r = rbase + tx;
@@ -510,12 +506,13 @@ void tc_release(bem_ctx* ctx) {
 }
 
 // Packs L (columns kcol..kcol+kw-1, rows r0..nn-1) into K slots
-// koff..koff+kw-1 of Lhat, optionally through a gather list.
+// koff..koff+kw-1 of Lhat, optionally through a row map (problem b's map at
+// gmap + b * gstride: the storage row of L that is row r now).
 int tc_pack_l(bem_ctx* ctx, const float2* A, size_t lda, size_t bstride, int nn, int kcol, int kw, int r0, int koff,
-              int batch, const int* gperm, int gstride) {
+              int batch, const int* gmap, size_t gstride) {
   if (r0 >= nn) return BEM_OK;
   k_pack_l21<<<dim3((nn - r0 + 31) / 32, batch), 256, 0, ctx->stream>>>(A, lda, bstride, nn, kcol, kw, r0, koff,
-                                                                        ctx->tc.lhat, 2 * nn, gperm, gstride);
+                                                                        ctx->tc.lhat, 2 * nn, gmap, gstride);
   ctx->launches++;
   BEM_CUDA(ctx, cudaGetLastError());
   return BEM_OK;
@@ -524,7 +521,7 @@ int tc_pack_l(bem_ctx* ctx, const float2* A, size_t lda, size_t bstride, int nn,
 // C -= Lhat U for rows [r0, nn) and columns [c0, cend) of `batch` FP32
 // systems, K = kw (packed Lhat and U_re/U_im; U row urow_off + (c - c0)).
 int tc_gemm(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int r0, int c0, int cend, int kw,
-            int urow_off, int batch) {
+            int urow_off, int batch, int kbase) {
   TcWork& W = ctx->tc;
   const int ncols = nn + 1;
   if (r0 >= nn || c0 >= cend) return BEM_OK;
@@ -546,6 +543,7 @@ int tc_gemm(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int r0,
   t.c0 = c0;
   t.ncols = ncols;
   t.kw = kw;
+  t.kbase = kbase;
   t.cend = cend;
   t.urow_off = urow_off;
   t.mtiles = (nn - r0 + kTcRows - 1) / kTcRows;
@@ -569,7 +567,7 @@ int tc_trailing_update(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int 
   if (r0 >= nn) return BEM_OK;
   int rc = tc_pack_l(ctx, A, lda, bstride, nn, k, w, r0, 0, batch, nullptr, 0);
   if (rc) return rc;
-  return tc_gemm(ctx, A, lda, bstride, nn, r0, r0, nn + 1, w, 0, batch);
+  return tc_gemm(ctx, A, lda, bstride, nn, r0, r0, nn + 1, w, 0, batch, 0);
 }
 
 }  // namespace bem

@@ -1879,13 +1879,34 @@ constexpr size_t kLtTile = (size_t)64 * kLtLd * sizeof(float2);
 // with X21 = -X22 L21 X11 at 16 and at 32 (one output per thread of 1024);
 // the zero block above the diagonal (rows 0-31, columns 32-63) holds the
 // intermediate L21 X11.  Row-major [64][64] per problem.
+// In a group of gsize panels (panel gi of it, gi >= 0), it also keeps the
+// group's row maps: map j (of the group's panel j < gsize - 1) gives, for a
+// position x now, the position the row held after panel j (where L of panel
+// j stores it). Panel gi replays its interchanges on maps j < gi and starts
+// map gi as the identity below its rows.
 __global__ void __launch_bounds__(1024) k_l11_inv(const float2* __restrict__ Abase, size_t lda, size_t bstride, int k,
-                                                 int w, float2* out) {
+                                                  int w, float2* out, const int* __restrict__ perm, int perm_stride,
+                                                  int* gmap, int nn, int gi, int gsize) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* s_inv = reinterpret_cast<float2*>(smem_raw);  // [64][kLtLd]
   float2* s_b = s_inv + 64 * kLtLd;                      // [64][kLtLd] L11
   const int prob = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const float2* A = Abase + (size_t)prob * bstride;
+  if (gi >= 0) {
+    int* gm = gmap + (size_t)prob * kGroupMaps * nn;
+    const int* pl = perm + (size_t)prob * perm_stride;
+    const int count = pl[0];
+    const int j = tid >> 7, e = tid & 127;  // map j, entry e (at most 128 entries, 3 maps)
+    int val = 0, dst = -1;
+    if (j < gi && j < kGroupMaps && e < count) {
+      val = gm[(size_t)j * nn + pl[2 + 2 * e]];
+      dst = pl[1 + 2 * e];
+    }
+    __syncthreads();  // every read before any write
+    if (dst >= 0) gm[(size_t)j * nn + dst] = val;
+    if (gi < gsize - 1 && gi < kGroupMaps)
+      for (int x = k + w + tid; x < nn; x += blockDim.x) gm[(size_t)gi * nn + x] = x;
+  }
   // L11 (unit lower, w x w at (k, k)) into s_b, row-major; s_inv = I.
   for (int idx = tid; idx < 64 * 64; idx += blockDim.x) {
     const int i = idx & 63, c = idx >> 6;
@@ -1951,12 +1972,13 @@ template <bool PRE>
 __global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, size_t bstride, int k, int w, int c0,
                                                      int ncols, const int* __restrict__ perm, int perm_stride,
                                                      float* ure, float* uim, int urows, int ubase, int koff,
-                                                     int kprev, const float2* __restrict__ linv) {
+                                                     int kfirst, int nprev, int cdefer, const int* __restrict__ gmap,
+                                                     int nn, const float2* __restrict__ linv) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* s_inv = reinterpret_cast<float2*>(smem_raw);  // [64][kLtLd] L11^-1, row-major
   float2* s_bb = s_inv + 64 * kLtLd;                     // [2][64][kLtLd] tiles (panel rows x columns), two stages
-  float2* s_lb = s_bb + 2 * 64 * kLtLd;                  // PRE: previous panel's L at this panel's rows
-  float2* s_upb = s_lb + 64 * kLtLd;                     // PRE: [2][64][kLtLd] previous panel's U rows of the tiles
+  float2* s_lb = s_bb + 2 * 64 * kLtLd;                  // PRE: an earlier panel's L at this panel's rows
+  float2* s_up = s_lb + 64 * kLtLd;                      // PRE: that panel's U rows of the tile
   __shared__ int s_src[64];                              // source row of panel row i
   __shared__ int s_xd[64], s_xs[64];                     // displaced rows: dst <- src
   __shared__ int s_nx;
@@ -1979,24 +2001,31 @@ __global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, 
     cp_async_commit();
   }
   __syncthreads();  // s_src
-  if (PRE) {  // Lb(i, t) = L(src(k + i), kprev + t)
+  // Lb_j(i, t) = L(map_j(k + i), kfirst + 64 j + t): earlier panel j's L at this panel's rows
+  const int* gm = gmap + (size_t)prob * kGroupMaps * nn;
+  auto load_lb = [&](int j) {
     for (int idx = tid; idx < 64 * 64; idx += blockDim.x) {
       const int i = idx & 63, t = idx >> 6;
-      cp_async8(&s_lb[i * kLtLd + t], i < w ? &A[(size_t)(kprev + t) * lda + s_src[i]] : A, i < w);
+      const bool ok = i < w;
+      cp_async8(&s_lb[i * kLtLd + t], ok ? &A[(size_t)(kfirst + 64 * j + t) * lda + gm[(size_t)j * nn + k + i]] : A,
+                ok);
     }
-  }
+  };
+  if (PRE && nprev == 1) load_lb(0);  // one earlier panel: its Lb serves every tile
   cp_async_commit();
 
   // warp tile: rows [16 * (warp & 3), +16) x columns [32 * (warp >> 2), +32)
   const int g = lane >> 2, t4 = lane & 3, mrow = 16 * (warp & 3), ncol = 32 * (warp >> 2);
-  // acc = M B for this warp's tile, M (64 x 64) and B (64 x 64) complex in
+  // acc += M B for this warp's tile, M (64 x 64) and B (64 x 64) complex in
   // shared memory; split: each operand as a TF32 pair hi + lo and three
   // products per real product (hi hi + hi lo + lo hi), about FP32 accuracy.
-  auto cproduct = [&](const float2* M, const float2* Bm, float (&pr)[4][4], float (&pi)[4][4], bool split) {
+  auto zero_acc = [&](float (&pr)[4][4], float (&pi)[4][4]) {
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt)
 #pragma unroll
       for (int e = 0; e < 4; ++e) pr[nt][e] = pi[nt][e] = 0.f;
+  };
+  auto cproduct = [&](const float2* M, const float2* Bm, float (&pr)[4][4], float (&pi)[4][4], bool split) {
 #pragma unroll 2
     for (int ks = 0; ks < 8; ++ks) {
       const int kc = ks * 8 + t4;
@@ -2041,20 +2070,18 @@ __global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, 
   };
 
   const int ntiles = (ncols - c0 + 63) / 64;
-  // A tile's inputs into stage st by cp.async (8-byte elements, zero-filled
-  // outside the panel rows and past the last column): one commit group.
+  // A tile's gathered panel rows into stage st by cp.async (8-byte elements,
+  // zero-filled outside the panel rows and past the last column).
   auto issue = [&](int tile, int st) {
     if (tile < ntiles) {
       const int cbase = c0 + tile * 64, tw = min(64, ncols - cbase);
       float2* b = s_bb + (size_t)st * 64 * kLtLd;
-      float2* up = s_upb + (size_t)st * 64 * kLtLd;
       const int i = tid & 63, cg = tid >> 6;
 #pragma unroll
       for (int u = 0; u < 16; ++u) {
         const int c = cg + 4 * u;
         const bool ok = c < tw && i < w;
         cp_async8(&b[i * kLtLd + c], ok ? &A[(size_t)(cbase + c) * lda + s_src[i]] : A, ok);
-        if (PRE) cp_async8(&up[i * kLtLd + c], c < tw ? &A[(size_t)(cbase + c) * lda + kprev + i] : A, c < tw);
       }
     }
     cp_async_commit();
@@ -2066,9 +2093,7 @@ __global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, 
     const int st = it & 1;
     const int cbase = c0 + tile * 64, tw = min(64, ncols - cbase);
     float2* sb = s_bb + (size_t)st * 64 * kLtLd;
-    float2* sup = s_upb + (size_t)st * 64 * kLtLd;
-    issue(tile + gridDim.x, st ^ 1);  // the next tile streams in meanwhile
-    cp_async_wait<1>();
+    cp_async_wait<0>();
     __syncthreads();
     // displaced rows: their sources, loaded now and stored after the products
     float2 xv[16];
@@ -2082,8 +2107,22 @@ __global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, 
       }
     }
     float pr[4][4], pi[4][4];
-    if (PRE) {  // B -= Lb Uprev
-      cproduct(s_lb, sup, pr, pi, false);
+    if (PRE && cbase >= cdefer) {  // B -= sum_j Lb_j Uprev_j: the group's deferred update of these rows
+      zero_acc(pr, pi);
+      for (int j = 0; j < nprev; ++j) {
+        if (nprev > 1) load_lb(j);
+        const int i = tid & 63, cg = tid >> 6;
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+          const int c = cg + 4 * u;
+          cp_async8(&s_up[i * kLtLd + c], c < tw ? &A[(size_t)(cbase + c) * lda + kfirst + 64 * j + i] : A, c < tw);
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        cproduct(s_lb, s_up, pr, pi, false);
+        __syncthreads();  // s_lb, s_up reloaded for the next panel
+      }
 #pragma unroll
       for (int nt = 0; nt < 4; ++nt)
 #pragma unroll
@@ -2095,6 +2134,8 @@ __global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, 
         }
       __syncthreads();
     }
+    issue(tile + gridDim.x, st ^ 1);  // the next tile streams in meanwhile
+    zero_acc(pr, pi);
     cproduct(s_inv, sb, pr, pi, true);  // U12 = L11^-1 B
     __syncthreads();                     // every warp has read the tile
 #pragma unroll
@@ -3425,92 +3466,137 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     L.panels.push_back({k, w});
     return BEM_OK;
   };
-  auto laswp = [&](bool pre, int k, int w, int c0, const int* perm_p, int ubase, int koff, int kprev) -> int {
+  // L11^-1 of the panel at k (for k_laswp_tc) and, for panel gi of a group
+  // of gsize, the group's row maps (k_l11_inv).
+  auto linv_maps = [&](int k, int w, const int* perm_p, int gi, int gsize) -> int {
+    LuWork& LW = ctx->lu;
+    const size_t lbytes = (size_t)batch * 64 * 64 * sizeof(float2);
+    if (LW.linv_bytes < lbytes) {
+      cudaFree(LW.linv);
+      LW.linv = nullptr;
+      LW.linv_bytes = 0;
+      BEM_CUDA(ctx, cudaMalloc(&LW.linv, lbytes));
+      LW.linv_bytes = lbytes;
+    }
+    const size_t mbytes = (size_t)batch * kGroupMaps * nn * sizeof(int);
+    if (LW.gmap_bytes < mbytes) {
+      cudaFree(LW.gmap);
+      LW.gmap = nullptr;
+      LW.gmap_bytes = 0;
+      BEM_CUDA(ctx, cudaMalloc(&LW.gmap, mbytes));
+      LW.gmap_bytes = mbytes;
+    }
+    BEM_CUDA(ctx, cudaFuncSetAttribute(k_l11_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * kLtTile)));
+    k_l11_inv<<<batch, 1024, 2 * kLtTile, ctx->stream>>>(static_cast<const float2*>(A), lda, bstride, k, w, LW.linv,
+                                                         perm_p, kPermStride, LW.gmap, nn, gi, gsize);
+    ctx->launches++;
+    BEM_CUDA(ctx, cudaGetLastError());
+    return BEM_OK;
+  };
+  // Interchanges + U12 of the panel at k for columns [c0, ncols), packed for
+  // the tensor cores at K slot koff (rows c - ubase).  Columns from cdefer
+  // on first take the deferred update of the nprev earlier panels of the
+  // group (at kfirst, kfirst + 64, ...); gi/gsize: the panel's place in its
+  // group (-1: none).
+  auto laswp = [&](int k, int w, int c0, const int* perm_p, int ubase, int koff, int kfirst, int nprev, int cdefer,
+                   int gi, int gsize) -> int {
     const int cols = ncols - c0;
     if (cols <= 0) return BEM_OK;
-    const int blocks = std::max(1, std::min((cols + 31) / 32, (4 * ctx->num_sms + batch - 1) / batch));
+    const bool pre = nprev > 0;
     // rows k..k+w-1 (and the displaced rows) of every column read and written once
     ProfScope ps(ctx, 2, 0.0, 2.0 * (double)cols * (2 * w) * es * batch);
     float* ure = tc ? ctx->tc.ure : nullptr;
     float* uim = tc ? ctx->tc.uim : nullptr;
     if (sizeof(R) == 4 && ctx->laswp_tc) {
-      // one CTA per SM (registers; shared memory for three or six 64 x 64 tiles)
+      int rc = linv_maps(k, w, perm_p, gi, gsize);
+      if (rc) return rc;
+      // one CTA per SM (registers; shared memory for three or five 64 x 64 tiles)
       const int ntiles = (cols + 63) / 64;
       const int per = std::max(1, ctx->num_sms / batch);
       const int tb = std::min(ntiles, per);
-      const size_t sm = (pre ? 6 : 3) * kLtTile;
+      const size_t sm = (pre ? 5 : 3) * kLtTile;
       float2* A2 = static_cast<float2*>(A);
       LuWork& LW = ctx->lu;
-      const size_t lbytes = (size_t)batch * 64 * 64 * sizeof(float2);
-      if (LW.linv_bytes < lbytes) {
-        cudaFree(LW.linv);
-        LW.linv = nullptr;
-        LW.linv_bytes = 0;
-        BEM_CUDA(ctx, cudaMalloc(&LW.linv, lbytes));
-        LW.linv_bytes = lbytes;
-      }
-      BEM_CUDA(ctx, cudaFuncSetAttribute(k_l11_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * kLtTile)));
-      k_l11_inv<<<batch, 1024, 2 * kLtTile, ctx->stream>>>(A2, lda, bstride, k, w, LW.linv);
-      ctx->launches++;
       if (pre) {
         BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_laswp_tc<true><<<dim3(tb, batch), 256, sm, ctx->stream>>>(
-            A2, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kprev, LW.linv);
+        k_laswp_tc<true><<<dim3(tb, batch), 256, sm, ctx->stream>>>(A2, lda, bstride, k, w, c0, ncols, perm_p,
+                                                                     kPermStride, ure, uim, nn + 1, ubase, koff,
+                                                                     kfirst, nprev, cdefer, LW.gmap, nn, LW.linv);
       } else {
         BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_laswp_tc<false><<<dim3(tb, batch), 256, sm, ctx->stream>>>(
-            A2, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kprev, LW.linv);
+        k_laswp_tc<false><<<dim3(tb, batch), 256, sm, ctx->stream>>>(A2, lda, bstride, k, w, c0, ncols, perm_p,
+                                                                      kPermStride, ure, uim, nn + 1, ubase, koff,
+                                                                      kfirst, 0, ncols, LW.gmap, nn, LW.linv);
       }
       ctx->launches++;
       BEM_CUDA(ctx, cudaGetLastError());
       return BEM_OK;
     }
+    if (gi >= 0 && sizeof(R) == 4) {  // the grouped packs read L through the row maps
+      int rc = linv_maps(k, w, perm_p, gi, gsize);
+      if (rc) return rc;
+    }
+    // substitution kernel: at most one earlier panel (pairs), deferred everywhere
+    const int blocks = std::max(1, std::min((cols + 31) / 32, (4 * ctx->num_sms + batch - 1) / batch));
     if (pre)
       k_laswp_trsm<R, true><<<dim3(blocks, batch), 256, 2 * lsmem, ctx->stream>>>(
-          A, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kprev);
+          A, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kfirst);
     else
       k_laswp_trsm<R, false><<<dim3(blocks, batch), 256, lsmem, ctx->stream>>>(
-          A, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kprev);
+          A, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kfirst);
     ctx->launches++;
     BEM_CUDA(ctx, cudaGetLastError());
     return BEM_OK;
   };
   for (int k = 0; k < nn;) {
     const int m = nn - k;
-    // Two 64-column panels per trailing update (K = 128) on the tensor-core
-    // path: panel 1's update reaches only the next 64 columns (panel 2) at
-    // once; for the columns right of both it is deferred and applied with
-    // panel 2's in one GEMM, with panel 1's L rows taken in panel 2's row
-    // order (its gather list) and panel 2's U rows finished by the deferred
-    // update of their own rows (k_laswp_trsm<PRE>).  A keeps the factors of
-    // the one-panel-at-a-time LU, so the solves are unchanged.
-    if (tc && ctx->lu_pairs && m > 128 && panel_nb(m) == 64 && panel_nb(m - 64) == 64) {
-      int w1 = 0, w2 = 0, *p1 = nullptr, *p2 = nullptr;
-      int rc = run_panel(k, w1, p1);
-      if (rc) return rc;
-      const int c0 = k + 64, c1 = k + 128;
-      rc = laswp(false, k, 64, c0, p1, c0, 0, 0);
-      if (rc) return rc;
-      {
-        ProfScope ps(ctx, 3, 8.0 * (double)(nn - c0) * 64.0 * 64.0 * batch,
-                     2.0 * (double)(nn - c0) * 64.0 * es * batch);
-        rc = tc_pack_l(ctx, static_cast<float2*>(A), lda, bstride, nn, k, 64, c0, 0, batch, nullptr, 0);
-        if (!rc) rc = tc_gemm(ctx, static_cast<float2*>(A), lda, bstride, nn, c0, c0, c1, 64, 0, batch);
+    // G = 2 or 4 64-column panels per trailing update (K = 64 G) on the
+    // tensor-core path.  Within the group the LU is right-looking: panel i's
+    // update of the group's remaining columns is applied at once (a narrow
+    // update).  For the columns past the group it is deferred: their rows
+    // receive the later panels' interchanges without it, each panel's U rows
+    // there first get the earlier panels' deferred update (their L read at
+    // this panel's rows through the group's row maps), and the rest is one
+    // K = 64 G update whose Lhat takes every earlier panel's L rows through
+    // its row map.  A keeps the factors of the one-panel-at-a-time LU (L in
+    // panel order), so the solves are unchanged.
+    const bool tcg = tc && sizeof(R) == 4;
+    const bool fit4 = m > 256 && panel_nb(m) == 64 && panel_nb(m - 64) == 64 && panel_nb(m - 128) == 64 &&
+                      panel_nb(m - 192) == 64;
+    const bool fit2 = m > 128 && panel_nb(m) == 64 && panel_nb(m - 64) == 64;
+    const int G = (tcg && ctx->lu_quads && ctx->laswp_tc && fit4) ? 4 : ((tcg && ctx->lu_pairs && fit2) ? 2 : 1);
+    if (G > 1) {
+      const int kG = k + 64 * G, ubase = k + 64;
+      float2* A2 = static_cast<float2*>(A);
+      for (int i = 0; i < G; ++i) {
+        const int ki = k + 64 * i;
+        int wi = 0, *pi = nullptr;
+        int rc = run_panel(ki, wi, pi);
+        if (rc) return rc;
+        rc = laswp(ki, 64, ki + 64, pi, ubase, 64 * i, k, i, kG, i, G);
+        if (rc) return rc;
+        if (i < G - 1) {  // panel i's update of the group's remaining columns
+          const int r0 = ki + 64;
+          ProfScope ps(ctx, 3, 8.0 * (double)(nn - r0) * (double)(kG - r0) * 64.0 * batch,
+                       2.0 * (double)(nn - r0) * (double)(kG - r0) * es * batch);
+          rc = tc_pack_l(ctx, A2, lda, bstride, nn, ki, 64, r0, 64 * i, batch, nullptr, 0);
+          if (!rc) rc = tc_gemm(ctx, A2, lda, bstride, nn, r0, r0, kG, 64, r0 - ubase, batch, 64 * i);
+          if (rc) return rc;
+        }
+      }
+      if (kG < nn) {
+        ProfScope ps(ctx, 3, 8.0 * (double)(nn - kG) * (double)(ncols - kG) * 64.0 * G * batch,
+                     2.0 * (double)(nn - kG) * (double)(ncols - kG) * es * batch);
+        for (int j = 0; j < G; ++j) {
+          const int* gm = j < G - 1 ? ctx->lu.gmap + (size_t)j * nn : nullptr;
+          int rc = tc_pack_l(ctx, A2, lda, bstride, nn, k + 64 * j, 64, kG, 64 * j, batch, gm,
+                             (size_t)kGroupMaps * nn);
+          if (rc) return rc;
+        }
+        int rc = tc_gemm(ctx, A2, lda, bstride, nn, kG, kG, ncols, 64 * G, kG - ubase, batch, 0);
         if (rc) return rc;
       }
-      rc = run_panel(c0, w2, p2);
-      if (rc) return rc;
-      rc = laswp(true, c0, 64, c1, p2, c0, 64, k);
-      if (rc) return rc;
-      if (c1 < nn) {
-        ProfScope ps(ctx, 3, 8.0 * (double)(nn - c1) * (double)(ncols - c1) * 128.0 * batch,
-                     2.0 * (double)(nn - c1) * (double)(ncols - c1) * es * batch);
-        rc = tc_pack_l(ctx, static_cast<float2*>(A), lda, bstride, nn, k, 64, c1, 0, batch, p2, kPermStride);
-        if (!rc) rc = tc_pack_l(ctx, static_cast<float2*>(A), lda, bstride, nn, c0, 64, c1, 64, batch, nullptr, 0);
-        if (!rc) rc = tc_gemm(ctx, static_cast<float2*>(A), lda, bstride, nn, c1, c1, ncols, 128, 64, batch);
-        if (rc) return rc;
-      }
-      k = c1;
+      k = kG;
       continue;
     }
     int w = 0, *perm_p = nullptr;
@@ -3519,7 +3605,7 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     const int c0 = k + w;
     if (c0 < ncols) {
       const int cols = ncols - c0;
-      rc = laswp(false, k, w, c0, perm_p, c0, 0, 0);
+      rc = laswp(k, w, c0, perm_p, c0, 0, k, 0, c0, -1, 1);
       if (rc) return rc;
       if (c0 < nn) {
         ProfScope ps(ctx, 3, 8.0 * (double)(nn - c0) * (double)cols * (double)w * batch,

@@ -524,7 +524,8 @@ KERNELS = {
     "panel": "k_panel_push (LU panel, one 16-CTA cluster per problem; pivot candidates pushed by remote "
              "stores before one cluster barrier per column)",
     "laswp_trsm": "k_l11_inv + k_laswp_tc (row interchanges + U12 = L11^-1 A12 on TF32 tensor cores, FP32)",
-    "gemm": "k_pack_l21 + k_gemm_tc (FP32 LU trailing update, tcgen05 kind::tf32, K = 128, TMA reduce-add)",
+    "gemm": "k_pack_l21 + k_gemm_tc (FP32 LU trailing update, tcgen05 kind::tf32, K = 256 per four-panel group, "
+            "TMA reduce-add)",
     "solves": "k_tri_inv + k_trsv_f32 (cooperative forward + back substitution with inverted diagonal blocks)",
     "residual": "k_resid_partial + k_resid_final (FP64 refinement residual)",
 }
