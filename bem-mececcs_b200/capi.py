@@ -142,8 +142,9 @@ class Context:
     INT_OPTIONS = ("gemm_ctas", "trsv_ctas")
 
     def set_option(self, name: str, value) -> None:
-        """bem_ctx_set_option: switches tcgen05, trsv_coop, lu_pairs,
-        panel_calu, graphs; CTA budgets gemm_ctas, trsv_ctas (0 = device)."""
+        """bem_ctx_set_option: switches tcgen05, trsv_coop, lu_pairs, lu_quads,
+        panel_calu, panel_push, panel_async, laswp_tc, trsv_inv, graphs; CTA
+        budgets gemm_ctas, trsv_ctas (0 = device)."""
         v = int(value) if name in self.INT_OPTIONS else int(bool(value))
         self.check(self.L.bem_ctx_set_option(self.h, name.encode(), v), "bem_ctx_set_option")
 

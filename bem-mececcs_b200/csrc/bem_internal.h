@@ -199,6 +199,7 @@ struct bem_ctx {
   int sw_nn = 0, sw_bsz = 0, sw_mixed = 0, sw_iters = 0;  // shape of the last directly enqueued step
   bool panel_calu = false;    // FP32 LU panels: tournament pivoting per 8-column sub-panel
   bool panel_push = true;     // cluster panels exchange pivots by remote stores before the barrier
+  bool panel_async = true;    // ... as st.async into mbarrier-counted mailboxes, no per-column cluster barrier
   bool lu_pairs = true;       // FP32 tensor-core LU: two 64-column panels per trailing update (K = 128)
   bool lu_quads = true;       // ... four (K = 256) where four 64-column panels fit
   // SM shares for contexts that run concurrently on one GPU (0: the whole device)

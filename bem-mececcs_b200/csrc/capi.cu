@@ -147,6 +147,7 @@ int bem_ctx_create(int device, bem_ctx** out) {
   if (const char* env = getenv("BEM_TRSV_INV")) ctx->trsv_inv = env[0] != '0';
   if (const char* env = getenv("BEM_LASWP_TC")) ctx->laswp_tc = env[0] != '0';
   if (const char* env = getenv("BEM_LU_QUADS")) ctx->lu_quads = env[0] != '0';
+  if (const char* env = getenv("BEM_PANEL_ASYNC")) ctx->panel_async = env[0] != '0';
   *out = ctx;
   return BEM_OK;
 }
@@ -543,6 +544,7 @@ static bool* option_slot(bem_ctx* ctx, const char* name) {
   if (!strcmp(name, "lu_quads")) return &ctx->lu_quads;
   if (!strcmp(name, "panel_calu")) return &ctx->panel_calu;
   if (!strcmp(name, "panel_push")) return &ctx->panel_push;
+  if (!strcmp(name, "panel_async")) return &ctx->panel_async;
   if (!strcmp(name, "graphs")) return &ctx->use_graphs;
   return nullptr;
 }

@@ -146,6 +146,7 @@ struct PanelArgs {
   int* status;
   int* pstart;     // panel starts for the later solves: [pidx] = k, [pidx + 1] = k + w
   int pidx;
+  int async_mail;  // k_panel_push: mailboxes filled by st.async (mbarrier complete_tx), no per-column cluster barrier
   // grid fallback only:
   void* slot_val;
   int* slot_row;
@@ -643,6 +644,14 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], 
 
 constexpr int kPushMoves = 16;  // positions that a sub-panel's 8 interchanges can touch
 
+// 16 bytes into CTA `rank`'s copy of p, completing that many bytes of the
+// transaction count of its copy of mbarrier mb (the receiver waits on it).
+__device__ __forceinline__ void dsm_st4_async(const void* p, unsigned rank, uint4 v, const uint64_t* mb) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(
+                   map_rank(p, rank)),
+               "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w), "r"(map_rank(mb, rank))
+               : "memory");
+}
 __device__ __forceinline__ void dsm_st4(const void* p, unsigned rank, uint4 v) {
   asm volatile("st.shared::cluster.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(map_rank(p, rank)), "r"(v.x), "r"(v.y),
                "r"(v.z), "r"(v.w)
@@ -723,6 +732,7 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
   __shared__ int s_pdst[2 * NB], s_psrc[2 * NB];
   __shared__ int s_pcount;
   __shared__ int s_ipiv[NB];
+  __shared__ uint64_t s_mb[2];  // [column parity]: the mailboxes' arrivals (async_mail)
 
   const unsigned rank = cluster_rank();
   const int prob = blockIdx.y, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -743,7 +753,16 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
     s_psrc[tid] = k + tid;
   }
   if (rank == 0 && tid == 0) s_pcount = w;
+  const bool amail = a.async_mail != 0;
+  if (amail && tid == 0) {
+    mbar_init(&s_mb[0], 1);
+    mbar_init(&s_mb[1], 1);
+  }
   __syncthreads();
+  if (amail) cluster_sync();  // every CTA's mbarriers exist before the first push
+  // bytes arriving in a CTA per column: every CTA's candidate (1 + KW words) and row gj (KW words)
+  const unsigned mail_bytes = (unsigned)(cs * (1 + KW) + KW) * 16u;
+  unsigned mph = 0;  // phase bits of s_mb[0], s_mb[1]
 
   const int grow = tid < rcount ? rbase + tid : INT_MAX;  // my row (position)
   const C czero{R(0), R(0)};
@@ -788,6 +807,7 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
       if (jj >= sw) break;
       const int j = s0 + jj, gj = k + j, par = j & 1;
       const int owner = j / rp;
+      if (amail && tid == 0) mbar_expect_tx(&s_mb[par], mail_bytes);  // arms this column's mailboxes
       // 1. Candidates: the best row of every warp stages its 8 values (and
       //    the thread holding row gj stages that row) before the CTA barrier.
       //    A NaN counts as 0, so every column has a pivot: row gj itself is
@@ -873,16 +893,32 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
         }
         if (lane < cs)
           for (int wi = warp; wi < NWORD; wi += NW) {
-            if (wi == 0)
+            if (amail) {  // every word goes out (the receiver counts bytes), row gj from its owner
+              if (wi == 0)
+                dsm_st4_async(&s_box[par][rank][0], lane, cword, &s_mb[par]);
+              else if (wi <= KW)
+                dsm_st4_async(&s_box[par][rank][wi], lane, s_wt[par][ww][wi - 1], &s_mb[par]);
+              else if ((int)rank == owner)
+                dsm_st4_async(&s_dbox[par][wi - 1 - KW], lane, s_gw[par][wi - 1 - KW], &s_mb[par]);
+            } else if (wi == 0) {
               dsm_st4(&s_box[par][rank][0], lane, cword);
-            else if (wi <= KW) {
+            } else if (wi <= KW) {
               if (cr != INT_MAX) dsm_st4(&s_box[par][rank][wi], lane, s_wt[par][ww][wi - 1]);
             } else if ((int)rank == owner) {
               dsm_st4(&s_dbox[par][wi - 1 - KW], lane, s_gw[par][wi - 1 - KW]);
             }
           }
       }
-      cluster_sync();
+      if (amail) {
+        // the column's mailboxes are full when the mbarrier's phase completes; a
+        // wait that runs out sets the status and later waits are skipped (the
+        // kernel still meets every cluster barrier)
+        if (*(volatile int*)&a.status[ST_TIMEOUT] == 0 && !mbar_wait(&s_mb[par], (mph >> par) & 1u))
+          atomicExch(&a.status[ST_TIMEOUT], 1);
+        mph ^= 1u << par;
+      } else {
+        cluster_sync();
+      }
       // 3. The winner, by every warp from its own CTA's mailboxes.
       int prow, wsrc;
       if constexpr (sizeof(R) == 4) {
@@ -3425,6 +3461,7 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     pa.status = ctx->d_status;
     pa.pstart = L.pstart;
     pa.pidx = (int)L.panels.size();
+    pa.async_mail = ctx->panel_async ? 1 : 0;
     const int nb = panel_nb(m);
     ProfScope ps(ctx, 1, 0.0, 2.0 * (double)m * std::min(nb ? nb : 64, m) * es * batch);
     if (nb) {

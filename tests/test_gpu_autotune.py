@@ -26,7 +26,8 @@ def test_options_give_the_same_solutions():
     again, _ = sol.sweep(freqs, form="mixed", batch=7, refine=3)
     assert np.array_equal(again, ref)
     for opt, val in (("graphs", False), ("lu_pairs", False), ("panel_calu", True), ("trsv_coop", False),
-                     ("panel_push", False), ("trsv_inv", False), ("laswp_tc", False), ("lu_quads", False)):
+                     ("panel_push", False), ("trsv_inv", False), ("laswp_tc", False), ("lu_quads", False),
+                     ("panel_async", False)):
         sol.ctx.set_option(opt, val)
         assert sol.ctx.get_option(opt) == val
         x, _ = sol.sweep(freqs, form="mixed", batch=7, refine=3)
