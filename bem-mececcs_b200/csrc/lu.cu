@@ -2014,7 +2014,7 @@ __global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, 
   float2* s_inv = reinterpret_cast<float2*>(smem_raw);  // [64][kLtLd] L11^-1, row-major
   float2* s_bb = s_inv + 64 * kLtLd;                     // [2][64][kLtLd] tiles (panel rows x columns), two stages
   float2* s_lb = s_bb + 2 * 64 * kLtLd;                  // PRE: an earlier panel's L at this panel's rows
-  float2* s_up = s_lb + 64 * kLtLd;                      // PRE: that panel's U rows of the tile
+  float2* s_upb = s_lb + 64 * kLtLd;                     // PRE: [2][64][kLtLd] that panel's U rows of the tile
   __shared__ int s_src[64];                              // source row of panel row i
   __shared__ int s_xd[64], s_xs[64];                     // displaced rows: dst <- src
   __shared__ int s_nx;
@@ -2039,15 +2039,25 @@ __global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, 
   __syncthreads();  // s_src
   // Lb_j(i, t) = L(map_j(k + i), kfirst + 64 j + t): earlier panel j's L at this panel's rows
   const int* gm = gmap + (size_t)prob * kGroupMaps * nn;
-  auto load_lb = [&](int j) {
+  auto load_lb_to = [&](float2* dst, int j) {
     for (int idx = tid; idx < 64 * 64; idx += blockDim.x) {
       const int i = idx & 63, t = idx >> 6;
       const bool ok = i < w;
-      cp_async8(&s_lb[i * kLtLd + t], ok ? &A[(size_t)(kfirst + 64 * j + t) * lda + gm[(size_t)j * nn + k + i]] : A,
+      cp_async8(&dst[i * kLtLd + t], ok ? &A[(size_t)(kfirst + 64 * j + t) * lda + gm[(size_t)j * nn + k + i]] : A,
                 ok);
     }
   };
-  if (PRE && nprev == 1) load_lb(0);  // one earlier panel: its Lb serves every tile
+  auto load_lb = [&](int j) { load_lb_to(s_lb, j); };
+  // earlier panel j's U rows of the tile at cbase (tw columns)
+  auto load_up_to = [&](float2* dst, int j, int cbase, int tw) {
+    const int i = tid & 63, cg = tid >> 6;
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const int c = cg + 4 * u;
+      cp_async8(&dst[i * kLtLd + c], c < tw ? &A[(size_t)(cbase + c) * lda + kfirst + 64 * j + i] : A, c < tw);
+    }
+  };
+  if (PRE) load_lb(0);
   cp_async_commit();
 
   // warp tile: rows [16 * (warp & 3), +16) x columns [32 * (warp >> 2), +32)
@@ -2108,7 +2118,9 @@ __global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, 
   const int ntiles = (ncols - c0 + 63) / 64;
   // A tile's gathered panel rows into stage st by cp.async (8-byte elements,
   // zero-filled outside the panel rows and past the last column).
-  auto issue = [&](int tile, int st) {
+  // With it, for a deferred tile, the first earlier panel's U rows (and its
+  // Lb again when the tile before used s_lb for a third panel).
+  auto issue = [&](int tile, int st, bool lb0) {
     if (tile < ntiles) {
       const int cbase = c0 + tile * 64, tw = min(64, ncols - cbase);
       float2* b = s_bb + (size_t)st * 64 * kLtLd;
@@ -2119,10 +2131,14 @@ __global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, 
         const bool ok = c < tw && i < w;
         cp_async8(&b[i * kLtLd + c], ok ? &A[(size_t)(cbase + c) * lda + s_src[i]] : A, ok);
       }
+      if (PRE && cbase >= cdefer) {
+        load_up_to(s_upb + (size_t)st * 64 * kLtLd, 0, cbase, tw);
+        if (lb0) load_lb(0);
+      }
     }
     cp_async_commit();
   };
-  issue(blockIdx.x, 0);
+  issue(blockIdx.x, 0, false);
   for (int it = 0;; ++it) {
     const int tile = blockIdx.x + it * gridDim.x;
     if (tile >= ntiles) break;
@@ -2144,20 +2160,28 @@ __global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, 
     }
     float pr[4][4], pi[4][4];
     if (PRE && cbase >= cdefer) {  // B -= sum_j Lb_j Uprev_j: the group's deferred update of these rows
+      // Two operand slots: slot 0 = (s_lb, this stage's U buffer), which the
+      // tile's own loads filled with panel 0's; slot 1 = the other stage's
+      // tile and U buffers, idle until the next tile is issued.  Panel j + 1's
+      // operands load into the other slot while panel j's product runs.
+      float2* const lb0 = s_lb;
+      float2* const lb1 = s_bb + (size_t)(st ^ 1) * 64 * kLtLd;
+      float2* const up0 = s_upb + (size_t)st * 64 * kLtLd;
+      float2* const up1 = s_upb + (size_t)(st ^ 1) * 64 * kLtLd;
       zero_acc(pr, pi);
       for (int j = 0; j < nprev; ++j) {
-        if (nprev > 1) load_lb(j);
-        const int i = tid & 63, cg = tid >> 6;
-#pragma unroll
-        for (int u = 0; u < 16; ++u) {
-          const int c = cg + 4 * u;
-          cp_async8(&s_up[i * kLtLd + c], c < tw ? &A[(size_t)(cbase + c) * lda + kfirst + 64 * j + i] : A, c < tw);
+        const bool odd = j & 1;
+        if (j + 1 < nprev) {
+          load_lb_to(odd ? lb0 : lb1, j + 1);
+          load_up_to(odd ? up0 : up1, j + 1, cbase, tw);
+          cp_async_commit();
+          cp_async_wait<1>();
+        } else {
+          cp_async_wait<0>();
         }
-        cp_async_commit();
-        cp_async_wait<0>();
         __syncthreads();
-        cproduct(s_lb, s_up, pr, pi, false);
-        __syncthreads();  // s_lb, s_up reloaded for the next panel
+        cproduct(odd ? lb1 : lb0, odd ? up1 : up0, pr, pi, false);
+        __syncthreads();  // slot sl is refilled two panels on
       }
 #pragma unroll
       for (int nt = 0; nt < 4; ++nt)
@@ -2170,7 +2194,7 @@ __global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, 
         }
       __syncthreads();
     }
-    issue(tile + gridDim.x, st ^ 1);  // the next tile streams in meanwhile
+    issue(tile + gridDim.x, st ^ 1, nprev >= 3);  // the next tile streams in meanwhile
     zero_acc(pr, pi);
     cproduct(s_inv, sb, pr, pi, true);  // U12 = L11^-1 B
     __syncthreads();                     // every warp has read the tile
@@ -3547,11 +3571,11 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     if (sizeof(R) == 4 && ctx->laswp_tc) {
       int rc = linv_maps(k, w, perm_p, gi, gsize);
       if (rc) return rc;
-      // one CTA per SM (registers; shared memory for three or five 64 x 64 tiles)
+      // one CTA per SM (registers; shared memory for three or six 64 x 64 tiles)
       const int ntiles = (cols + 63) / 64;
       const int per = std::max(1, ctx->num_sms / batch);
       const int tb = std::min(ntiles, per);
-      const size_t sm = (pre ? 5 : 3) * kLtTile;
+      const size_t sm = (pre ? 6 : 3) * kLtTile;
       float2* A2 = static_cast<float2*>(A);
       LuWork& LW = ctx->lu;
       if (pre) {
