@@ -278,10 +278,44 @@ int tc_ensure(bem_ctx* ctx, int nn, int batch);
 void tc_release(bem_ctx* ctx);
 int tc_trailing_update(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int k, int w, int batch);
 int tc_pack_l(bem_ctx* ctx, const float2* A, size_t lda, size_t bstride, int nn, int kcol, int kw, int r0, int koff,
-              int batch, const int* gmap, size_t gstride);
+              int batch, const int* gmap, size_t gstride, int npanels = 1, int nmaps = 1);
 int tc_gemm(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int r0, int c0, int cend, int kw,
             int urow_off, int batch, int kbase);
 constexpr int kTcKPitch = 256;  // floats per packed tensor-core operand row
+
+// One 32-row block of the packed tensor-core operand Lhat (256 threads):
+// L(r, k..k+kw-1) for rows rbase..rbase+31 (L's storage row map[r], or r)
+// goes to rows 2(r - r0) + part of `out`, K slots koff..koff+kw-1, rounded to
+// TF32.  Uses a [64][33] shared tile and 32 shared ints; the caller
+// synchronises before the next block reuses them.
+__device__ __forceinline__ void pack_l_rows(const float2* __restrict__ Ap, size_t lda, int nn, int k, int kw, int r0,
+                                            int rbase, int koff, float* out, const int* __restrict__ map,
+                                            float2 (*tile)[33], int* s_src) {
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 8 x 32
+  if (threadIdx.x < 32) {
+    const int r = rbase + threadIdx.x;
+    s_src[threadIdx.x] = (map && r < nn) ? map[r] : r;
+  }
+  __syncthreads();
+  const int src = s_src[tx];
+  for (int c = ty; c < 64; c += 8) {
+    const int r = rbase + tx;
+    float2 v = make_float2(0.f, 0.f);
+    if (c < kw && r < nn) v = Ap[(size_t)(k + c) * lda + src];
+    tile[c][tx] = v;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < 32 * 2 * 64; idx += blockDim.x) {
+    const int c = idx & 63, rr = idx >> 6;  // rr = 2*local_row + part
+    const int lr = rr >> 1, part = rr & 1;
+    const int r = rbase + lr;
+    if (r >= nn || c >= kw) continue;
+    const float2 v = tile[c][lr];
+    unsigned t;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(part ? v.y : v.x));
+    out[(size_t)(2 * (r - r0) + part) * kTcKPitch + koff + c] = __uint_as_float(t);
+  }
+}
 int measure_fp64_peak(bem_ctx* ctx, double* tflops);
 int measure_fma_peaks(bem_ctx* ctx, double* fp64_tflops, double* fp32_tflops);
 int measure_tf32_peak(bem_ctx* ctx, int n, double* tflops);

@@ -313,41 +313,18 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
 // With a gather list (a later panel's interchanges: count, then dst/src
 // pairs), row r takes L from the row that the list moves to r, i.e. L in the
 // later panel's row order; A itself is not changed.
+// Panel z (blockIdx.z) of npanels consecutive 64-column panels: columns
+// k + 64 z.., K slots koff + 64 z.., through problem b's row map z (at
+// gmap + b * gstride + z * nn) when z < nmaps.
 __global__ void __launch_bounds__(256) k_pack_l21(const float2* __restrict__ A, size_t lda, size_t bstride, int nn,
                                                   int k, int kw, int r0, int koff, float* lhat, int lrows,
-                                                  const int* __restrict__ gmap, size_t gstride) {
+                                                  const int* __restrict__ gmap, size_t gstride, int nmaps) {
   __shared__ float2 tile[64][33];
   __shared__ int s_src[32];
-  const int b = blockIdx.y;
-  const float2* Ap = A + (size_t)b * bstride;
-  const int rbase = r0 + blockIdx.x * 32;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 8 x 32
-  if (threadIdx.x < 32) {
-    const int r = rbase + threadIdx.x;
-    // the row of L's storage that is row r now (a row map of a panel group), or r
-    s_src[threadIdx.x] = (gmap && r < nn) ? gmap[(size_t)b * gstride + r] : r;
-  }
-  __syncthreads();
-  const int src = s_src[tx];
-  for (int c = ty; c < 64; c += 8) {
-    const int r = rbase + tx;
-    float2 v = make_float2(0.f, 0.f);
-    if (c < kw && r < nn) v = Ap[(size_t)(k + c) * lda + src];
-    tile[c][tx] = v;
-  }
-  __syncthreads();
-  float* out = lhat + (size_t)b * lrows * kKPitch;
-  for (int idx = threadIdx.x; idx < 32 * 2 * 64; idx += blockDim.x) {
-    const int c = idx & 63, rr = idx >> 6;  // rr = 2*local_row + part
-    const int lr = rr >> 1, p = rr & 1;
-    const int r = rbase + lr;
-    if (r >= nn || c >= kw) continue;
-    const float2 v = tile[c][lr];
-    const float x = p ? v.y : v.x;
-    unsigned t;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(x));
-    out[(size_t)(2 * (r - r0) + p) * kKPitch + koff + c] = __uint_as_float(t);
-  }
+  const int b = blockIdx.y, z = blockIdx.z;
+  const int* map = (gmap && z < nmaps) ? gmap + (size_t)b * gstride + (size_t)z * nn : nullptr;
+  pack_l_rows(A + (size_t)b * bstride, lda, nn, k + 64 * z, kw, r0, r0 + blockIdx.x * 32, koff + 64 * z,
+              lhat + (size_t)b * lrows * kKPitch, map, tile, s_src);
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -507,12 +484,14 @@ void tc_release(bem_ctx* ctx) {
 
 // Packs L (columns kcol..kcol+kw-1, rows r0..nn-1) into K slots
 // koff..koff+kw-1 of Lhat, optionally through a row map (problem b's map at
-// gmap + b * gstride: the storage row of L that is row r now).
+// gmap + b * gstride: the storage row of L that is row r now); with npanels
+// > 1, also the next 64-column panels into the next K slots in the same
+// launch, the first nmaps of them through the maps that follow.
 int tc_pack_l(bem_ctx* ctx, const float2* A, size_t lda, size_t bstride, int nn, int kcol, int kw, int r0, int koff,
-              int batch, const int* gmap, size_t gstride) {
+              int batch, const int* gmap, size_t gstride, int npanels, int nmaps) {
   if (r0 >= nn) return BEM_OK;
-  k_pack_l21<<<dim3((nn - r0 + 31) / 32, batch), 256, 0, ctx->stream>>>(A, lda, bstride, nn, kcol, kw, r0, koff,
-                                                                        ctx->tc.lhat, 2 * nn, gmap, gstride);
+  k_pack_l21<<<dim3((nn - r0 + 31) / 32, batch, npanels), 256, 0, ctx->stream>>>(
+      A, lda, bstride, nn, kcol, kw, r0, koff, ctx->tc.lhat, 2 * nn, gmap, gstride, gmap ? nmaps : 0);
   ctx->launches++;
   BEM_CUDA(ctx, cudaGetLastError());
   return BEM_OK;

@@ -2009,7 +2009,8 @@ __global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, 
                                                      int ncols, const int* __restrict__ perm, int perm_stride,
                                                      float* ure, float* uim, int urows, int ubase, int koff,
                                                      int kfirst, int nprev, int cdefer, const int* __restrict__ gmap,
-                                                     int nn, const float2* __restrict__ linv) {
+                                                     int nn, const float2* __restrict__ linv, float* lhat, int lrows,
+                                                     int pk_r0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* s_inv = reinterpret_cast<float2*>(smem_raw);  // [64][kLtLd] L11^-1, row-major
   float2* s_bb = s_inv + 64 * kLtLd;                     // [2][64][kLtLd] tiles (panel rows x columns), two stages
@@ -2232,6 +2233,19 @@ __global__ void __launch_bounds__(256, 1) k_laswp_tc(float2* Abase, size_t lda, 
     __syncthreads();  // this stage is refilled two tiles on
   }
   cp_async_wait<0>();
+  if (pk_r0 >= 0 && pk_r0 < nn) {
+    // this panel's L21 (rows pk_r0..nn-1) packed for the update that follows,
+    // at its K slot, 32-row blocks dealt to the CTAs (the tiles' shared memory)
+    __shared__ int s_psrc[32];
+    __syncthreads();
+    auto tile = reinterpret_cast<float2(*)[33]>(s_bb);
+    float* out = lhat + (size_t)prob * lrows * kTcKPitch;
+    const int nblk = (nn - pk_r0 + 31) / 32;
+    for (int bi = blockIdx.x; bi < nblk; bi += gridDim.x) {
+      pack_l_rows(A, lda, nn, k, w, pk_r0, pk_r0 + 32 * bi, koff, out, nullptr, tile, s_psrc);
+      __syncthreads();
+    }
+  }
 }
 // ---------------------------------------------------------------------------
 // Trailing update C -= L21 U12 on the tensor cores, complex as 4 real products.
@@ -3559,8 +3573,11 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
   // on first take the deferred update of the nprev earlier panels of the
   // group (at kfirst, kfirst + 64, ...); gi/gsize: the panel's place in its
   // group (-1: none).
+  // pack_r0 >= 0: also pack this panel's L21 (rows pack_r0..) at K slot koff
+  // for the update that follows (packed = true when done here).
   auto laswp = [&](int k, int w, int c0, const int* perm_p, int ubase, int koff, int kfirst, int nprev, int cdefer,
-                   int gi, int gsize) -> int {
+                   int gi, int gsize, int pack_r0, bool& packed) -> int {
+    packed = false;
     const int cols = ncols - c0;
     if (cols <= 0) return BEM_OK;
     const bool pre = nprev > 0;
@@ -3578,19 +3595,22 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
       const size_t sm = (pre ? 6 : 3) * kLtTile;
       float2* A2 = static_cast<float2*>(A);
       LuWork& LW = ctx->lu;
+      const int pk = (ure && pack_r0 >= 0) ? pack_r0 : -1;
+      float* lhat = ctx->tc.lhat;
       if (pre) {
         BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_laswp_tc<true><<<dim3(tb, batch), 256, sm, ctx->stream>>>(A2, lda, bstride, k, w, c0, ncols, perm_p,
-                                                                     kPermStride, ure, uim, nn + 1, ubase, koff,
-                                                                     kfirst, nprev, cdefer, LW.gmap, nn, LW.linv);
+        k_laswp_tc<true><<<dim3(tb, batch), 256, sm, ctx->stream>>>(
+            A2, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kfirst, nprev,
+            cdefer, LW.gmap, nn, LW.linv, lhat, 2 * nn, pk);
       } else {
         BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_laswp_tc<false><<<dim3(tb, batch), 256, sm, ctx->stream>>>(A2, lda, bstride, k, w, c0, ncols, perm_p,
-                                                                      kPermStride, ure, uim, nn + 1, ubase, koff,
-                                                                      kfirst, 0, ncols, LW.gmap, nn, LW.linv);
+        k_laswp_tc<false><<<dim3(tb, batch), 256, sm, ctx->stream>>>(
+            A2, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kfirst, 0, ncols,
+            LW.gmap, nn, LW.linv, lhat, 2 * nn, pk);
       }
       ctx->launches++;
       BEM_CUDA(ctx, cudaGetLastError());
+      packed = pk >= 0;
       return BEM_OK;
     }
     if (gi >= 0 && sizeof(R) == 4) {  // the grouped packs read L through the row maps
@@ -3634,13 +3654,14 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
         int wi = 0, *pi = nullptr;
         int rc = run_panel(ki, wi, pi);
         if (rc) return rc;
-        rc = laswp(ki, 64, ki + 64, pi, ubase, 64 * i, k, i, kG, i, G);
+        bool packed = false;
+        rc = laswp(ki, 64, ki + 64, pi, ubase, 64 * i, k, i, kG, i, G, i < G - 1 ? ki + 64 : -1, packed);
         if (rc) return rc;
         if (i < G - 1) {  // panel i's update of the group's remaining columns
           const int r0 = ki + 64;
           ProfScope ps(ctx, 3, 8.0 * (double)(nn - r0) * (double)(kG - r0) * 64.0 * batch,
                        2.0 * (double)(nn - r0) * (double)(kG - r0) * es * batch);
-          rc = tc_pack_l(ctx, A2, lda, bstride, nn, ki, 64, r0, 64 * i, batch, nullptr, 0);
+          if (!packed) rc = tc_pack_l(ctx, A2, lda, bstride, nn, ki, 64, r0, 64 * i, batch, nullptr, 0);
           if (!rc) rc = tc_gemm(ctx, A2, lda, bstride, nn, r0, r0, kG, 64, r0 - ubase, batch, 64 * i);
           if (rc) return rc;
         }
@@ -3648,13 +3669,10 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
       if (kG < nn) {
         ProfScope ps(ctx, 3, 8.0 * (double)(nn - kG) * (double)(ncols - kG) * 64.0 * G * batch,
                      2.0 * (double)(nn - kG) * (double)(ncols - kG) * es * batch);
-        for (int j = 0; j < G; ++j) {
-          const int* gm = j < G - 1 ? ctx->lu.gmap + (size_t)j * nn : nullptr;
-          int rc = tc_pack_l(ctx, A2, lda, bstride, nn, k + 64 * j, 64, kG, 64 * j, batch, gm,
-                             (size_t)kGroupMaps * nn);
-          if (rc) return rc;
-        }
-        int rc = tc_gemm(ctx, A2, lda, bstride, nn, kG, kG, ncols, 64 * G, kG - ubase, batch, 0);
+        // every panel's L at its K slot in one launch, panels 0..G-2 through their row maps
+        int rc = tc_pack_l(ctx, A2, lda, bstride, nn, k, 64, kG, 0, batch, ctx->lu.gmap, (size_t)kGroupMaps * nn,
+                           G, G - 1);
+        if (!rc) rc = tc_gemm(ctx, A2, lda, bstride, nn, kG, kG, ncols, 64 * G, kG - ubase, batch, 0);
         if (rc) return rc;
       }
       k = kG;
@@ -3666,13 +3684,17 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     const int c0 = k + w;
     if (c0 < ncols) {
       const int cols = ncols - c0;
-      rc = laswp(k, w, c0, perm_p, c0, 0, k, 0, c0, -1, 1);
+      bool packed = false;
+      rc = laswp(k, w, c0, perm_p, c0, 0, k, 0, c0, -1, 1, tc ? c0 : -1, packed);
       if (rc) return rc;
       if (c0 < nn) {
         ProfScope ps(ctx, 3, 8.0 * (double)(nn - c0) * (double)cols * (double)w * batch,
                      2.0 * (double)(nn - c0) * (double)cols * es * batch);
         if (tc) {
-          rc = tc_trailing_update(ctx, static_cast<float2*>(A), lda, bstride, nn, k, w, batch);
+          if (packed)
+            rc = tc_gemm(ctx, static_cast<float2*>(A), lda, bstride, nn, c0, c0, nn + 1, w, 0, batch, 0);
+          else
+            rc = tc_trailing_update(ctx, static_cast<float2*>(A), lda, bstride, nn, k, w, batch);
           if (rc) return rc;
         } else if (sizeof(R) == 8) {
           dim3 grid((nn - c0 + GBM - 1) / GBM, (cols + GBN - 1) / GBN, batch);
