@@ -1928,6 +1928,14 @@ __global__ void __launch_bounds__(1024) k_l11_inv(const float2* __restrict__ Aba
   float2* s_b = s_inv + 64 * kLtLd;                      // [64][kLtLd] L11
   const int prob = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const float2* A = Abase + (size_t)prob * bstride;
+  // L11 (unit lower, w x w at (k, k)) into registers first: these loads
+  // overlap the row maps' dependent loads below
+  float2 lv[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int idx = tid + q * 1024, i = idx & 63, c = idx >> 6;
+    lv[q] = (i < w && c < w) ? A[(size_t)(k + c) * lda + k + i] : make_float2(0.f, 0.f);
+  }
   if (gi >= 0) {
     int* gm = gmap + (size_t)prob * kGroupMaps * nn;
     const int* pl = perm + (size_t)prob * perm_stride;
@@ -1943,10 +1951,11 @@ __global__ void __launch_bounds__(1024) k_l11_inv(const float2* __restrict__ Aba
     if (gi < gsize - 1 && gi < kGroupMaps)
       for (int x = k + w + tid; x < nn; x += blockDim.x) gm[(size_t)gi * nn + x] = x;
   }
-  // L11 (unit lower, w x w at (k, k)) into s_b, row-major; s_inv = I.
-  for (int idx = tid; idx < 64 * 64; idx += blockDim.x) {
-    const int i = idx & 63, c = idx >> 6;
-    s_b[i * kLtLd + c] = (i < w && c < w) ? A[(size_t)(k + c) * lda + k + i] : make_float2(0.f, 0.f);
+  // L11 into s_b, row-major; s_inv = I (1024 threads, 4 entries each)
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int idx = tid + q * 1024, i = idx & 63, c = idx >> 6;
+    s_b[i * kLtLd + c] = lv[q];
     s_inv[i * kLtLd + c] = make_float2(i == c ? 1.f : 0.f, 0.f);
   }
   __syncthreads();
@@ -1962,13 +1971,13 @@ __global__ void __launch_bounds__(1024) k_l11_inv(const float2* __restrict__ Aba
     for (int i = 0; i < 16; ++i) x[i] = zf{i == c ? 1.f : 0.f, 0.f};
 #pragma unroll
     for (int i = 1; i < 16; ++i) {
-      zf acc{0.f, 0.f};
+      zf acc{0.f, 0.f}, acc2{0.f, 0.f};  // two chains: even and odd t
 #pragma unroll
       for (int t = 0; t < i; ++t) {  // x_t = 0 for t < c
         const float2 l = at(s_b, b0 + i, b0 + t);
-        cfms(acc, zf{l.x, l.y}, x[t]);
+        cfms((t & 1) ? acc2 : acc, zf{l.x, l.y}, x[t]);
       }
-      if (i > c) x[i] = acc;
+      if (i > c) x[i] = zf{acc.re + acc2.re, acc.im + acc2.im};
     }
 #pragma unroll
     for (int i = 0; i < 16; ++i) at(s_inv, b0 + i, b0 + c) = make_float2(x[i].re, x[i].im);
@@ -1979,22 +1988,26 @@ __global__ void __launch_bounds__(1024) k_l11_inv(const float2* __restrict__ Aba
     const int npair = 64 / (2 * h), outs = npair * h * h;
     for (int idx = tid; idx < outs; idx += blockDim.x) {  // T = L21 X11 into the scratch block
       const int pp = idx / (h * h), i = (idx / h) % h, j = idx % h, o = pp * 2 * h;
-      zf acc{0.f, 0.f};
-      for (int t = 0; t < h; ++t) {
+      zf acc{0.f, 0.f}, acc2{0.f, 0.f};  // two chains: even and odd t
+      for (int t = 0; t < h; t += 2) {
         const float2 l = at(s_b, o + h + i, o + t), x = at(s_inv, o + t, o + j);
+        const float2 l2 = at(s_b, o + h + i, o + t + 1), x2 = at(s_inv, o + t + 1, o + j);
         cfms(acc, zf{l.x, l.y}, zf{x.x, x.y});
+        cfms(acc2, zf{l2.x, l2.y}, zf{x2.x, x2.y});
       }
-      at(s_inv, pp * h + i, 32 + j) = make_float2(-acc.re, -acc.im);  // acc = -T
+      at(s_inv, pp * h + i, 32 + j) = make_float2(-acc.re - acc2.re, -acc.im - acc2.im);  // acc = -T
     }
     __syncthreads();
     for (int idx = tid; idx < outs; idx += blockDim.x) {  // X21 = -X22 T
       const int pp = idx / (h * h), i = (idx / h) % h, j = idx % h, o = pp * 2 * h;
-      zf acc{0.f, 0.f};
-      for (int t = 0; t < h; ++t) {
+      zf acc{0.f, 0.f}, acc2{0.f, 0.f};
+      for (int t = 0; t < h; t += 2) {
         const float2 x = at(s_inv, o + h + i, o + h + t), tt = at(s_inv, pp * h + t, 32 + j);
+        const float2 x2 = at(s_inv, o + h + i, o + h + t + 1), tt2 = at(s_inv, pp * h + t + 1, 32 + j);
         cfms(acc, zf{x.x, x.y}, zf{tt.x, tt.y});
+        cfms(acc2, zf{x2.x, x2.y}, zf{tt2.x, tt2.y});
       }
-      at(s_inv, o + h + i, o + j) = make_float2(acc.re, acc.im);  // acc = -X22 T
+      at(s_inv, o + h + i, o + j) = make_float2(acc.re + acc2.re, acc.im + acc2.im);  // acc = -X22 T
     }
     __syncthreads();
   }
