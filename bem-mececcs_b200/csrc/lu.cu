@@ -7,21 +7,27 @@
 // of B equal-size problems (A_b = A + b * bstride) is factored in lockstep.
 //
 //   for each panel of w columns starting at k (w adapts to the panel height):
-//     k_panel_cluster  one thread-block cluster (16 CTAs) per problem holds the
-//                      panel rows in shared memory; per column the pivot
-//                      candidates and rows are exchanged over distributed
-//                      shared memory with one hardware cluster barrier.  Pivot =
+//     k_panel_push     one thread-block cluster (16 CTAs) per problem holds the
+//                      panel rows in shared memory; per column every CTA pushes
+//                      its pivot candidate (and the owner row gj) into mailboxes
+//                      in every CTA (st.async, counted by an mbarrier).  Pivot =
 //                      first row of largest |re|+|im| (LAPACK IZAMAX); rows are
-//                      interchanged as ZGETF2 does.
+//                      interchanged as ZGETF2 does.  k_panel_cluster (pull form)
+//                      and k_panel_calu (tournament pivoting) are options.
 //     k_panel_grid     fallback for panels too tall for one cluster: the same
 //                      algorithm over a cooperative grid with a bounded
 //                      software grid barrier.
-//     k_laswp_trsm     the panel's row interchanges applied to every column to
-//                      the right (one gather per column) and U12 = L11^-1 A12.
+//     k_l11_inv +      FP32: L11^-1 once per panel, then the panel's row
+//     k_laswp_tc       interchanges on every column to the right and U12 =
+//                      L11^-1 A12 on TF32 tensor cores (with the deferred update
+//                      of the earlier panels of a group); k_laswp_trsm does the
+//                      same by substitution (FP64).
 //     k_gemm_f64       A22 -= L21 U12 on the FP64 tensor cores (DMMA m8n8k4).
-//     k_gemm_tf32      the same for FP32 storage on the TF32 tensor cores.
-//   k_backsub          U x = y, one launch per 64-row block, the diagonal
-//                      block staged in shared memory.
+//     k_gemm_tc        (gemm_tc.cu) the FP32 update on tcgen05, K = 64 G for a
+//                      group of G = 1, 2 or 4 panels; k_gemm_tf32 on mma.sync.
+//   k_trsv_f32 /       forward + back substitution in one cooperative launch
+//   k_trsv             (FP32 with inverted diagonal blocks from k_tri_inv;
+//                      FP64 by substitution); k_backsub per 64-row block.
 //
 // Row interchanges are never applied to columns left of a panel; each panel's
 // interchanges are kept (ipiv and a dst/src gather list) so that later solves

@@ -553,8 +553,8 @@ def _roofline(name, k, peaks, mpeaks):
     if name == "gemm":
         tf = k["work"] / secs / 1e12
         peak = mpeaks["tf32_umma_n128"]
-        out["traffic_note"] = ("ncu, one K = 128 launch of 2 problems: dram read+write = 1.03 x the algorithmic "
-                               "C bytes (profiles/k_gemm_tc_2160.md)")
+        out["traffic_note"] = ("ncu, one K = 256 launch of 2 problems: dram read+write = 1.11 x the algorithmic "
+                               "C bytes (profiles/k_gemm_tc_k256_2160.md)")
         out["tensor"] = {"achieved_tflops": round(tf, 2), "peak_tflops": round(peak, 1),
                          "frac": round(tf / peak, 4),
                          "peak_source": "measured: tcgen05 kind::tf32 M=128 N=128 issue-rate "
