@@ -10,9 +10,10 @@ elements: 2160 boundary elements, NPG = 4, n = 6480 complex unknowns.  The
 per-mesh static work (GHMATECE) is done once before timing.
 
 Headline (`value`): the mixed+batched form, one step = one lockstep batch of
-8 frequency solves (FP64 assembly, FP32 LU on TF32 tensor cores, FP64
-iterative refinement), checked against the plain FP64 path at 1e-8.  The
-plain FP64 GPU path (one frequency at a time) is measured in the same run.
+`bem_sweep_batch_limit` frequency solves, 7 on this mesh (FP64 assembly,
+FP32 LU on TF32 tensor cores, FP64 iterative refinement), checked against
+the plain FP64 path at 1e-8.  The plain FP64 GPU path (one frequency at a
+time) is measured in the same run.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -77,6 +78,30 @@ def parse_args():
 def dist_env():
     return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
             int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def frequency_shard(freqs, rank, world):
+    """This replica's frequencies: every world-th one from its rank on.  The
+    shares are disjoint, cover the sweep and differ in length by at most one;
+    no rank needs another's data."""
+    return freqs[rank::world]
+
+
+def max_over_ranks(x, world, device):
+    """The slowest rank's time (ms): the job ends when its last replica does.
+    One all-reduce, taken by every rank at the same point."""
+    if world == 1:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, units_per_rank, ms):
+    """Whole-job throughput: the units all replicas processed over the slowest
+    replica's time."""
+    return world * units_per_rank / (ms * 1e-3)
 
 
 # ---------------------------------------------------------------------------
@@ -191,7 +216,7 @@ def run_ours(args):
 
     s, d = meshgen.config_mesh("c2_2160")
     freqs = meshgen.sweep_frequencies(128, seed=3)
-    mine = freqs[rank::world]
+    mine = frequency_shard(freqs, rank, world)
     sol = BemSolver(s, device=local)
     limit = sol.sweep_batch_limit("mixed")
     B, R = (min(args.batch, limit) if args.batch > 0 else limit), args.refine
@@ -218,13 +243,6 @@ def run_ours(args):
     def barrier():
         if world > 1:
             torch.distributed.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
 
     def timed(fn, steps, prof=False):
         barrier()
@@ -288,7 +306,7 @@ def run_ours(args):
     time.sleep(0.3)
     t_mix = timed(lambda i: sweep_step(args.warmup + i), args.steps)
     clocks = sampler.stop()
-    ms_mix = max_over_ranks(t_mix["ms"])
+    ms_mix = max_over_ranks(t_mix["ms"], world, f"cuda:{local}")
     # per-kernel-class times, launches and algorithmic bytes: a separate
     # profiled pass (CUDA events around every launch; no graph replay)
     t_prof = timed(lambda i: sweep_step(args.warmup + args.steps + i), max(3, args.steps // 2), prof=True)
@@ -303,7 +321,7 @@ def run_ours(args):
         plain_step(i)
     ctx.sync()
     t_plain = timed(plain_step, kp, prof=True)
-    ms_plain = max_over_ranks(t_plain["ms"])
+    ms_plain = max_over_ranks(t_plain["ms"], world, f"cuda:{local}")
 
     # --- end to end through the C-ABI with host buffers (e2e) ---
     zdfi_pin = torch.empty(nn * 16, dtype=torch.uint8, pin_memory=True).numpy().view(np.complex128)
@@ -318,14 +336,14 @@ def run_ours(args):
 
     e2e_step(0)
     t_e2e = timed(e2e_step, args.steps)
-    e2e_ms = max_over_ranks(t_e2e["ms"])
+    e2e_ms = max_over_ranks(t_e2e["ms"], world, f"cuda:{local}")
     if not np.all(np.isfinite(x_pin)):
         raise RuntimeError("non-finite solution")
 
     mpeaks = ctx.peaks()
-    value = world * args.steps * B / (ms_mix * 1e-3)
-    value_plain = world * kp / (ms_plain * 1e-3)
-    e2e_value = world * args.steps * B / (e2e_ms * 1e-3)
+    value = job_rate(world, args.steps * B, ms_mix)
+    value_plain = job_rate(world, kp, ms_plain)
+    e2e_value = job_rate(world, args.steps * B, e2e_ms)
     pm = t_prof["prof"]
     pp = t_plain["prof"]
     shares = {k: round(v["ms"] / t_prof["ms"], 4) for k, v in pm.items()}
