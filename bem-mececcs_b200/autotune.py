@@ -2,9 +2,10 @@
 
 The choices it makes are the library's algorithm switches and the lockstep
 batch: the FP32 panel's pivoting (per column, or tournament per 8-column
-sub-panel), one or two panels per tensor-core trailing update (K = 64 or
-128), CUDA-graph replay of the batch step, and the number of problems in
-lockstep (up to bem_sweep_batch_limit).  Each candidate is timed on the
+sub-panel), four, two or one panels per tensor-core trailing update
+(K = 256, 128 or 64; four take precedence where they fit), CUDA-graph replay
+of the batch step, and the number of problems in lockstep (up to
+bem_sweep_batch_limit).  Each candidate is timed on the
 resident mesh on real frequencies (after one untimed batch) and the fastest
 is kept in a JSON cache keyed by GPU, problem size and form, so that later
 processes apply it without tuning again.
@@ -22,6 +23,7 @@ import time
 import numpy as np
 
 DEFAULT_SPACE = {
+    "lu_quads": (True, False),
     "panel_calu": (False, True),
     "lu_pairs": (True, False),
     "graphs": (True, False),
