@@ -242,7 +242,7 @@ def format_results(r: Results) -> str:
     def row(idx, vals, w=5):
         return f"{idx:{w}d}" + "".join(f"  {_fmt_d(z.real)},{_fmt_d(z.imag)}" for z in vals)
 
-    out = ["", " " + "*" * 79, "", f"{'':30s}FREQU\xcaNCIA = {r.freq:14.7E}".replace("E", "D"), "",
+    out = ["", " " + "*" * 79, "", f"{'':30s}FREQ\xdc\xcaNCIA = {_fmt_d(r.freq, 14, 7)}", "",
            " " + "*" * 79, "", " RESULTADOS", "", "  N\xd3S DO CONTORNO", "",
            " ELEM      DESLOCAMENTO X           DESLOCAMENTOT Y           DESLOCAMENTO Z", ""]
     out += [row(i + 1, v) for i, v in enumerate(r.disp)]

@@ -85,6 +85,17 @@ def test_results_format_roundtrip(tmp_path, golden_dir):
     assert max(err.values()) == 0.0
 
 
+@pytest.mark.parametrize("tag", ["240", "2160"])
+def test_results_block_is_byte_exact(golden_dir, tag):
+    """format_results re-creates the shipped result block (Outputec.for:21-59)
+    byte for byte from the parsed values: labels, Fortran D formats, spacing."""
+    path = os.path.join(golden_dir, f"SSOLO{tag}D_-5+5.SOL")
+    lines = open(path, encoding="latin-1").read().split("\n")
+    i = next(k for k, ln in enumerate(lines) if "FREQ\xdc\xcaNCIA =" in ln)
+    block = "\n".join(lines[i - 3:])
+    assert formats.format_results(formats.parse_results(path)[0]) == block
+
+
 def test_oracle_static_solve_satisfies_its_system():
     """The static extension's restatement: H x = G dfi after the swap, and
     the prescribed values come back unchanged through the un-swap."""
