@@ -1,0 +1,68 @@
+"""The reference's golden-file checker (src/dtester.c), compiled into
+oracle/_ref/dtester by `make -C oracle ref`, run on a result written in the
+reference's output layout: the golden file's header (the echo of the input
+data, which the checker reads the mesh sizes from), then the result block of
+Outputec.for:21-59 (formats.format_results)."""
+import os
+import re
+import subprocess
+
+from bem_mececcs_b200 import formats
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DTESTER = os.path.join(ROOT, "oracle", "_ref", "dtester")
+ENC = "latin-1"
+KEYS = ("disp", "traction", "idisp", "sigma")
+
+
+def available() -> bool:
+    return os.access(DTESTER, os.X_OK)
+
+
+def build() -> bool:
+    """Builds the checker where the reference tree is present; True if it exists."""
+    if not available():
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"],
+                       capture_output=True)
+    return available()
+
+
+def header(gold_path: str) -> str:
+    """The golden file's lines before its result block."""
+    lines = open(gold_path, encoding=ENC).read().split("\n")
+    i = next(k for k, ln in enumerate(lines) if "FREQ\xdc\xcaNCIA =" in ln)
+    return "\n".join(lines[:i - 3]) + "\n"
+
+
+def write(path: str, gold_path: str, res: "formats.Results") -> None:
+    with open(path, "w", encoding=ENC) as fh:
+        fh.write(header(gold_path) + formats.format_results(res))
+
+
+def run(ours: str, gold_path: str):
+    """(exit status, the four errors the checker prints)."""
+    p = subprocess.run([DTESTER, ours, gold_path], capture_output=True, text=True, encoding=ENC)
+    vals = [float(v) for v in re.findall(r":\s*([-+0-9.E]+)\s*$", p.stdout, re.M)]
+    if len(vals) != 4:
+        raise AssertionError(f"unexpected checker output: {p.stdout!r} {p.stderr!r}")
+    return p.returncode, dict(zip(KEYS, vals))
+
+
+def judge(res: "formats.Results", gold_path: str, workdir: str):
+    """Writes `res` beside the golden header and runs the checker on it.
+    Returns (exit status, the checker's four errors, formats.dtester_errors
+    on the same two files).  The file holds 4 printed digits, so the last two
+    agree with each other, not with the metric taken on `res` in memory."""
+    ours = os.path.join(workdir, "ours_" + os.path.basename(gold_path))
+    write(ours, gold_path, res)
+    rc, ref_err = run(ours, gold_path)
+    file_err = formats.dtester_errors(formats.parse_results(ours)[0],
+                                      formats.parse_results(gold_path)[0])
+    return rc, ref_err, file_err
+
+
+def result_block(gold_path: str) -> str:
+    """The golden file's result block, from its frequency line to the end."""
+    lines = open(gold_path, encoding=ENC).read().split("\n")
+    i = next(k for k, ln in enumerate(lines) if "FREQ\xdc\xcaNCIA =" in ln)
+    return "\n".join(lines[i - 3:])

@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import oracle
+import refcheck
 from bem_mececcs_b200 import capi, formats, host, meshgen
 from bem_mececcs_b200.solver import BemSolver
 from gpu_util import rel
@@ -108,7 +109,9 @@ def test_interec1_seam_matches_native():
     assert rel(zdsol, ozd) < TOL
 
 
-def _golden_on_gpu(golden_dir, stem):
+def _golden_on_gpu(golden_dir, stem, workdir):
+    """dtester's errors of the all-GPU result (restated metric), and the
+    reference's own checker run on it where oracle/_ref/dtester is built."""
     s = formats.read_static(os.path.join(golden_dir, f"ESOLO{stem}E_-5+5.DAT"))
     d = formats.read_dynamic(os.path.join(golden_dir, f"ESOLO{stem}D_-5+5.DAT"), s.nbe)
     sol = BemSolver(s)
@@ -120,17 +123,27 @@ def _golden_on_gpu(golden_dir, stem):
     sol.ctx.close()
     mine = formats.Results(fr, disp.reshape(-1, 3), trac.reshape(-1, 3),
                            zdsol.reshape(-1, 3), zssol.reshape(-1, 9))
-    gold = formats.parse_results(os.path.join(golden_dir, f"SSOLO{stem}D_-5+5.SOL"))[0]
-    return formats.dtester_errors(mine, gold)
+    gold_path = os.path.join(golden_dir, f"SSOLO{stem}D_-5+5.SOL")
+    err = formats.dtester_errors(mine, formats.parse_results(gold_path)[0])
+    ref = refcheck.judge(mine, gold_path, workdir) if refcheck.available() else None
+    return err, ref
 
 
-def test_golden_240_all_on_gpu(golden_dir):
-    """src/tests.sh:38-50 with boundary AND interior results from the GPU."""
-    err = _golden_on_gpu(golden_dir, "240")
+def _check(err, ref):
     assert all(v <= 1e-3 for v in err.values()), err
+    if ref is not None:
+        rc, ref_err, file_err = ref
+        assert rc == 0, ref_err
+        for k, v in ref_err.items():
+            assert v <= 1e-3 and v == pytest.approx(file_err[k], rel=1e-5, abs=1e-12), \
+                (k, ref_err, file_err)
+
+
+def test_golden_240_all_on_gpu(golden_dir, tmp_path):
+    """src/tests.sh:38-50 with boundary AND interior results from the GPU."""
+    _check(*_golden_on_gpu(golden_dir, "240", str(tmp_path)))
 
 
 @pytest.mark.slow
-def test_golden_2160_all_on_gpu(golden_dir):
-    err = _golden_on_gpu(golden_dir, "2160")
-    assert all(v <= 1e-3 for v in err.values()), err
+def test_golden_2160_all_on_gpu(golden_dir, tmp_path):
+    _check(*_golden_on_gpu(golden_dir, "2160", str(tmp_path)))

@@ -7,7 +7,9 @@ oracle/_ref/dtester; these tests write the oracle's solution of ESOLO240 and
 ESOLO2160 in the reference's output layout (the golden file's header, then
 the result block of Outputec.for) and require that
 
-- the reference's checker accepts it (exit status 0),
+- the oracle's result block, printed to the golden file's 4 digits, is the
+  shipped one byte for byte, and the reference's checker accepts it (exit
+  status 0, every error zero),
 - the four errors it prints equal formats.dtester_errors, the restatement the
   GPU parity tests use, to the printed precision,
 - a mistake planted in the oracle's output (one displacement moved by 2e-3) is
@@ -16,44 +18,22 @@ the result block of Outputec.for) and require that
 Skipped where neither the built checker nor the reference tree is present.
 """
 import os
-import re
-import subprocess
 
 import numpy as np
 import pytest
 
 import oracle
+import refcheck
 from bem_mececcs_b200 import formats
 
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-DTESTER = os.path.join(ROOT, "oracle", "_ref", "dtester")
 EPS = 1.0e-3  # src/dtester.c:24
-_ENC = "latin-1"
 
 
 @pytest.fixture(scope="module")
 def dtester():
-    if not os.access(DTESTER, os.X_OK):
-        r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"],
-                           capture_output=True)
-        if r.returncode != 0 or not os.access(DTESTER, os.X_OK):
-            pytest.skip("the reference's checker is not built and its source is absent")
-    return DTESTER
-
-
-def _header(gold_path):
-    """The golden file's lines before its first result block (the echo of the
-    input data, which the checker reads the mesh sizes from)."""
-    lines = open(gold_path, encoding=_ENC).read().split("\n")
-    i = next(k for k, ln in enumerate(lines) if "FREQ\xdc\xcaNCIA =" in ln)
-    return "\n".join(lines[:i - 3]) + "\n"
-
-
-def _run_dtester(exe, ours, gold):
-    p = subprocess.run([exe, ours, gold], capture_output=True, text=True, encoding=_ENC)
-    vals = [float(v) for v in re.findall(r":\s*([-+0-9.E]+)\s*$", p.stdout, re.M)]
-    assert len(vals) == 4, p.stdout
-    return p.returncode, dict(zip(("disp", "traction", "idisp", "sigma"), vals))
+    if not refcheck.build():
+        pytest.skip("the reference's checker is not built and its source is absent")
+    return refcheck.DTESTER
 
 
 def _oracle_results(golden_dir, tag):
@@ -68,20 +48,19 @@ def _oracle_results(golden_dir, tag):
                            zdsol.reshape(-1, 3), zssol.reshape(-1, 9))
 
 
-def _write(path, header, res):
-    with open(path, "w", encoding=_ENC) as fh:
-        fh.write(header + formats.format_results(res))
-
-
 @pytest.mark.parametrize("tag", ["240", pytest.param("2160", marks=pytest.mark.slow)])
 def test_reference_checker_accepts_the_oracle(tmp_path, golden_dir, dtester, tag):
     gold_path = os.path.join(golden_dir, f"SSOLO{tag}D_-5+5.SOL")
     res = _oracle_results(golden_dir, tag)
     ours = str(tmp_path / f"ours{tag}.SOL")
-    _write(ours, _header(gold_path), res)
+    refcheck.write(ours, gold_path, res)
 
-    rc, ref_err = _run_dtester(dtester, ours, gold_path)
+    rc, ref_err = refcheck.run(ours, gold_path)
     assert rc == 0, ref_err
+    # printed to the golden file's 4 digits, the oracle's result block is the
+    # shipped one byte for byte, so every error the checker prints is zero
+    assert formats.format_results(res) == refcheck.result_block(gold_path)
+    assert all(v == 0.0 for v in ref_err.values()), ref_err
     # the restated metric on the same two files
     mine = formats.parse_results(ours)[0]
     gold = formats.parse_results(gold_path)[0]
@@ -97,9 +76,9 @@ def test_reference_checker_rejects_a_planted_mistake(tmp_path, golden_dir, dtest
     res.disp = res.disp.copy()
     res.disp[17, 1] += 2.0e-3
     ours = str(tmp_path / "planted.SOL")
-    _write(ours, _header(gold_path), res)
+    refcheck.write(ours, gold_path, res)
 
-    rc, ref_err = _run_dtester(dtester, ours, gold_path)
+    rc, ref_err = refcheck.run(ours, gold_path)
     assert rc == 1 and ref_err["disp"] > EPS
     err = formats.dtester_errors(formats.parse_results(ours)[0],
                                  formats.parse_results(gold_path)[0])
@@ -113,6 +92,6 @@ def test_reference_checker_rejects_a_planted_mistake(tmp_path, golden_dir, dtest
 def test_reference_checker_on_the_golden_file_itself(golden_dir, dtester):
     for tag in ("240", "2160"):
         g = os.path.join(golden_dir, f"SSOLO{tag}D_-5+5.SOL")
-        rc, ref_err = _run_dtester(dtester, g, g)
+        rc, ref_err = refcheck.run(g, g)
         assert rc == 0 and all(v == 0.0 for v in ref_err.values())
         assert np.all(np.isfinite(formats.parse_results(g)[0].sigma))
