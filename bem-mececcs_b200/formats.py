@@ -1,8 +1,9 @@
 """Input and output file formats of BEM-MECECCS.
 
-The static input (read by INPUTECE, src/Inputece.for:16-108), the dynamic
-input (INPUTECD, src/Inputecd.for:7-139) and the per-frequency result block
-of the dynamic output (OUTPUTEC, src/Outputec.for:9-68).  Files are Latin-1
+The static input (read by INPUTECE, src/Inputece.for:16-108) and its echo in
+the static output, the dynamic input (INPUTECD, src/Inputecd.for:7-139) and
+the per-frequency result block of the dynamic output (OUTPUTEC,
+src/Outputec.for:9-68).  Files are Latin-1
 text; numbers are read with Fortran list-directed semantics: every READ
 statement starts on a new record, takes as many values as it needs across
 records and drops the rest of its last record.
@@ -138,6 +139,35 @@ def write_static(path, s: StaticInput) -> None:
     out += [" " + " ".join(f"{int(v)}." for v in row) for row in s.cone]
     with open(path, "w", encoding=_ENC) as fh:
         fh.write("\n".join(out) + "\n")
+
+
+def format_static_echo(s: StaticInput) -> str:
+    """The static output file: INPUTECE's echo of what it read, with the
+    element centroids it computes (src/Inputece.for:29-104; formats 100, 200,
+    300, 400, 500, 550).  The reference's known-answer test requires this file
+    to equal the shipped SSOLO*E_-5+5.SOL byte for byte (src/tests.sh:43)."""
+    def d(v, w, k):
+        return _fmt_d(float(v), w, k)
+
+    out = ["", " " + "*" * 79, "", f"{s.title[:75]:<75s}", "", "", "DADOS", "",
+           f"  N\xdaMERO DE ELEMENTOS DA MALHA= {s.n:4d}",
+           f"  N\xdaMERO DE ELEMENTOS DE CONTORNO= {s.nbe:4d}",
+           f"  N\xdaMERO DE PONTOS EXTREMOS DOS ELEMENTOS= {s.np:4d}",
+           f"  N\xdaMERO DE PONTOS DE GAUSS= {s.npg:3d}",
+           f"  M\xd3DULO DE CISALHAMENTO= {d(s.ge, 14, 7)}",
+           f"  COEFICIENTE DE POISSON= {d(s.rnu, 14, 7)}",
+           "", "", "  COORDENADAS DOS PONTOS EXTREMOS DOS ELEMENTOS DE CONTORNO", "",
+           f"    PONTO{'':10s}X{'':18s}Y{'':18s}Z"]
+    out += [f"    {i + 1:4d}" + "".join(f"     {d(v, 14, 7)}" for v in xyz)
+            for i, xyz in enumerate(zip(s.cx, s.cy, s.cz))]
+    out += ["", "", "  CONECTIVIDADE DOS ELEMENTOS DE CONTORNO", "",
+            f" ELEMENTO{'':3s}EXTR I{'':3s}EXTR J{'':3s}EXTR K{'':3s}EXTR L"
+            f"{'':5s}XMED{'':8s}YMED{'':8s}ZMED"]
+    cxm, cym, czm = s.centroids()
+    out += [f"{i + 1:6d}" + "".join(f"{int(c):9d}" for c in s.cone[i]) + "  "
+            + "".join(d(v, 12, 4) for v in (cxm[i], cym[i], czm[i]))
+            for i in range(s.n)]
+    return "\n".join(out) + "\n"
 
 
 def write_dynamic(path, d: DynamicInput) -> None:

@@ -86,6 +86,27 @@ def test_results_format_roundtrip(tmp_path, golden_dir):
 
 
 @pytest.mark.parametrize("tag", ["240", "2160"])
+def test_static_echo_is_byte_exact(golden_dir, tag):
+    """src/tests.sh:41-46: the static output (INPUTECE's echo with the element
+    centroids the solver collocates at) equals the shipped SSOLO*E file byte
+    for byte, from the reader and the centroids the product path uses."""
+    s = formats.read_static(os.path.join(golden_dir, f"ESOLO{tag}E_-5+5.DAT"))
+    with open(os.path.join(golden_dir, f"SSOLO{tag}E_-5+5.SOL"), encoding="latin-1") as fh:
+        gold = fh.read()
+    assert formats.format_static_echo(s) == gold
+
+
+def test_fixtures_match_their_checksums(golden_dir):
+    import hashlib
+    with open(os.path.join(golden_dir, "SHA256SUMS")) as fh:
+        sums = [ln.split() for ln in fh if ln.strip()]
+    assert len(sums) == 8
+    for digest, name in sums:
+        with open(os.path.join(golden_dir, name), "rb") as fh:
+            assert hashlib.sha256(fh.read()).hexdigest() == digest, name
+
+
+@pytest.mark.parametrize("tag", ["240", "2160"])
 def test_results_block_is_byte_exact(golden_dir, tag):
     """format_results re-creates the shipped result block (Outputec.for:21-59)
     byte for byte from the parsed values: labels, Fortran D formats, spacing."""
