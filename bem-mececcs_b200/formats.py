@@ -3,10 +3,10 @@
 The static input (read by INPUTECE, src/Inputece.for:16-108) and its echo in
 the static output, the dynamic input (INPUTECD, src/Inputecd.for:7-139) and
 the per-frequency result block of the dynamic output (OUTPUTEC,
-src/Outputec.for:9-68).  Files are Latin-1
-text; numbers are read with Fortran list-directed semantics: every READ
-statement starts on a new record, takes as many values as it needs across
-records and drops the rest of its last record.
+src/Outputec.for:9-68).  Files are Latin-1 text; numbers are read with
+Fortran list-directed semantics: every READ statement starts on a new
+record, takes as many values as it needs across records and drops the rest
+of its last record.
 """
 from __future__ import annotations
 
@@ -170,6 +170,59 @@ def format_static_echo(s: StaticInput) -> str:
     return "\n".join(out) + "\n"
 
 
+def format_dynamic_echo(s: StaticInput, d: DynamicInput, material) -> str:
+    """The head of the dynamic output file: INPUTECD's echo of the mesh and of
+    what it read, with the derived complex material `material` = (ZGE, ZCS,
+    ZCP) (src/Inputecd.for:23-136; formats 100, 200, 230, 250, 300, 400, 500,
+    550, 600, 650, 700, 750).  The result blocks of format_results follow it."""
+    def f(v, w, k):
+        return _fmt_d(float(v), w, k)
+
+    zge, zcs, zcp = material
+    out = ["", " " + "*" * 79, "", f"{d.title[:75]:<75s}", "", "", "DADOS", "",
+           f"  N\xdaMERO DE ELEMENTOS DA MALHA= {s.n:4d}",
+           f"  N\xdaMERO DE ELEMENTOS DE CONTORNO= {s.nbe:4d}",
+           f"  N\xdaMERO DE PONTOS EXTREMOS DOS ELEMENTOS= {s.np:4d}",
+           f"  N\xdaMERO DE PONTOS INTERNOS= {d.l:3d}",
+           f"  N\xdaMERO DE PONTOS DE GAUSS= {s.npg:3d}",
+           f"  N\xdaMERO DE FREQ\xdc\xcaNCIAS= {d.nfr:3d}",
+           f"  M\xd3DULO DE CISALHAMENTO (REAL)= {f(s.ge, 14, 7)}",
+           f"  COEFICIENTE DE POISSON= {f(s.rnu, 14, 7)}",
+           f"  COEFICIENTE DE AMORTECIMENTO= {f(d.dam, 14, 7)}",
+           f"  DENSIDADE DE MASSA= {f(d.rho, 14, 7)}",
+           "", "", "DADOS DERIVADOS", "",
+           f"  M\xd3DULO DE CISALHAMENTO (COMPLEXO)= {f(zge.real, 14, 7)}{f(zge.imag, 14, 7)}",
+           f"  VELOCIDADE DA ONDA-S (COMPLEXO)= {f(zcs.real, 14, 7)}{f(zcs.imag, 14, 7)}",
+           f"  VELOCIDADE DA ONDA-P (COMPLEXO)= {f(zcp.real, 14, 7)}{f(zcp.imag, 14, 7)}",
+           "", "  FREQUENCIAS", ""]
+    fr = list(d.freqs)
+    out += ["".join(f"  {f(v, 14, 7)}" for v in fr[k:k + 5]) for k in range(0, len(fr), 5)]
+    out += ["", "", "  COORDENADAS DOS PONTOS EXTREMOS DOS ELEMENTOS DA MALHA", "",
+            f"    PONTO{'':10s}X{'':18s}Y{'':18s}Z"]
+    out += [f"    {i + 1:4d}" + "".join(f"     {f(v, 14, 7)}" for v in xyz)
+            for i, xyz in enumerate(zip(s.cx, s.cy, s.cz))]
+    out += ["", "", "  CONECTIVIDADE DOS ELEMENTOS DA MALHA", "",
+            f" ELEMENTO{'':3s}EXTR I{'':3s}EXTR J{'':3s}EXTR K{'':3s}EXTR L"
+            f"{'':5s}XMED{'':8s}YMED{'':8s}ZMED"]
+    cxm, cym, czm = s.centroids()
+    out += [f"{i + 1:6d}" + "".join(f"{int(c):9d}" for c in s.cone[i]) + "  "
+            + "".join(f(v, 12, 4) for v in (cxm[i], cym[i], czm[i]))
+            for i in range(s.n)]
+    out += ["", "", "  CONDI\xc7\xd5ES DE CONTORNO", "",
+            (f"{'':8s}" + f"VALOR PRESCRITO{'':10s}" * 3).rstrip(),  # a final nX writes nothing
+            f" ELEM{'':6s}DIRE\xc7\xc3O X{'':4s}C\xd3DIGO{'':6s}DIRE\xc7\xc3O Y{'':4s}C\xd3DIGO"
+            f"{'':6s}DIRE\xc7\xc3O Z{'':4s}C\xd3DIGO"]
+    out += [(f"{i + 1:4d}" + "".join(f"    {f(d.bc[3 * i + j], 10, 3)}      {int(d.kode[3 * i + j]):3d}  "
+                                     for j in range(3))).rstrip()
+            for i in range(s.nbe)]
+    if d.l > 0:
+        out += ["", "", "  COORDENADAS DOS PONTOS INTERNOS ", "",
+                f"    PONTO{'':10s}X{'':18s}Y{'':17s} Z"]
+        out += [f"    {i + 1:3d}" + "".join(f(v, 19, 7) for v in xyz)
+                for i, xyz in enumerate(zip(d.cxi, d.cyi, d.czi))]
+    return "\n".join(out) + "\n"
+
+
 def write_dynamic(path, d: DynamicInput) -> None:
     """Writes a file INPUTECD reads back unchanged."""
     out = [d.title, " ", f"{d.l} {d.nfr} {_r(d.dam)} {_r(d.rho)}", ""]
@@ -289,6 +342,15 @@ def format_results(r: Results) -> str:
         out += [row(i + 1, v, 4) for i, v in enumerate(r.sigma)]
     out.append(" " + "*" * 230)
     return "\n".join(out) + "\n"
+
+
+def write_dynamic_output(path, s: StaticInput, d: DynamicInput, material, results) -> None:
+    """The dynamic output file the reference writes: INPUTECD's echo, then one
+    OUTPUTEC block per frequency (`results`, a list of Results)."""
+    with open(path, "w", encoding=_ENC) as fh:
+        fh.write(format_dynamic_echo(s, d, material))
+        for r in results:
+            fh.write(format_results(r))
 
 
 def dtester_errors(a: Results, b: Results) -> dict:

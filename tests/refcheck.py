@@ -1,13 +1,13 @@
 """The reference's golden-file checker (src/dtester.c), compiled into
-oracle/_ref/dtester by `make -C oracle ref`, run on a result written in the
-reference's output layout: the golden file's header (the echo of the input
-data, which the checker reads the mesh sizes from), then the result block of
-Outputec.for:21-59 (formats.format_results)."""
+oracle/_ref/dtester by `make -C oracle ref`, run on a dynamic output file
+written the way the reference writes it (formats.write_dynamic_output:
+INPUTECD's echo, from which the checker reads the mesh sizes, then the
+OUTPUTEC result block)."""
 import os
 import re
 import subprocess
 
-from bem_mececcs_b200 import formats
+from bem_mececcs_b200 import formats, host
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DTESTER = os.path.join(ROOT, "oracle", "_ref", "dtester")
@@ -27,16 +27,9 @@ def build() -> bool:
     return available()
 
 
-def header(gold_path: str) -> str:
-    """The golden file's lines before its result block."""
-    lines = open(gold_path, encoding=ENC).read().split("\n")
-    i = next(k for k, ln in enumerate(lines) if "FREQ\xdc\xcaNCIA =" in ln)
-    return "\n".join(lines[:i - 3]) + "\n"
-
-
-def write(path: str, gold_path: str, res: "formats.Results") -> None:
-    with open(path, "w", encoding=ENC) as fh:
-        fh.write(header(gold_path) + formats.format_results(res))
+def write(path: str, s, d, res: "formats.Results") -> None:
+    """The output file of the run (s, d) whose only frequency gave `res`."""
+    formats.write_dynamic_output(path, s, d, host.material(s.ge, s.rnu, d.dam, d.rho), [res])
 
 
 def run(ours: str, gold_path: str):
@@ -48,13 +41,13 @@ def run(ours: str, gold_path: str):
     return p.returncode, dict(zip(KEYS, vals))
 
 
-def judge(res: "formats.Results", gold_path: str, workdir: str):
-    """Writes `res` beside the golden header and runs the checker on it.
+def judge(s, d, res: "formats.Results", gold_path: str, workdir: str):
+    """Writes the output file of the run (s, d) and runs the checker on it.
     Returns (exit status, the checker's four errors, formats.dtester_errors
     on the same two files).  The file holds 4 printed digits, so the last two
     agree with each other, not with the metric taken on `res` in memory."""
     ours = os.path.join(workdir, "ours_" + os.path.basename(gold_path))
-    write(ours, gold_path, res)
+    write(ours, s, d, res)
     rc, ref_err = run(ours, gold_path)
     file_err = formats.dtester_errors(formats.parse_results(ours)[0],
                                       formats.parse_results(gold_path)[0])

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import oracle
-from bem_mececcs_b200 import formats, meshgen
+from bem_mececcs_b200 import formats, host, meshgen
 
 EPS = 1.0e-3  # src/dtester.c:24
 
@@ -94,6 +94,32 @@ def test_static_echo_is_byte_exact(golden_dir, tag):
     with open(os.path.join(golden_dir, f"SSOLO{tag}E_-5+5.SOL"), encoding="latin-1") as fh:
         gold = fh.read()
     assert formats.format_static_echo(s) == gold
+
+
+@pytest.mark.parametrize("tag", ["240", "2160"])
+def test_dynamic_echo_is_byte_exact(golden_dir, tag):
+    """The head of the shipped SSOLO*D file (INPUTECD's echo, with the derived
+    complex material ZGE, ZCS, ZCP that the product path computes) byte for byte."""
+    s = formats.read_static(os.path.join(golden_dir, f"ESOLO{tag}E_-5+5.DAT"))
+    d = formats.read_dynamic(os.path.join(golden_dir, f"ESOLO{tag}D_-5+5.DAT"), s.nbe)
+    with open(os.path.join(golden_dir, f"SSOLO{tag}D_-5+5.SOL"), encoding="latin-1") as fh:
+        lines = fh.read().split("\n")
+    i = next(k for k, ln in enumerate(lines) if "FREQ\xdc\xcaNCIA =" in ln)
+    echo = formats.format_dynamic_echo(s, d, host.material(s.ge, s.rnu, d.dam, d.rho))
+    assert echo == "\n".join(lines[:i - 3]) + "\n"
+
+
+@pytest.mark.parametrize("tag", ["240", pytest.param("2160", marks=pytest.mark.slow)])
+def test_oracle_output_file_is_the_shipped_one(tmp_path, golden_dir, tag):
+    """src/tests.sh:48-53 at its strictest: the oracle's whole dynamic output
+    file (echo + result block, 4 printed digits) IS SSOLO*D_-5+5.SOL."""
+    s = formats.read_static(os.path.join(golden_dir, f"ESOLO{tag}E_-5+5.DAT"))
+    d = formats.read_dynamic(os.path.join(golden_dir, f"ESOLO{tag}D_-5+5.DAT"), s.nbe)
+    mine, _ = _run(golden_dir, tag)
+    out = tmp_path / "out.sol"
+    formats.write_dynamic_output(out, s, d, host.material(s.ge, s.rnu, d.dam, d.rho), [mine])
+    with open(os.path.join(golden_dir, f"SSOLO{tag}D_-5+5.SOL"), "rb") as fh:
+        assert out.read_bytes() == fh.read()
 
 
 def test_fixtures_match_their_checksums(golden_dir):

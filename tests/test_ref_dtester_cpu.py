@@ -4,8 +4,8 @@ src/tests.sh:38-117 judges a run by compiling src/dtester.c and running it on
 the run's output file against the shipped SSOLO*D_-5+5.SOL.  oracle/Makefile
 (`make -C oracle ref`) compiles that checker from the reference tree into
 oracle/_ref/dtester; these tests write the oracle's solution of ESOLO240 and
-ESOLO2160 in the reference's output layout (the golden file's header, then
-the result block of Outputec.for) and require that
+ESOLO2160 as the reference's output file (formats.write_dynamic_output) and
+require that
 
 - the oracle's result block, printed to the golden file's 4 digits, is the
   shipped one byte for byte, and the reference's checker accepts it (exit
@@ -44,16 +44,16 @@ def _oracle_results(golden_dir, tag):
     fr = d.freqs[0]
     disp, tr, _ = p.solve(fr)
     zdsol, zssol = p.interior(fr, disp, tr)
-    return formats.Results(fr, disp.reshape(-1, 3), tr.reshape(-1, 3),
-                           zdsol.reshape(-1, 3), zssol.reshape(-1, 9))
+    return s, d, formats.Results(fr, disp.reshape(-1, 3), tr.reshape(-1, 3),
+                                 zdsol.reshape(-1, 3), zssol.reshape(-1, 9))
 
 
 @pytest.mark.parametrize("tag", ["240", pytest.param("2160", marks=pytest.mark.slow)])
 def test_reference_checker_accepts_the_oracle(tmp_path, golden_dir, dtester, tag):
     gold_path = os.path.join(golden_dir, f"SSOLO{tag}D_-5+5.SOL")
-    res = _oracle_results(golden_dir, tag)
+    s, d, res = _oracle_results(golden_dir, tag)
     ours = str(tmp_path / f"ours{tag}.SOL")
-    refcheck.write(ours, gold_path, res)
+    refcheck.write(ours, s, d, res)
 
     rc, ref_err = refcheck.run(ours, gold_path)
     assert rc == 0, ref_err
@@ -72,11 +72,11 @@ def test_reference_checker_accepts_the_oracle(tmp_path, golden_dir, dtester, tag
 
 def test_reference_checker_rejects_a_planted_mistake(tmp_path, golden_dir, dtester):
     gold_path = os.path.join(golden_dir, "SSOLO240D_-5+5.SOL")
-    res = _oracle_results(golden_dir, "240")
+    s, d, res = _oracle_results(golden_dir, "240")
     res.disp = res.disp.copy()
     res.disp[17, 1] += 2.0e-3
     ours = str(tmp_path / "planted.SOL")
-    refcheck.write(ours, gold_path, res)
+    refcheck.write(ours, s, d, res)
 
     rc, ref_err = refcheck.run(ours, gold_path)
     assert rc == 1 and ref_err["disp"] > EPS
