@@ -382,7 +382,8 @@ def run_ours(args):
         "speedup_vs_plain_fp64": round(value / value_plain, 3),
         "roofline": roof,
         "rooflines_all": {k: {kk: v[kk] for kk in ("achieved", "frac", "ms") if kk in v} |
-                          ({"tensor_frac": v["tensor"]["frac"]} if "tensor" in v else {})
+                          ({"tensor_frac": v["tensor"]["frac"]} if "tensor" in v else {}) |
+                          ({"fp64_frac": v["fp64"]["frac"]} if "fp64" in v else {})
                           for k, v in roof_all.items()},
         "peaks_measured_tflops": mpeaks,
         "kernel_share": shares,
@@ -537,6 +538,14 @@ def _peaks():
         return {}
 
 
+# Flops of one Stokes evaluation with its Gauss-weighted accumulation into H
+# and G, and of one element's geometry at one Gauss point, counted once on the
+# reference's arithmetic (SOLFUND, NONSINGD) by an operation-counting
+# restatement of the oracle that a test keeps equal to these figures.  Two
+# complex exponentials (2 exp + 2 sincos calls) per evaluation come on top.
+STOKES_FLOPS_PER_EVAL = 613
+GEOMETRY_FLOPS_PER_GAUSS_POINT = 98
+
 KERNELS = {
     "assembly": "k_dyn_diag + k_dyn_offdiag + k_rhs_reduce (FP64 Stokes assembly, BC swap, RHS)",
     "panel": "k_panel_push (LU panel, one 16-CTA cluster per problem; pivot candidates pushed by remote "
@@ -577,8 +586,15 @@ def _roofline(name, k, peaks, mpeaks):
                          "frac": round(tf / peak, 4),
                          "peak_source": "measured: tcgen05 kind::tf32 M=128 N=128 issue-rate "
                                         "microbenchmark (bem_measure_peaks)"}
-    if name == "assembly":
-        out["stokes_evals_per_s"] = round(k["work"] / secs, 1)
+    if name == "assembly" and secs > 0:
+        evals = k["work"] / secs
+        out["stokes_evals_per_s"] = round(evals, 1)
+        tf = evals * STOKES_FLOPS_PER_EVAL / 1e12
+        fp64 = mpeaks.get("fp64_fma") if isinstance(mpeaks, dict) else None
+        out["fp64"] = {"achieved_tflops": round(tf, 2), "flops_per_eval": STOKES_FLOPS_PER_EVAL,
+                       "transcendentals_per_eval": "2 exp + 2 sincos, not in the flops",
+                       "peak_tflops": fp64, "frac": round(tf / fp64, 4) if fp64 else None,
+                       "peak_source": "measured: FP64 FMA issue-rate microbenchmark (bem_measure_peaks)"}
     return out
 
 
