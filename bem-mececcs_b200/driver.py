@@ -1,0 +1,72 @@
+"""The reference's driver over its files: one mesh, every frequency.
+
+`run_case` does what the reference's main program does with its four file
+arguments (src/Main.for:85-200): read the static input and echo it
+(INPUTECE), compute the static diagonals (GHMATECE), read the dynamic input
+and echo it (INPUTECD), then per frequency assemble and solve (GHMATECD,
+LINSOLVE), un-swap and evaluate the interior points (INTEREC) and append the
+frequency's result block (OUTPUTEC).  The files it writes are the reference's
+formats (formats.format_static_echo, formats.write_dynamic_output).
+
+Frequencies are solved one at a time in FP64 (form "plain", what the
+reference does), or all together by the lockstep sweep of the mixed form
+(FP32 LU on tensor cores + FP64 refinement, form "mixed"), whose solutions
+are un-swapped on the host.
+
+Every frequency starts from the boundary conditions read from the file.  The
+reference's CPU build un-swaps into its ZDFI array in place
+(src/Interec.for:62-66 on the array set once at src/Main.for:158), so with
+more than one frequency and any KODE = 0 its later frequencies start from the
+previous frequency's tractions; that is not reproduced.  With one frequency
+or KODE = 1 everywhere (the shipped cases) the two agree.  The reference also
+lists FR, |ZFI(157)| and |ZFI(166)| on a unit it never opens
+(src/Outputec.for:61, a compiler-named file); that side file is not written.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import formats
+from .solver import BemSolver, unswap_host
+
+_ENC = "latin-1"
+
+
+def run_case(input_e, input_d, output_e, output_d, *, form: str = "plain", refine: int = 3,
+             device: int = 0, solver_factory=None) -> list:
+    """Runs the case of the four files; returns the list of Results (one per
+    frequency) that output_d holds.  `solver_factory(static, device)` makes
+    the solver (BemSolver by default)."""
+    if form not in ("plain", "mixed"):
+        raise ValueError(f"form must be 'plain' or 'mixed', not {form!r}")
+    s = formats.read_static(input_e)
+    with open(output_e, "w", encoding=_ENC) as fh:
+        fh.write(formats.format_static_echo(s))
+    make = solver_factory or (lambda st, dev: BemSolver(st, device=dev))
+    sol = make(s, device)
+    try:
+        sol.ghmatece()
+        d = formats.read_dynamic(input_d, s.nbe)
+        zdfi = np.asarray(d.bc, dtype=np.complex128)
+        sol.set_bc(d.kode, zdfi, d.dam, d.rho)
+        freqs = [float(f) for f in d.freqs]
+        if form == "mixed" and freqs:
+            x, _ = sol.sweep(freqs, form="mixed", batch=sol.sweep_batch_limit("mixed"), refine=refine)
+            bound = [unswap_host(x[i], d.kode, zdfi, sol.material[0]) for i in range(len(freqs))]
+        else:
+            bound = None
+        results = []
+        for i, fr in enumerate(freqs):
+            disp, trac = bound[i] if bound is not None else sol.solve_frequency(fr)
+            if d.l > 0:
+                zdsol, zssol = sol.interior(fr, disp, trac, d.cxi, d.cyi, d.czi)
+            else:
+                zdsol, zssol = np.zeros(0, dtype=np.complex128), np.zeros(0, dtype=np.complex128)
+            results.append(formats.Results(fr, np.asarray(disp).reshape(-1, 3),
+                                           np.asarray(trac).reshape(-1, 3),
+                                           np.asarray(zdsol).reshape(-1, 3),
+                                           np.asarray(zssol).reshape(-1, 9)))
+        formats.write_dynamic_output(output_d, s, d, sol.material, results)
+        return results
+    finally:
+        sol.ctx.close()

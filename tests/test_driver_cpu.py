@@ -1,0 +1,125 @@
+"""driver.run_case, the reference's main program over its four files
+(src/Main.for:85-200), with an oracle-backed stand-in for the GPU solver.
+
+The stand-in has BemSolver's interface and answers from the oracle, so the
+driver's own work (reading, echoing, the frequency loop, the un-swap of the
+mixed form, interior points, writing) is checked here on the CPU: on the
+reference's ESOLO240 case both output files must be the shipped ones byte for
+byte, and a multi-frequency case with prescribed displacements must give each
+frequency the solution of its own system from the file's boundary conditions.
+The GPU solver behind the same calls is checked in tests/test_gpu_driver.py.
+"""
+import os
+import types
+
+import numpy as np
+import pytest
+
+import oracle
+from bem_mececcs_b200 import driver, formats, host
+
+
+class OracleSolver:
+    """BemSolver's interface, answered by the oracle (test only)."""
+
+    def __init__(self, s, d):
+        self.s, self.d = s, d
+        self.p = oracle.OracleProblem(s, d)
+        self.ctx = types.SimpleNamespace(close=lambda: None)
+        self.calls = []
+
+    def ghmatece(self):
+        self.calls.append("ghmatece")
+        self.p.ghmatece()
+
+    def set_bc(self, kode, zdfi, dam, rho):
+        self.calls.append("set_bc")
+        assert np.array_equal(kode, self.d.kode) and np.array_equal(zdfi, self.d.bc)
+        self.material = host.material(self.s.ge, self.s.rnu, dam, rho)
+
+    def solve_frequency(self, fr):
+        self.calls.append(("solve", fr))
+        disp, trac, _ = self.p.solve(fr, use_openblas=False)
+        return disp, trac
+
+    def sweep_batch_limit(self, form):
+        return 7
+
+    def sweep(self, freqs, *, form, batch, refine):
+        self.calls.append(("sweep", tuple(freqs), form, batch))
+        return np.array([self.p.solve(f, use_openblas=False)[2] for f in freqs]), np.zeros(len(freqs))
+
+    def interior(self, fr, disp, trac, cxi, cyi, czi):
+        self.calls.append(("interior", fr))
+        return self.p.interior(fr, disp, trac)
+
+
+def _factory(d, made):
+    def make(s, device):
+        sol = OracleSolver(s, d)
+        made.append(sol)
+        return sol
+    return make
+
+
+@pytest.mark.parametrize("form", ["plain", "mixed"])
+def test_reference_case_files_come_out_byte_identical(tmp_path, golden_dir, form):
+    ein = os.path.join(golden_dir, "ESOLO240E_-5+5.DAT")
+    din = os.path.join(golden_dir, "ESOLO240D_-5+5.DAT")
+    s = formats.read_static(ein)
+    d = formats.read_dynamic(din, s.nbe)
+    made = []
+    eout, dout = tmp_path / "SSOLO240E.DAT", tmp_path / "SSOLO240D.DAT"
+    res = driver.run_case(ein, din, eout, dout, form=form, solver_factory=_factory(d, made))
+    assert len(res) == 1 and res[0].freq == d.freqs[0]
+    for out, gold in ((eout, "SSOLO240E_-5+5.SOL"), (dout, "SSOLO240D_-5+5.SOL")):
+        with open(os.path.join(golden_dir, gold), "rb") as fh:
+            assert out.read_bytes() == fh.read(), gold
+    calls = made[0].calls
+    assert calls[:2] == ["ghmatece", "set_bc"]
+    if form == "mixed":
+        assert calls[2] == ("sweep", (float(d.freqs[0]),), "mixed", 7)
+    else:
+        assert calls[2] == ("solve", float(d.freqs[0]))
+
+
+def test_every_frequency_starts_from_the_file_boundary_conditions(tmp_path, golden_dir):
+    """Three frequencies, a third of the components with prescribed
+    displacement: each block is the solution of that frequency's own system
+    from the file's BCs (the reference's in-place ZDFI update is not carried
+    from one frequency to the next)."""
+    ein = os.path.join(golden_dir, "ESOLO240E_-5+5.DAT")
+    s = formats.read_static(ein)
+    d = formats.read_dynamic(os.path.join(golden_dir, "ESOLO240D_-5+5.DAT"), s.nbe)
+    rng = np.random.default_rng(8)
+    d.freqs = np.array([0.5, 1.0, 2.25])
+    d.nfr = 3
+    d.kode = np.where(rng.random(d.kode.size) < 0.33, 0, 1).astype(np.int32)
+    d.bc = np.where(d.kode == 0, 0.01 * rng.standard_normal(d.kode.size), d.bc)
+    din = tmp_path / "d.dat"
+    formats.write_dynamic(din, d)
+    d2 = formats.read_dynamic(din, s.nbe)
+    outs = {}
+    for form in ("plain", "mixed"):
+        made = []
+        res = driver.run_case(ein, din, tmp_path / f"e_{form}", tmp_path / f"d_{form}", form=form,
+                              solver_factory=_factory(d2, made))
+        back = formats.parse_results(tmp_path / f"d_{form}")
+        assert [b.freq for b in back] == pytest.approx([0.5, 1.0, 2.25])
+        p = oracle.OracleProblem(s, d2)
+        p.ghmatece()
+        for r, fr in zip(res, (0.5, 1.0, 2.25)):
+            disp, trac, _ = p.solve(fr, use_openblas=False)
+            assert np.allclose(r.disp.ravel(), disp, rtol=0, atol=1e-13 * np.abs(disp).max())
+            assert np.allclose(r.traction.ravel(), trac, rtol=0, atol=1e-13 * np.abs(trac).max())
+            # prescribed displacements come back as given, every frequency
+            assert np.array_equal(r.disp.ravel()[d2.kode == 0], d2.bc[d2.kode == 0])
+        outs[form] = (tmp_path / f"d_{form}").read_bytes()
+    assert outs["plain"] == outs["mixed"]
+
+
+def test_unknown_form_is_refused(tmp_path, golden_dir):
+    with pytest.raises(ValueError):
+        driver.run_case(os.path.join(golden_dir, "ESOLO240E_-5+5.DAT"),
+                        os.path.join(golden_dir, "ESOLO240D_-5+5.DAT"),
+                        tmp_path / "e", tmp_path / "d", form="fp16")
