@@ -127,6 +127,13 @@ def read_dynamic(path, nbe: int) -> DynamicInput:
                         p[:, 0].copy(), p[:, 1].copy(), p[:, 2].copy())
 
 
+def _fmt_i(v, width: int) -> str:
+    """Fortran Iw: right-justified, or `width` asterisks when the number does
+    not fit."""
+    t = str(int(v))
+    return t.rjust(width) if len(t) <= width else "*" * width
+
+
 def _r(v) -> str:
     """Shortest decimal that reads back to the same double."""
     return repr(float(v))
@@ -150,21 +157,21 @@ def format_static_echo(s: StaticInput) -> str:
         return _fmt_d(float(v), w, k)
 
     out = ["", " " + "*" * 79, "", f"{s.title[:75]:<75s}", "", "", "DADOS", "",
-           f"  N\xdaMERO DE ELEMENTOS DA MALHA= {s.n:4d}",
-           f"  N\xdaMERO DE ELEMENTOS DE CONTORNO= {s.nbe:4d}",
-           f"  N\xdaMERO DE PONTOS EXTREMOS DOS ELEMENTOS= {s.np:4d}",
-           f"  N\xdaMERO DE PONTOS DE GAUSS= {s.npg:3d}",
+           f"  N\xdaMERO DE ELEMENTOS DA MALHA= {_fmt_i(s.n, 4)}",
+           f"  N\xdaMERO DE ELEMENTOS DE CONTORNO= {_fmt_i(s.nbe, 4)}",
+           f"  N\xdaMERO DE PONTOS EXTREMOS DOS ELEMENTOS= {_fmt_i(s.np, 4)}",
+           f"  N\xdaMERO DE PONTOS DE GAUSS= {_fmt_i(s.npg, 3)}",
            f"  M\xd3DULO DE CISALHAMENTO= {d(s.ge, 14, 7)}",
            f"  COEFICIENTE DE POISSON= {d(s.rnu, 14, 7)}",
            "", "", "  COORDENADAS DOS PONTOS EXTREMOS DOS ELEMENTOS DE CONTORNO", "",
            f"    PONTO{'':10s}X{'':18s}Y{'':18s}Z"]
-    out += [f"    {i + 1:4d}" + "".join(f"     {d(v, 14, 7)}" for v in xyz)
+    out += [f"    {_fmt_i(i + 1, 4)}" + "".join(f"     {d(v, 14, 7)}" for v in xyz)
             for i, xyz in enumerate(zip(s.cx, s.cy, s.cz))]
     out += ["", "", "  CONECTIVIDADE DOS ELEMENTOS DE CONTORNO", "",
             f" ELEMENTO{'':3s}EXTR I{'':3s}EXTR J{'':3s}EXTR K{'':3s}EXTR L"
             f"{'':5s}XMED{'':8s}YMED{'':8s}ZMED"]
     cxm, cym, czm = s.centroids()
-    out += [f"{i + 1:6d}" + "".join(f"{int(c):9d}" for c in s.cone[i]) + "  "
+    out += [_fmt_i(i + 1, 6) + "".join(_fmt_i(c, 9) for c in s.cone[i]) + "  "
             + "".join(d(v, 12, 4) for v in (cxm[i], cym[i], czm[i]))
             for i in range(s.n)]
     return "\n".join(out) + "\n"
@@ -180,12 +187,12 @@ def format_dynamic_echo(s: StaticInput, d: DynamicInput, material) -> str:
 
     zge, zcs, zcp = material
     out = ["", " " + "*" * 79, "", f"{d.title[:75]:<75s}", "", "", "DADOS", "",
-           f"  N\xdaMERO DE ELEMENTOS DA MALHA= {s.n:4d}",
-           f"  N\xdaMERO DE ELEMENTOS DE CONTORNO= {s.nbe:4d}",
-           f"  N\xdaMERO DE PONTOS EXTREMOS DOS ELEMENTOS= {s.np:4d}",
-           f"  N\xdaMERO DE PONTOS INTERNOS= {d.l:3d}",
-           f"  N\xdaMERO DE PONTOS DE GAUSS= {s.npg:3d}",
-           f"  N\xdaMERO DE FREQ\xdc\xcaNCIAS= {d.nfr:3d}",
+           f"  N\xdaMERO DE ELEMENTOS DA MALHA= {_fmt_i(s.n, 4)}",
+           f"  N\xdaMERO DE ELEMENTOS DE CONTORNO= {_fmt_i(s.nbe, 4)}",
+           f"  N\xdaMERO DE PONTOS EXTREMOS DOS ELEMENTOS= {_fmt_i(s.np, 4)}",
+           f"  N\xdaMERO DE PONTOS INTERNOS= {_fmt_i(d.l, 3)}",
+           f"  N\xdaMERO DE PONTOS DE GAUSS= {_fmt_i(s.npg, 3)}",
+           f"  N\xdaMERO DE FREQ\xdc\xcaNCIAS= {_fmt_i(d.nfr, 3)}",
            f"  M\xd3DULO DE CISALHAMENTO (REAL)= {f(s.ge, 14, 7)}",
            f"  COEFICIENTE DE POISSON= {f(s.rnu, 14, 7)}",
            f"  COEFICIENTE DE AMORTECIMENTO= {f(d.dam, 14, 7)}",
@@ -199,26 +206,26 @@ def format_dynamic_echo(s: StaticInput, d: DynamicInput, material) -> str:
     out += ["".join(f"  {f(v, 14, 7)}" for v in fr[k:k + 5]) for k in range(0, len(fr), 5)]
     out += ["", "", "  COORDENADAS DOS PONTOS EXTREMOS DOS ELEMENTOS DA MALHA", "",
             f"    PONTO{'':10s}X{'':18s}Y{'':18s}Z"]
-    out += [f"    {i + 1:4d}" + "".join(f"     {f(v, 14, 7)}" for v in xyz)
+    out += [f"    {_fmt_i(i + 1, 4)}" + "".join(f"     {f(v, 14, 7)}" for v in xyz)
             for i, xyz in enumerate(zip(s.cx, s.cy, s.cz))]
     out += ["", "", "  CONECTIVIDADE DOS ELEMENTOS DA MALHA", "",
             f" ELEMENTO{'':3s}EXTR I{'':3s}EXTR J{'':3s}EXTR K{'':3s}EXTR L"
             f"{'':5s}XMED{'':8s}YMED{'':8s}ZMED"]
     cxm, cym, czm = s.centroids()
-    out += [f"{i + 1:6d}" + "".join(f"{int(c):9d}" for c in s.cone[i]) + "  "
+    out += [_fmt_i(i + 1, 6) + "".join(_fmt_i(c, 9) for c in s.cone[i]) + "  "
             + "".join(f(v, 12, 4) for v in (cxm[i], cym[i], czm[i]))
             for i in range(s.n)]
     out += ["", "", "  CONDI\xc7\xd5ES DE CONTORNO", "",
             (f"{'':8s}" + f"VALOR PRESCRITO{'':10s}" * 3).rstrip(),  # a final nX writes nothing
             f" ELEM{'':6s}DIRE\xc7\xc3O X{'':4s}C\xd3DIGO{'':6s}DIRE\xc7\xc3O Y{'':4s}C\xd3DIGO"
             f"{'':6s}DIRE\xc7\xc3O Z{'':4s}C\xd3DIGO"]
-    out += [(f"{i + 1:4d}" + "".join(f"    {f(d.bc[3 * i + j], 10, 3)}      {int(d.kode[3 * i + j]):3d}  "
-                                     for j in range(3))).rstrip()
+    out += [(_fmt_i(i + 1, 4) + "".join(f"    {f(d.bc[3 * i + j], 10, 3)}      "
+                                        f"{_fmt_i(d.kode[3 * i + j], 3)}  " for j in range(3))).rstrip()
             for i in range(s.nbe)]
     if d.l > 0:
         out += ["", "", "  COORDENADAS DOS PONTOS INTERNOS ", "",
                 f"    PONTO{'':10s}X{'':18s}Y{'':17s} Z"]
-        out += [f"    {i + 1:3d}" + "".join(f(v, 19, 7) for v in xyz)
+        out += [f"    {_fmt_i(i + 1, 3)}" + "".join(f(v, 19, 7) for v in xyz)
                 for i, xyz in enumerate(zip(d.cxi, d.cyi, d.czi))]
     return "\n".join(out) + "\n"
 
@@ -304,17 +311,17 @@ def parse_results(path) -> list:
 
 
 def _fmt_d(v: float, width: int = 11, digits: int = 4) -> str:
-    """Fortran Dw.d: 0.dddd D+ee with the leading zero kept."""
+    """Fortran Dw.d: 0.dddd D+ee with the leading zero kept (a three-digit
+    exponent drops the D).  The digits are the correctly rounded decimal
+    expansion of the double, taken from Python's %e conversion."""
     if v == 0.0:
         body = "0." + "0" * digits + "D+00"
     else:
-        e = int(np.floor(np.log10(abs(v)))) + 1
-        m = abs(v) / 10.0 ** e
-        mant = round(m, digits)
-        if mant >= 1.0:
-            mant /= 10.0
-            e += 1
-        body = f"0.{int(round(mant * 10 ** digits)):0{digits}d}D{'+' if e >= 0 else '-'}{abs(e):02d}"
+        t = f"{abs(v):.{digits - 1}e}"  # d.ddde+XX, rounding carries included
+        e = int(t[digits + 2:]) + 1
+        mant = t[0] + t[2:digits + 1]
+        body = (f"0.{mant}D{'+' if e >= 0 else '-'}{abs(e):02d}" if abs(e) < 100
+                else f"0.{mant}{'+' if e >= 0 else '-'}{abs(e):03d}")
         if v < 0:
             body = "-" + body
     return body.rjust(width)
@@ -323,7 +330,7 @@ def _fmt_d(v: float, width: int = 11, digits: int = 4) -> str:
 def format_results(r: Results) -> str:
     """The OUTPUTEC block (Outputec.for:21-59) for one frequency."""
     def row(idx, vals, w=5):
-        return f"{idx:{w}d}" + "".join(f"  {_fmt_d(z.real)},{_fmt_d(z.imag)}" for z in vals)
+        return _fmt_i(idx, w) + "".join(f"  {_fmt_d(z.real)},{_fmt_d(z.imag)}" for z in vals)
 
     out = ["", " " + "*" * 79, "", f"{'':30s}FREQ\xdc\xcaNCIA = {_fmt_d(r.freq, 14, 7)}", "",
            " " + "*" * 79, "", " RESULTADOS", "", "  N\xd3S DO CONTORNO", "",
