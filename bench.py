@@ -163,15 +163,31 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU baseline: the oracle's restatement of the reference CPU path.
 # ---------------------------------------------------------------------------
+_TIMING_LIB: list = []
+
+
+def _timing_build(oracle):
+    """The oracle compiled with the reference's CPU flags on this host, once
+    per process: (library path or None, what was timed)."""
+    if not _TIMING_LIB:
+        path, why = oracle.timing_lib(tempfile.mkdtemp(prefix="bem_cpu_"))
+        flags = " ".join(oracle.REFERENCE_CFLAGS)
+        _TIMING_LIB.append((path, f"oracle port built with the reference's flags ({flags})" if path else
+                            f"oracle port, parity build -O2 (the {flags} build failed: {why})"))
+    return _TIMING_LIB[0]
+
+
 def cpu_freq_solve_seconds(s, d, zh_sys, zfi_sys, fr, *, budget_s=8.0):
     """Time of one frequency solve on the host: GHMATECD (OpenMP over element
     columns, timed on a bounded sample of columns and scaled), ZGEMV and
-    ZGESV (OpenBLAS, all threads) on the full system.  Returns
+    ZGESV (OpenBLAS, all threads) on the full system.  GHMATECD runs the
+    oracle compiled the way the reference compiles its CPU path.  Returns
     (seconds, sample description, threads)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from scipy.linalg import lapack
-    p = oracle.OracleProblem(s, d)
+    lib_path, built = _timing_build(oracle)
+    p = oracle.OracleProblem(s, d, lib_path=lib_path)
     p.ghmatece()
     nbe = s.nbe
     zh = np.zeros(p.nn * p.nn, dtype=np.complex128)
@@ -198,7 +214,7 @@ def cpu_freq_solve_seconds(s, d, zh_sys, zfi_sys, fr, *, budget_s=8.0):
     except Exception:
         threads = os.cpu_count()
     sample = (f"GHMATECD on {cols} of {nbe} element columns (scaled x{nbe / cols:.1f}, "
-              f"{t_asm:.2f} s est.), full ZGEMV+ZGESV n={p.nn} ({t_lu:.2f} s)")
+              f"{t_asm:.2f} s est.; {built}), full ZGEMV+ZGESV n={p.nn} ({t_lu:.2f} s, OpenBLAS)")
     return t_asm + t_lu, sample, int(threads)
 
 

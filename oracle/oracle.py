@@ -33,38 +33,72 @@ def build() -> str:
     return path
 
 
-def lib():
+_BOUND: dict = {}
+
+# The reference builds its CPU path with these (src/Makefile:17-18); the
+# timing variant of the oracle uses them, the parity build does not.
+REFERENCE_CFLAGS = ["-march=native", "-Ofast", "-funroll-loops", "-fopenmp"]
+
+
+def timing_lib(outdir: str):
+    """Compiles bem_oracle.c with the reference's CPU flags into outdir (on
+    the machine that will run it: -march=native).  Returns (path, "") or,
+    when that fails, (None, the compiler's complaint).  For timing only:
+    -Ofast gives up the parity build's bit-for-bit arithmetic."""
+    out = os.path.join(outdir, "liboracle_ofast.so")
+    cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
+    try:
+        r = subprocess.run([cc, *REFERENCE_CFLAGS, "-fPIC", "-std=c11", "-shared", "-o", out,
+                            os.path.join(_HERE, "bem_oracle.c"), "-lm"],
+                           capture_output=True, text=True, timeout=300)
+    except (OSError, subprocess.TimeoutExpired) as e:
+        return None, str(e)
+    if r.returncode != 0:
+        return None, (r.stderr.strip().splitlines() or ["compiler failed"])[-1]
+    return out, ""
+
+
+def lib(path: str | None = None):
+    """The oracle's ctypes library: the parity build (liboracle.so) unless
+    `path` names another build of bem_oracle.c."""
     global _LIB
+    if path is not None:
+        if path not in _BOUND:
+            _BOUND[path] = _bind(ctypes.CDLL(path))
+        return _BOUND[path]
     if _LIB is None:
         path = os.path.join(_HERE, "liboracle.so")
         if not os.path.exists(path):
             build()
-        L = ctypes.CDLL(path)
-        L.orc_gauleg.argtypes = [_int, _d, _d]
-        L.orc_normvec.argtypes = [_int, _i, _d, _d, _d, _d]
-        L.orc_centroids.argtypes = [_int, _i, _d, _d, _d, _d, _d, _d]
-        L.orc_material.argtypes = [_dbl, _dbl, _dbl, _dbl, _d, _d, _d]
-        L.orc_static_consts.argtypes = [_dbl, _dbl, _d]
-        geo = [_int, _int, _int, _int, _i, _d, _d, _d]
-        L.orc_ghmatece.argtypes = geo + [_d, _d, _d, _d, _d, _d, _dbl, _dbl, _d, _d,
-                                         ctypes.c_void_p]
-        L.orc_ghmatecd.argtypes = geo + [_d, _d, _d, _d, _d, _d, _d, _d, _d, _d, _dbl,
-                                         _d, _d, _c, _c]
-        L.orc_ghmatecd_cols.argtypes = geo + [_d, _d, _d, _d, _d, _d, _d, _d, _d, _d, _dbl,
-                                              _d, _d, _int, _int, _c, _c]
-        L.orc_boundary_conditions.argtypes = [_int, _c, _c, _i, _d]
-        L.orc_zgemv.argtypes = [_int, _c, _c, _c]
-        L.orc_zgesv.argtypes = [_int, _c, _i, _c]
-        L.orc_unswap.argtypes = [_int, _i, _d, _c, _c]
-        L.orc_interior_disp.argtypes = geo + [_d, _d, _d, _int, _d, _d, _d, _d, _d, _d,
-                                              _dbl, _c, _c, _c]
-        L.orc_interior_stress.argtypes = geo + [_d, _d, _d, _int, _d, _d, _d, _d, _d,
-                                                _d, _dbl, _dbl, _c, _c, _c]
-        L.orc_solfund.argtypes = [_d, _d, _d, _d, _d, _d, _dbl, _c, _c]
-        L.orc_static_solve.argtypes = geo + [_d, _d, _d, _d, _d, _d, _dbl, _dbl, _i, _d, _d, _d,
-                                             ctypes.c_void_p, ctypes.c_void_p]
-        _LIB = L
+        _LIB = _bind(ctypes.CDLL(path))
     return _LIB
+
+
+def _bind(L):
+    L.orc_gauleg.argtypes = [_int, _d, _d]
+    L.orc_normvec.argtypes = [_int, _i, _d, _d, _d, _d]
+    L.orc_centroids.argtypes = [_int, _i, _d, _d, _d, _d, _d, _d]
+    L.orc_material.argtypes = [_dbl, _dbl, _dbl, _dbl, _d, _d, _d]
+    L.orc_static_consts.argtypes = [_dbl, _dbl, _d]
+    geo = [_int, _int, _int, _int, _i, _d, _d, _d]
+    L.orc_ghmatece.argtypes = geo + [_d, _d, _d, _d, _d, _d, _dbl, _dbl, _d, _d,
+                                     ctypes.c_void_p]
+    L.orc_ghmatecd.argtypes = geo + [_d, _d, _d, _d, _d, _d, _d, _d, _d, _d, _dbl,
+                                     _d, _d, _c, _c]
+    L.orc_ghmatecd_cols.argtypes = geo + [_d, _d, _d, _d, _d, _d, _d, _d, _d, _d, _dbl,
+                                          _d, _d, _int, _int, _c, _c]
+    L.orc_boundary_conditions.argtypes = [_int, _c, _c, _i, _d]
+    L.orc_zgemv.argtypes = [_int, _c, _c, _c]
+    L.orc_zgesv.argtypes = [_int, _c, _i, _c]
+    L.orc_unswap.argtypes = [_int, _i, _d, _c, _c]
+    L.orc_interior_disp.argtypes = geo + [_d, _d, _d, _int, _d, _d, _d, _d, _d, _d,
+                                          _dbl, _c, _c, _c]
+    L.orc_interior_stress.argtypes = geo + [_d, _d, _d, _int, _d, _d, _d, _d, _d,
+                                            _d, _dbl, _dbl, _c, _c, _c]
+    L.orc_solfund.argtypes = [_d, _d, _d, _d, _d, _d, _dbl, _c, _c]
+    L.orc_static_solve.argtypes = geo + [_d, _d, _d, _d, _d, _d, _dbl, _dbl, _i, _d, _d, _d,
+                                         ctypes.c_void_p, ctypes.c_void_p]
+    return L
 
 
 def gauleg(npg: int):
@@ -112,8 +146,11 @@ def zgesv(a: np.ndarray, b: np.ndarray, *, use_openblas: bool | None = None):
 class OracleProblem:
     """One mesh with its dynamic input, set up as src/Main.for:108-158 does."""
 
-    def __init__(self, static, dynamic):
+    def __init__(self, static, dynamic, lib_path: str | None = None):
+        """lib_path: another build of bem_oracle.c (timing_lib) instead of
+        the parity build."""
         self.s, self.d = static, dynamic
+        self._lib = lib(lib_path)
         s = static
         self.cone = s.cone_fortran()
         self.cx = np.ascontiguousarray(s.cx, dtype=np.float64)
@@ -121,9 +158,9 @@ class OracleProblem:
         self.cz = np.ascontiguousarray(s.cz, dtype=np.float64)
         self.gi, self.ome = gauleg(s.npg)
         self.etas = np.zeros(3 * s.n)
-        lib().orc_normvec(s.n, self.cone, self.cx, self.cy, self.cz, self.etas)
+        self._lib.orc_normvec(s.n, self.cone, self.cx, self.cy, self.cz, self.etas)
         self.cxm, self.cym, self.czm = (np.zeros(s.n) for _ in range(3))
-        lib().orc_centroids(s.n, self.cone, self.cx, self.cy, self.cz,
+        self._lib.orc_centroids(s.n, self.cone, self.cx, self.cy, self.cz,
                             self.cxm, self.cym, self.czm)
         self.c = static_consts(s.ge, s.rnu)
         self.zge, self.zcs, self.zcp = material(s.ge, s.rnu, dynamic.dam, dynamic.rho)
@@ -139,7 +176,7 @@ class OracleProblem:
         self.hestdiag = np.zeros(9 * s.nbe)
         self.gestdiag = np.zeros(9 * s.nbe)
         hest = np.zeros(9 * s.nbe * s.n) if want_hest else None
-        st = lib().orc_ghmatece(*self._geo(), self.cxm, self.cym, self.czm, self.etas,
+        st = self._lib.orc_ghmatece(*self._geo(), self.cxm, self.cym, self.czm, self.etas,
                                 self.gi, self.ome, s.ge, s.rnu, self.hestdiag,
                                 self.gestdiag,
                                 hest.ctypes.data_as(ctypes.c_void_p) if hest is not None
@@ -155,7 +192,7 @@ class OracleProblem:
         nn = self.nn
         zh = np.zeros(nn * nn, dtype=np.complex128)
         zg = np.zeros(nn * nn, dtype=np.complex128)
-        st = lib().orc_ghmatecd(*self._geo(), self.cxm, self.cym, self.czm, self.etas,
+        st = self._lib.orc_ghmatecd(*self._geo(), self.cxm, self.cym, self.czm, self.etas,
                                 self.gi, self.ome, self.c, self.zge, self.zcs, self.zcp,
                                 float(fr), self.hestdiag, self.gestdiag, zh, zg)
         if st != 0:
@@ -169,7 +206,7 @@ class OracleProblem:
         nn = self.nn
         zh = np.zeros(nn * nn, dtype=np.complex128) if zh is None else zh
         zg = np.zeros(nn * nn, dtype=np.complex128) if zg is None else zg
-        st = lib().orc_ghmatecd_cols(*self._geo(), self.cxm, self.cym, self.czm, self.etas,
+        st = self._lib.orc_ghmatecd_cols(*self._geo(), self.cxm, self.cym, self.czm, self.etas,
                                      self.gi, self.ome, self.c, self.zge, self.zcs, self.zcp,
                                      float(fr), self.hestdiag, self.gestdiag, int(jlo), int(jhi),
                                      zh, zg)
@@ -190,7 +227,7 @@ class OracleProblem:
         g = np.zeros(nn * nn) if want_matrices else None
         hp = h.ctypes.data_as(ctypes.c_void_p) if want_matrices else None
         gp = g.ctypes.data_as(ctypes.c_void_p) if want_matrices else None
-        st = lib().orc_static_solve(*self._geo(), self.cxm, self.cym, self.czm, self.etas,
+        st = self._lib.orc_static_solve(*self._geo(), self.cxm, self.cym, self.czm, self.etas,
                                     self.gi, self.ome, float(s.ge), float(s.rnu), kode, dfi,
                                     disp, trac, hp, gp)
         if st != 0:
@@ -203,11 +240,11 @@ class OracleProblem:
         zh, zg = self.ghmatecd(fr)
         zh0, zg0 = zh.copy(), zg.copy()
         kode = np.ascontiguousarray(self.d.kode, dtype=np.int32)
-        lib().orc_boundary_conditions(self.nn, zh, zg, kode, self.zge)
+        self._lib.orc_boundary_conditions(self.nn, zh, zg, kode, self.zge)
         if zdfi is None:
             zdfi = self.d.bc.astype(np.complex128)
         zfi = np.zeros(self.nn, dtype=np.complex128)
-        lib().orc_zgemv(self.nn, zg, np.ascontiguousarray(zdfi, dtype=np.complex128), zfi)
+        self._lib.orc_zgemv(self.nn, zg, np.ascontiguousarray(zdfi, dtype=np.complex128), zfi)
         return zh, zfi, zh0, zg0
 
     def solve(self, fr: float, *, use_openblas: bool | None = None, zdfi=None):
@@ -218,7 +255,7 @@ class OracleProblem:
         disp = x.copy()
         tr = (self.d.bc.astype(np.complex128) if zdfi is None else
               np.asarray(zdfi, dtype=np.complex128)).copy()
-        lib().orc_unswap(self.nn, np.ascontiguousarray(self.d.kode, dtype=np.int32),
+        self._lib.orc_unswap(self.nn, np.ascontiguousarray(self.d.kode, dtype=np.int32),
                          self.zge, disp, tr)
         return disp, tr, x
 
@@ -229,11 +266,11 @@ class OracleProblem:
         if d.l <= 0:
             return zdsol, zssol
         pts = [np.ascontiguousarray(a, dtype=np.float64) for a in (d.cxi, d.cyi, d.czi)]
-        st = lib().orc_interior_disp(*self._geo(), self.etas, self.gi, self.ome, d.l,
+        st = self._lib.orc_interior_disp(*self._geo(), self.etas, self.gi, self.ome, d.l,
                                      *pts, self.zge, self.zcs, self.zcp, float(fr),
                                      np.ascontiguousarray(zfi), np.ascontiguousarray(zdfi),
                                      zdsol)
-        st |= lib().orc_interior_stress(*self._geo(), self.etas, self.gi, self.ome, d.l,
+        st |= self._lib.orc_interior_stress(*self._geo(), self.etas, self.gi, self.ome, d.l,
                                         *pts, self.zge, self.zcs, self.zcp, d.rho,
                                         float(fr), np.ascontiguousarray(zfi),
                                         np.ascontiguousarray(zdfi), zssol)

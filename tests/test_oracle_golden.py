@@ -159,3 +159,20 @@ def test_oracle_static_solve_satisfies_its_system():
     assert np.linalg.norm(H @ x - G @ dfi) < 1e-12 * np.linalg.norm(G @ dfi)
     k0 = d.kode == 0
     assert np.array_equal(disp[k0], dfi[k0]) and np.array_equal(trac[~k0], dfi[~k0])
+
+
+def test_timing_build_computes_the_same_system(tmp_path):
+    """The benchmark's CPU leg times bem_oracle.c built with the reference's
+    flags (-march=native -Ofast ...); it must still compute GHMATECD, to the
+    rounding that fast-math allows."""
+    path, why = oracle.timing_lib(str(tmp_path))
+    if path is None:
+        pytest.skip(f"no compiler for the timing build: {why}")
+    s, d = meshgen.config_mesh("c1_240")
+    ref = oracle.OracleProblem(s, d)
+    fast = oracle.OracleProblem(s, d, lib_path=path)
+    assert fast._lib is not ref._lib
+    zh0, zg0 = ref.ghmatecd(1.0)
+    zh1, zg1 = fast.ghmatecd(1.0)
+    assert np.linalg.norm(zh1 - zh0) <= 1e-11 * np.linalg.norm(zh0)
+    assert np.linalg.norm(zg1 - zg0) <= 1e-11 * np.linalg.norm(zg0)
