@@ -176,3 +176,45 @@ def test_timing_build_computes_the_same_system(tmp_path):
     zh1, zg1 = fast.ghmatecd(1.0)
     assert np.linalg.norm(zh1 - zh0) <= 1e-11 * np.linalg.norm(zh0)
     assert np.linalg.norm(zg1 - zg0) <= 1e-11 * np.linalg.norm(zg0)
+
+
+def test_oracle_reports_a_collapsed_element():
+    """The GPU test's failure case, on the oracle: an element collapsed onto a
+    line has DET < 1e-5, where the reference's CPU routines stop with
+    'NONSING : ERRO, JACOBIANO NULO OU NEGATIVO' (src/Nonsinge.for:88,
+    src/Nonsingd.for:89-94) and its GPU kernels return status 1 with 'Matriz
+    Singular' (src/kernels/Ghmatecd_cu.cu:438); the oracle's static and
+    dynamic assemblies both report status 1."""
+    s, d = meshgen.config_mesh("c1_240")
+    c = s.cone[5] - 1
+    s.cx[c[2]], s.cy[c[2]] = s.cx[c[1]], s.cy[c[1]]
+    s.cx[c[3]], s.cy[c[3]] = s.cx[c[0]], s.cy[c[0]]
+    p = oracle.OracleProblem(s, d)
+    with pytest.raises(RuntimeError, match="GHMATECE status 1"):
+        p.ghmatece()
+    p.hestdiag = np.zeros(9 * s.nbe)  # skip the static part to reach GHMATECD
+    p.gestdiag = np.zeros(9 * s.nbe)
+    with pytest.raises(RuntimeError, match="GHMATECD status 1"):
+        p.ghmatecd(1.0)
+
+
+@pytest.mark.parametrize("use_openblas", [False, True])
+def test_oracle_zgesv_reports_a_singular_matrix(use_openblas):
+    rng = np.random.default_rng(4)
+    a = rng.standard_normal((40, 40)) + 1j * rng.standard_normal((40, 40))
+    a[:, 17] = 0.0
+    with pytest.raises(np.linalg.LinAlgError):
+        oracle.zgesv(a, np.ones(40, dtype=np.complex128), use_openblas=use_openblas)
+
+
+def test_smallest_enclosed_mesh_solves():
+    """One boundary element (n = 3) in its enclosure: the smallest system."""
+    s = meshgen.enclosed_grid(1, 1, jitter=0.0, seed=0, depth=2.5, layers=1)
+    d = meshgen.traction_patch(s, radius=2.0, freqs=(1.0,))
+    assert s.nbe == 1
+    p = oracle.OracleProblem(s, d)
+    p.ghmatece()
+    zh, zfi, _, _ = p.system(1.0)
+    disp, trac, x = p.solve(1.0, use_openblas=False)
+    a = zh.reshape(3, 3, order="F")
+    assert np.all(np.isfinite(x)) and np.linalg.norm(a @ x - zfi) <= 1e-13 * np.linalg.norm(zfi)
