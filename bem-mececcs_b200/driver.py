@@ -24,6 +24,8 @@ lists FR, |ZFI(157)| and |ZFI(166)| on a unit it never opens
 """
 from __future__ import annotations
 
+import time
+
 import numpy as np
 
 from . import formats
@@ -33,33 +35,59 @@ _ENC = "latin-1"
 
 
 def run_case(input_e, input_d, output_e, output_d, *, form: str = "plain", refine: int = 3,
-             device: int = 0, solver_factory=None) -> list:
+             device: int = 0, solver_factory=None, log=None) -> list:
     """Runs the case of the four files; returns the list of Results (one per
     frequency) that output_d holds.  `solver_factory(static, device)` makes
-    the solver (BemSolver by default)."""
+    the solver (BemSolver by default).  `log` (e.g. print), if given,
+    receives the reference's stage-time lines ("Tempo gasto alocando os
+    vetores compartilhados: <s>", "<ROUTINE>: Tempo na GPU: <s>" for
+    GHMATECE and per frequency GHMATECD, LINSOLVE and INTEREC1; src/Main.for:
+    135, src/Ghmatece.for:244-245, src/Ghmatecd.for:224-226,
+    src/Linsolve.for:54-57, src/Interec.for:171-173), which the reference's
+    analysis script reads.  The interior stresses are computed in the same
+    kernel as the interior displacements, so INTEREC1 covers both and no
+    SIGMAEC line is written; the mixed form's lockstep sweep reports one
+    "SWEEP: Tempo na GPU: <s>" line in place of GHMATECD and LINSOLVE."""
     if form not in ("plain", "mixed"):
         raise ValueError(f"form must be 'plain' or 'mixed', not {form!r}")
     s = formats.read_static(input_e)
     with open(output_e, "w", encoding=_ENC) as fh:
         fh.write(formats.format_static_echo(s))
     make = solver_factory or (lambda st, dev: BemSolver(st, device=dev))
+    t0 = time.perf_counter()
     sol = make(s, device)
+    stage = _Stages(sol, log)
+    stage.done("Tempo gasto alocando os vetores compartilhados:", t0)
     try:
+        t0 = time.perf_counter()
         sol.ghmatece()
+        stage.done("GHMATECE: Tempo na GPU:", t0)
         d = formats.read_dynamic(input_d, s.nbe)
         zdfi = np.asarray(d.bc, dtype=np.complex128)
         sol.set_bc(d.kode, zdfi, d.dam, d.rho)
         freqs = [float(f) for f in d.freqs]
         if form == "mixed" and freqs:
+            t0 = time.perf_counter()
             x, _ = sol.sweep(freqs, form="mixed", batch=sol.sweep_batch_limit("mixed"), refine=refine)
+            stage.done("SWEEP: Tempo na GPU:", t0)
             bound = [unswap_host(x[i], d.kode, zdfi, sol.material[0]) for i in range(len(freqs))]
         else:
             bound = None
         results = []
         for i, fr in enumerate(freqs):
-            disp, trac = bound[i] if bound is not None else sol.solve_frequency(fr)
+            if bound is not None:
+                disp, trac = bound[i]
+            else:
+                t0 = time.perf_counter()
+                sol.ghmatecd(fr)
+                t0 = stage.done("GHMATECD: Tempo na GPU:", t0)
+                sol.linsolve()
+                stage.done("LINSOLVE: Tempo na GPU:", t0)
+                disp, trac = sol.interec()
             if d.l > 0:
+                t0 = time.perf_counter()
                 zdsol, zssol = sol.interior(fr, disp, trac, d.cxi, d.cyi, d.czi)
+                stage.done("INTEREC1: Tempo na GPU:", t0)
             else:
                 zdsol, zssol = np.zeros(0, dtype=np.complex128), np.zeros(0, dtype=np.complex128)
             results.append(formats.Results(fr, np.asarray(disp).reshape(-1, 3),
@@ -70,3 +98,19 @@ def run_case(input_e, input_d, output_e, output_d, *, form: str = "plain", refin
         return results
     finally:
         sol.ctx.close()
+
+
+class _Stages:
+    """Stage timer: waits for the device, logs '<label> <seconds>' in the
+    reference's list-directed style and returns the end time."""
+
+    def __init__(self, sol, log):
+        self.sol, self.log = sol, log
+
+    def done(self, label: str, t0: float) -> float:
+        if self.log is None:
+            return time.perf_counter()
+        self.sol.ctx.sync()
+        t = time.perf_counter()
+        self.log(f" {label} {t - t0:24.16E}")
+        return t

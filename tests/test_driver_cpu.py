@@ -10,6 +10,7 @@ frequency the solution of its own system from the file's boundary conditions.
 The GPU solver behind the same calls is checked in tests/test_gpu_driver.py.
 """
 import os
+import re
 import types
 
 import numpy as np
@@ -25,7 +26,7 @@ class OracleSolver:
     def __init__(self, s, d):
         self.s, self.d = s, d
         self.p = oracle.OracleProblem(s, d)
-        self.ctx = types.SimpleNamespace(close=lambda: None)
+        self.ctx = types.SimpleNamespace(close=lambda: None, sync=lambda: None)
         self.calls = []
 
     def ghmatece(self):
@@ -37,10 +38,16 @@ class OracleSolver:
         assert np.array_equal(kode, self.d.kode) and np.array_equal(zdfi, self.d.bc)
         self.material = host.material(self.s.ge, self.s.rnu, dam, rho)
 
-    def solve_frequency(self, fr):
+    def ghmatecd(self, fr):
         self.calls.append(("solve", fr))
-        disp, trac, _ = self.p.solve(fr, use_openblas=False)
-        return disp, trac
+        self.fr = fr
+
+    def linsolve(self):
+        self.last = self.p.solve(self.fr, use_openblas=False)
+        return self.last[2]
+
+    def interec(self):
+        return self.last[0], self.last[1]
 
     def sweep_batch_limit(self, form):
         return 7
@@ -123,3 +130,33 @@ def test_unknown_form_is_refused(tmp_path, golden_dir):
         driver.run_case(os.path.join(golden_dir, "ESOLO240E_-5+5.DAT"),
                         os.path.join(golden_dir, "ESOLO240D_-5+5.DAT"),
                         tmp_path / "e", tmp_path / "d", form="fp16")
+
+
+# src/analyser.py:12,27-34: how the reference's analysis script reads a run's log
+_FLOAT = r"([-+]?(\d+(\.\d*)?|\.\d+)([eE][-+]?\d+)?)"
+_ANALYSER = {"SHARED": r"Tempo gasto alocando os vetores compartilhados:\s*" + _FLOAT,
+             "GHMATECE": r"GHMATECE: Tempo na ...:\s*" + _FLOAT,
+             "GHMATECD": r"GHMATECD: Tempo na ...:\s*" + _FLOAT,
+             "LINSOLVE": r"LINSOLVE: Tempo na ...:\s*" + _FLOAT,
+             "INTEREC1": r"INTEREC1: Tempo na ...:\s*" + _FLOAT}
+
+
+@pytest.mark.parametrize("form", ["plain", "mixed"])
+def test_stage_log_reads_like_the_reference(tmp_path, golden_dir, form):
+    ein = os.path.join(golden_dir, "ESOLO240E_-5+5.DAT")
+    din = os.path.join(golden_dir, "ESOLO240D_-5+5.DAT")
+    s = formats.read_static(ein)
+    d = formats.read_dynamic(din, s.nbe)
+    lines = []
+    driver.run_case(ein, din, tmp_path / "e", tmp_path / "d", form=form,
+                    solver_factory=_factory(d, []), log=lines.append)
+    found = {}
+    for ln in lines:
+        for key, rx in _ANALYSER.items():
+            m = re.search(rx, ln)
+            if m:
+                found[key] = float(m.group(1))
+    want = {"SHARED", "GHMATECE", "INTEREC1"} | ({"GHMATECD", "LINSOLVE"} if form == "plain" else set())
+    assert set(found) == want, lines
+    assert all(v >= 0.0 for v in found.values())
+    assert any(ln.strip().startswith("SWEEP: Tempo na GPU:") for ln in lines) == (form == "mixed")
