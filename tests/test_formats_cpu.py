@@ -51,3 +51,32 @@ def test_result_block_roundtrip_at_a_large_mesh(tmp_path):
     for a, b in ((back.disp, r.disp), (back.traction, r.traction)):
         for part in (np.real, np.imag):
             assert np.all(np.abs(part(a) - part(b)) <= 5e-4 * np.abs(part(b)) + 1e-300)
+
+
+def test_truncated_input_file_is_reported(tmp_path, golden_dir):
+    """A bad file fails on the host with the reader's error, before any device
+    work: the static input cut in the middle of its connectivity, and the
+    dynamic input cut in its boundary conditions."""
+    import os
+    src = open(os.path.join(golden_dir, "ESOLO240E_-5+5.DAT"), encoding="latin-1").read().split("\n")
+    cut = tmp_path / "e.dat"
+    cut.write_text("\n".join(src[: len(src) // 2]) + "\n", encoding="latin-1")
+    with pytest.raises(EOFError, match="past the end"):
+        formats.read_static(cut)
+    s = formats.read_static(os.path.join(golden_dir, "ESOLO240E_-5+5.DAT"))
+    dsrc = open(os.path.join(golden_dir, "ESOLO240D_-5+5.DAT"), encoding="latin-1").read().split("\n")
+    dcut = tmp_path / "d.dat"
+    dcut.write_text("\n".join(dsrc[:20]) + "\n", encoding="latin-1")
+    with pytest.raises(EOFError):
+        formats.read_dynamic(dcut, s.nbe)
+
+
+def test_non_numeric_field_is_reported(tmp_path, golden_dir):
+    import os
+    src = open(os.path.join(golden_dir, "ESOLO240E_-5+5.DAT"), encoding="latin-1").read().split("\n")
+    i = next(k for k in range(1, len(src)) if src[k].strip())  # the N, NBE, NP, NPG, GE, RNU record
+    src[i] = src[i].replace(src[i].split()[0], "24O", 1)      # a letter O for a zero
+    bad = tmp_path / "e.dat"
+    bad.write_text("\n".join(src), encoding="latin-1")
+    with pytest.raises(ValueError):
+        formats.read_static(bad)
