@@ -11,7 +11,8 @@ formats (formats.format_static_echo, formats.write_dynamic_output).
 Frequencies are solved one at a time in FP64 (form "plain", what the
 reference does), or all together by the lockstep sweep of the mixed form
 (FP32 LU on tensor cores + FP64 refinement, form "mixed"), whose solutions
-are un-swapped on the host.
+are un-swapped on the host; a frequency whose refinement does not converge
+is solved again in FP64 (BemSolver.sweep's fallback).
 
 Every frequency starts from the boundary conditions read from the file.  The
 reference's CPU build un-swaps into its ZDFI array in place
@@ -32,6 +33,9 @@ from . import formats
 from .solver import BemSolver, unswap_host
 
 _ENC = "latin-1"
+# A mixed-form problem whose last refinement step still changed the solution
+# by more than this (relative) is solved again in FP64.
+MIXED_FALLBACK_TOL = 1e-9
 
 
 def run_case(input_e, input_d, output_e, output_d, *, form: str = "plain", refine: int = 3,
@@ -68,8 +72,12 @@ def run_case(input_e, input_d, output_e, output_d, *, form: str = "plain", refin
         freqs = [float(f) for f in d.freqs]
         if form == "mixed" and freqs:
             t0 = time.perf_counter()
-            x, _ = sol.sweep(freqs, form="mixed", batch=sol.sweep_batch_limit("mixed"), refine=refine)
+            x, _ = sol.sweep(freqs, form="mixed", batch=sol.sweep_batch_limit("mixed"), refine=refine,
+                             fallback_tol=MIXED_FALLBACK_TOL)
             stage.done("SWEEP: Tempo na GPU:", t0)
+            for i in sol.fallbacks:
+                if log is not None:
+                    log(f" MIXED: refinement did not converge at FR = {freqs[i]!r}; solved in FP64")
             bound = [unswap_host(x[i], d.kode, zdfi, sol.material[0]) for i in range(len(freqs))]
         else:
             bound = None

@@ -131,9 +131,28 @@ class BemSolver:
         return zdsol, zssol
 
     def sweep(self, freqs, *, form: str = "mixed", batch: int = 8, refine: int = 3,
-              want_x: bool = True):
+              want_x: bool = True, fallback_tol: float | None = None):
         """Frequency sweep on the resident mesh (bem_sweep).  Returns
-        (x[nfreq, nn] raw solutions or None, last relative correction)."""
+        (x[nfreq, nn] raw solutions or None, last relative correction).
+
+        fallback_tol (mixed form, refine > 0, x wanted): a problem whose last
+        refinement correction is above it, or not finite, has not converged
+        (refinement stalls when the FP32 factors are too far from the FP64
+        matrix); it is solved again in the plain FP64 form and its index is
+        listed in self.fallbacks.  Its correction is left as reported."""
+        self.fallbacks = []
+        x, corr = self._sweep_raw(freqs, form, batch, refine, want_x)
+        if fallback_tol is None or form != "mixed" or not want_x or refine <= 0:
+            return x, corr
+        idx = [i for i, c in enumerate(corr) if not c <= fallback_tol]
+        if idx:
+            plain_batch = max(1, min(batch, self.sweep_batch_limit("plain")))
+            xp, _ = self._sweep_raw(f64(freqs)[idx], "plain", plain_batch, refine, True)
+            x[idx] = xp
+            self.fallbacks = idx
+        return x, corr
+
+    def _sweep_raw(self, freqs, form, batch, refine, want_x):
         freqs = f64(freqs)
         nf = freqs.size
         zge, zcs, zcp = self.material

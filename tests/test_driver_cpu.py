@@ -18,6 +18,7 @@ import pytest
 
 import oracle
 from bem_mececcs_b200 import driver, formats, host
+from bem_mececcs_b200.solver import BemSolver
 
 
 class OracleSolver:
@@ -49,12 +50,24 @@ class OracleSolver:
     def interec(self):
         return self.last[0], self.last[1]
 
+    stall = ()  # frequencies whose mixed refinement the stand-in reports as stalled
+
     def sweep_batch_limit(self, form):
         return 7
 
-    def sweep(self, freqs, *, form, batch, refine):
+    sweep = BemSolver.sweep  # the real fallback logic over the stand-in's raw sweep
+
+    def _sweep_raw(self, freqs, form, batch, refine, want_x):
+        freqs = [float(f) for f in freqs]
         self.calls.append(("sweep", tuple(freqs), form, batch))
-        return np.array([self.p.solve(f, use_openblas=False)[2] for f in freqs]), np.zeros(len(freqs))
+        x = np.array([self.p.solve(f, use_openblas=False)[2] for f in freqs])
+        corr = np.zeros(len(freqs))
+        if form == "mixed":
+            for i, f in enumerate(freqs):
+                if f in self.stall:  # a stalled refinement: a wrong x, a large correction
+                    x[i] *= 1.5
+                    corr[i] = 1e-3
+        return x, corr
 
     def interior(self, fr, disp, trac, cxi, cyi, czi):
         self.calls.append(("interior", fr))
@@ -160,3 +173,25 @@ def test_stage_log_reads_like_the_reference(tmp_path, golden_dir, form):
     assert set(found) == want, lines
     assert all(v >= 0.0 for v in found.values())
     assert any(ln.strip().startswith("SWEEP: Tempo na GPU:") for ln in lines) == (form == "mixed")
+
+
+def test_mixed_form_falls_back_to_fp64_where_refinement_stalls(tmp_path, golden_dir):
+    ein = os.path.join(golden_dir, "ESOLO240E_-5+5.DAT")
+    din = os.path.join(golden_dir, "ESOLO240D_-5+5.DAT")
+    s = formats.read_static(ein)
+    d = formats.read_dynamic(din, s.nbe)
+    made, lines = [], []
+
+    def make(st, device):
+        sol = OracleSolver(st, d)
+        sol.stall = (float(d.freqs[0]),)
+        made.append(sol)
+        return sol
+
+    dout = tmp_path / "d"
+    driver.run_case(ein, din, tmp_path / "e", dout, form="mixed", solver_factory=make, log=lines.append)
+    assert made[0].fallbacks == [0]
+    assert [c[2] for c in made[0].calls if c[0] == "sweep"] == ["mixed", "plain"]
+    assert any("solved in FP64" in ln for ln in lines)
+    with open(os.path.join(golden_dir, "SSOLO240D_-5+5.SOL"), "rb") as fh:
+        assert dout.read_bytes() == fh.read()
