@@ -52,3 +52,40 @@ def test_converged_problems_are_left_alone():
     sol = FakeRaw([1e-15, 2e-14])
     x, _ = sol.sweep([1.0, 2.0], form="mixed", batch=2, refine=3, fallback_tol=1e-9)
     assert sol.fallbacks == [] and len(sol.raw_calls) == 1 and np.all(x.real[:, 0] == [1.0, 2.0])
+
+
+def _refine(a, b, steps):
+    """The mixed form's refinement, restated in numpy: complex64 LU with
+    partial pivoting (LAPACK cgetrf), then `steps` rounds of r = b - A x in
+    FP64, d = LU32^-1 r, x += d.  Returns x and max|d|/max|x| of the last d."""
+    from scipy.linalg import lu_factor, lu_solve
+    lu = lu_factor(a.astype(np.complex64))
+    x = lu_solve(lu, b.astype(np.complex64)).astype(np.complex128)
+    corr = np.inf
+    for _ in range(steps):
+        r = b - a @ x
+        d = lu_solve(lu, r.astype(np.complex64)).astype(np.complex128)
+        x = x + d
+        corr = np.abs(d).max() / np.abs(x).max()
+    return x, corr
+
+
+@pytest.mark.parametrize("cond", [1e1, 1e3, 1e5, 1e6, 1e7, 1e8, 1e9])
+def test_fallback_threshold_separates_converged_from_stalled(cond):
+    """Over conditioning from benign to beyond FP32: after 3 steps, a last
+    correction <= 1e-9 (the driver's threshold) comes with an error <= 1e-8
+    (the mixed form's target), and the systems FP32 factors cannot handle
+    (cond * 2^-24 >= 1) all exceed the threshold and go to FP64."""
+    rng = np.random.default_rng(int(np.log10(cond)))
+    n = 160
+    q1, _ = np.linalg.qr(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    q2, _ = np.linalg.qr(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    a = (q1 * np.logspace(0, -np.log10(cond), n)) @ q2.conj().T
+    b = a @ (rng.standard_normal(n) + 1j * rng.standard_normal(n))
+    x_ref = np.linalg.solve(a, b)
+    x, corr = _refine(a, b, 3)
+    err = np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref)
+    if corr <= 1e-9:
+        assert err <= 1e-8, (cond, corr, err)
+    if cond * 2.0 ** -24 >= 1.0:
+        assert not corr <= 1e-9, (cond, corr, err)
