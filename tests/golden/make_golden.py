@@ -9,17 +9,26 @@ centroids, src/Inputece.for:29-104) must match byte for byte
 (src/tests.sh:43).  These data files are copied verbatim (they are inputs and
 outputs, not source); run this script in a container where the reference is
 mounted.
+
+Two of the meshes of the reference's own benchmark (src/bench.sh:3, inputs
+only, from malhas.zip at the reference's root) are copied too: E510 (a soil
+trench, 510 boundary + 5 enclosing elements) and Esoil_1600 (1600 + 5), both
+NPG=8 with L=76 interior points.  They carry no shipped outputs; they pin the
+readers on the reference's own files and give the oracle (and the GPU) a
+second geometry class.
 """
 import hashlib
 import os
 import shutil
 import sys
+import zipfile
 
 SRC = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
 HERE = os.path.dirname(os.path.abspath(__file__))
 FILES = ["ESOLO240E_-5+5.DAT", "ESOLO240D_-5+5.DAT", "SSOLO240D_-5+5.SOL",
          "ESOLO2160E_-5+5.DAT", "ESOLO2160D_-5+5.DAT", "SSOLO2160D_-5+5.SOL",
          "SSOLO240E_-5+5.SOL", "SSOLO2160E_-5+5.SOL"]
+ZIPPED = ["E510e.dat", "E510d.dat", "Esoil_1600e.dat", "Esoil_1600d.dat"]
 
 if __name__ == "__main__":
     with open(os.path.join(HERE, "SHA256SUMS"), "w") as out:
@@ -28,4 +37,10 @@ if __name__ == "__main__":
             shutil.copyfile(os.path.join(SRC, f), dst)
             with open(dst, "rb") as fh:
                 out.write(f"{hashlib.sha256(fh.read()).hexdigest()}  {f}\n")
-    print("copied", len(FILES), "fixtures")
+        with zipfile.ZipFile(os.path.join(SRC, os.pardir, "malhas.zip")) as z:
+            for f in ZIPPED:
+                data = z.read(f)
+                with open(os.path.join(HERE, f), "wb") as fh:
+                    fh.write(data)
+                out.write(f"{hashlib.sha256(data).hexdigest()}  {f}\n")
+    print("copied", len(FILES) + len(ZIPPED), "fixtures")

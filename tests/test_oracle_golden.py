@@ -126,7 +126,7 @@ def test_fixtures_match_their_checksums(golden_dir):
     import hashlib
     with open(os.path.join(golden_dir, "SHA256SUMS")) as fh:
         sums = [ln.split() for ln in fh if ln.strip()]
-    assert len(sums) == 8
+    assert len(sums) == 12
     for digest, name in sums:
         with open(os.path.join(golden_dir, name), "rb") as fh:
             assert hashlib.sha256(fh.read()).hexdigest() == digest, name
