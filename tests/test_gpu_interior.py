@@ -11,6 +11,7 @@ import pytest
 
 import oracle
 import refcheck
+import refmetrics
 from bem_mececcs_b200 import capi, formats, host, meshgen
 from bem_mececcs_b200.solver import BemSolver
 from gpu_util import rel
@@ -44,6 +45,7 @@ def test_interior_matches_oracle():
     p = oracle.OracleProblem(s, d)
     ozd, ozs = p.interior(fr, disp, trac)
     assert rel(zdsol, ozd) < TOL
+    assert refmetrics.zdsol(zdsol, ozd)[2]  # ASSERT_ZDSOL
     assert rel(zssol, ozs) < TOL
     # without stresses: the same displacements
     zd2, zs2 = sol.interior(fr, disp, trac, cxi, cyi, czi, stresses=False)
@@ -107,6 +109,7 @@ def test_interec1_seam_matches_native():
     d.l, d.cxi, d.cyi, d.czi = 6, cxi, cyi, czi
     ozd, _ = oracle.OracleProblem(s, d).interior(fr, disp, trac)
     assert rel(zdsol, ozd) < TOL
+    assert refmetrics.zdsol(zdsol, ozd)[2]  # ASSERT_ZDSOL
 
 
 def _golden_on_gpu(golden_dir, stem, workdir):

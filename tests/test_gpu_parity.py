@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
+import refmetrics
 from bem_mececcs_b200 import formats, meshgen
 from bem_mececcs_b200.capi import BEM_ERR_DEGENERATE, BEM_ERR_SINGULAR, BemError, Context
 from bem_mececcs_b200.solver import BemSolver, solve_dense
@@ -112,6 +113,9 @@ def test_dynamic_mixed_kode(ctx):
     assert rel(x, ox) < TOL
     disp, trac = sol.interec()
     assert rel(disp, odisp) < TOL and rel(trac, otrac) < TOL
+    # the reference's own GPU-vs-CPU checks (-DTEST_CUDA) on the same arrays
+    assert refmetrics.ghmatecd_zh_zfi(zh, ozh, zfi, ozfi, s.nbe)[2]
+    assert refmetrics.zfi(x, ox)[2]
 
 
 def test_golden_240_end_to_end(ctx, golden_dir):
@@ -123,10 +127,12 @@ def test_golden_240_end_to_end(ctx, golden_dir):
     ohd, ogd, _ = p.ghmatece()
     sol, hd, gd = _setup(s, d, ctx)
     assert rel(hd, ohd) < 1e-12 and rel(gd, ogd) < 1e-12
+    assert refmetrics.ghmatece_h_g(hd, ohd, gd, ogd, s.nbe)[2]  # ASSERT_GHMATECE_H_G
     fr = d.freqs[0]
     disp, trac = sol.solve_frequency(fr)
     odisp, _, _ = p.solve(fr, use_openblas=False)
     assert rel(disp, odisp) < TOL
+    assert refmetrics.zfi(disp, odisp)[2]  # ASSERT_ZFI
     zdsol, zssol = p.interior(fr, disp, trac)
     mine = formats.Results(fr, disp.reshape(-1, 3), trac.reshape(-1, 3),
                            zdsol.reshape(-1, 3), zssol.reshape(-1, 9))
