@@ -27,6 +27,7 @@ from .capi import (BEM_FAST_SINGULAR, BEM_FORM_MIXED, BEM_FORM_PLAIN, BEM_KEEP_P
 class BemSolver:
     def __init__(self, static, device: int = 0, ctx: Context | None = None):
         self.s = static
+        self._own_ctx = ctx is None
         self.ctx = ctx or Context(device)
         s = static
         self.nn = 3 * s.nbe
@@ -45,6 +46,20 @@ class BemSolver:
         self.kode = None
         self.zdfi = None
         self.material = None
+
+    def close(self):
+        """Frees the device state: the context, when this solver created it
+        (a context passed in belongs to the caller)."""
+        if self._own_ctx and self.ctx is not None:
+            self.ctx.close()
+        self.ctx = None if self._own_ctx else self.ctx
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+        return False
 
     def ghmatece(self, compute_gest: bool = True):
         hd = np.zeros(9 * self.s.nbe)

@@ -89,3 +89,26 @@ def test_fallback_threshold_separates_converged_from_stalled(cond):
         assert err <= 1e-8, (cond, corr, err)
     if cond * 2.0 ** -24 >= 1.0:
         assert not corr <= 1e-9, (cond, corr, err)
+
+
+class _FakeCtx:
+    def __init__(self):
+        self.closed = 0
+
+    def close(self):
+        self.closed += 1
+
+
+def test_close_frees_only_a_context_the_solver_made():
+    own = BemSolver.__new__(BemSolver)
+    own._own_ctx, own.ctx = True, _FakeCtx()
+    c = own.ctx
+    with own as sol:
+        assert sol is own
+    assert c.closed == 1 and own.ctx is None
+    own.close()  # twice is harmless
+    assert c.closed == 1
+    shared = BemSolver.__new__(BemSolver)
+    shared._own_ctx, shared.ctx = False, _FakeCtx()
+    shared.close()
+    assert shared.ctx.closed == 0
