@@ -218,3 +218,23 @@ def test_smallest_enclosed_mesh_solves():
     disp, trac, x = p.solve(1.0, use_openblas=False)
     a = zh.reshape(3, 3, order="F")
     assert np.all(np.isfinite(x)) and np.linalg.norm(a @ x - zfi) <= 1e-13 * np.linalg.norm(zfi)
+
+
+def test_parity_bound_resolves_small_physics_changes():
+    """The 1e-10 relative bound the GPU is held to has teeth: a change of one
+    part in 1e8 in the Poisson ratio or in omega moves the assembled system by
+    8e-10 and 4.7e-9, so a device path computing a slightly different problem
+    cannot pass it."""
+    import copy
+    s, d = meshgen.config_mesh("c1_240")
+
+    def system(s1, fr):
+        p = oracle.OracleProblem(s1, d)
+        p.ghmatece()
+        return p.system(fr)[0]
+
+    zh0 = system(s, 1.0)
+    s2 = copy.deepcopy(s)
+    s2.rnu *= 1 + 1e-8
+    for zh in (system(s2, 1.0), system(s, 1.0 + 1e-8)):
+        assert np.linalg.norm(zh - zh0) / np.linalg.norm(zh0) > 5e-10
