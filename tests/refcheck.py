@@ -41,7 +41,7 @@ def run(ours: str, gold_path: str):
     return p.returncode, dict(zip(KEYS, vals))
 
 
-def judge(s, d, res: "formats.Results", gold_path: str, workdir: str):
+def check_run(s, d, res: "formats.Results", gold_path: str, workdir: str):
     """Writes the output file of the run (s, d) and runs the checker on it.
     Returns (exit status, the checker's four errors, formats.dtester_errors
     on the same two files).  The file holds 4 printed digits, so the last two

@@ -128,7 +128,7 @@ def _golden_on_gpu(golden_dir, stem, workdir):
                            zdsol.reshape(-1, 3), zssol.reshape(-1, 9))
     gold_path = os.path.join(golden_dir, f"SSOLO{stem}D_-5+5.SOL")
     err = formats.dtester_errors(mine, formats.parse_results(gold_path)[0])
-    ref = refcheck.judge(s, d, mine, gold_path, workdir) if refcheck.available() else None
+    ref = refcheck.check_run(s, d, mine, gold_path, workdir) if refcheck.available() else None
     return err, ref
 
 

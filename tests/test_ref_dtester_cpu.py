@@ -1,6 +1,6 @@
 """The reference's own golden-file checker on the oracle's output.
 
-src/tests.sh:38-117 judges a run by compiling src/dtester.c and running it on
+src/tests.sh:38-117 checks a run by compiling src/dtester.c and running it on
 the run's output file against the shipped SSOLO*D_-5+5.SOL.  oracle/Makefile
 (`make -C oracle ref`) compiles that checker from the reference tree into
 oracle/_ref/dtester; these tests write the oracle's solution of ESOLO240 and
