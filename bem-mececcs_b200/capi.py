@@ -88,6 +88,7 @@ def lib():
     L.bem_prof_bytes.argtypes = [vp, vp]
     L.bem_measure_fp64_peak.argtypes = [vp, vp]
     L.bem_measure_peaks.argtypes = [vp, vp]
+    L.bem_wait_selftest.argtypes = [vp, ip]
     L.bem_static_solve.argtypes = [vp, vp, dp, vp, vp, vp, vp]
     L.bem_batch_solve.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, ip, ip, vp, vp]
     L.bem_interior.argtypes = [vp, vp, vp, vp, dp, dp, ip, vp, vp, vp, vp, vp, vp, vp]
@@ -139,12 +140,13 @@ class Context:
         except Exception:
             pass
 
-    INT_OPTIONS = ("gemm_ctas", "trsv_ctas")
+    INT_OPTIONS = ("gemm_ctas", "trsv_ctas", "wait_limit_ms")
 
     def set_option(self, name: str, value) -> None:
         """bem_ctx_set_option: switches tcgen05, trsv_coop, lu_pairs, lu_quads,
         panel_calu, panel_push, panel_async, laswp_tc, trsv_inv, graphs; CTA
-        budgets gemm_ctas, trsv_ctas (0 = device)."""
+        budgets gemm_ctas, trsv_ctas (0 = device); wait_limit_ms, the bound of
+        every device-side wait (1..60000, default 2000)."""
         v = int(value) if name in self.INT_OPTIONS else int(bool(value))
         self.check(self.L.bem_ctx_set_option(self.h, name.encode(), v), "bem_ctx_set_option")
 
@@ -174,6 +176,12 @@ class Context:
         return {k: {"ms": float(ms[i]), "launches": int(n[i]), "work": float(work[i]),
                     "bytes": float(nbytes[i])}
                 for i, k in enumerate(PROF_CLASSES)}
+
+    def wait_selftest(self, which: int) -> int:
+        """bem_wait_selftest: the status of one bounded wait on an event that
+        never happens (0: bulk-copy mbarrier, 1: grid barrier); BEM_ERR_TIMEOUT
+        when the wait gave up as it should."""
+        return int(self.L.bem_wait_selftest(self.h, int(which)))
 
     def fp64_peak_tflops(self) -> float:
         out = np.zeros(1)

@@ -370,9 +370,10 @@ __global__ void __launch_bounds__(128) k_dyn_offdiag(DynParams p) {
     mbar_expect_tx(&s_bar, bytes);
     bulk_g2s(s_gq, p.gq + (size_t)J0 * p.ng, bytes, &s_bar);
   }
-  if (!mbar_wait(&s_bar, 0)) {
+  const unsigned long long wlim = wait_limit(p.status);
+  if (!mbar_wait(&s_bar, 0, wlim)) {
     if (threadIdx.x == 0) atomicExch(&p.status[ST_TIMEOUT], 1);
-    mbar_wait(&s_bar, 0);  // let the copy in flight land before leaving
+    mbar_wait(&s_bar, 0, wlim);  // let the copy in flight land before leaving
     return;
   }
 
@@ -898,7 +899,10 @@ double2* g_noalloc_addr[kNoAllocMaxDevices] = {};
 
 // Device address of g_noalloc_scratch on the current device, looked up on the
 // first call per device.  On the host the array's name stands for a host-side
-// shadow, never for device memory, so only this address goes to kernels.
+// shadow, never for device memory, so only this address goes to kernels.  The
+// cached address belongs to the device's current context: after a
+// cudaDeviceReset the module may load at another address, so the cache does
+// not survive a reset (the header says so).
 int noalloc_scratch(bem_ctx* ctx, double2** out) {
   if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices)
     return fail(ctx, BEM_ERR_ARG, "bem_ghmatecd_noalloc: device index out of range");
@@ -987,6 +991,9 @@ int bem_ghmatecd_noalloc(bem_ctx* ctx, const double zge[2], const double zcs[2],
   p.status = ctx->d_status;
   p.kb[0] = make_consts(zge, zcs, zcp, fr);
 
+  // timed as the assembly class when profiling is on, like bem_ghmatecd:
+  // work = Stokes evaluations, bytes = the system written once
+  ProfScope ps(ctx, 0, (double)m.nbe * (double)m.nbe * (double)m.ng, (double)nn * (nn + 1) * 16.0);
   k_dyn_diag<<<dim3((m.nbe + 127) / 128, 1, 1), 128, 0, ctx->stream>>>(p);
   ctx->launches++;
   BEM_CUDA(ctx, cudaGetLastError());

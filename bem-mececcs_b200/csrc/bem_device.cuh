@@ -11,9 +11,23 @@ namespace bem {
 
 // Status words in device memory (ctx->d_status[]).
 enum DevStatus { ST_DEGENERATE = 0, ST_SINGULAR = 1, ST_TIMEOUT = 2, ST_COUNT = 4 };
+// After the status words: two mesh flags (ints 4, 5), the context's wait
+// limit (a u64 of nanoseconds at ints 6-7, 8-byte aligned; 0 = the default)
+// and the counter of the wait self-test's grid barrier (int 8).
+constexpr int ST_WAIT_LIMIT = 6;
+constexpr int ST_SELFTEST_CTR = 8;
+constexpr int ST_WORDS = 16;  // ints of ctx->d_status
 
-// Bounded device waits give up after this many nanoseconds of %globaltimer.
+// Bounded device waits give up after this many nanoseconds of %globaltimer
+// unless the context sets its own limit (option "wait_limit_ms").
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s
+
+// The wait limit of the context that owns `status`; read once per kernel.
+__device__ __forceinline__ unsigned long long wait_limit(const int* status) {
+  const unsigned long long v =
+      status ? *reinterpret_cast<const volatile unsigned long long*>(status + ST_WAIT_LIMIT) : 0ull;
+  return v ? v : kWaitLimitNs;
+}
 
 template <typename R>
 struct cpx {
@@ -141,11 +155,12 @@ __device__ __forceinline__ void red_release_gpu_add(unsigned* p, unsigned v) {
 
 // Grid-wide barrier of a cooperative launch over `nblocks` CTAs.  `ctr` is
 // zeroed before the launch; barrier number `epoch` (1, 2, ...) completes when
-// the counter reaches epoch * nblocks.  The wait is bounded: on timeout (or
-// when another CTA has already timed out) it sets status[ST_TIMEOUT] and
-// returns false; callers then leave the kernel.
+// the counter reaches epoch * nblocks.  The wait is bounded by limit_ns (the
+// context's wait_limit): on timeout (or when another CTA has already timed
+// out) it sets status[ST_TIMEOUT] and returns false; callers then leave the
+// kernel.
 __device__ __forceinline__ bool grid_barrier(unsigned* ctr, unsigned epoch, unsigned nblocks,
-                                             int* status) {
+                                             int* status, unsigned long long limit_ns) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -157,7 +172,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* ctr, unsigned epoch, unsi
     unsigned spins = 0;
     while (ld_acquire_gpu(ctr) < target) {
       if ((++spins & 255u) == 0) {
-        if (*(volatile int*)&status[ST_TIMEOUT] != 0 || globaltimer_ns() - t0 > kWaitLimitNs) {
+        if (*(volatile int*)&status[ST_TIMEOUT] != 0 || globaltimer_ns() - t0 > limit_ns) {
           atomicExch(&status[ST_TIMEOUT], 1);
           ok = 0;
           break;
@@ -191,7 +206,8 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
       : "memory");
 }
 // Bounded wait for phase `parity` of the mbarrier; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity,
+                                          unsigned long long limit_ns = kWaitLimitNs) {
   const unsigned long long t0 = globaltimer_ns();
   unsigned spins = 0;
   while (true) {
@@ -202,7 +218,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
         : "r"(smem_u32(bar)), "r"(parity)
         : "memory");
     if (done) return true;
-    if ((++spins & 63u) == 0 && globaltimer_ns() - t0 > kWaitLimitNs) return false;
+    if ((++spins & 63u) == 0 && globaltimer_ns() - t0 > limit_ns) return false;
   }
 }
 

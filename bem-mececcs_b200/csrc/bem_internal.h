@@ -205,6 +205,7 @@ struct bem_ctx {
   // SM shares for contexts that run concurrently on one GPU (0: the whole device)
   int gemm_ctas = 0;          // CTAs of the persistent tensor-core trailing update
   int trsv_ctas = 0;          // CTAs of one cooperative triangular solve (all problems together)
+  int wait_limit_ms = 2000;   // bound of every device-side wait (copy of the device word)
 };
 
 namespace bem {
@@ -321,5 +322,7 @@ int measure_fma_peaks(bem_ctx* ctx, double* fp64_tflops, double* fp32_tflops);
 int measure_tf32_peak(bem_ctx* ctx, int n, double* tflops);
 
 int check_status(bem_ctx* ctx);
+// The failure-path self-test kernel (bem_wait_selftest), lu.cu.
+int wait_selftest(bem_ctx* ctx, int which);
 
 }  // namespace bem

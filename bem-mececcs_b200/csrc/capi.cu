@@ -131,8 +131,8 @@ int bem_ctx_create(int device, bem_ctx** out) {
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_status, 8 * sizeof(int));
-  if (e == cudaSuccess) e = cudaMemset(ctx->d_status, 0, 8 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_status, ST_WORDS * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_status, 0, ST_WORDS * sizeof(int));  // wait limit 0: the default
   if (e != cudaSuccess) {
     delete ctx;
     return e == cudaErrorMemoryAllocation ? BEM_ERR_NOMEM : BEM_ERR_CUDA;
@@ -557,9 +557,24 @@ static int* int_option_slot(bem_ctx* ctx, const char* name) {
   return nullptr;
 }
 
+constexpr int kWaitLimitMaxMs = 60000;
+
 int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
   if (!ctx || !name) return BEM_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!strcmp(name, "wait_limit_ms")) {
+    // kept in the context's device status words: every bounded wait reads it
+    // at the start of its kernel, captured graphs included
+    if (value < 1 || value > kWaitLimitMaxMs)
+      return fail(ctx, BEM_ERR_ARG, "wait_limit_ms must be in 1..60000");
+    const unsigned long long ns = (unsigned long long)value * 1000000ull;
+    cudaSetDevice(ctx->device);
+    BEM_CUDA(ctx, cudaMemcpyAsync(ctx->d_status + ST_WAIT_LIMIT, &ns, sizeof ns, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    BEM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->wait_limit_ms = value;
+    return BEM_OK;
+  }
   bool* slot = option_slot(ctx, name);
   int* islot = slot ? nullptr : int_option_slot(ctx, name);
   if (!slot && !islot) return fail(ctx, BEM_ERR_ARG, std::string("unknown option ") + name);
@@ -577,6 +592,10 @@ int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
 int bem_ctx_get_option(bem_ctx* ctx, const char* name, int* value) {
   if (!ctx || !name || !value) return BEM_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!strcmp(name, "wait_limit_ms")) {
+    *value = ctx->wait_limit_ms;
+    return BEM_OK;
+  }
   if (bool* slot = option_slot(ctx, name)) {
     *value = *slot ? 1 : 0;
     return BEM_OK;
@@ -646,6 +665,13 @@ int bem_prof_read(bem_ctx* ctx, double* ms, long long* launches, double* work) {
     if (work) work[c] = P.work[c];
   }
   return BEM_OK;
+}
+
+int bem_wait_selftest(bem_ctx* ctx, int which) {
+  if (!ctx || (which != 0 && which != 1)) return BEM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  return wait_selftest(ctx, which);
 }
 
 int bem_measure_fp64_peak(bem_ctx* ctx, double* tflops) {

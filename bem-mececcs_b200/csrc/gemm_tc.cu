@@ -135,9 +135,10 @@ struct TcArgs {
 };
 
 // Bounded wait; on timeout raise the kernel-wide abort flag and the status word.
-__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* status) {
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* status,
+                                              unsigned long long limit_ns) {
   if (*abort_flag) return false;
-  if (mbar_wait(bar, parity)) return true;
+  if (mbar_wait(bar, parity, limit_ns)) return true;
   *abort_flag = 1;
   atomicExch(&status[ST_TIMEOUT], 1);
   return false;
@@ -180,6 +181,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
   tc_fence_after();
   const uint32_t tmem = s_tmem;
   volatile int* abort_flag = &s_abort;
+  const unsigned long long wlim = wait_limit(a.status);
 
   if (warp == 0 && lane == 0) {
     // ---- TMA producer: operand K-chunks through a kStages ring; C tiles
@@ -204,7 +206,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
       const int ly = b * a.lrows + 2 * tm * kTcRows;
       const int uy = b * a.urows + a.urow_off + tn * kTcCols;
       for (int h = 0; h < nchunks; ++h) {
-        if (!wait_or_abort(&empty[s], ph ^ 1u, abort_flag, a.status)) {
+        if (!wait_or_abort(&empty[s], ph ^ 1u, abort_flag, a.status, wlim)) {
           ok = false;
           break;
         }
@@ -228,11 +230,11 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
     bool ok = true;
     for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++it) {
       const int buf = it & 1;
-      if (!wait_or_abort(&t_empty[buf], ((uint32_t)(it >> 1) & 1u) ^ 1u, abort_flag, a.status)) break;
+      if (!wait_or_abort(&t_empty[buf], ((uint32_t)(it >> 1) & 1u) ^ 1u, abort_flag, a.status, wlim)) break;
       tc_fence_after();
       const uint32_t d1 = tmem + (uint32_t)buf * 256u, d2 = d1 + 128u;
       for (int h = 0; h < nchunks; ++h) {
-        if (!wait_or_abort(&full[s], ph, abort_flag, a.status)) {
+        if (!wait_or_abort(&full[s], ph, abort_flag, a.status, wlim)) {
           ok = false;
           break;
         }
@@ -265,7 +267,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
     int it = 0;
     for (int t = blockIdx.x; t < total; t += gridDim.x, ++it) {
       const int buf = it & 1;
-      if (!__all_sync(0xffffffffu, wait_or_abort(&t_full[buf], (uint32_t)(it >> 1) & 1u, abort_flag, a.status)))
+      if (!__all_sync(0xffffffffu, wait_or_abort(&t_full[buf], (uint32_t)(it >> 1) & 1u, abort_flag, a.status, wlim)))
         break;
       tc_fence_after();
       const int b = t / (a.mtiles * a.ntiles);
@@ -421,7 +423,7 @@ __global__ void __launch_bounds__(128, 1) k_umma_peak(int iters, int n, int* sta
       for (int kk = 0; kk < 4; ++kk)
         umma_tf32(tmem, sdesc(sa + 32u * kk), sdesc(sb + 32u * kk), idesc, (it | kk) ? 1u : 0u);
     umma_commit(&done);
-    if (!mbar_wait(&done, 0)) atomicExch(&status[ST_TIMEOUT], 1);
+    if (!mbar_wait(&done, 0, wait_limit(status))) atomicExch(&status[ST_TIMEOUT], 1);
   }
   __syncthreads();
   if (warp == 0) {

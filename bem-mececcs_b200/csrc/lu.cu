@@ -733,6 +733,7 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
   __shared__ unsigned s_rk[2][NW];
   __shared__ int s_rr[2][NW];
   __shared__ int s_mdst[kPushMoves], s_msrc[kPushMoves], s_ment[kPushMoves], s_mcnt;
+  const unsigned long long wlim = wait_limit(a.status);  // the context's bound on every wait
   __shared__ int s_ppos[kPushMoves], s_pcnt;  // published rows (positions)
   __shared__ int s_pent[SW];                  // published row holding each pivot row's right part
   __shared__ int s_pdst[2 * NB], s_psrc[2 * NB];
@@ -919,7 +920,7 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
         // the column's mailboxes are full when the mbarrier's phase completes; a
         // wait that runs out sets the status and later waits are skipped (the
         // kernel still meets every cluster barrier)
-        if (*(volatile int*)&a.status[ST_TIMEOUT] == 0 && !mbar_wait(&s_mb[par], (mph >> par) & 1u))
+        if (*(volatile int*)&a.status[ST_TIMEOUT] == 0 && !mbar_wait(&s_mb[par], (mph >> par) & 1u, wlim))
           atomicExch(&a.status[ST_TIMEOUT], 1);
         mph ^= 1u << par;
       } else {
@@ -1667,6 +1668,7 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel_grid(PanelArgs a) {
   __shared__ int s_pcount;
 
   const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned long long wlim = wait_limit(a.status);
   E* A = static_cast<E*>(a.A);
   const int rp = a.rp, w = a.w, k = a.k, G = a.cs;
   const int rbase = k + b * rp;
@@ -1701,7 +1703,7 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel_grid(PanelArgs a) {
     const int lbr = s_best;
     if (lbr != INT_MAX && tid < w) cand[((size_t)par * G + b) * NB + tid] = s_a[tid * rp + (lbr - rbase)];
     if (gj >= rbase && gj < rbase + rcount && tid < w) drow[par * NB + tid] = s_a[tid * rp + (gj - rbase)];
-    if (!grid_barrier(a.bar, (unsigned)(j + 1), (unsigned)G, a.status)) return;
+    if (!grid_barrier(a.bar, (unsigned)(j + 1), (unsigned)G, a.status, wlim)) return;
     if (tid == 0) __threadfence();
     if (warp == 0) {
       R v = R(-1);
@@ -2663,6 +2665,7 @@ __global__ void __launch_bounds__(256) k_trsv(TrsvArgs a) {
   __shared__ C s_rd[kTrsvBlk];  // reciprocals of the diagonal of U (backward)
   const int prob = blockIdx.x / a.group, rank = blockIdx.x % a.group, G = a.group;
   if (prob >= a.batch) return;
+  const unsigned long long wlim = wait_limit(a.status);
   const E* A = static_cast<const E*>(a.A) + (size_t)prob * a.bstride;
   E* v = static_cast<E*>(a.v) + (size_t)prob * a.vstride;
   E* b1 = static_cast<E*>(a.w) + (size_t)prob * 2 * a.nn;
@@ -2733,12 +2736,12 @@ __global__ void __launch_bounds__(256) k_trsv(TrsvArgs a) {
         kprev = k;
         wprev = w;
       }
-      if (!grid_barrier(ctr, ++epoch, G, a.status)) return;
+      if (!grid_barrier(ctr, ++epoch, G, a.status, wlim)) return;
     }
     if (wprev > 0) {  // the last panel was even: its rows still go to v
       if (rank == 0)
         for (int i = threadIdx.x; i < wprev; i += blockDim.x) stc<R>(&v[kprev + i], s_xprev[i]);
-      if (!grid_barrier(ctr, ++epoch, G, a.status)) return;
+      if (!grid_barrier(ctr, ++epoch, G, a.status, wlim)) return;
     }
   }
 
@@ -2774,7 +2777,7 @@ __global__ void __launch_bounds__(256) k_trsv(TrsvArgs a) {
       const int lo = min(b0, rank * per), hi = min(b0, lo + per);
       trsv_rows<R>(A, a.lda, b0, wb, s_x, v, v, lo, hi, s_part);
     }
-    if (!grid_barrier(ctr, ++epoch, G, a.status)) return;
+    if (!grid_barrier(ctr, ++epoch, G, a.status, wlim)) return;
   }
   const int per = (nn + G - 1) / G;
   const int lo = min(nn, rank * per), hi = min(nn, lo + per);
@@ -2877,6 +2880,7 @@ __global__ void __launch_bounds__(256) k_trsv_f32(const __grid_constant__ CUtens
   __shared__ int s_ok;
   const int prob = blockIdx.x / a.group, rank = blockIdx.x % a.group, G = a.group;
   if (prob >= a.batch) return;
+  const unsigned long long wlim = wait_limit(a.status);
   float2* v = static_cast<float2*>(a.v) + (size_t)prob * a.vstride;
   float2* b1 = static_cast<float2*>(a.w) + (size_t)prob * 2 * a.nn;
   float2* xo = b1 + a.nn;
@@ -3044,8 +3048,9 @@ __global__ void __launch_bounds__(256) k_trsv_f32(const __grid_constant__ CUtens
     }
     if (!fwd && rank == 0)
       for (int i = tid; i < w; i += blockDim.x) stc<float>(&xo[c0 + i], s_x[i]);
-    if (!mbar_wait(&s_bar, phase)) {
+    if (!mbar_wait(&s_bar, phase, wlim)) {
       atomicExch(&a.status[ST_TIMEOUT], 1);
+      mbar_wait(&s_bar, phase, wlim);  // let the box in flight land before leaving
       return;
     }
     phase ^= 1u;
@@ -3076,7 +3081,7 @@ __global__ void __launch_bounds__(256) k_trsv_f32(const __grid_constant__ CUtens
       unsigned spins = 0;
       while (ld_acquire_gpu(ctr) < target) {
         if ((++spins & 255u) == 0) {
-          if (*(volatile int*)&a.status[ST_TIMEOUT] != 0 || globaltimer_ns() - t0 > kWaitLimitNs) {
+          if (*(volatile int*)&a.status[ST_TIMEOUT] != 0 || globaltimer_ns() - t0 > wlim) {
             atomicExch(&a.status[ST_TIMEOUT], 1);
             ok = 0;
             break;
@@ -3086,11 +3091,17 @@ __global__ void __launch_bounds__(256) k_trsv_f32(const __grid_constant__ CUtens
       s_ok = ok;
     }
     __syncthreads();
-    if (!s_ok) return;
+    if (!s_ok) {
+      if (st + 1 < nsteps) mbar_wait(&s_bar, phase, wlim);  // the next step's box, issued above, lands first
+      return;
+    }
     if (st == nf - 1 && wprev > 0) {  // the last panel was even: its rows still go to v
       if (rank == 0)
         for (int i = tid; i < wprev; i += blockDim.x) stc<float>(&v[kprev + i], s_xprev[i]);
-      if (!grid_barrier(ctr, ++epoch, G, a.status)) return;
+      if (!grid_barrier(ctr, ++epoch, G, a.status, wlim)) {
+        if (st + 1 < nsteps) mbar_wait(&s_bar, phase, wlim);  // the next step's box lands first
+        return;
+      }
     }
   }
   int lo, hi;
@@ -3941,6 +3952,40 @@ int measure_fma_peaks(bem_ctx* ctx, double* fp64_tflops, double* fp32_tflops) {
   int rc = measure_fma_t<double>(ctx, 4096, fp64_tflops);
   if (rc) return rc;
   return measure_fma_t<float>(ctx, 16384, fp32_tflops);
+}
+
+// ---------------------------------------------------------------------------
+// Failure-path self-test: the library's two kinds of bounded device wait, each
+// on something that never happens, under the context's wait limit.  which = 0:
+// an mbarrier armed for 16 bytes of a bulk copy that is never issued (the wait
+// of every TMA load); which = 1: a software grid barrier that expects one CTA
+// more than the launch has (the wait of the cooperative kernels).  Both give
+// up after the limit, record ST_TIMEOUT and return; nothing is in flight.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(32) k_wait_selftest(int which, int* status) {
+  __shared__ __align__(8) uint64_t s_bar;
+  const unsigned long long wlim = wait_limit(status);
+  if (which == 0) {
+    if (threadIdx.x == 0) {
+      mbar_init(&s_bar, 1);
+      mbar_expect_tx(&s_bar, 16u);  // the one arrival, and 16 bytes that never come
+    }
+    __syncthreads();
+    const bool ok = mbar_wait(&s_bar, 0, wlim);
+    if (!ok && threadIdx.x == 0) atomicExch(&status[ST_TIMEOUT], 1);
+  } else {
+    unsigned* ctr = reinterpret_cast<unsigned*>(status + ST_SELFTEST_CTR);
+    grid_barrier(ctr, 1u, gridDim.x + 1u, status, wlim);
+  }
+}
+
+int wait_selftest(bem_ctx* ctx, int which) {
+  BEM_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->stream));
+  BEM_CUDA(ctx, cudaMemsetAsync(ctx->d_status + ST_SELFTEST_CTR, 0, sizeof(int), ctx->stream));
+  k_wait_selftest<<<1, 32, 0, ctx->stream>>>(which, ctx->d_status);
+  ctx->launches++;
+  BEM_CUDA(ctx, cudaGetLastError());
+  return check_status(ctx);
 }
 
 }  // namespace bem

@@ -60,9 +60,14 @@ def parse_args():
                     help="frequencies per lockstep batch (0: the library's limit for this mesh, "
                          "bem_sweep_batch_limit)")
     ap.add_argument("--refine", type=int, default=3, help="FP64 refinement steps (mixed form)")
-    ap.add_argument("--serve-count", type=int, default=40,
-                    help="requests of the serving stream replayed in the served measurement "
-                         "(0 skips the stream; the 128-request served sweep always runs)")
+    ap.add_argument("--serve-count", type=int, default=2000,
+                    help="requests of the serving stream replayed in the mixed form (0 skips the "
+                         "stream; the 128-request served sweep always runs)")
+    ap.add_argument("--serve-plain-count", type=int, default=120,
+                    help="requests of the same stream (its first ones) replayed in the plain FP64 form, "
+                         "whose service rate is far below the arrival rate")
+    ap.add_argument("--no-precision", action="store_true",
+                    help="skip the precision block (per-result errors against the FP64 oracle)")
     ap.add_argument("--no-serve", action="store_true", help="skip the served measurements")
     ap.add_argument("--small-count", type=int, default=512,
                     help="small meshes (24..600 elements) of the batching measurement (0 skips it)")
@@ -358,9 +363,24 @@ def run_ours(args):
     if not np.all(np.isfinite(x_pin)):
         raise RuntimeError("non-finite solution")
 
+    # --- the plain FP64 form batched as the mixed one is (bem_sweep PLAIN) ---
+    Bp = sol.sweep_batch_limit("plain")
+
+    def plain_sweep_step(i):
+        fr = capi.f64([mine[(i * Bp + j) % len(mine)] for j in range(Bp)])
+        ctx.check(L.bem_sweep(h, capi.ptr(zge2), capi.ptr(zcs2), capi.ptr(zcp2), capi.ptr(c),
+                              capi.ptr(fr), Bp, capi.BEM_FORM_PLAIN, Bp, 0, None, None), "bem_sweep")
+
+    plain_sweep_step(0)
+    ctx.sync()
+    kpb = max(2, args.steps // 4)
+    t_plain_b = timed(lambda i: plain_sweep_step(1 + i), kpb)
+    ms_plain_b = max_over_ranks(t_plain_b["ms"], world, f"cuda:{local}")
+
     mpeaks = ctx.peaks()
     value = job_rate(world, args.steps * B, ms_mix)
     value_plain = job_rate(world, kp, ms_plain)
+    value_plain_b = job_rate(world, kpb * Bp, ms_plain_b)
     e2e_value = job_rate(world, args.steps * B, e2e_ms)
     pm = t_prof["prof"]
     pp = t_plain["prof"]
@@ -391,13 +411,10 @@ def run_ours(args):
                    "step": f"one batch of {B} frequency solves",
                    "n": nn, "parallelism": f"replicas x{world} (frequency-sharded)",
                    "l2": "inputs larger than L2: each 6480x6481 complex128 system is 672 MB"},
-        "accuracy": {"max_rel_err_vs_plain_fp64": max_err, "tolerance": 1e-8,
-                     "last_correction": float(max(corr))},
-        "plain_fp64": {"value": round(value_plain, 3), "unit": UNIT,
-                       "ms_per_solve": round(ms_plain / kp, 3), "steps": kp,
-                       "gemm_tflops": round(plain_gemm, 3) if plain_gemm else None,
-                       "kernel_share": {k: round(v["ms"] / t_plain["ms"], 4) for k, v in pp.items()}},
-        "speedup_vs_plain_fp64": round(value / value_plain, 3),
+        "gpu_launches": int(t_mix["launches"]),
+        "clocks": clocks,
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT,
+                "h2d_bytes_per_step": int(nn * 16 + nn * 4), "d2h_bytes_per_step": int(B * nn * 16)},
         "roofline": roof,
         "rooflines_all": {k: {kk: v[kk] for kk in ("achieved", "frac", "ms") if kk in v} |
                           ({"tensor_frac": v["tensor"]["frac"]} if "tensor" in v else {}) |
@@ -408,30 +425,127 @@ def run_ours(args):
         "kernels": pm,
         "kernels_steps": max(3, args.steps // 2),
         "cuda_graphs": os.environ.get("BEM_GRAPHS", "1") != "0",
-        "e2e": {"value": round(e2e_value, 3), "unit": UNIT,
-                "h2d_bytes_per_step": int(nn * 16 + nn * 4), "d2h_bytes_per_step": int(B * nn * 16)},
         "static_per_mesh": {"ghmatece_ms": round(static_ms, 3),
                             "kelvin_evals": s.nbe * (s.n - 1) * s.npg ** 2 + 4 * s.nbe * s.npg ** 2,
                             "note": "GHMATECE once per mesh (HESTdiag + GESTdiag on the device), host wall "
                                     "clock of the first call, set-up included; outside the timed sweep"},
-        "gpu_launches": int(t_mix["launches"]),
-        "clocks": clocks,
+        "accuracy": {"max_rel_err_vs_plain_fp64": max_err, "tolerance": 1e-8,
+                     "last_correction": float(max(corr))},
+        "plain_fp64": {"value": round(value_plain, 3), "unit": UNIT,
+                       "form": "one frequency at a time: bem_ghmatecd + bem_linsolve (the reference's order)",
+                       "ms_per_solve": round(ms_plain / kp, 3), "steps": kp,
+                       "gemm_tflops": round(plain_gemm, 3) if plain_gemm else None,
+                       "kernel_share": {k: round(v["ms"] / t_plain["ms"], 4) for k, v in pp.items()}},
+        "plain_fp64_batched": {"value": round(value_plain_b, 3), "unit": UNIT,
+                               "form": f"bem_sweep PLAIN, {Bp} frequencies per step in lockstep, FP64 LU",
+                               "ms_per_step": round(ms_plain_b / kpb, 3), "steps": kpb},
+        "speedup_vs_plain_fp64": round(value / value_plain, 3),
+        "speedup_vs_plain_fp64_batched": round(value / value_plain_b, 3),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sol.ghmatecd(float(mine[0]))
         zh_sys, zfi_sys = sol.get_system()
         secs, sample, threads = cpu_freq_solve_seconds(s, d, zh_sys, zfi_sys, float(mine[0]))
+        del zh_sys, zfi_sys
         line["cpu_baseline"] = {"value": round(1.0 / secs, 5), "unit": UNIT, "cores": threads,
                                 "kind": "port", "sample": sample}
     ctx.close()
+    if rank == 0 and not args.no_precision:
+        line["precision"] = run_precision(args, local)
     if not args.no_serve:
         line["served"] = run_served(args, s, d, mine, local)
     if args.small_count > 0:
         line["batched_small_meshes"] = run_small_batch(args, local)
+    line["summary"] = _summary(line)
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def _summary(line):
+    """The figures a reader needs first, compact and last on the line (a log
+    that keeps only the end of the output still holds them)."""
+    out = {"mixed_batched": line["value"], "e2e": line["e2e"]["value"],
+           "plain_fp64": line["plain_fp64"]["value"],
+           "plain_fp64_batched": line["plain_fp64_batched"]["value"],
+           "speedup_vs_plain_fp64": line["speedup_vs_plain_fp64"],
+           "speedup_vs_plain_fp64_batched": line["speedup_vs_plain_fp64_batched"],
+           "plain_gemm_tflops": line["plain_fp64"]["gemm_tflops"],
+           "max_rel_err_mixed_vs_plain": float(f"{line['accuracy']['max_rel_err_vs_plain_fp64']:.3g}"),
+           "roofline": {"class": line["roofline"].get("class"), "frac": line["roofline"]["frac"],
+                        "traffic_per_launch": line["roofline"]["traffic"]}}
+    if "cpu_baseline" in line:
+        out["cpu_baseline"] = line["cpu_baseline"]["value"]
+    pr = line.get("precision")
+    if pr:
+        out["rel_err_vs_oracle_2160"] = {k: {f: float(f"{max(v[f].values()):.3g}") for f in ("mixed", "plain")}
+                                         for k, v in pr["c3_2160_vs_oracle"].items()}
+        out["rel_err_mixed_vs_plain_8640"] = {k: float(f"{v:.3g}") for k, v in pr["c3_8640_vs_plain_gpu"].items()}
+    sv = line.get("served")
+    if sv:
+        out["served_sweep_2160"] = {"mixed": sv["sweep_2160"]["mixed"]["solves_per_s"],
+                                    "plain": sv["sweep_2160"]["plain"]["solves_per_s"],
+                                    "speedup": sv["sweep_2160"]["speedup_mixed_vs_plain"]}
+        if "stream" in sv:
+            out["served_stream"] = {f: {k: sv["stream"][f][k] for k in
+                                        ("requests", "completed", "solves_per_s", "p50_ms", "p99_ms")}
+                                    for f in ("mixed", "plain") if f in sv["stream"]}
+    sb = line.get("batched_small_meshes")
+    if sb:
+        out["small_meshes"] = {"batch_mixed": sb["batch_mixed"]["solves_per_s"],
+                               "batch_plain": sb["batch_plain"]["solves_per_s"],
+                               "one_by_one_plain": sb["one_by_one_plain"]["solves_per_s"]}
+    return out
+
+
+PRECISION_OMEGAS = (0.5, 2.0, 8.0)
+
+
+def run_precision(args, device):
+    """The precision form's per-result errors.  2160 elements (the jittered
+    mesh of seed 1) at omega 0.5, 2, 8: the mixed and the plain GPU solutions
+    against the FP64 oracle's (raw solution, boundary displacements and
+    tractions after the un-swap).  8640 elements (seed 2, n = 25920): the
+    mixed form against the plain FP64 GPU path, which the oracle pins
+    wherever both run (the oracle would need tens of GB and minutes per
+    omega at this size)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from bem_mececcs_b200.solver import BemSolver, unswap_host
+
+    def rel(a, b):
+        return float(np.linalg.norm(np.ravel(a - b)) / np.linalg.norm(np.ravel(b)))
+
+    out = {"note": "relative 2-norm errors per result; mixed target <= 1e-8, plain parity <= 1e-10"}
+    s3, d3 = meshgen.config_mesh("c3_2160")
+    with BemSolver(s3, device=device) as sol:
+        sol.ghmatece()
+        sol.set_bc(d3.kode, d3.bc.astype(np.complex128), d3.dam, d3.rho)
+        xm, corr = sol.sweep(d3.freqs, form="mixed", batch=len(d3.freqs), refine=args.refine)
+        xp, _ = sol.sweep(d3.freqs, form="plain", batch=len(d3.freqs))
+        zge = sol.material[0]
+    p = oracle.OracleProblem(s3, d3)
+    p.ghmatece()
+    res = {}
+    for i, fr in enumerate(d3.freqs):
+        odisp, otrac, ox = p.solve(float(fr), use_openblas=True)
+        r = {}
+        for form, x in (("mixed", xm[i]), ("plain", xp[i])):
+            disp, trac = unswap_host(x, d3.kode, d3.bc, zge)
+            r[form] = {"x": rel(x, ox), "disp": rel(disp, odisp), "trac": rel(trac, otrac)}
+        r["last_correction"] = float(corr[i])
+        res[f"{fr:g}"] = r
+    out["c3_2160_vs_oracle"] = res
+    s4, d4 = meshgen.config_mesh("c3_8640")
+    with BemSolver(s4, device=device) as sol:
+        sol.ghmatece()
+        sol.set_bc(d4.kode, d4.bc.astype(np.complex128), d4.dam, d4.rho)
+        xm, corr = sol.sweep(d4.freqs, form="mixed", batch=1, refine=args.refine)
+        xp, _ = sol.sweep(d4.freqs, form="plain", batch=1)
+    out["c3_8640_vs_plain_gpu"] = {f"{fr:g}": rel(xm[i], xp[i]) for i, fr in enumerate(d4.freqs)}
+    out["c3_8640_last_correction"] = {f"{fr:g}": float(corr[i]) for i, fr in enumerate(d4.freqs)}
+    return out
 
 
 def run_small_batch(args, device):
@@ -496,10 +610,11 @@ def _served_summary(st, wall_s):
 def run_served(args, s, d, mine, device):
     """The serving form (bem_server_*, one request per (mesh, omega, BCs)):
     (1) this rank's share of the 128-frequency sweep on the 2160 mesh,
-    submitted as one burst of requests; (2) the first --serve-count requests
-    of the seeded serving stream (Poisson arrivals at 50/s, 240..12000
-    elements, 30% right-hand-side-only), replayed in real time.  Mixed and
-    plain FP64, HBM budget 160 GB.  Latency = submit to result on the host."""
+    submitted as one burst of requests; (2) the seeded serving stream
+    (Poisson arrivals at 50/s, 240..12000 elements, 30% right-hand-side-only),
+    replayed in real time: its first --serve-count requests (all 2000 by
+    default) in the mixed form, its first --serve-plain-count in the plain
+    FP64 form.  HBM budget 160 GB.  Latency = submit to result on the host."""
     from bem_mececcs_b200 import serve
     mat = (s.ge, s.rnu, d.dam, d.rho)
     bc = d.bc.astype(np.complex128)
@@ -520,18 +635,21 @@ def run_served(args, s, d, mine, device):
                                             max(sweep["plain"]["solves_per_s"], 1e-9), 3)
     out["sweep_2160"] = sweep
     if args.serve_count > 0:
-        reqs = serve.serving_workload(count=args.serve_count)
+        reqs = serve.serving_workload(count=max(args.serve_count, args.serve_plain_count))
         meshes, prepared = {}, []
         for r in reqs:
             if r.key not in meshes:
                 meshes[r.key] = serve.request_mesh(r)
             prepared.append((r, *serve.request_bc(meshes[r.key], r)))
-        stream = {"requests": len(reqs), "arrival_rate_per_s": 50.0,
+        stream = {"stream_length": len(reqs), "arrival_rate_per_s": 50.0,
                   "elements": [int(min(r.grid[0] * r.grid[1] for r in reqs)),
                                int(max(r.grid[0] * r.grid[1] for r in reqs))]}
-        for form in ("mixed", "plain"):
+        for form, count in (("mixed", args.serve_count), ("plain", args.serve_plain_count)):
+            if count <= 0:
+                continue
             srv = serve.Server(device=device, budget_bytes=160e9, form=form, refine=args.refine)
-            ids_mesh = {k: srv.add_mesh(m) for k, m in meshes.items()}
+            last = max(r.key for r, _, _ in prepared[:count])
+            ids_mesh = {k: srv.add_mesh(m) for k, m in meshes.items() if k <= last}
             wm = serve.request_mesh(serve.Request(0.0, (12, 10), 1, 0.0, mat, (0, 0, 1)))
             w = srv.add_mesh(wm)
             srv.wait(srv.submit(w, mat, 1.0, *serve.request_bc(wm, serve.Request(
@@ -539,14 +657,14 @@ def run_served(args, s, d, mine, device):
             srv.reset_stats()
             t0 = time.perf_counter()
             ids = []
-            for r, rbc, rk in prepared:
+            for r, rbc, rk in prepared[:count]:
                 dt = r.t - (time.perf_counter() - t0)
                 if dt > 0:
                     time.sleep(dt)
                 ids.append(srv.submit(ids_mesh[r.key], r.material, r.fr, rbc, rk))
             for i in ids:
                 srv.wait(i, timeout=1800.0)
-            stream[form] = _served_summary(srv.stats(), time.perf_counter() - t0)
+            stream[form] = _served_summary(srv.stats(), time.perf_counter() - t0) | {"requests": count}
             srv.close()
         out["stream"] = stream
     return out
@@ -586,15 +704,25 @@ NOTES = {
 }
 
 
+# DRAM bytes (read + write) per algorithmic byte of the trailing update, from
+# one ncu capture of a K = 256 k_gemm_tc launch on 2 problems of n = 6480
+# (1.165 GB against 1.044 GB of C read and written once).  The launch's
+# traffic is C (the operands stay in L2), so it grows in proportion to the
+# algorithmic bytes and scales to any launch by them.
+GEMM_DRAM_PER_ALGO_BYTE = 1.165 / 1.044
+
+
 def _roofline(name, k, peaks, mpeaks):
     """Roofline of one kernel class over the timed region: achieved
     algorithmic bytes (bem_prof_bytes) per second against the measured HBM
-    copy bandwidth; the trailing update also against the tcgen05 TF32 peak."""
+    copy bandwidth; the trailing update also against the tcgen05 TF32 peak.
+    traffic: DRAM bytes per launch (average over the class's launches), where
+    an ncu capture gives the ratio to the algorithmic bytes."""
     secs = k["ms"] * 1e-3
     hbm = peaks.get("hbm_gbs", 6650.0)
     gbs = k.get("bytes", 0.0) / secs / 1e9 if secs > 0 else 0.0
-    out = {"bound": "hbm", "kernel": KERNELS.get(name, name), "achieved": round(gbs, 1), "peak": hbm,
-           "unit": "GB/s", "frac": round(gbs / hbm, 4), "traffic": None,
+    out = {"bound": "hbm", "class": name, "kernel": KERNELS.get(name, name), "achieved": round(gbs, 1),
+           "peak": hbm, "unit": "GB/s", "frac": round(gbs / hbm, 4), "traffic": None,
            "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
            "ms": round(k["ms"], 3), "launches": k["launches"]}
     if name in NOTES:
@@ -602,8 +730,12 @@ def _roofline(name, k, peaks, mpeaks):
     if name == "gemm":
         tf = k["work"] / secs / 1e12
         peak = mpeaks["tf32_umma_n128"]
-        out["traffic_note"] = ("ncu, one K = 256 launch of 2 problems: dram read+write = 1.11 x the algorithmic "
-                               "C bytes (profiles/k_gemm_tc_k256_2160.md)")
+        per_launch = k.get("bytes", 0.0) / max(1, k["launches"])
+        out["traffic"] = round(GEMM_DRAM_PER_ALGO_BYTE * per_launch)
+        out["algorithmic_bytes_per_launch"] = round(per_launch)
+        out["traffic_note"] = ("bytes per launch: dram read+write / algorithmic C bytes = "
+                               f"{GEMM_DRAM_PER_ALGO_BYTE:.3f} from ncu on one K = 256 launch of 2 problems "
+                               "(profiles/k_gemm_tc_k256_2160.md), times this run's algorithmic bytes per launch")
         out["tensor"] = {"achieved_tflops": round(tf, 2), "peak_tflops": round(peak, 1),
                          "frac": round(tf / peak, 4),
                          "peak_source": "measured: tcgen05 kind::tf32 M=128 N=128 issue-rate "

@@ -135,7 +135,11 @@ int bem_ctx_set_stream(bem_ctx *ctx, void *stream);
  * Integer budgets for a context that shares the GPU with another one running
  * at the same time (0, the default, means the whole device): "gemm_ctas"
  * (CTAs of the persistent FP32 trailing update) and "trsv_ctas" (CTAs of one
- * cooperative triangular solve, over all problems of the batch). */
+ * cooperative triangular solve, over all problems of the batch).
+ * "wait_limit_ms" (1..60000, default 2000): how long any device-side wait of
+ * ctx's kernels (a bulk-copy mbarrier, a cluster mailbox, a software grid
+ * barrier) may last before the kernel gives up, records a timeout and
+ * returns; the call then reports BEM_ERR_TIMEOUT. */
 int bem_ctx_set_option(bem_ctx *ctx, const char *name, int value);
 int bem_ctx_get_option(bem_ctx *ctx, const char *name, int *value);
 const char *bem_status_string(int status);
@@ -190,8 +194,11 @@ int bem_get_preswap(bem_ctx *ctx, double *zh, double *zg);
  * assembly's scratch (2 x 9 nbe + chunks x nn complex128 words, chunks =
  * ceil(nbe / min(64, 1024 / npg^2))) comes from one fixed 8 MiB array that
  * each device holds until the process exits; a larger mesh is rejected with
- * BEM_ERR_ARG (nbe <= 3136 at npg <= 4, 1618 at npg = 8).  The first call on a device
- * looks up that array's device address; make it before any stream capture.
+ * BEM_ERR_ARG (nbe <= 3136 at npg <= 4, 2520 at 5, 2128 at 6, 1801 at 7, 1618 at
+ * npg = 8).  The first call on a device looks up that array's device address
+ * and keeps it for the life of the process; make it before any stream
+ * capture.  The kept address does not survive cudaDeviceReset on that device:
+ * after a reset this entry point must not be called again in the process.
  * All calls on a device share the array: calls that overlap on the GPU
  * (other streams, other contexts of the same device) race.  Asynchronous on
  * ctx's stream; a device-side timeout shows at the next bem_sync. */
@@ -293,6 +300,16 @@ int bem_prof_read(bem_ctx *ctx, double *ms, long long *launches,
  * factors read once per solve, the FP64 matrix once per residual, the
  * systems written by the assembly). */
 int bem_prof_bytes(bem_ctx *ctx, double *bytes);
+
+/* Failure-path self-test.  No counterpart in the reference (its CUDA waits
+ * are unbounded): runs one small kernel with the library's bounded wait of
+ * kind `which` on an event that never happens -- 0: an mbarrier armed for a
+ * bulk copy that is never issued; 1: a software grid barrier that expects one
+ * CTA more than the launch has -- under ctx's "wait_limit_ms".  The kernel
+ * gives up after that limit and returns, and the call reports
+ * BEM_ERR_TIMEOUT; ctx stays usable (the next call clears the status).
+ * Nothing faults or hangs. */
+int bem_wait_selftest(bem_ctx *ctx, int which);
 
 /* Measures this GPU's FP64 tensor-core (DMMA) throughput with a
  * register-resident mma.sync loop; writes TFLOP/s. */

@@ -23,7 +23,9 @@ import shutil
 import sys
 import zipfile
 
-SRC = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
+# The reference's src/ directory: the first argument, else BEM_REFERENCE_TREE/src.
+SRC = (sys.argv[1] if len(sys.argv) > 1 else
+       os.path.join(os.environ["BEM_REFERENCE_TREE"], "src") if "BEM_REFERENCE_TREE" in os.environ else None)
 HERE = os.path.dirname(os.path.abspath(__file__))
 FILES = ["ESOLO240E_-5+5.DAT", "ESOLO240D_-5+5.DAT", "SSOLO240D_-5+5.SOL",
          "ESOLO2160E_-5+5.DAT", "ESOLO2160D_-5+5.DAT", "SSOLO2160D_-5+5.SOL",
@@ -31,6 +33,8 @@ FILES = ["ESOLO240E_-5+5.DAT", "ESOLO240D_-5+5.DAT", "SSOLO240D_-5+5.SOL",
 ZIPPED = ["E510e.dat", "E510d.dat", "Esoil_1600e.dat", "Esoil_1600d.dat"]
 
 if __name__ == "__main__":
+    if SRC is None:
+        sys.exit("usage: make_golden.py <reference>/src  (or set BEM_REFERENCE_TREE)")
     with open(os.path.join(HERE, "SHA256SUMS"), "w") as out:
         for f in FILES:
             dst = os.path.join(HERE, f)

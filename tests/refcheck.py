@@ -22,8 +22,11 @@ def available() -> bool:
 def build() -> bool:
     """Builds the checker where the reference tree is present; True if it exists."""
     if not available():
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"],
-                       capture_output=True)
+        import __graft_entry__
+        ref = __graft_entry__.reference_tree()
+        if ref:
+            subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={ref}"],
+                           capture_output=True)
     return available()
 
 

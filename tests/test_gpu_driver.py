@@ -15,11 +15,15 @@ from bem_mececcs_b200 import driver, formats
 pytestmark = pytest.mark.gpu
 
 
-def test_reference_case_through_the_driver(tmp_path, golden_dir):
+@pytest.mark.parametrize("form", ["plain", "mixed"])
+def test_reference_case_through_the_driver(tmp_path, golden_dir, form):
+    """Both forms of the driver: plain (one frequency at a time in FP64, what
+    the reference does) and mixed (the lockstep sweep, FP32 LU on tensor
+    cores + FP64 refinement) on the reference's NPG = 8 known-answer mesh."""
     ein = os.path.join(golden_dir, "ESOLO240E_-5+5.DAT")
     din = os.path.join(golden_dir, "ESOLO240D_-5+5.DAT")
     eout, dout = str(tmp_path / "SSOLO240E.DAT"), str(tmp_path / "SSOLO240D.DAT")
-    res = driver.run_case(ein, din, eout, dout, form="plain", device=0)
+    res = driver.run_case(ein, din, eout, dout, form=form, device=0)
     assert len(res) == 1
     with open(os.path.join(golden_dir, "SSOLO240E_-5+5.SOL"), "rb") as fh:
         assert open(eout, "rb").read() == fh.read()
