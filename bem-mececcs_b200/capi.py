@@ -144,7 +144,7 @@ class Context:
 
     def set_option(self, name: str, value) -> None:
         """bem_ctx_set_option: switches tcgen05, trsv_coop, lu_pairs, lu_quads,
-        panel_calu, panel_push, panel_async, laswp_tc, trsv_inv, graphs; CTA
+        f64_pairs, tc_pair, panel_calu, panel_push, panel_async, laswp_tc, trsv_inv, graphs; CTA
         budgets gemm_ctas, trsv_ctas (0 = device); wait_limit_ms, the bound of
         every device-side wait (1..60000, default 2000)."""
         v = int(value) if name in self.INT_OPTIONS else int(bool(value))

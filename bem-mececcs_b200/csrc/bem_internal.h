@@ -112,7 +112,8 @@ struct TcWork {
   float* lhat = nullptr;  // [batch][2nn][64]  re/im rows of L21, TF32
   float* ure = nullptr;   // [batch][nn+1][64] Re U12, K-major, TF32
   float* uim = nullptr;   // [batch][nn+1][64] Im U12
-  void* maps = nullptr;   // 4 TMA tensor maps (host copies, passed by value)
+  void* maps = nullptr;   // 6 TMA tensor maps (host copies, passed by value)
+  int pair_clusters = 0;  // resident CTA pairs of k_gemm_tc2 (0: not yet queried)
   float2* cbase = nullptr;  // systems the C map (maps[3]) was made for
   size_t clda = 0, cbstride = 0;
   int cbatch = 0;
@@ -202,6 +203,8 @@ struct bem_ctx {
   bool panel_async = true;    // ... as st.async into mbarrier-counted mailboxes, no per-column cluster barrier
   bool lu_pairs = true;       // FP32 tensor-core LU: two 64-column panels per trailing update (K = 128)
   bool lu_quads = true;       // ... four (K = 256) where four 64-column panels fit
+  bool f64_pairs = true;      // FP64 LU: two panels per trailing update (K = 2 x panel width)
+  bool tc_pair = false;       // FP32 trailing update by CTA pairs (k_gemm_tc2, tcgen05 cta_group::2)
   // SM shares for contexts that run concurrently on one GPU (0: the whole device)
   int gemm_ctas = 0;          // CTAs of the persistent tensor-core trailing update
   int trsv_ctas = 0;          // CTAs of one cooperative triangular solve (all problems together)

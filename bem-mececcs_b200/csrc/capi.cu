@@ -148,6 +148,8 @@ int bem_ctx_create(int device, bem_ctx** out) {
   if (const char* env = getenv("BEM_LASWP_TC")) ctx->laswp_tc = env[0] != '0';
   if (const char* env = getenv("BEM_LU_QUADS")) ctx->lu_quads = env[0] != '0';
   if (const char* env = getenv("BEM_PANEL_ASYNC")) ctx->panel_async = env[0] != '0';
+  if (const char* env = getenv("BEM_F64_PAIRS")) ctx->f64_pairs = env[0] != '0';
+  if (const char* env = getenv("BEM_TC_PAIR")) ctx->tc_pair = env[0] == '1';
   *out = ctx;
   return BEM_OK;
 }
@@ -542,6 +544,8 @@ static bool* option_slot(bem_ctx* ctx, const char* name) {
   if (!strcmp(name, "laswp_tc")) return &ctx->laswp_tc;
   if (!strcmp(name, "lu_pairs")) return &ctx->lu_pairs;
   if (!strcmp(name, "lu_quads")) return &ctx->lu_quads;
+  if (!strcmp(name, "f64_pairs")) return &ctx->f64_pairs;
+  if (!strcmp(name, "tc_pair")) return &ctx->tc_pair;
   if (!strcmp(name, "panel_calu")) return &ctx->panel_calu;
   if (!strcmp(name, "panel_push")) return &ctx->panel_push;
   if (!strcmp(name, "panel_async")) return &ctx->panel_async;

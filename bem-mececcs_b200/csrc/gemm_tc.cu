@@ -310,6 +310,238 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
   }
 }
 
+// ---------------------------------------------------------------------------
+// k_gemm_tc2: the same update by CTA pairs (a cluster of 2 CTAs on one TPC,
+// option "tc_pair").  A pair owns a 128-complex-row x 128-column tile of C:
+// each CTA stages its own 64 complex rows of Lhat (128 real rows) and half of
+// the tile's U columns (64 of U_re and U_im) per K chunk, the even CTA issues
+// tcgen05.mma.cta_group::2 with M = 256, N = 128 (each CTA's tensor memory
+// receives its own 128 real rows over all 128 columns) and each CTA's
+// epilogue reduce-adds its own rows as in k_gemm_tc.  Per K chunk the pair
+// reads 64 KB from L2 for a 128 x 128 complex tile where two single CTAs read
+// 96 KB.  Protocol (no multicast load anywhere): every CTA loads into its own
+// shared memory and the copies complete bytes of the even CTA's `full`
+// barrier (cp.async.bulk.tensor.cta_group::2), which the even CTA alone
+// arms; its MMA thread frees a stage in both CTAs with one multicast
+// tcgen05.commit, signals both CTAs' accumulators full the same way, and
+// waits until the four epilogue warps of both CTAs have arrived on its
+// `t_empty`.  Tensor memory is allocated and freed by warp 1 of each CTA
+// (cta_group::2).  Every wait is bounded.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kHalfChunk = 64 * 32 * 4;           // U box of the pair: 64 rows x 32 floats = 8 KB
+constexpr uint32_t kStage2Bytes = kChunk + 2 * kHalfChunk;  // 32 KB per CTA and stage
+constexpr int kStages2 = 4;
+constexpr size_t kTc2Smem = (size_t)kStages2 * kStage2Bytes + 2 * kHalfBytes + 1024;
+
+__device__ __forceinline__ unsigned pair_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void pair_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// Shared::cluster address of this CTA's variable p in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t pair_addr(const void* p, unsigned rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+  return r;
+}
+// TMA load into this CTA's shared memory whose completed bytes go to the
+// mbarrier at shared::cluster address `bar` (the even CTA's).
+__device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+      "[%4];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void umma_tf32_pair(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                               uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+// Arrives on the mbarrier at the same offset in both CTAs of the pair once the
+// MMAs issued so far are complete.
+__device__ __forceinline__ void umma_commit_pair(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+          smem_u32(bar)),
+      "h"((unsigned short)0x3)
+      : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t bar) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__global__ void __launch_bounds__(256, 1) k_gemm_tc2(const __grid_constant__ CUtensorMap tm_l,
+                                                     const __grid_constant__ CUtensorMap tm_ure,
+                                                     const __grid_constant__ CUtensorMap tm_uim,
+                                                     const __grid_constant__ CUtensorMap tm_c, TcArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  unsigned char* ring = smem;                                                 // kStages2 x (Lhat, U_re, U_im)
+  float* stage_c = reinterpret_cast<float*>(smem + kStages2 * kStage2Bytes);  // 2 x [64 cols][128 floats]
+  __shared__ uint64_t full[kStages2], empty[kStages2], t_full[2], t_empty[2];
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_abort;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned rank = pair_rank();
+  const bool even = rank == 0;
+  const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+  const int total = a.mtiles * a.ntiles * a.batch;  // mtiles: 128-complex-row tiles here
+  const int nchunks = (a.kw + 31) / 32;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages2; ++s) {
+      mbar_init(&full[s], 1);   // the even CTA's expect_tx (bytes of both CTAs)
+      mbar_init(&empty[s], 1);  // the multicast commit of the even CTA's MMA thread
+    }
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&t_full[s], 1);   // multicast commit
+      mbar_init(&t_empty[s], 8);  // the 4 epilogue warps of both CTAs (even CTA's copy)
+    }
+    s_abort = 0;
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  pair_sync();  // both CTAs' barriers are initialised before any remote arrival
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  volatile int* abort_flag = &s_abort;
+  const unsigned long long wlim = wait_limit(a.status);
+  const int tile_rows = 2 * kTcRows;  // complex rows per pair tile
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer of this CTA's operand halves (both CTAs) ----
+    int s = 0;
+    uint32_t ph = 0;
+    bool ok = true;
+    for (int t = pair; t < total && ok; t += npairs) {
+      const int b = t / (a.mtiles * a.ntiles);
+      const int rem = t % (a.mtiles * a.ntiles);
+      const int tm = rem % a.mtiles, tn = rem / a.mtiles;
+      const int ly = b * a.lrows + 2 * (tm * tile_rows + (int)rank * kTcRows);
+      const int uy = b * a.urows + a.urow_off + tn * kTcCols + (int)rank * (kTcCols / 2);
+      for (int h = 0; h < nchunks; ++h) {
+        if (!wait_or_abort(&empty[s], ph ^ 1u, abort_flag, a.status, wlim)) {
+          ok = false;
+          break;
+        }
+        unsigned char* st = ring + (size_t)s * kStage2Bytes;
+        const uint32_t fb = pair_addr(&full[s], 0);
+        if (even) mbar_expect_tx(&full[s], 2 * kStage2Bytes);
+        tma_load_2d_pair(st, &tm_l, a.kbase + 32 * h, ly, fb);
+        tma_load_2d_pair(st + kChunk, &tm_ure, a.kbase + 32 * h, uy, fb);
+        tma_load_2d_pair(st + kChunk + kHalfChunk, &tm_uim, a.kbase + 32 * h, uy, fb);
+        if (++s == kStages2) {
+          s = 0;
+          ph ^= 1u;
+        }
+      }
+    }
+  } else if (warp == 1 && lane == 0 && even) {
+    // ---- MMA issuer of the pair ----
+    const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcCols >> 3) << 17) |
+                           ((uint32_t)(256 >> 4) << 24);
+    int s = 0;
+    uint32_t ph = 0;
+    int it = 0;
+    bool ok = true;
+    for (int t = pair; t < total && ok; t += npairs, ++it) {
+      const int buf = it & 1;
+      if (!wait_or_abort(&t_empty[buf], ((uint32_t)(it >> 1) & 1u) ^ 1u, abort_flag, a.status, wlim)) break;
+      tc_fence_after();
+      const uint32_t d1 = tmem + (uint32_t)buf * 256u, d2 = d1 + 128u;
+      for (int h = 0; h < nchunks; ++h) {
+        if (!wait_or_abort(&full[s], ph, abort_flag, a.status, wlim)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sbase = smem_u32(ring + (size_t)s * kStage2Bytes);
+        const int ks = min(4, (a.kw - 32 * h) / 8);
+        for (int kk = 0; kk < ks; ++kk) {
+          const uint32_t off = (uint32_t)kk * 32u;
+          const uint64_t da = sdesc(sbase + off);
+          const uint64_t dre = sdesc(sbase + kChunk + off);
+          const uint64_t dim = sdesc(sbase + kChunk + kHalfChunk + off);
+          const uint32_t acc = (h > 0 || kk > 0) ? 1u : 0u;
+          umma_tf32_pair(d1, da, dre, idesc, acc);
+          umma_tf32_pair(d2, da, dim, idesc, acc);
+        }
+        umma_commit_pair(&empty[s]);
+        if (++s == kStages2) {
+          s = 0;
+          ph ^= 1u;
+        }
+      }
+      if (ok) umma_commit_pair(&t_full[buf]);
+    }
+  } else if (warp >= 4) {
+    // ---- epilogue of this CTA's 64 complex rows (both CTAs) ----
+    const int e = warp - 4;
+    const int rho = 32 * e + lane;
+    const int p = lane & 1;
+    const bool issuer = (e == 0 && lane == 0);
+    const uint32_t te0 = pair_addr(&t_empty[0], 0), te1 = pair_addr(&t_empty[1], 0);
+    int it = 0;
+    for (int t = pair; t < total; t += npairs, ++it) {
+      const int buf = it & 1;
+      if (!__all_sync(0xffffffffu, wait_or_abort(&t_full[buf], (uint32_t)(it >> 1) & 1u, abort_flag, a.status, wlim)))
+        break;
+      tc_fence_after();
+      const int b = t / (a.mtiles * a.ntiles);
+      const int rem = t % (a.mtiles * a.ntiles);
+      const int tm = rem % a.mtiles, tn = rem / a.mtiles;
+      const int row0 = a.r0 + tm * tile_rows + (int)rank * kTcRows;  // this CTA's first complex row
+      const uint32_t tbase = tmem + (uint32_t)buf * 256u + ((uint32_t)(32 * e) << 16);
+      for (int hc = 0; hc < 2; ++hc) {
+        float* ct = stage_c + (size_t)hc * (kHalfBytes / 4);
+        if (issuer) tma_wait_read_1();
+        epi_bar_sync();
+        for (int c = 0; c < 64; c += 16) {
+          float v1[16], v2[16];
+          tmem_ld16(tbase + (uint32_t)(64 * hc + c), v1);
+          tmem_ld16(tbase + 128u + (uint32_t)(64 * hc + c), v2);
+          tmem_ld_wait();
+          const int colbase = a.c0 + tn * kTcCols + 64 * hc + c;
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const float x = __shfl_xor_sync(0xffffffffu, v2[i], 1);
+            const float val = p ? (v1[i] + x) : (v1[i] - x);
+            ct[(c + i) * 128 + rho] = colbase + i < a.cend ? -val : 0.0f;
+          }
+        }
+        if (hc == 1) {
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive_remote(buf ? te1 : te0);
+        }
+        fence_proxy_async();
+        epi_bar_sync();
+        if (issuer && row0 < a.nn) tma_reduce_add_3d(&tm_c, 2 * row0, a.c0 + tn * kTcCols + 64 * hc, b, ct);
+      }
+    }
+    if (issuer) tma_store_wait_all();
+  }
+  __syncthreads();
+  pair_sync();  // the pair's MMAs, commits and remote arrivals are all done
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  }
+}
+
 // Lhat: rows 2(r - r0) + p of problem b hold part p of L(r, k..k+kw-1),
 // K-major at K slots koff..koff+kw-1 of a kKPitch-float row, rounded to TF32.
 // With a gather list (a later panel's interchanges: count, then dst/src
@@ -345,13 +577,13 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// 2-D map over `rows` rows of 64 floats (256-byte rows), 32 x 128 boxes, 128B swizzle.
-bool make_map(CUtensorMap* m, float* base, size_t rows) {
+// 2-D map over `rows` rows of kKPitch floats, 32 x box_rows boxes, 128B swizzle.
+bool make_map(CUtensorMap* m, float* base, size_t rows, unsigned box_rows = 128) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return false;
   cuuint64_t dims[2] = {kKPitch, (cuuint64_t)rows};
   cuuint64_t strides[1] = {kKPitch * sizeof(float)};
-  cuuint32_t box[2] = {32, 128};
+  cuuint32_t box[2] = {32, box_rows};
   cuuint32_t estr[2] = {1, 1};
   return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -465,13 +697,17 @@ int tc_ensure(bem_ctx* ctx, int nn, int batch) {
   BEM_CUDA(ctx, cudaMemset(W.lhat, 0, lrows * kKPitch * sizeof(float)));
   BEM_CUDA(ctx, cudaMemset(W.ure, 0, urows * kKPitch * sizeof(float)));
   BEM_CUDA(ctx, cudaMemset(W.uim, 0, urows * kKPitch * sizeof(float)));
-  W.maps = new CUtensorMap[4];
+  // maps: 0 Lhat, 1-2 U_re/U_im (128-row boxes), 3 C (made per system), 4-5 U_re/U_im in
+  // the 64-row boxes of the CTA-pair kernel
+  W.maps = new CUtensorMap[6];
   CUtensorMap* maps = static_cast<CUtensorMap*>(W.maps);
-  if (!make_map(&maps[0], W.lhat, lrows) || !make_map(&maps[1], W.ure, urows) || !make_map(&maps[2], W.uim, urows))
+  if (!make_map(&maps[0], W.lhat, lrows) || !make_map(&maps[1], W.ure, urows) || !make_map(&maps[2], W.uim, urows) ||
+      !make_map(&maps[4], W.ure, urows, 64) || !make_map(&maps[5], W.uim, urows, 64))
     return fail(ctx, BEM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   W.lrows_cap = lrows;
   W.urows_cap = urows;
   BEM_CUDA(ctx, cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+  BEM_CUDA(ctx, cudaFuncSetAttribute(k_gemm_tc2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTc2Smem));
   return BEM_OK;
 }
 
@@ -533,8 +769,48 @@ int tc_gemm(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int r0,
   t.lrows = 2 * nn;
   t.urows = nn + 1;
   t.status = ctx->d_status;
-  const int total = t.mtiles * t.ntiles * batch;
   const int ctas = ctx->gemm_ctas > 0 ? std::min(ctx->gemm_ctas, ctx->num_sms) : ctx->num_sms;
+  if (ctx->tc_pair) {
+    // CTA pairs: 128-complex-row tiles, as many pairs as can be resident at once
+    t.mtiles = (nn - r0 + 2 * kTcRows - 1) / (2 * kTcRows);
+    const int total = t.mtiles * t.ntiles * batch;
+    if (W.pair_clusters == 0) {
+      cudaLaunchConfig_t q = {};
+      q.gridDim = dim3(2, 1, 1);
+      q.blockDim = dim3(256, 1, 1);
+      q.dynamicSmemBytes = kTc2Smem;
+      cudaLaunchAttribute qa[1];
+      qa[0].id = cudaLaunchAttributeClusterDimension;
+      qa[0].val.clusterDim.x = 2;
+      qa[0].val.clusterDim.y = 1;
+      qa[0].val.clusterDim.z = 1;
+      q.attrs = qa;
+      q.numAttrs = 1;
+      int n = 0;
+      if (cudaOccupancyMaxActiveClusters(&n, k_gemm_tc2, &q) != cudaSuccess || n < 1) {
+        cudaGetLastError();
+        return fail(ctx, BEM_ERR_CUDA, "no resident CTA pair for the paired tensor-core update");
+      }
+      W.pair_clusters = n;
+    }
+    const int pairs = std::max(1, std::min({total, W.pair_clusters, ctas / 2}));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * pairs, 1, 1);
+    cfg.blockDim = dim3(256, 1, 1);
+    cfg.dynamicSmemBytes = kTc2Smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    BEM_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_gemm_tc2, maps[0], maps[4], maps[5], maps[3], t));
+    ctx->launches++;
+    return BEM_OK;
+  }
+  const int total = t.mtiles * t.ntiles * batch;
   const int grid = std::min(total, ctas);
   k_gemm_tc<<<grid, 256, kTcSmem, ctx->stream>>>(maps[0], maps[1], maps[2], maps[3], t);
   ctx->launches++;

@@ -1764,11 +1764,14 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel_grid(PanelArgs a) {
 
 // Row interchanges of one panel applied to columns [c0, ncols) as a gather,
 // then U12 = L11^-1 A12 (unit lower).  One warp per column; problem = blockIdx.y.
+// PRE: the previous panel (columns kprev..kprev+wprev-1, wprev = 16, 32, 48
+// or 64) has not yet updated this panel's rows; its deferred product comes
+// first.
 template <typename R, bool PRE>
 __global__ void __launch_bounds__(256) k_laswp_trsm(void* Av, size_t lda, size_t bstride, int k, int w, int c0,
                                                     int ncols, const int* __restrict__ perm, int perm_stride,
                                                     float* ure, float* uim, int urows, int ubase, int koff,
-                                                    int kprev) {
+                                                    int kprev, int wprev) {
   using E = typename Elt<R>::T;
   using C = cpx<R>;
   constexpr int NB = 64;
@@ -1786,7 +1789,7 @@ __global__ void __launch_bounds__(256) k_laswp_trsm(void* Av, size_t lda, size_t
     // interchanges holds the old row src(k + i).  64 rows x 4 groups of 16
     // columns, all loads of a thread issued before its stores.
     const int i = threadIdx.x & 63, jg = threadIdx.x >> 6;
-    if (i < w) {
+    if (i < w && jg * 16 < wprev) {
       const int src = pl[2 * i + 1];
       E t[16];
 #pragma unroll
@@ -1820,8 +1823,8 @@ __global__ void __launch_bounds__(256) k_laswp_trsm(void* Av, size_t lda, size_t
 #pragma unroll
       for (int h = 0; h < 2; ++h) x[q][h] = ok && xd[h] >= 0 ? ldc<R>(&cp[xs[h]]) : C{R(0), R(0)};
       if (PRE) {
-        u0[q] = ok ? ldc<R>(&cp[kprev + lane]) : C{R(0), R(0)};
-        u1[q] = ok ? ldc<R>(&cp[kprev + lane + 32]) : C{R(0), R(0)};
+        u0[q] = ok && lane < wprev ? ldc<R>(&cp[kprev + lane]) : C{R(0), R(0)};
+        u1[q] = ok && lane + 32 < wprev ? ldc<R>(&cp[kprev + lane + 32]) : C{R(0), R(0)};
       }
     }
     __syncwarp();
@@ -1835,8 +1838,8 @@ __global__ void __launch_bounds__(256) k_laswp_trsm(void* Av, size_t lda, size_t
     }
     if (PRE) {
       // The previous panel's deferred update of this panel's rows:
-      // v -= L(rows, kprev..kprev+63) U(kprev..kprev+63, col).
-      for (int j = 0; j < NB; ++j) {
+      // v -= L(rows, kprev..kprev+wprev-1) U(kprev..kprev+wprev-1, col).
+      for (int j = 0; j < wprev; ++j) {
         const C l0 = s_Lb[j * NB + lane], l1 = s_Lb[j * NB + lane + 32];
 #pragma unroll
         for (int q = 0; q < QC; ++q) {
@@ -2287,16 +2290,45 @@ constexpr int AS_STRIDE = GBM + 2;  // == 2 mod 8
 constexpr int BS_STRIDE = GBK + 4;  // == 4 mod 8
 constexpr size_t kGemmSmem = (size_t)2 * (GBK * AS_STRIDE + GBN * BS_STRIDE) * sizeof(double2);
 
+// With gperm (a panel pair of the plain LU): the first wg of the K columns
+// are the earlier panel's L, whose rows have not taken the later panel's
+// interchanges; row r of C reads them at the row the later panel's gather
+// list moved to r (count, then dst/src pairs; problem z's list at
+// gperm + z * gperm_stride).
 __global__ void __launch_bounds__(256) k_gemm_f64(double2* Abase, size_t lda, size_t bstride, int nn, int k, int w,
-                                                  int r0, int c0, int ncols) {
+                                                  int r0, int c0, int ncols, const int* __restrict__ gperm,
+                                                  int gperm_stride, int wg) {
   extern __shared__ __align__(16) double2 g_smem[];
   auto As = reinterpret_cast<double2(*)[GBK][AS_STRIDE]>(g_smem);
   auto Bs = reinterpret_cast<double2(*)[GBN][BS_STRIDE]>(g_smem + 2 * GBK * AS_STRIDE);
+  __shared__ int s_map[GBM];  // storage row of the gathered L columns for each tile row
   double2* A = Abase + (size_t)blockIdx.z * bstride;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warps
   const int row0 = r0 + blockIdx.x * GBM, col0 = c0 + blockIdx.y * GBN;
+
+  // The tile of C is read at the end: start bringing it into L2 now.
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int gr = row0 + wm * 32 + mt * 8 + g, gc = col0 + wn * 16 + nt * 8 + 2 * t + e;
+        if (gr < nn && gc < ncols) asm volatile("prefetch.global.L2 [%0];" ::"l"(&A[(size_t)gc * lda + gr]));
+      }
+  if (tid < GBM) s_map[tid] = row0 + tid;
+  __syncthreads();
+  if (gperm && wg > 0) {
+    const int* pl = gperm + (size_t)blockIdx.z * gperm_stride;
+    const int cnt = pl[0];
+    for (int e = tid; e < cnt; e += blockDim.x) {
+      const int dst = pl[1 + 2 * e];
+      if (dst >= row0 && dst < row0 + GBM) s_map[dst - row0] = pl[2 + 2 * e];
+    }
+  }
+  __syncthreads();
 
   auto load_chunk = [&](int stage, int kc) {
 #pragma unroll
@@ -2305,7 +2337,8 @@ __global__ void __launch_bounds__(256) k_gemm_f64(double2* Abase, size_t lda, si
       const int kk = idx >> 6, m = idx & 63;
       const int gr = row0 + m, gk = kc + kk;
       const bool ok = gr < nn && gk < w;
-      cp_async16(&As[stage][kk][m], ok ? &A[(size_t)(k + gk) * lda + gr] : A, ok);
+      const int sr = gk < wg ? s_map[m] : gr;
+      cp_async16(&As[stage][kk][m], ok ? &A[(size_t)(k + gk) * lda + sr] : A, ok);
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -3651,10 +3684,10 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     const int blocks = std::max(1, std::min((cols + 31) / 32, (4 * ctx->num_sms + batch - 1) / batch));
     if (pre)
       k_laswp_trsm<R, true><<<dim3(blocks, batch), 256, 2 * lsmem, ctx->stream>>>(
-          A, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kfirst);
+          A, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kfirst, k - kfirst);
     else
       k_laswp_trsm<R, false><<<dim3(blocks, batch), 256, lsmem, ctx->stream>>>(
-          A, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kfirst);
+          A, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kfirst, 0);
     ctx->launches++;
     BEM_CUDA(ctx, cudaGetLastError());
     return BEM_OK;
@@ -3708,6 +3741,51 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
       k = kG;
       continue;
     }
+    // FP64: two panels of the same width nb per trailing update (K = 2 nb).
+    // Panel 1's update reaches panel 2's columns at once (a narrow update);
+    // past the pair, panel 2's interchanges reach rows that have not taken
+    // panel 1's update, panel 2's U rows first take it (k_laswp_trsm<PRE>,
+    // panel 1's L read at panel 2's rows through its gather list), and the
+    // rest is one K = 2 nb update whose first nb columns read panel 1's L
+    // through the same list.  A keeps the factors of the one-panel-at-a-time
+    // LU, so the solves are unchanged.
+    const int nbp = sizeof(R) == 8 && ctx->f64_pairs ? panel_nb(m) : 0;
+    if (nbp > 0 && m > 2 * nbp && panel_nb(m - nbp) == nbp) {
+      double2* A2 = static_cast<double2*>(A);
+      int w1 = 0, w2 = 0, *p1 = nullptr, *p2 = nullptr;
+      int rc = run_panel(k, w1, p1);
+      if (rc) return rc;
+      const int k2 = k + w1;
+      bool packed = false;
+      rc = laswp(k, w1, k2, p1, k2, 0, k, 0, k2, -1, 1, -1, packed);
+      if (rc) return rc;
+      {  // panel 1's update of panel 2's columns
+        ProfScope ps(ctx, 3, 8.0 * (double)(nn - k2) * (double)nbp * (double)w1 * batch,
+                     2.0 * (double)(nn - k2) * (double)nbp * es * batch);
+        dim3 grid((nn - k2 + GBM - 1) / GBM, (nbp + GBN - 1) / GBN, batch);
+        k_gemm_f64<<<grid, 256, kGemmSmem, ctx->stream>>>(A2, lda, bstride, nn, k, w1, k2, k2, k2 + nbp, nullptr,
+                                                         0, 0);
+        ctx->launches++;
+        BEM_CUDA(ctx, cudaGetLastError());
+      }
+      rc = run_panel(k2, w2, p2);
+      if (rc) return rc;
+      const int kG = k2 + w2;
+      rc = laswp(k2, w2, kG, p2, kG, 0, k, 1, kG, -1, 1, -1, packed);
+      if (rc) return rc;
+      if (kG < nn) {
+        const int cols = ncols - kG;
+        ProfScope ps(ctx, 3, 8.0 * (double)(nn - kG) * (double)cols * (double)(w1 + w2) * batch,
+                     2.0 * (double)(nn - kG) * (double)cols * es * batch);
+        dim3 grid((nn - kG + GBM - 1) / GBM, (cols + GBN - 1) / GBN, batch);
+        k_gemm_f64<<<grid, 256, kGemmSmem, ctx->stream>>>(A2, lda, bstride, nn, k, w1 + w2, kG, kG, ncols, p2,
+                                                         kPermStride, w1);
+        ctx->launches++;
+        BEM_CUDA(ctx, cudaGetLastError());
+      }
+      k = kG;
+      continue;
+    }
     int w = 0, *perm_p = nullptr;
     int rc = run_panel(k, w, perm_p);
     if (rc) return rc;
@@ -3729,7 +3807,7 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
         } else if (sizeof(R) == 8) {
           dim3 grid((nn - c0 + GBM - 1) / GBM, (cols + GBN - 1) / GBN, batch);
           k_gemm_f64<<<grid, 256, kGemmSmem, ctx->stream>>>(static_cast<double2*>(A), lda, bstride, nn, k, w, c0, c0,
-                                                           ncols);
+                                                           ncols, nullptr, 0, 0);
           ctx->launches++;
         } else {
           dim3 grid((nn - c0 + TBM - 1) / TBM, (cols + TBN - 1) / TBN, batch);

@@ -123,15 +123,18 @@ int bem_ctx_set_stream(bem_ctx *ctx, void *stream);
  * autotuner: "tcgen05" (FP32 trailing update on tcgen05, else TF32
  * mma.sync), "trsv_coop" (one cooperative launch per triangular solve),
  * "lu_pairs" (two 64-column panels per FP32 trailing update, K = 128),
- * "lu_quads" (four, K = 256, where they fit), "panel_calu" (FP32 panels with
+ * "lu_quads" (four, K = 256, where they fit), "f64_pairs" (FP64 LU: two
+ * panels per trailing update, K = twice the panel width), "tc_pair" (the FP32
+ * trailing update by CTA pairs on tcgen05 cta_group::2, M = 256 per pair),
+ * "panel_calu" (FP32 panels with
  * tournament pivoting), "panel_push" (cluster panels push their pivot
  * candidates by remote stores), "panel_async" (... as st.async into
  * mbarrier-counted mailboxes, without a cluster barrier per column),
  * "laswp_tc" (FP32 row interchanges + U12 on the tensor cores), "trsv_inv"
  * (FP32 solves with inverted diagonal blocks), "graphs" (bem_sweep replays a
  * captured step).  Defaults: tcgen05, trsv_coop, lu_pairs, lu_quads,
- * panel_push, panel_async, laswp_tc, trsv_inv and graphs on; panel_calu
- * off.
+ * f64_pairs, panel_push, panel_async, laswp_tc, trsv_inv and graphs on;
+ * panel_calu and tc_pair off.
  * Integer budgets for a context that shares the GPU with another one running
  * at the same time (0, the default, means the whole device): "gemm_ctas"
  * (CTAs of the persistent FP32 trailing update) and "trsv_ctas" (CTAs of one

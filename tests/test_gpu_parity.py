@@ -43,6 +43,28 @@ def test_lu_random(ctx, n):
     assert rel(x, ref) < 1e-11 * max(1.0, np.linalg.cond(a) / 100)
 
 
+@pytest.mark.parametrize("pairs", [True, False], ids=["f64_pairs", "one_panel"])
+def test_lu_tall_panels_pairs(ctx, pairs):
+    """n = 4000: the FP64 panels above 3440 rows are 32 columns wide, so two
+    of them share one K = 64 trailing update (f64_pairs), the first panel's L
+    read through the second's gather list.  Rows are shuffled so that every
+    panel pivots across the pair; the result must not depend on the scheme."""
+    n = 4000
+    rng = np.random.default_rng(40)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    a = a[rng.permutation(n)] * np.exp(rng.uniform(-3, 3, n))[:, None]  # uneven row scales: real pivoting
+    b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    ctx.set_option("f64_pairs", pairs)
+    try:
+        x = solve_dense(ctx, a, b)
+    finally:
+        ctx.set_option("f64_pairs", True)
+    # normwise backward error at FP64 level, and the same solution as LAPACK's
+    berr = np.linalg.norm(a @ x - b) / (np.linalg.norm(a) * np.linalg.norm(x) + np.linalg.norm(b))
+    assert berr < 1e-15
+    assert rel(x, np.linalg.solve(a, b)) < 1e-10
+
+
 def test_lu_needs_pivoting(ctx):
     n = 200
     rng = np.random.default_rng(3)

@@ -93,3 +93,25 @@ def test_sweep_mixed_c2_2160():
     for i in range(3):
         assert rel(xm[i], xp[i]) < 1e-8, (freqs[i], rel(xm[i], xp[i]))
     ctx.close()
+
+
+@pytest.mark.parametrize("batch", [1, 4])
+def test_sweep_mixed_cta_pair_update(c1, batch):
+    """The FP32 trailing update by CTA pairs (option tc_pair: tcgen05
+    cta_group::2, each pair one 128 x 128 complex tile) gives the refined
+    solution at the FP64 level, as the one-CTA update does, and its
+    unrefined FP32 solution is as close to the oracle's."""
+    s, d, p, sol = c1
+    x1, _ = sol.sweep(FREQS, form="mixed", batch=batch, refine=0)
+    sol.ctx.set_option("tc_pair", True)
+    try:
+        x2, _ = sol.sweep(FREQS, form="mixed", batch=batch, refine=0)
+        x3, corr = sol.sweep(FREQS, form="mixed", batch=batch, refine=3)
+    finally:
+        sol.ctx.set_option("tc_pair", False)
+    for i, fr in enumerate(FREQS):
+        ox = _oracle_x(p, fr)
+        e1, e2 = rel(x1[i], ox), rel(x2[i], ox)
+        assert e2 < 1e-4 and e2 < 10 * max(e1, 1e-7), (batch, fr, e1, e2)
+        assert rel(x3[i], ox) < 1e-10, (batch, fr)
+        assert corr[i] < 1e-9
