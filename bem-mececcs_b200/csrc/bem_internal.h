@@ -5,6 +5,7 @@
 
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -209,6 +210,7 @@ struct bem_ctx {
   int gemm_ctas = 0;          // CTAs of the persistent tensor-core trailing update
   int trsv_ctas = 0;          // CTAs of one cooperative triangular solve (all problems together)
   int wait_limit_ms = 2000;   // bound of every device-side wait (copy of the device word)
+  std::unordered_map<long long, int> lockstep_cache;  // lu_lockstep_capacity by (size, precision)
 };
 
 namespace bem {

@@ -2295,7 +2295,7 @@ constexpr size_t kGemmSmem = (size_t)2 * (GBK * AS_STRIDE + GBN * BS_STRIDE) * s
 // interchanges; row r of C reads them at the row the later panel's gather
 // list moved to r (count, then dst/src pairs; problem z's list at
 // gperm + z * gperm_stride).
-__global__ void __launch_bounds__(256) k_gemm_f64(double2* Abase, size_t lda, size_t bstride, int nn, int k, int w,
+__global__ void __launch_bounds__(256, 2) k_gemm_f64(double2* Abase, size_t lda, size_t bstride, int nn, int k, int w,
                                                   int r0, int c0, int ncols, const int* __restrict__ gperm,
                                                   int gperm_stride, int wg) {
   extern __shared__ __align__(16) double2 g_smem[];
@@ -3370,7 +3370,13 @@ static int lockstep_capacity_t(bem_ctx* ctx, int nn) {
 // Problems whose panels run in one wave: the first (tallest) panel's cluster
 // kernel, as many clusters as can be resident at once.
 int lu_lockstep_capacity(bem_ctx* ctx, int nn, bool fp32) {
-  return fp32 ? lockstep_capacity_t<float>(ctx, nn) : lockstep_capacity_t<double>(ctx, nn);
+  // occupancy queries are host calls of tens of microseconds: remember each answer
+  const long long key = 2LL * nn + (fp32 ? 1 : 0);
+  auto it = ctx->lockstep_cache.find(key);
+  if (it != ctx->lockstep_cache.end()) return it->second;
+  const int cap = fp32 ? lockstep_capacity_t<float>(ctx, nn) : lockstep_capacity_t<double>(ctx, nn);
+  ctx->lockstep_cache[key] = cap;
+  return cap;
 }
 
 // One cooperative k_trsv launch over `batch` problems: forward (with the
