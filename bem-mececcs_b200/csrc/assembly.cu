@@ -542,9 +542,9 @@ int launch_static(bem_ctx* ctx, const double c[4], int compute_gest, double* hes
   // static_chunks holds the capacity of static_part in chunks of nbe*9 doubles
   // for the current mesh (reset to 0 by bem_mesh_upload).
   if (chunks > ctx->static_chunks) {
-    if (ctx->static_part) cudaFree(ctx->static_part);
+    if (ctx->static_part) dev_free(ctx, ctx->static_part);
     ctx->static_part = nullptr;
-    BEM_CUDA(ctx, cudaMalloc(&ctx->static_part, (size_t)chunks * m.nbe * 9 * sizeof(double)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &ctx->static_part, (size_t)chunks * m.nbe * 9 * sizeof(double)));
     ctx->static_chunks = chunks;
   }
   StaticParams p{};
@@ -722,9 +722,9 @@ int launch_dynamic(bem_ctx* ctx, const double zge[2], const double zcs[2], const
   System& s = ctx->sys;
   const int chunks = rhs_chunks(ctx);
   if (chunks > s.rhs_chunks) {
-    if (s.rhs_part) cudaFree(s.rhs_part);
+    if (s.rhs_part) dev_free(ctx, s.rhs_part);
     s.rhs_part = nullptr;
-    BEM_CUDA(ctx, cudaMalloc(&s.rhs_part, (size_t)chunks * s.nn * sizeof(double2)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &s.rhs_part, (size_t)chunks * s.nn * sizeof(double2)));
     s.rhs_chunks = chunks;
   }
   (void)m;

@@ -211,12 +211,33 @@ struct bem_ctx {
   int trsv_ctas = 0;          // CTAs of one cooperative triangular solve (all problems together)
   int wait_limit_ms = 2000;   // bound of every device-side wait (copy of the device word)
   std::unordered_map<long long, int> lockstep_cache;  // lu_lockstep_capacity by (size, precision)
+  unsigned long long alloc_epoch = 0;  // device allocations so far (dev_alloc)
+  unsigned long long sg_epoch = 0;     // alloc_epoch when the sweep step was captured
 };
 
 namespace bem {
 
 int fail(bem_ctx* ctx, int code, const std::string& msg);
 int cuda_fail(bem_ctx* ctx, cudaError_t e, const char* what);
+
+// Device memory of a context comes from the device's stream-ordered pool,
+// allocated and freed on the context's stream.  cudaFree synchronises the
+// whole device, so a process that creates and drops contexts while others
+// compute (the server evicting a cached problem while other requests run)
+// would stall every stream on each drop; cudaFreeAsync does not.  The
+// allocation waits for the context's own stream only, so the memory is
+// ready for any stream and for synchronous copies as cudaMalloc's would be.
+// Every allocation also advances ctx->alloc_epoch: a captured sweep step
+// names the buffers it was captured with and is replayed only while no
+// buffer of the context has been (re)allocated since.
+template <typename T>
+cudaError_t dev_alloc(bem_ctx* ctx, T** p, size_t bytes) {
+  ++ctx->alloc_epoch;
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(p), bytes, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  return e;
+}
+void dev_free(bem_ctx* ctx, void* p);
 
 #define BEM_CUDA(ctx, call)                                   \
   do {                                                        \

@@ -16,6 +16,10 @@ int fail(bem_ctx* ctx, int code, const std::string& msg) {
   return code;
 }
 
+void dev_free(bem_ctx* ctx, void* p) {
+  if (p) cudaFreeAsync(p, ctx->stream);
+}
+
 int cuda_fail(bem_ctx* ctx, cudaError_t e, const char* what) {
   std::string m = std::string(what) + ": " + cudaGetErrorString(e);
   return fail(ctx, e == cudaErrorMemoryAllocation ? BEM_ERR_NOMEM : BEM_ERR_CUDA, m);
@@ -32,40 +36,40 @@ int check_status(bem_ctx* ctx) {
   return BEM_OK;
 }
 
-static void free_mesh(Mesh& m) {
-  cudaFree(m.gq);
-  cudaFree(m.eta);
-  cudaFree(m.colloc);
-  cudaFree(m.corner);
-  cudaFree(m.degen);
+static void free_mesh(bem_ctx* ctx, Mesh& m) {
+  dev_free(ctx, m.gq);
+  dev_free(ctx, m.eta);
+  dev_free(ctx, m.colloc);
+  dev_free(ctx, m.corner);
+  dev_free(ctx, m.degen);
   m = Mesh{};
 }
 
-static void free_system(System& s) {
-  cudaFree(s.A);
-  cudaFree(s.zh_pre);
-  cudaFree(s.zg_pre);
-  cudaFree(s.diag_h);
-  cudaFree(s.diag_g);
-  cudaFree(s.rhs_part);
-  cudaFree(s.x);
+static void free_system(bem_ctx* ctx, System& s) {
+  dev_free(ctx, s.A);
+  dev_free(ctx, s.zh_pre);
+  dev_free(ctx, s.zg_pre);
+  dev_free(ctx, s.diag_h);
+  dev_free(ctx, s.diag_g);
+  dev_free(ctx, s.rhs_part);
+  dev_free(ctx, s.x);
   s = System{};
 }
 
 static int ensure_system(bem_ctx* ctx, int nn, bool preswap) {
   System& s = ctx->sys;
   if (s.nn != nn || !s.A) {
-    free_system(s);
+    free_system(ctx, s);
     s.nn = nn;
     s.lda = (size_t)nn;
-    BEM_CUDA(ctx, cudaMalloc(&s.A, s.lda * (size_t)(nn + 1) * sizeof(double2)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &s.A, s.lda * (size_t)(nn + 1) * sizeof(double2)));
     const int nbe = (nn + 2) / 3;
-    BEM_CUDA(ctx, cudaMalloc(&s.diag_h, (size_t)nbe * 9 * sizeof(double2)));
-    BEM_CUDA(ctx, cudaMalloc(&s.diag_g, (size_t)nbe * 9 * sizeof(double2)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &s.diag_h, (size_t)nbe * 9 * sizeof(double2)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &s.diag_g, (size_t)nbe * 9 * sizeof(double2)));
   }
   if (preswap && !s.zh_pre) {
-    BEM_CUDA(ctx, cudaMalloc(&s.zh_pre, (size_t)nn * nn * sizeof(double2)));
-    BEM_CUDA(ctx, cudaMalloc(&s.zg_pre, (size_t)nn * nn * sizeof(double2)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &s.zh_pre, (size_t)nn * nn * sizeof(double2)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &s.zg_pre, (size_t)nn * nn * sizeof(double2)));
   }
   return BEM_OK;
 }
@@ -131,13 +135,24 @@ int bem_ctx_create(int device, bem_ctx** out) {
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_status, ST_WORDS * sizeof(int));
-  if (e == cudaSuccess) e = cudaMemset(ctx->d_status, 0, ST_WORDS * sizeof(int));  // wait limit 0: the default
+  ctx->stream = ctx->own_stream;
+  if (e == cudaSuccess) {
+    // The device's stream-ordered pool keeps what contexts free, so that the
+    // next context's buffers come from it without a new device allocation.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      unsigned long long keep = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    e = dev_alloc(ctx, &ctx->d_status, ST_WORDS * sizeof(int));
+  }
+  if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_status, 0, ST_WORDS * sizeof(int), ctx->stream);  // wait limit 0: the default
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) {
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return e == cudaErrorMemoryAllocation ? BEM_ERR_NOMEM : BEM_ERR_CUDA;
   }
-  ctx->stream = ctx->own_stream;
   if (const char* env = getenv("BEM_TF32_MMA_SYNC")) ctx->use_tcgen05 = env[0] != '1';
   if (const char* env = getenv("BEM_TRSV_LEGACY")) ctx->use_trsv_coop = env[0] != '1';
   if (const char* env = getenv("BEM_LU_PAIRS")) ctx->lu_pairs = env[0] != '0';
@@ -158,28 +173,31 @@ int bem_ctx_destroy(bem_ctx* ctx) {
   if (!ctx) return BEM_OK;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  free_mesh(ctx->mesh);
-  free_system(ctx->sys);
-  cudaFree(ctx->hestdiag);
-  cudaFree(ctx->gestdiag);
-  cudaFree(ctx->zdfi);
-  cudaFree(ctx->kode);
-  cudaFree(ctx->d_status);
-  cudaFree(ctx->static_part);
+  // everything of ctx is idle now: free it on the context's own stream (the
+  // caller's stream may be gone by the time the frees run)
+  ctx->stream = ctx->own_stream;
+  free_mesh(ctx, ctx->mesh);
+  free_system(ctx, ctx->sys);
+  dev_free(ctx, ctx->hestdiag);
+  dev_free(ctx, ctx->gestdiag);
+  dev_free(ctx, ctx->zdfi);
+  dev_free(ctx, ctx->kode);
+  dev_free(ctx, ctx->d_status);
+  dev_free(ctx, ctx->static_part);
   LuWork& L = ctx->lu;
-  cudaFree(L.ipiv);
-  cudaFree(L.perm);
-  cudaFree(L.slot_val);
-  cudaFree(L.slot_row);
-  cudaFree(L.cand);
-  cudaFree(L.drow);
-  cudaFree(L.barrier);
-  cudaFree(L.trsv_w);
-  cudaFree(L.tinv);
-  cudaFree(L.linv);
-  cudaFree(L.gmap);
-  cudaFree(L.trsv_ctr);
-  cudaFree(L.pstart);
+  dev_free(ctx, L.ipiv);
+  dev_free(ctx, L.perm);
+  dev_free(ctx, L.slot_val);
+  dev_free(ctx, L.slot_row);
+  dev_free(ctx, L.cand);
+  dev_free(ctx, L.drow);
+  dev_free(ctx, L.barrier);
+  dev_free(ctx, L.trsv_w);
+  dev_free(ctx, L.tinv);
+  dev_free(ctx, L.linv);
+  dev_free(ctx, L.gmap);
+  dev_free(ctx, L.trsv_ctr);
+  dev_free(ctx, L.pstart);
   for (bem_ctx* w : ctx->workers) bem_ctx_destroy(w);
   ctx->workers.clear();
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
@@ -195,6 +213,10 @@ int bem_ctx_destroy(bem_ctx* ctx) {
 int bem_ctx_set_stream(bem_ctx* ctx, void* stream) {
   if (!ctx) return BEM_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  // work and frees already enqueued on the old stream finish before the
+  // context's buffers are used, or freed, on the new one
+  BEM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
   return BEM_OK;
 }
@@ -218,7 +240,7 @@ int bem_mesh_upload(bem_ctx* ctx, int n, int nbe, int np, int npg, const int* co
     if (cone[i] < 1 || cone[i] > np) return fail(ctx, BEM_ERR_ARG, "bem_mesh_upload: node number out of range");
   cudaSetDevice(ctx->device);
   BEM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  free_mesh(ctx->mesh);
+  free_mesh(ctx, ctx->mesh);
   Mesh& m = ctx->mesh;
   m.n = n;
   m.nbe = nbe;
@@ -229,17 +251,17 @@ int bem_mesh_upload(bem_ctx* ctx, int n, int nbe, int np, int npg, const int* co
     m.gi[i] = gi[i];
     m.ome[i] = ome[i];
   }
-  BEM_CUDA(ctx, cudaMalloc(&m.gq, (size_t)n * m.ng * sizeof(double4)));
-  BEM_CUDA(ctx, cudaMalloc(&m.eta, (size_t)n * sizeof(double4)));
-  BEM_CUDA(ctx, cudaMalloc(&m.colloc, (size_t)n * sizeof(double4)));
-  BEM_CUDA(ctx, cudaMalloc(&m.corner, (size_t)n * 12 * sizeof(double)));
-  BEM_CUDA(ctx, cudaMalloc(&m.degen, (size_t)n * sizeof(int)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &m.gq, (size_t)n * m.ng * sizeof(double4)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &m.eta, (size_t)n * sizeof(double4)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &m.colloc, (size_t)n * sizeof(double4)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &m.corner, (size_t)n * 12 * sizeof(double)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &m.degen, (size_t)n * sizeof(int)));
   // Staging copies of the raw mesh arrays (freed after the precompute).
   const size_t nd = (size_t)3 * np + 6 * (size_t)n;
   double* d_raw = nullptr;
   int* d_cone = nullptr;
-  BEM_CUDA(ctx, cudaMalloc(&d_raw, nd * sizeof(double)));
-  BEM_CUDA(ctx, cudaMalloc(&d_cone, (size_t)4 * n * sizeof(int)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &d_raw, nd * sizeof(double)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &d_cone, (size_t)4 * n * sizeof(int)));
   double *dcx = d_raw, *dcy = dcx + np, *dcz = dcy + np, *detas = dcz + np, *dcxm = detas + 3 * (size_t)n,
          *dcym = dcxm + n, *dczm = dcym + n;
   cudaStream_t st = ctx->stream;
@@ -253,28 +275,28 @@ int bem_mesh_upload(bem_ctx* ctx, int n, int nbe, int np, int npg, const int* co
   BEM_CUDA(ctx, cudaMemcpyAsync(d_cone, cone, 4 * (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st));
   int rc = launch_geometry(ctx, dcx, dcy, dcz, d_cone, detas, dcxm, dcym, dczm);
   BEM_CUDA(ctx, cudaStreamSynchronize(st));
-  cudaFree(d_raw);
-  cudaFree(d_cone);
+  dev_free(ctx, d_raw);
+  dev_free(ctx, d_cone);
   if (rc) return rc;
   int flags[2];
   BEM_CUDA(ctx, cudaMemcpy(flags, ctx->d_status + ST_COUNT, sizeof flags, cudaMemcpyDeviceToHost));
   ctx->have_mesh = true;
   ctx->have_hest = ctx->have_gest = ctx->have_dyn = false;
   // Per-mesh buffers sized by nbe are reallocated on the next use.
-  cudaFree(ctx->zdfi);
-  cudaFree(ctx->kode);
+  dev_free(ctx, ctx->zdfi);
+  dev_free(ctx, ctx->kode);
   ctx->zdfi = nullptr;
   ctx->kode = nullptr;
-  cudaFree(ctx->static_part);
+  dev_free(ctx, ctx->static_part);
   ctx->static_part = nullptr;
   ctx->static_chunks = 0;
   release_sweep(ctx);
   ctx->sys.assembled = ctx->sys.solved = false;
-  cudaFree(ctx->hestdiag);
-  cudaFree(ctx->gestdiag);
+  dev_free(ctx, ctx->hestdiag);
+  dev_free(ctx, ctx->gestdiag);
   ctx->hestdiag = ctx->gestdiag = nullptr;
-  BEM_CUDA(ctx, cudaMalloc(&ctx->hestdiag, (size_t)nbe * 9 * sizeof(double)));
-  BEM_CUDA(ctx, cudaMalloc(&ctx->gestdiag, (size_t)nbe * 9 * sizeof(double)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &ctx->hestdiag, (size_t)nbe * 9 * sizeof(double)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &ctx->gestdiag, (size_t)nbe * 9 * sizeof(double)));
   // Remember the degenerate flags: [0] any element, [1] boundary elements.
   ctx->mesh_flag_all = flags[0];
   ctx->mesh_flag_bnd = flags[1];
@@ -326,7 +348,7 @@ int bem_static_h(bem_ctx* ctx, const double c[4], double* hest_out) {
   cudaSetDevice(ctx->device);
   const size_t count = (size_t)3 * ctx->mesh.nbe * 3 * ctx->mesh.n;
   double* d = nullptr;
-  BEM_CUDA(ctx, cudaMalloc(&d, count * sizeof(double)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &d, count * sizeof(double)));
   BEM_CUDA(ctx, cudaMemsetAsync(d, 0, count * sizeof(double), ctx->stream));
   int rc = launch_static(ctx, c, 0, d);
   if (!rc) {
@@ -334,7 +356,7 @@ int bem_static_h(bem_ctx* ctx, const double c[4], double* hest_out) {
     if (e != cudaSuccess) rc = cuda_fail(ctx, e, "copy static H");
   }
   if (!rc) rc = check_status(ctx);
-  cudaFree(d);
+  dev_free(ctx, d);
   if (!rc) ctx->have_hest = true;
   return rc;
 }
@@ -346,8 +368,8 @@ int bem_dyn_upload(bem_ctx* ctx, const double* zdfi, const int* kode) {
   cudaSetDevice(ctx->device);
   const int nn = 3 * ctx->mesh.nbe;
   if (!ctx->zdfi) {
-    BEM_CUDA(ctx, cudaMalloc(&ctx->zdfi, (size_t)nn * sizeof(double2)));
-    BEM_CUDA(ctx, cudaMalloc(&ctx->kode, (size_t)nn * sizeof(int)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &ctx->zdfi, (size_t)nn * sizeof(double2)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &ctx->kode, (size_t)nn * sizeof(int)));
   }
   BEM_CUDA(ctx, cudaMemcpyAsync(ctx->zdfi, zdfi, (size_t)nn * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
   BEM_CUDA(ctx, cudaMemcpyAsync(ctx->kode, kode, (size_t)nn * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
@@ -459,9 +481,9 @@ int bem_static_solve(bem_ctx* ctx, const double c[4], double ge, const int* kode
   double* Gs = nullptr;
   double* d_dfi = nullptr;
   int* d_kode = nullptr;
-  BEM_CUDA(ctx, cudaMalloc(&Gs, (size_t)nn * nn * sizeof(double)));
-  BEM_CUDA(ctx, cudaMalloc(&d_dfi, (size_t)nn * sizeof(double)));
-  BEM_CUDA(ctx, cudaMalloc(&d_kode, (size_t)nn * sizeof(int)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &Gs, (size_t)nn * nn * sizeof(double)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &d_dfi, (size_t)nn * sizeof(double)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &d_kode, (size_t)nn * sizeof(int)));
   BEM_CUDA(ctx, cudaMemcpyAsync(d_dfi, dfi, (size_t)nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   BEM_CUDA(ctx, cudaMemcpyAsync(d_kode, kode, (size_t)nn * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   BEM_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->stream));
@@ -478,9 +500,9 @@ int bem_static_solve(bem_ctx* ctx, const double c[4], double ge, const int* kode
     rc = check_status(ctx);
   }
   cudaStreamSynchronize(ctx->stream);
-  cudaFree(Gs);
-  cudaFree(d_dfi);
-  cudaFree(d_kode);
+  dev_free(ctx, Gs);
+  dev_free(ctx, d_dfi);
+  dev_free(ctx, d_kode);
   if (rc) return rc;
   // Interec.for:59-67 with the real GE.
   for (int i = 0; i < nn; ++i) {

@@ -129,10 +129,28 @@ struct TcArgs {
   int cend;         // columns >= cend are left unchanged
   int urow_off;     // packed U row of column c0
   int mtiles, ntiles, batch;
+  int band;         // m-tiles per band of the tile order (see tile_of)
   int lrows;        // Lhat rows per problem (2*nn)
   int urows;        // U rows per problem (nn+1)
   int* status;
 };
+
+// Tile t of a launch -> (problem b, m-tile tm, n-tile tn).  Tiles run in
+// bands of a.band m-tiles: every n-tile of one band before the next band, m
+// fastest inside a band.  The band's rows of Lhat (a few MB) stay in L2 while
+// all of U streams past them once per band; with m fastest over the whole
+// height instead, a tall system's Lhat (74 MB at n = 36000) would be read
+// from HBM again for every n-tile.
+__device__ __forceinline__ void tile_of(int t, const TcArgs& a, int& b, int& tm, int& tn) {
+  const int per = a.mtiles * a.ntiles;
+  b = t / per;
+  const int rem = t % per;
+  const int bi = rem / (a.band * a.ntiles);
+  const int r2 = rem - bi * a.band * a.ntiles;
+  const int bm = min(a.band, a.mtiles - bi * a.band);
+  tn = r2 / bm;
+  tm = bi * a.band + r2 % bm;
+}
 
 // Bounded wait; on timeout raise the kernel-wide abort flag and the status word.
 __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* status,
@@ -188,9 +206,9 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
     //      kPrefetch ahead are prefetched into L2 for the reduce-adds ----
     auto prefetch_c = [&](int t) {
       if (t >= total) return;
-      const int b = t / (a.mtiles * a.ntiles);
-      const int rem = t % (a.mtiles * a.ntiles);
-      const int x = 2 * (a.r0 + (rem % a.mtiles) * kTcRows), y = a.c0 + (rem / a.mtiles) * kTcCols;
+      int b, tm, tn;
+      tile_of(t, a, b, tm, tn);
+      const int x = 2 * (a.r0 + tm * kTcRows), y = a.c0 + tn * kTcCols;
       tma_prefetch_3d(&tm_c, x, y, b);
       tma_prefetch_3d(&tm_c, x, y + 64, b);
     };
@@ -200,9 +218,8 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
     bool ok = true;
     for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
       prefetch_c(t + kPrefetch * gridDim.x);
-      const int b = t / (a.mtiles * a.ntiles);
-      const int rem = t % (a.mtiles * a.ntiles);
-      const int tm = rem % a.mtiles, tn = rem / a.mtiles;
+      int b, tm, tn;
+      tile_of(t, a, b, tm, tn);
       const int ly = b * a.lrows + 2 * tm * kTcRows;
       const int uy = b * a.urows + a.urow_off + tn * kTcCols;
       for (int h = 0; h < nchunks; ++h) {
@@ -270,9 +287,8 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
       if (!__all_sync(0xffffffffu, wait_or_abort(&t_full[buf], (uint32_t)(it >> 1) & 1u, abort_flag, a.status, wlim)))
         break;
       tc_fence_after();
-      const int b = t / (a.mtiles * a.ntiles);
-      const int rem = t % (a.mtiles * a.ntiles);
-      const int tm = rem % a.mtiles, tn = rem / a.mtiles;
+      int b, tm, tn;
+      tile_of(t, a, b, tm, tn);
       const uint32_t tbase = tmem + (uint32_t)buf * 256u + ((uint32_t)(32 * e) << 16);
       for (int hc = 0; hc < 2; ++hc) {
         float* ct = stage_c + (size_t)hc * (kHalfBytes / 4);
@@ -427,9 +443,8 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc2(const __grid_constant__ CUt
     uint32_t ph = 0;
     bool ok = true;
     for (int t = pair; t < total && ok; t += npairs) {
-      const int b = t / (a.mtiles * a.ntiles);
-      const int rem = t % (a.mtiles * a.ntiles);
-      const int tm = rem % a.mtiles, tn = rem / a.mtiles;
+      int b, tm, tn;
+      tile_of(t, a, b, tm, tn);
       const int ly = b * a.lrows + 2 * (tm * tile_rows + (int)rank * kTcRows);
       const int uy = b * a.urows + a.urow_off + tn * kTcCols + (int)rank * (kTcCols / 2);
       for (int h = 0; h < nchunks; ++h) {
@@ -500,9 +515,8 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc2(const __grid_constant__ CUt
       if (!__all_sync(0xffffffffu, wait_or_abort(&t_full[buf], (uint32_t)(it >> 1) & 1u, abort_flag, a.status, wlim)))
         break;
       tc_fence_after();
-      const int b = t / (a.mtiles * a.ntiles);
-      const int rem = t % (a.mtiles * a.ntiles);
-      const int tm = rem % a.mtiles, tn = rem / a.mtiles;
+      int b, tm, tn;
+      tile_of(t, a, b, tm, tn);
       const int row0 = a.r0 + tm * tile_rows + (int)rank * kTcRows;  // this CTA's first complex row
       const uint32_t tbase = tmem + (uint32_t)buf * 256u + ((uint32_t)(32 * e) << 16);
       for (int hc = 0; hc < 2; ++hc) {
@@ -691,9 +705,9 @@ int tc_ensure(bem_ctx* ctx, int nn, int batch) {
   const size_t lrows = (size_t)2 * nn * batch, urows = (size_t)(nn + 1) * batch;
   if (W.lhat && lrows <= W.lrows_cap && urows <= W.urows_cap) return BEM_OK;
   tc_release(ctx);
-  BEM_CUDA(ctx, cudaMalloc(&W.lhat, lrows * kKPitch * sizeof(float)));
-  BEM_CUDA(ctx, cudaMalloc(&W.ure, urows * kKPitch * sizeof(float)));
-  BEM_CUDA(ctx, cudaMalloc(&W.uim, urows * kKPitch * sizeof(float)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &W.lhat, lrows * kKPitch * sizeof(float)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &W.ure, urows * kKPitch * sizeof(float)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &W.uim, urows * kKPitch * sizeof(float)));
   BEM_CUDA(ctx, cudaMemset(W.lhat, 0, lrows * kKPitch * sizeof(float)));
   BEM_CUDA(ctx, cudaMemset(W.ure, 0, urows * kKPitch * sizeof(float)));
   BEM_CUDA(ctx, cudaMemset(W.uim, 0, urows * kKPitch * sizeof(float)));
@@ -713,9 +727,9 @@ int tc_ensure(bem_ctx* ctx, int nn, int batch) {
 
 void tc_release(bem_ctx* ctx) {
   TcWork& W = ctx->tc;
-  cudaFree(W.lhat);
-  cudaFree(W.ure);
-  cudaFree(W.uim);
+  dev_free(ctx, W.lhat);
+  dev_free(ctx, W.ure);
+  dev_free(ctx, W.uim);
   delete[] static_cast<CUtensorMap*>(W.maps);
   W = TcWork{};
 }
@@ -764,6 +778,7 @@ int tc_gemm(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int r0,
   t.cend = cend;
   t.urow_off = urow_off;
   t.mtiles = (nn - r0 + kTcRows - 1) / kTcRows;
+  t.band = 48;  // 48 x 64 complex rows: 6 MB of Lhat at K = 256
   t.ntiles = (cend - c0 + kTcCols - 1) / kTcCols;
   t.batch = batch;
   t.lrows = 2 * nn;
@@ -773,6 +788,7 @@ int tc_gemm(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int r0,
   if (ctx->tc_pair) {
     // CTA pairs: 128-complex-row tiles, as many pairs as can be resident at once
     t.mtiles = (nn - r0 + 2 * kTcRows - 1) / (2 * kTcRows);
+    t.band = 24;  // 24 x 128 complex rows: 6 MB of Lhat at K = 256
     const int total = t.mtiles * t.ntiles * batch;
     if (W.pair_clusters == 0) {
       cudaLaunchConfig_t q = {};

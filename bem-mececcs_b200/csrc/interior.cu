@@ -198,10 +198,10 @@ __global__ void k_interior_reduce(const double2* __restrict__ part, int l, int c
 }  // namespace
 
 void release_interior(bem_ctx* ctx) {
-  cudaFree(ctx->int_pts);
-  cudaFree(ctx->int_ut);
-  cudaFree(ctx->int_part);
-  cudaFree(ctx->int_out);
+  dev_free(ctx, ctx->int_pts);
+  dev_free(ctx, ctx->int_ut);
+  dev_free(ctx, ctx->int_part);
+  dev_free(ctx, ctx->int_out);
   ctx->int_pts = nullptr;
   ctx->int_ut = nullptr;
   ctx->int_part = nullptr;
@@ -218,10 +218,10 @@ int interior_points(bem_ctx* ctx, const double zge[2], const double zcs[2], cons
   const int chunks = (nbe + kIntThreads - 1) / kIntThreads;
   if ((size_t)l > ctx->int_cap_l || (size_t)nn > ctx->int_cap_nn) {
     release_interior(ctx);
-    BEM_CUDA(ctx, cudaMalloc(&ctx->int_pts, (size_t)l * sizeof(double4)));
-    BEM_CUDA(ctx, cudaMalloc(&ctx->int_ut, (size_t)2 * nn * sizeof(double2)));
-    BEM_CUDA(ctx, cudaMalloc(&ctx->int_part, (size_t)l * chunks * kIntOut * sizeof(double2)));
-    BEM_CUDA(ctx, cudaMalloc(&ctx->int_out, (size_t)l * kIntOut * sizeof(double2)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &ctx->int_pts, (size_t)l * sizeof(double4)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &ctx->int_ut, (size_t)2 * nn * sizeof(double2)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &ctx->int_part, (size_t)l * chunks * kIntOut * sizeof(double2)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &ctx->int_out, (size_t)l * kIntOut * sizeof(double2)));
     ctx->int_cap_l = (size_t)l;
     ctx->int_cap_nn = (size_t)nn;
   }

@@ -3148,24 +3148,24 @@ __global__ void __launch_bounds__(256) k_trsv_f32(const __grid_constant__ CUtens
 int lu_ensure_workspace(bem_ctx* ctx, int nn, int batch) {
   LuWork& L = ctx->lu;
   if (L.cap_nn >= nn && L.cap_batch >= batch && L.ipiv) return BEM_OK;
-  cudaFree(L.ipiv);
-  cudaFree(L.perm);
+  dev_free(ctx, L.ipiv);
+  dev_free(ctx, L.perm);
   L.ipiv = nullptr;
   L.perm = nullptr;
-  BEM_CUDA(ctx, cudaMalloc(&L.ipiv, (size_t)nn * batch * sizeof(int)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &L.ipiv, (size_t)nn * batch * sizeof(int)));
   const int max_panels = (nn + 15) / 16 + 1;
-  BEM_CUDA(ctx, cudaMalloc(&L.perm, (size_t)max_panels * kPermStride * batch * sizeof(int)));
-  cudaFree(L.pstart);
+  BEM_CUDA(ctx, dev_alloc(ctx, &L.perm, (size_t)max_panels * kPermStride * batch * sizeof(int)));
+  dev_free(ctx, L.pstart);
   L.pstart = nullptr;
-  BEM_CUDA(ctx, cudaMalloc(&L.pstart, (size_t)(max_panels + 1) * sizeof(int)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &L.pstart, (size_t)(max_panels + 1) * sizeof(int)));
   L.cap_nn = nn;
   L.cap_batch = batch;
   if (!L.slot_val) {
-    BEM_CUDA(ctx, cudaMalloc(&L.slot_val, 2 * kMaxGrid * sizeof(double)));
-    BEM_CUDA(ctx, cudaMalloc(&L.slot_row, 2 * kMaxGrid * sizeof(int)));
-    BEM_CUDA(ctx, cudaMalloc(&L.cand, (size_t)2 * kMaxGrid * 64 * sizeof(double2)));
-    BEM_CUDA(ctx, cudaMalloc(&L.drow, 2 * 64 * sizeof(double2)));
-    BEM_CUDA(ctx, cudaMalloc(&L.barrier, sizeof(unsigned)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &L.slot_val, 2 * kMaxGrid * sizeof(double)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &L.slot_row, 2 * kMaxGrid * sizeof(int)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &L.cand, (size_t)2 * kMaxGrid * 64 * sizeof(double2)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &L.drow, 2 * 64 * sizeof(double2)));
+    BEM_CUDA(ctx, dev_alloc(ctx, &L.barrier, sizeof(unsigned)));
   }
   return BEM_OK;
 }
@@ -3418,10 +3418,10 @@ static int trsv_f32(bem_ctx* ctx, const void* A, size_t lda, size_t bstride, int
   if (!L.tinv_valid) {
     const size_t bytes = (size_t)batch * (npan + nblk) * kTrsvBlk * kTrsvBlk * sizeof(float2);
     if (L.tinv_bytes < bytes) {
-      cudaFree(L.tinv);
+      dev_free(ctx, L.tinv);
       L.tinv = nullptr;
       L.tinv_bytes = 0;
-      BEM_CUDA(ctx, cudaMalloc(&L.tinv, bytes));
+      BEM_CUDA(ctx, dev_alloc(ctx, &L.tinv, bytes));
       L.tinv_bytes = bytes;
     }
     ProfScope ps(ctx, 4, 8.0 * (double)(npan + nblk) * kTrsvBlk * kTrsvBlk * kTrsvBlk / 3.0 * batch,
@@ -3469,13 +3469,13 @@ static int trsv_coop(bem_ctx* ctx, const void* A, size_t lda, size_t bstride, in
   LuWork& L = ctx->lu;
   const size_t wbytes = (size_t)2 * nn * batch * sizeof(E);
   if (L.trsv_w_bytes < wbytes) {
-    cudaFree(L.trsv_w);
+    dev_free(ctx, L.trsv_w);
     L.trsv_w = nullptr;
     L.trsv_w_bytes = 0;
-    BEM_CUDA(ctx, cudaMalloc(&L.trsv_w, wbytes));
+    BEM_CUDA(ctx, dev_alloc(ctx, &L.trsv_w, wbytes));
     L.trsv_w_bytes = wbytes;
   }
-  if (!L.trsv_ctr) BEM_CUDA(ctx, cudaMalloc(&L.trsv_ctr, kMaxBatch * sizeof(unsigned)));
+  if (!L.trsv_ctr) BEM_CUDA(ctx, dev_alloc(ctx, &L.trsv_ctr, kMaxBatch * sizeof(unsigned)));
   if (batch < 1 || batch > kMaxBatch) return fail(ctx, BEM_ERR_ARG, "batch size out of range");
   if constexpr (sizeof(R) == 4) {
     if (ctx->trsv_inv) {
@@ -3616,18 +3616,18 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     LuWork& LW = ctx->lu;
     const size_t lbytes = (size_t)batch * 64 * 64 * sizeof(float2);
     if (LW.linv_bytes < lbytes) {
-      cudaFree(LW.linv);
+      dev_free(ctx, LW.linv);
       LW.linv = nullptr;
       LW.linv_bytes = 0;
-      BEM_CUDA(ctx, cudaMalloc(&LW.linv, lbytes));
+      BEM_CUDA(ctx, dev_alloc(ctx, &LW.linv, lbytes));
       LW.linv_bytes = lbytes;
     }
     const size_t mbytes = (size_t)batch * kGroupMaps * nn * sizeof(int);
     if (LW.gmap_bytes < mbytes) {
-      cudaFree(LW.gmap);
+      dev_free(ctx, LW.gmap);
       LW.gmap = nullptr;
       LW.gmap_bytes = 0;
-      BEM_CUDA(ctx, cudaMalloc(&LW.gmap, mbytes));
+      BEM_CUDA(ctx, dev_alloc(ctx, &LW.gmap, mbytes));
       LW.gmap_bytes = mbytes;
     }
     BEM_CUDA(ctx, cudaFuncSetAttribute(k_l11_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * kLtTile)));
@@ -3973,7 +3973,7 @@ int measure_fp64_peak(bem_ctx* ctx, double* tflops) {
   const int blocks = ctx->num_sms * 4, threads = 256, iters = 8192;
   double* out = nullptr;
   cudaEvent_t e0, e1;
-  BEM_CUDA(ctx, cudaMalloc(&out, (size_t)blocks * threads * sizeof(double)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &out, (size_t)blocks * threads * sizeof(double)));
   BEM_CUDA(ctx, cudaEventCreate(&e0));
   BEM_CUDA(ctx, cudaEventCreate(&e1));
   k_dmma_peak<<<blocks, threads, 0, ctx->stream>>>(out, iters / 8);  // warm-up
@@ -3988,7 +3988,7 @@ int measure_fp64_peak(bem_ctx* ctx, double* tflops) {
   *tflops = flops / (ms * 1e-3) / 1e12;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  cudaFree(out);
+  dev_free(ctx, out);
   return BEM_OK;
 }
 
@@ -4014,7 +4014,7 @@ static int measure_fma_t(bem_ctx* ctx, int iters, double* tflops) {
   const int blocks = ctx->num_sms * 8, threads = 256;
   T* out = nullptr;
   cudaEvent_t e0, e1;
-  BEM_CUDA(ctx, cudaMalloc(&out, (size_t)blocks * threads * sizeof(T)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &out, (size_t)blocks * threads * sizeof(T)));
   BEM_CUDA(ctx, cudaEventCreate(&e0));
   BEM_CUDA(ctx, cudaEventCreate(&e1));
   k_fma_peak<T><<<blocks, threads, 0, ctx->stream>>>(out, iters / 8);  // warm-up
@@ -4028,7 +4028,7 @@ static int measure_fma_t(bem_ctx* ctx, int iters, double* tflops) {
   *tflops = 2.0 * 8.0 * (double)blocks * threads * iters / (ms * 1e-3) / 1e12;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  cudaFree(out);
+  dev_free(ctx, out);
   return BEM_OK;
 }
 

@@ -144,17 +144,17 @@ __global__ void k_pad_rest(T* A, size_t lda, int n, int npad) {
   if (col >= n || r >= n) A[(size_t)col * lda + r] = v;
 }
 
-void free_sweep(SweepBuf& S) {
-  cudaFree(S.A64);
-  cudaFree(S.A32);
-  cudaFree(S.x64);
-  cudaFree(S.v32);
-  cudaFree(S.part);
-  cudaFree(S.diag_h);
-  cudaFree(S.diag_g);
-  cudaFree(S.rhs_part);
-  cudaFree(S.norm);
-  cudaFree(S.G64);
+void free_sweep(bem_ctx* ctx, SweepBuf& S) {
+  dev_free(ctx, S.A64);
+  dev_free(ctx, S.A32);
+  dev_free(ctx, S.x64);
+  dev_free(ctx, S.v32);
+  dev_free(ctx, S.part);
+  dev_free(ctx, S.diag_h);
+  dev_free(ctx, S.diag_g);
+  dev_free(ctx, S.rhs_part);
+  dev_free(ctx, S.norm);
+  dev_free(ctx, S.G64);
   S = SweepBuf{};
 }
 
@@ -165,23 +165,26 @@ int ensure_sweep(bem_ctx* ctx, int batch, bool mixed, bool keep_g = false) {
   const int chunks = rhs_chunks(ctx);
   if (S.nn == nn && S.batch >= batch && (!mixed || S.A32) && (!keep_g || S.G64) && S.rhs_chunks >= chunks)
     return BEM_OK;
-  free_sweep(S);
+  // A captured step names these buffers: let it finish and drop it before they go.
+  BEM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  release_sweep_graph(ctx);
+  free_sweep(ctx, S);
   S.nn = nn;
   S.batch = batch;
   S.lda = (size_t)((nn + 1) & ~1);  // even: 16-byte aligned column strides for the FP32 TMA maps
   S.a_stride = S.lda * (size_t)(nn + 1);
   S.rhs_chunks = chunks;
   S.resid_chunks = (nn + kResidCols - 1) / kResidCols;
-  BEM_CUDA(ctx, cudaMalloc(&S.A64, S.a_stride * batch * sizeof(double2)));
-  if (mixed) BEM_CUDA(ctx, cudaMalloc(&S.A32, S.a_stride * batch * sizeof(float2)));
-  BEM_CUDA(ctx, cudaMalloc(&S.x64, (size_t)nn * batch * sizeof(double2)));
-  BEM_CUDA(ctx, cudaMalloc(&S.v32, (size_t)nn * batch * sizeof(float2)));
-  BEM_CUDA(ctx, cudaMalloc(&S.part, (size_t)S.resid_chunks * nn * batch * sizeof(double2)));
-  BEM_CUDA(ctx, cudaMalloc(&S.diag_h, (size_t)nbe * 9 * batch * sizeof(double2)));
-  BEM_CUDA(ctx, cudaMalloc(&S.diag_g, (size_t)nbe * 9 * batch * sizeof(double2)));
-  BEM_CUDA(ctx, cudaMalloc(&S.rhs_part, (size_t)chunks * nn * batch * sizeof(double2)));
-  BEM_CUDA(ctx, cudaMalloc(&S.norm, (size_t)2 * batch * (kMaxRefine + 1) * sizeof(unsigned long long)));
-  if (keep_g) BEM_CUDA(ctx, cudaMalloc(&S.G64, S.a_stride * batch * sizeof(double2)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &S.A64, S.a_stride * batch * sizeof(double2)));
+  if (mixed) BEM_CUDA(ctx, dev_alloc(ctx, &S.A32, S.a_stride * batch * sizeof(float2)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &S.x64, (size_t)nn * batch * sizeof(double2)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &S.v32, (size_t)nn * batch * sizeof(float2)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &S.part, (size_t)S.resid_chunks * nn * batch * sizeof(double2)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &S.diag_h, (size_t)nbe * 9 * batch * sizeof(double2)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &S.diag_g, (size_t)nbe * 9 * batch * sizeof(double2)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &S.rhs_part, (size_t)chunks * nn * batch * sizeof(double2)));
+  BEM_CUDA(ctx, dev_alloc(ctx, &S.norm, (size_t)2 * batch * (kMaxRefine + 1) * sizeof(unsigned long long)));
+  if (keep_g) BEM_CUDA(ctx, dev_alloc(ctx, &S.G64, S.a_stride * batch * sizeof(double2)));
   return BEM_OK;
 }
 
@@ -227,8 +230,8 @@ void release_sweep_graph(bem_ctx* ctx) {
 void release_sweep(bem_ctx* ctx) {
   drop_sweep_graph(ctx);
   ctx->sw_nn = 0;
-  free_sweep(ctx->sweep);
-  free_sweep(ctx->bbuf);
+  free_sweep(ctx, ctx->sweep);
+  free_sweep(ctx, ctx->bbuf);
 }
 
 int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], const double c[4],
@@ -285,7 +288,8 @@ int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double z
                       ctx->sw_iters == iters;  // a step of this shape already ran directly
     const bool graph = ctx->use_graphs && !ctx->prof.on && warm && bsz == batch;
     const bool have = ctx->sweep_exec && ctx->sg_nn == nn && ctx->sg_bsz == bsz &&
-                      ctx->sg_mixed == (int)mixed && ctx->sg_iters == iters;
+                      ctx->sg_mixed == (int)mixed && ctx->sg_iters == iters &&
+                      ctx->sg_epoch == ctx->alloc_epoch;  // none of its buffers moved since
     if (graph && have) {
       rc = dyn_graph_update(ctx, ctx->sweep_exec, ctx->sweep_dyn_nodes, db);
       if (rc) return rc;
@@ -310,6 +314,7 @@ int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double z
         ctx->sg_bsz = bsz;
         ctx->sg_mixed = (int)mixed;
         ctx->sg_iters = iters;
+        ctx->sg_epoch = ctx->alloc_epoch;
         ctx->sg_launches = ctx->launches - l0;
         BEM_CUDA(ctx, cudaGraphLaunch(ex, ctx->stream));
       } else {
@@ -394,16 +399,16 @@ int ensure_batchbuf(bem_ctx* d, const BatchNeed& q, bool mixed) {
                     q.resid_elems <= (size_t)S.resid_chunks && q.rhs_elems <= (size_t)S.rhs_chunks &&
                     q.max_nbe <= S.batch && (size_t)q.norm_batch <= S.norm_cap;
   if (fits) return BEM_OK;
-  free_sweep(S);
-  BEM_CUDA(d, cudaMalloc(&S.A64, q.a_elems * sizeof(double2)));
-  if (mixed) BEM_CUDA(d, cudaMalloc(&S.A32, q.a_elems * sizeof(float2)));
-  BEM_CUDA(d, cudaMalloc(&S.x64, q.vec_elems * sizeof(double2)));
-  BEM_CUDA(d, cudaMalloc(&S.v32, q.vec_elems * sizeof(float2)));
-  BEM_CUDA(d, cudaMalloc(&S.part, q.resid_elems * sizeof(double2)));
-  BEM_CUDA(d, cudaMalloc(&S.diag_h, (size_t)q.max_nbe * 9 * sizeof(double2)));
-  BEM_CUDA(d, cudaMalloc(&S.diag_g, (size_t)q.max_nbe * 9 * sizeof(double2)));
-  BEM_CUDA(d, cudaMalloc(&S.rhs_part, q.rhs_elems * sizeof(double2)));
-  BEM_CUDA(d, cudaMalloc(&S.norm, (size_t)2 * q.norm_batch * (kMaxRefine + 1) * sizeof(unsigned long long)));
+  free_sweep(d, S);
+  BEM_CUDA(d, dev_alloc(d, &S.A64, q.a_elems * sizeof(double2)));
+  if (mixed) BEM_CUDA(d, dev_alloc(d, &S.A32, q.a_elems * sizeof(float2)));
+  BEM_CUDA(d, dev_alloc(d, &S.x64, q.vec_elems * sizeof(double2)));
+  BEM_CUDA(d, dev_alloc(d, &S.v32, q.vec_elems * sizeof(float2)));
+  BEM_CUDA(d, dev_alloc(d, &S.part, q.resid_elems * sizeof(double2)));
+  BEM_CUDA(d, dev_alloc(d, &S.diag_h, (size_t)q.max_nbe * 9 * sizeof(double2)));
+  BEM_CUDA(d, dev_alloc(d, &S.diag_g, (size_t)q.max_nbe * 9 * sizeof(double2)));
+  BEM_CUDA(d, dev_alloc(d, &S.rhs_part, q.rhs_elems * sizeof(double2)));
+  BEM_CUDA(d, dev_alloc(d, &S.norm, (size_t)2 * q.norm_batch * (kMaxRefine + 1) * sizeof(unsigned long long)));
   // capacities, in elements (this buffer set is only read through views)
   S.a_stride = q.a_elems;
   S.nn = (int)q.vec_elems;

@@ -35,6 +35,13 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// Solves in flight at once.  Every LU keeps one 16-CTA cluster per panel and
+// the device holds about 9 of those at a time; admitting more than that only
+// queues their kernels behind each other on the GPU (measured: 94 concurrent
+// 6480-unknown solves ran 4x slower in total than 16), so a request that
+// fits the memory budget still waits here until a solve finishes.
+constexpr int kMaxInflight = 8;
+
 double ms_between(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
 }
@@ -71,7 +78,8 @@ struct Slot {
   size_t bytes = 0;
   unsigned long long last_use = 0;
   cudaEvent_t done = nullptr;
-  double* h_x = nullptr;  // pinned, 2 nn doubles
+  double* h_x = nullptr;  // pinned, 2 nn doubles (h_cap bytes)
+  size_t h_cap = 0;
   std::shared_ptr<SrvRequest> req;
 };
 
@@ -113,6 +121,11 @@ class Server {
     worker_.join();
     cudaSetDevice(device_);
     for (Slot& s : slots_) destroy_slot(s);
+    for (auto& b : pinned_free_) cudaFreeHost(b.second);
+    // hand the device memory the slots held back from the stream-ordered pool
+    cudaMemPool_t pool;
+    if (cudaDeviceSynchronize() == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, device_) == cudaSuccess)
+      cudaMemPoolTrimTo(pool, 0);
   }
 
   int add_mesh(SrvMesh&& m) {
@@ -213,7 +226,7 @@ class Server {
             ++busy;
           }
         }
-      for (auto it = queue_.begin(); it != queue_.end();) {
+      for (auto it = queue_.begin(); it != queue_.end() && busy < kMaxInflight;) {
         const int st = try_start(*it);
         if (st == 1) {
           it = queue_.erase(it);
@@ -288,9 +301,27 @@ class Server {
   void destroy_slot(Slot& s) {
     if (s.ctx) bem_ctx_destroy(s.ctx);
     if (s.done) cudaEventDestroy(s.done);
-    if (s.h_x) cudaFreeHost(s.h_x);
+    if (s.h_x) pinned_free_.push_back({s.h_cap, s.h_x});  // kept: cudaFreeHost would stall the device
     used_bytes_ -= std::min(used_bytes_, s.bytes);
     s = Slot{};
+  }
+
+  // A pinned result buffer of at least `bytes`, from the ones earlier slots left.
+  double* take_pinned(size_t bytes, size_t* cap) {
+    size_t best = pinned_free_.size();
+    for (size_t i = 0; i < pinned_free_.size(); ++i)
+      if (pinned_free_[i].first >= bytes && (best == pinned_free_.size() || pinned_free_[i].first < pinned_free_[best].first))
+        best = i;
+    if (best < pinned_free_.size()) {
+      auto b = pinned_free_[best];
+      pinned_free_.erase(pinned_free_.begin() + (long)best);
+      *cap = b.first;
+      return b.second;
+    }
+    double* p = nullptr;
+    if (cudaMallocHost(&p, bytes) != cudaSuccess) return nullptr;
+    *cap = bytes;
+    return p;
   }
 
   // Frees idle slots, least recently used first, until `need` more bytes fit.
@@ -347,7 +378,7 @@ class Server {
                              m.ome.data());
       if (st == BEM_OK && cudaEventCreateWithFlags(&fresh->done, cudaEventDisableTiming) != cudaSuccess)
         st = BEM_ERR_CUDA;
-      if (st == BEM_OK && cudaMallocHost(&fresh->h_x, 2 * (size_t)nn * sizeof(double)) != cudaSuccess)
+      if (st == BEM_OK && !(fresh->h_x = take_pinned(2 * (size_t)nn * sizeof(double), &fresh->h_cap)))
         st = BEM_ERR_NOMEM;
       if (st != BEM_OK) {
         destroy_slot(*fresh);
@@ -420,6 +451,7 @@ class Server {
   bool stop_ = false;
   std::vector<SrvMesh> meshes_;
   std::deque<Slot> slots_;  // stable addresses
+  std::vector<std::pair<size_t, double*>> pinned_free_;  // pinned buffers of destroyed slots
   std::deque<std::shared_ptr<SrvRequest>> queue_;
   std::unordered_map<long long, std::shared_ptr<SrvRequest>> reqs_;
   long long next_id_ = 0;

@@ -17,7 +17,10 @@
  *
  *  2. The native API (bem_*).  An explicit context per mesh, status codes
  *     instead of exit(), device-resident state that can be kept across
- *     frequencies, and an optional caller stream.
+ *     frequencies, and an optional caller stream.  A context's device memory
+ *     comes from the device's stream-ordered pool (cudaMallocAsync on the
+ *     context's stream; the pool keeps freed memory for later contexts), so
+ *     destroying a context does not synchronise the rest of the device.
  *
  * Layouts follow the reference (Fortran column-major):
  *   cone[k*n + i]            CONE(i+1,k+1), 1-based node numbers, n x 4
@@ -345,7 +348,9 @@ int bem_interior(bem_ctx *ctx, const double zge[2], const double zcs[2],
  * problem stays resident (H, its factors and the post-swap G): a later
  * request with the same mesh, material, omega and KODE but a new right-hand
  * side is solved with the cached factors (GEMV + solves).  Idle problems are
- * evicted least-recently-used when a new one needs room.  form:
+ * evicted least-recently-used when a new one needs room.  At most 8 solves
+ * run at once (more would only queue their kernels behind each other on the
+ * GPU); a request that fits the budget waits for one to finish.  form:
  * BEM_FORM_PLAIN or BEM_FORM_MIXED (with `refine` refinement steps). */
 typedef struct bem_server bem_server;
 int bem_server_create(int device, double budget_bytes, int form, int refine,

@@ -111,7 +111,8 @@ def test_noalloc_limit_boundary(npg, nbe_max, grid_ok, grid_over):
     sol.ctx.close()
 
     s = meshgen.planar_grid(*grid_ok, npg=npg)
-    d = meshgen.traction_patch(s)
+    d = meshgen.traction_patch(s, radius=3.0)  # reaches the centroids of every strip (|y| <= 2.5)
+    assert np.abs(d.bc).sum() > 0
     sol = BemSolver(s)
     sol.set_bc(d.kode, d.bc, d.dam, d.rho)
     nn = sol.nn
