@@ -206,6 +206,7 @@ struct bem_ctx {
   bool lu_quads = true;       // ... four (K = 256) where four 64-column panels fit
   bool f64_pairs = true;      // FP64 LU: two panels per trailing update (K = 2 x panel width)
   bool tc_pair = false;       // FP32 trailing update by CTA pairs (k_gemm_tc2, tcgen05 cta_group::2)
+  bool small_clusters = true; // panel clusters sized to the system (<= 256 rows per CTA), not always 16
   // SM shares for contexts that run concurrently on one GPU (0: the whole device)
   int gemm_ctas = 0;          // CTAs of the persistent tensor-core trailing update
   int trsv_ctas = 0;          // CTAs of one cooperative triangular solve (all problems together)

@@ -165,6 +165,7 @@ int bem_ctx_create(int device, bem_ctx** out) {
   if (const char* env = getenv("BEM_PANEL_ASYNC")) ctx->panel_async = env[0] != '0';
   if (const char* env = getenv("BEM_F64_PAIRS")) ctx->f64_pairs = env[0] != '0';
   if (const char* env = getenv("BEM_TC_PAIR")) ctx->tc_pair = env[0] == '1';
+  if (const char* env = getenv("BEM_SMALL_CLUSTERS")) ctx->small_clusters = env[0] != '0';
   *out = ctx;
   return BEM_OK;
 }
@@ -568,6 +569,7 @@ static bool* option_slot(bem_ctx* ctx, const char* name) {
   if (!strcmp(name, "lu_quads")) return &ctx->lu_quads;
   if (!strcmp(name, "f64_pairs")) return &ctx->f64_pairs;
   if (!strcmp(name, "tc_pair")) return &ctx->tc_pair;
+  if (!strcmp(name, "small_clusters")) return &ctx->small_clusters;
   if (!strcmp(name, "panel_calu")) return &ctx->panel_calu;
   if (!strcmp(name, "panel_push")) return &ctx->panel_push;
   if (!strcmp(name, "panel_async")) return &ctx->panel_async;

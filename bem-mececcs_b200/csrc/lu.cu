@@ -3325,6 +3325,20 @@ static int cluster_size(bem_ctx* ctx) {
   return cs;
 }
 
+// CTAs per panel cluster for an nn x nn system: the device's largest (16)
+// halved while every CTA still holds at most 256 panel rows (option
+// "small_clusters", on).  A panel costs about the same time per column
+// whatever the cluster size, so small systems need no more than a few CTAs
+// each, and the lockstep batches and concurrent classes of small problems
+// then fit many more problems on the device at once.  The 6480-unknown
+// sweep keeps 16.
+static int cluster_size_for(bem_ctx* ctx, int nn) {
+  int cs = cluster_size(ctx);
+  if (ctx->small_clusters)
+    while (cs > 2 && (nn + cs / 2 - 1) / (cs / 2) <= 256) cs /= 2;
+  return cs;
+}
+
 // Clusters of the panel kernel that can be resident at once (0 if unknown).
 template <typename R, int NB, int NT>
 static int cluster_capacity(int cs, int rp) {
@@ -3352,7 +3366,7 @@ static int cluster_capacity(int cs, int rp) {
 
 template <typename R>
 static int lockstep_capacity_t(bem_ctx* ctx, int nn) {
-  const int cs = cluster_size(ctx);
+  const int cs = cluster_size_for(ctx, nn);
   const int rp = (nn + cs - 1) / cs;
   if (rp > 512) return kMaxBatch;  // grid-panel fallback: problems take turns anyway
   const bool big = rp > 256;
@@ -3371,7 +3385,7 @@ static int lockstep_capacity_t(bem_ctx* ctx, int nn) {
 // kernel, as many clusters as can be resident at once.
 int lu_lockstep_capacity(bem_ctx* ctx, int nn, bool fp32) {
   // occupancy queries are host calls of tens of microseconds: remember each answer
-  const long long key = 2LL * nn + (fp32 ? 1 : 0);
+  const long long key = 4LL * nn + (fp32 ? 1 : 0) + (ctx->small_clusters ? 2 : 0);
   auto it = ctx->lockstep_cache.find(key);
   if (it != ctx->lockstep_cache.end()) return it->second;
   const int cap = fp32 ? lockstep_capacity_t<float>(ctx, nn) : lockstep_capacity_t<double>(ctx, nn);
@@ -3522,7 +3536,7 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
   LuWork& L = ctx->lu;
   const int ncols = nn + 1;
   const size_t es = sizeof(cpx<R>);
-  const int cs = cluster_size(ctx);
+  const int cs = cluster_size_for(ctx, nn);
   const size_t lsmem = 64 * 64 * es;
   const size_t bsmem = 64 * 64 * es;
   BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_trsm<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,

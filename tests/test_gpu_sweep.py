@@ -115,3 +115,19 @@ def test_sweep_mixed_cta_pair_update(c1, batch):
         assert e2 < 10 * max(e1, 1e-7), (batch, fr, e1, e2)
         assert rel(x3[i], ox) < 1e-10, (batch, fr)
         assert corr[i] < 1e-9
+
+
+def test_small_clusters_same_factors(c1):
+    """n = 720: the panel cluster shrinks from 16 CTAs to 4 (180 rows per
+    CTA).  The pivots and arithmetic of a column step do not depend on how
+    the rows are split, so both give the oracle's solution at 1e-10 and agree
+    with each other to rounding."""
+    s, d, p, sol = c1
+    xs = {}
+    for on in (True, False):
+        sol.ctx.set_option("small_clusters", on)
+        xs[on], _ = sol.sweep(FREQS[:3], form="plain", batch=3)
+    sol.ctx.set_option("small_clusters", True)
+    for i, fr in enumerate(FREQS[:3]):
+        assert rel(xs[True][i], _oracle_x(p, fr)) < 1e-10
+        assert rel(xs[True][i], xs[False][i]) < 1e-13
