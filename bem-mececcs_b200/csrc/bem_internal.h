@@ -300,6 +300,11 @@ int slot_solve_full(bem_ctx* ctx, const double zge[2], const double zcs[2], cons
                     double fr, bool mixed, int iters);
 int slot_solve_rhs(bem_ctx* ctx, bool mixed, int iters);
 const double2* slot_solution(bem_ctx* ctx, bool mixed, bool rhs_only);
+// `batch` frequencies with the same boundary conditions in one lockstep step
+// (not cached for right-hand-side reuse); problem b's raw solution.
+int slot_solve_batch(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], const double c[4],
+                     const double* freqs, int batch, bool mixed, int iters);
+const double2* slot_batch_solution(bem_ctx* ctx, bool mixed, int b);
 
 // Tensor-core FP32 trailing update (gemm_tc.cu).
 int tc_ensure(bem_ctx* ctx, int nn, int batch);

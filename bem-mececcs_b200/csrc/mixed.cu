@@ -687,6 +687,52 @@ int slot_solve_rhs(bem_ctx* ctx, bool mixed, int iters) {
   return refine_steps(ctx, S, 1, iters + 1, 0);
 }
 
+// Serving batches: `batch` frequencies of the resident mesh with the same
+// boundary conditions in lockstep (one assembly launch, one lockstep LU and
+// refinement), as one step of bem_sweep; not kept for right-hand-side reuse.
+int slot_solve_batch(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], const double c[4],
+                     const double* freqs, int batch, bool mixed, int iters) {
+  if (iters < 0 || iters > kMaxRefine) return fail(ctx, BEM_ERR_ARG, "refinement steps out of range");
+  if (batch < 1 || batch > kMaxBatch) return fail(ctx, BEM_ERR_ARG, "batch size out of range");
+  int rc = ensure_sweep(ctx, batch, mixed, false);
+  if (rc) return rc;
+  SweepBuf& S = ctx->sweep;
+  const int nn = S.nn;
+  BEM_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->stream));
+  DynBatch db{};
+  db.zge = zge;
+  db.zcs = zcs;
+  db.zcp = zcp;
+  db.c = c;
+  db.freqs = freqs;
+  db.batch = batch;
+  db.flags = BEM_FAST_SINGULAR;
+  db.A = S.A64;
+  db.lda = S.lda;
+  db.a_stride = S.a_stride;
+  db.A32 = mixed ? S.A32 : nullptr;
+  db.diag_h = S.diag_h;
+  db.diag_g = S.diag_g;
+  db.rhs_part = S.rhs_part;
+  rc = launch_dynamic_batch(ctx, db);
+  if (rc) return rc;
+  if (!mixed) return lu_factor_solve_batch(ctx, S.A64, S.lda, S.a_stride, nn, batch, false);
+  rc = lu_factor_solve_batch(ctx, S.A32, S.lda, S.a_stride, nn, batch, true);
+  if (rc) return rc;
+  k_x_init<<<dim3((nn + 255) / 256, batch), 256, 0, ctx->stream>>>(S.A32, S.lda, S.a_stride, nn, S.x64, nn);
+  ctx->launches++;
+  BEM_CUDA(ctx, cudaMemsetAsync(S.norm, 0, (size_t)2 * batch * (kMaxRefine + 1) * sizeof(unsigned long long),
+                                ctx->stream));
+  return refine_steps(ctx, S, batch, iters, 0);
+}
+
+// Raw solution of problem b of the last slot_solve_batch.
+const double2* slot_batch_solution(bem_ctx* ctx, bool mixed, int b) {
+  SweepBuf& S = ctx->sweep;
+  if (mixed) return S.x64 + (size_t)b * S.nn;
+  return S.A64 + (size_t)b * S.a_stride + (size_t)S.nn * S.lda;
+}
+
 const double2* slot_solution(bem_ctx* ctx, bool mixed, bool rhs_only) {
   SweepBuf& S = ctx->sweep;
   if (mixed || rhs_only) return S.x64;

@@ -78,9 +78,10 @@ struct Slot {
   size_t bytes = 0;
   unsigned long long last_use = 0;
   cudaEvent_t done = nullptr;
-  double* h_x = nullptr;  // pinned, 2 nn doubles (h_cap bytes)
+  double* h_x = nullptr;  // pinned, 2 nn doubles per problem (h_cap bytes)
   size_t h_cap = 0;
-  std::shared_ptr<SrvRequest> req;
+  int cap_probs = 1;      // problems the slot's bytes were admitted for
+  std::vector<std::shared_ptr<SrvRequest>> reqs;  // in flight: one, or a lockstep batch
 };
 
 // Inputecd.for:58-60 and Ghmatece.for:55-63 on the host.
@@ -216,22 +217,25 @@ class Server {
     std::unique_lock<std::mutex> lk(mu_);
     while (!stop_) {
       bool progress = false;
-      int busy = 0;
+      int busy = 0;  // problems in flight
       for (Slot& s : slots_)
         if (s.busy) {
           if (cudaEventQuery(s.done) == cudaSuccess) {
             finish(s);
             progress = true;
           } else {
-            ++busy;
+            busy += (int)s.reqs.size();
           }
         }
       for (auto it = queue_.begin(); it != queue_.end() && busy < kMaxInflight;) {
-        const int st = try_start(*it);
-        if (st == 1) {
-          it = queue_.erase(it);
+        const int st = try_start(*it, kMaxInflight - busy);
+        if (st > 0) {  // the request and any batched with it leave the queue
+          queue_.erase(std::remove_if(queue_.begin(), queue_.end(),
+                                      [](const std::shared_ptr<SrvRequest>& q) { return q->started; }),
+                       queue_.end());
+          it = queue_.begin();
           progress = true;
-          ++busy;
+          busy += st;
         } else if (st < 0) {
           it = queue_.erase(it);  // failed at admission: reported through wait()
           progress = true;
@@ -257,8 +261,8 @@ class Server {
   }
 
   void finish(Slot& s) {
-    std::shared_ptr<SrvRequest> r = s.req;
-    s.req.reset();
+    std::vector<std::shared_ptr<SrvRequest>> rs;
+    rs.swap(s.reqs);
     s.busy = false;
     int st;
     {
@@ -266,7 +270,12 @@ class Server {
       st = check_status(s.ctx);
     }
     if (st == BEM_OK && s.ctx->mesh_flag_bnd) st = BEM_ERR_DEGENERATE;
-    s.cached = (st == BEM_OK);
+    s.cached = (st == BEM_OK && rs.size() == 1);  // a batch's problems are not kept for reuse
+    s.last_use = ++tick_;
+    for (size_t b = 0; b < rs.size(); ++b) finish_one(rs[b], st, s.h_x + 2 * rs[b]->kode.size() * b);
+  }
+
+  void finish_one(const std::shared_ptr<SrvRequest>& r, int st, const double* hx) {
     if (st == BEM_OK) {
       // The un-swap of Interec.for:59-67: KODE = 0 entries exchange roles.
       double zge[2], zcs[2], zcp[2];
@@ -275,7 +284,7 @@ class Server {
       r->disp.resize(2 * nn);
       r->trac.resize(2 * nn);
       for (size_t i = 0; i < nn; ++i) {
-        const double xr = s.h_x[2 * i], xi = s.h_x[2 * i + 1];
+        const double xr = hx[2 * i], xi = hx[2 * i + 1];
         if (r->kode[i] == 0) {
           r->disp[2 * i] = r->bc[2 * i];
           r->disp[2 * i + 1] = r->bc[2 * i + 1];
@@ -289,7 +298,6 @@ class Server {
         }
       }
     }
-    s.last_use = ++tick_;
     complete(r, st);
   }
 
@@ -337,8 +345,23 @@ class Server {
     return true;
   }
 
-  // 1 started, 0 not yet (waits for memory or a slot), -1 failed.
-  int try_start(const std::shared_ptr<SrvRequest>& r) {
+  // Queued requests that can run in lockstep with r: same mesh, material,
+  // boundary conditions and KODE, any omega (a frequency sweep).
+  std::vector<std::shared_ptr<SrvRequest>> companions(const std::shared_ptr<SrvRequest>& r, int room) {
+    std::vector<std::shared_ptr<SrvRequest>> out;
+    for (const auto& q : queue_) {
+      if ((int)out.size() + 1 >= room) break;
+      if (q == r || q->started || q->mesh != r->mesh || std::memcmp(q->mat, r->mat, sizeof q->mat) != 0 ||
+          q->kode != r->kode || q->bc != r->bc)
+        continue;
+      out.push_back(q);
+    }
+    return out;
+  }
+
+  // Problems started (the request, and those batched with it), 0 not yet
+  // (waits for memory or a slot), -1 failed.  `room`: problems that may start.
+  int try_start(const std::shared_ptr<SrvRequest>& r, int room) {
     const SrvMesh& m = meshes_[r->mesh];
     const int nn = 3 * m.nbe;
     Slot* slot = nullptr;
@@ -349,18 +372,38 @@ class Server {
         rhs_only = true;
         break;
       }
+    std::vector<std::shared_ptr<SrvRequest>> batch{r};
+    if (!rhs_only) {
+      auto more = companions(r, std::min(room, kMaxBatch));
+      batch.insert(batch.end(), more.begin(), more.end());
+    }
+    const size_t per = slot_footprint(nn, m.nbe, m.npg * m.npg, mixed_) +
+                       (size_t)m.n * (m.npg * m.npg + 3) * sizeof(double4);
     if (!slot) {
       for (Slot& s : slots_)  // an idle slot of the same mesh: reuse its buffers
         if (s.ctx && !s.busy && s.mesh == r->mesh && (!slot || s.last_use < slot->last_use)) slot = &s;
     }
+    if (slot && !rhs_only && (int)batch.size() > slot->cap_probs) {
+      // a batch wider than the slot was admitted for: room for the difference, or one problem
+      if (!make_room(per * (batch.size() - slot->cap_probs))) batch.resize(slot->cap_probs);
+      else {
+        used_bytes_ += per * (batch.size() - slot->cap_probs);
+        peak_bytes_ = std::max(peak_bytes_, used_bytes_);
+        slot->bytes += per * (batch.size() - slot->cap_probs);
+        slot->cap_probs = (int)batch.size();
+      }
+    }
     if (!slot) {
-      const size_t need = slot_footprint(nn, m.nbe, m.npg * m.npg, mixed_) +
-                          (size_t)m.n * (m.npg * m.npg + 3) * sizeof(double4);
-      if (need > budget_) {
+      if (per > budget_) {
         complete(r, BEM_ERR_NOMEM);
         return -1;
       }
-      if (!make_room(need)) return 0;
+      while (batch.size() > 1 && per * batch.size() > budget_) batch.pop_back();
+      if (!make_room(per * batch.size())) {
+        batch.resize(1);
+        if (!make_room(per)) return 0;
+      }
+      const size_t need = per * batch.size();
       Slot* fresh = nullptr;
       for (Slot& s : slots_)
         if (!s.ctx) {
@@ -378,8 +421,6 @@ class Server {
                              m.ome.data());
       if (st == BEM_OK && cudaEventCreateWithFlags(&fresh->done, cudaEventDisableTiming) != cudaSuccess)
         st = BEM_ERR_CUDA;
-      if (st == BEM_OK && !(fresh->h_x = take_pinned(2 * (size_t)nn * sizeof(double), &fresh->h_cap)))
-        st = BEM_ERR_NOMEM;
       if (st != BEM_OK) {
         destroy_slot(*fresh);
         complete(r, st);
@@ -387,6 +428,7 @@ class Server {
       }
       fresh->mesh = r->mesh;
       fresh->bytes = need;
+      fresh->cap_probs = (int)batch.size();
       used_bytes_ += need;
       peak_bytes_ = std::max(peak_bytes_, used_bytes_);
       slot = fresh;
@@ -400,6 +442,14 @@ class Server {
       st = bem_dyn_upload(ctx, r->bc.data(), r->kode.data());
       std::lock_guard<std::mutex> g(ctx->mu);
       cudaSetDevice(device_);
+      if (batch.size() > 1)  // no more problems in lockstep than the panel kernel keeps resident
+        batch.resize(std::min(batch.size(), (size_t)std::max(1, lu_lockstep_capacity(ctx, nn, mixed_))));
+      const size_t hneed = 2 * (size_t)nn * sizeof(double) * batch.size();
+      if (st == BEM_OK && slot->h_cap < hneed) {
+        if (slot->h_x) pinned_free_.push_back({slot->h_cap, slot->h_x});
+        slot->h_x = take_pinned(hneed, &slot->h_cap);
+        if (!slot->h_x) st = BEM_ERR_NOMEM;
+      }
       if (st == BEM_OK && !rhs_only && !(slot->have_static && slot->st_ge == r->mat[0] && slot->st_nu == r->mat[1])) {
         st = cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->stream) == cudaSuccess
                  ? launch_static(ctx, c, 1, nullptr)
@@ -411,16 +461,25 @@ class Server {
           slot->st_nu = r->mat[1];
         }
       }
-      if (st == BEM_OK)
-        st = rhs_only ? slot_solve_rhs(ctx, mixed_, refine_)
-                      : slot_solve_full(ctx, zge, zcs, zcp, c, r->fr, mixed_, refine_);
       if (st == BEM_OK) {
-        const double2* x = slot_solution(ctx, mixed_, rhs_only);
-        if (cudaMemcpyAsync(slot->h_x, x, (size_t)nn * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream) !=
-                cudaSuccess ||
-            cudaEventRecord(slot->done, ctx->stream) != cudaSuccess)
+        if (rhs_only) {
+          st = slot_solve_rhs(ctx, mixed_, refine_);
+        } else if (batch.size() == 1) {
+          st = slot_solve_full(ctx, zge, zcs, zcp, c, r->fr, mixed_, refine_);
+        } else {
+          std::vector<double> fr;
+          for (const auto& q : batch) fr.push_back(q->fr);
+          st = slot_solve_batch(ctx, zge, zcs, zcp, c, fr.data(), (int)batch.size(), mixed_, refine_);
+        }
+      }
+      for (size_t b = 0; b < batch.size() && st == BEM_OK; ++b) {
+        const double2* x = batch.size() == 1 ? slot_solution(ctx, mixed_, rhs_only)
+                                             : slot_batch_solution(ctx, mixed_, (int)b);
+        if (cudaMemcpyAsync(slot->h_x + 2 * (size_t)nn * b, x, (size_t)nn * sizeof(double2), cudaMemcpyDeviceToHost,
+                            ctx->stream) != cudaSuccess)
           st = BEM_ERR_CUDA;
       }
+      if (st == BEM_OK && cudaEventRecord(slot->done, ctx->stream) != cudaSuccess) st = BEM_ERR_CUDA;
     }
     if (st != BEM_OK) {
       slot->cached = false;
@@ -429,16 +488,19 @@ class Server {
     }
     slot->busy = true;
     slot->cached = false;
-    slot->req = r;
+    slot->reqs = batch;
     std::memcpy(slot->mat, r->mat, sizeof slot->mat);
     slot->fr = r->fr;
     slot->kode = r->kode;
     slot->last_use = ++tick_;
-    r->started = true;
-    r->rhs_only = rhs_only;
-    r->bytes = slot->bytes;
-    r->t_start = Clock::now();
-    return 1;
+    const auto now = Clock::now();
+    for (const auto& q : batch) {
+      q->started = true;
+      q->rhs_only = rhs_only;
+      q->bytes = slot->bytes / batch.size();
+      q->t_start = now;
+    }
+    return (int)batch.size();
   }
 
   int device_;

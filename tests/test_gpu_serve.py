@@ -123,3 +123,27 @@ def test_admission_by_footprint():
         srv.wait(srv.submit(big, MAT, 1.0, bcb, kb))
     assert e.value.code == capi.BEM_ERR_NOMEM
     srv.close()
+
+
+@pytest.mark.parametrize("form", ["mixed", "plain"])
+def test_same_mesh_sweep_batched_in_lockstep(form):
+    """Requests for one mesh, material and load at several omegas, submitted
+    at once, run as lockstep batches in one slot (the sweep's form); each
+    result equals the same request solved alone, and the batch's problems
+    are not kept as cached factors."""
+    m = _mesh(14, 12, 4)
+    bc, kode = _bc(m, 0.0, 0.0, 1.5)
+    freqs = [0.4, 0.9, 1.7, 2.6, 3.3, 4.8, 6.1, 7.7, 9.5]
+    srv = serve.Server(form=form, refine=3)
+    mid = srv.add_mesh(m)
+    alone = [srv.wait(srv.submit(mid, MAT, f, bc, kode))[:2] for f in freqs]
+    srv.close()
+    srv = serve.Server(form=form, refine=3)
+    mid = srv.add_mesh(m)
+    ids = [srv.submit(mid, MAT, f, bc, kode) for f in freqs]
+    got = [srv.wait(i)[:2] for i in ids]
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == len(freqs) and st["max_busy"] >= 2  # several problems in flight together
+    for (d0, t0), (d1, t1) in zip(alone, got):
+        assert rel(d1, d0) < TOL and rel(t1, t0) < TOL
