@@ -99,6 +99,16 @@ struct LuWork {
   size_t linv_bytes = 0;
   int* gmap = nullptr;           // [batch][kGroupMaps][nn] row maps of a panel group (k_l11_inv)
   size_t gmap_bytes = 0;
+  // tall FP32 panels by tournament (tslu_panel): chunk copies and their pivots,
+  // the candidates, their row indices and pivots
+  float2* ts_s = nullptr;
+  int* ts_ipiv = nullptr;
+  int* ts_perm = nullptr;
+  float2* ts_c = nullptr;
+  int* ts_gid = nullptr;
+  int* ts_cipiv = nullptr;
+  int* ts_cperm = nullptr;
+  size_t ts_cap[7] = {0, 0, 0, 0, 0, 0, 0};  // elements allocated, in the order above
   float2* tinv = nullptr;        // FP32 solves: inverted diagonal blocks of the last factors
   size_t tinv_bytes = 0;
   bool tinv_valid = false;
@@ -207,6 +217,7 @@ struct bem_ctx {
   bool f64_pairs = true;      // FP64 LU: two panels per trailing update (K = 2 x panel width)
   bool tc_pair = false;       // FP32 trailing update by CTA pairs (k_gemm_tc2, tcgen05 cta_group::2)
   bool small_clusters = true; // panel clusters sized to the system (<= 256 rows per CTA), not always 16
+  bool panel_tslu = true;     // FP32 panels taller than a cluster: tournament pivoting instead of the grid kernel
   // SM shares for contexts that run concurrently on one GPU (0: the whole device)
   int gemm_ctas = 0;          // CTAs of the persistent tensor-core trailing update
   int trsv_ctas = 0;          // CTAs of one cooperative triangular solve (all problems together)
@@ -226,17 +237,16 @@ int cuda_fail(bem_ctx* ctx, cudaError_t e, const char* what);
 // whole device, so a process that creates and drops contexts while others
 // compute (the server evicting a cached problem while other requests run)
 // would stall every stream on each drop; cudaFreeAsync does not.  The
-// allocation waits for the context's own stream only, so the memory is
-// ready for any stream and for synchronous copies as cudaMalloc's would be.
-// Every allocation also advances ctx->alloc_epoch: a captured sweep step
-// names the buffers it was captured with and is replayed only while no
-// buffer of the context has been (re)allocated since.
+// memory is ready in the order of the context's stream, which is where the
+// library uses it (copies included); a context moved to another stream
+// (bem_ctx_set_stream) waits for its old one first.  Every allocation also
+// advances ctx->alloc_epoch: a captured sweep step names the buffers it was
+// captured with and is replayed only while no buffer of the context has been
+// (re)allocated since.
 template <typename T>
 cudaError_t dev_alloc(bem_ctx* ctx, T** p, size_t bytes) {
   ++ctx->alloc_epoch;
-  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(p), bytes, ctx->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-  return e;
+  return cudaMallocAsync(reinterpret_cast<void**>(p), bytes, ctx->stream);
 }
 void dev_free(bem_ctx* ctx, void* p);
 

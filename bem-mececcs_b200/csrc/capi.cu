@@ -166,6 +166,7 @@ int bem_ctx_create(int device, bem_ctx** out) {
   if (const char* env = getenv("BEM_F64_PAIRS")) ctx->f64_pairs = env[0] != '0';
   if (const char* env = getenv("BEM_TC_PAIR")) ctx->tc_pair = env[0] == '1';
   if (const char* env = getenv("BEM_SMALL_CLUSTERS")) ctx->small_clusters = env[0] != '0';
+  if (const char* env = getenv("BEM_PANEL_TSLU")) ctx->panel_tslu = env[0] != '0';
   *out = ctx;
   return BEM_OK;
 }
@@ -199,6 +200,13 @@ int bem_ctx_destroy(bem_ctx* ctx) {
   dev_free(ctx, L.gmap);
   dev_free(ctx, L.trsv_ctr);
   dev_free(ctx, L.pstart);
+  dev_free(ctx, L.ts_s);
+  dev_free(ctx, L.ts_ipiv);
+  dev_free(ctx, L.ts_perm);
+  dev_free(ctx, L.ts_c);
+  dev_free(ctx, L.ts_gid);
+  dev_free(ctx, L.ts_cipiv);
+  dev_free(ctx, L.ts_cperm);
   for (bem_ctx* w : ctx->workers) bem_ctx_destroy(w);
   ctx->workers.clear();
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
@@ -570,6 +578,7 @@ static bool* option_slot(bem_ctx* ctx, const char* name) {
   if (!strcmp(name, "f64_pairs")) return &ctx->f64_pairs;
   if (!strcmp(name, "tc_pair")) return &ctx->tc_pair;
   if (!strcmp(name, "small_clusters")) return &ctx->small_clusters;
+  if (!strcmp(name, "panel_tslu")) return &ctx->panel_tslu;
   if (!strcmp(name, "panel_calu")) return &ctx->panel_calu;
   if (!strcmp(name, "panel_push")) return &ctx->panel_push;
   if (!strcmp(name, "panel_async")) return &ctx->panel_async;

@@ -708,9 +708,9 @@ int tc_ensure(bem_ctx* ctx, int nn, int batch) {
   BEM_CUDA(ctx, dev_alloc(ctx, &W.lhat, lrows * kKPitch * sizeof(float)));
   BEM_CUDA(ctx, dev_alloc(ctx, &W.ure, urows * kKPitch * sizeof(float)));
   BEM_CUDA(ctx, dev_alloc(ctx, &W.uim, urows * kKPitch * sizeof(float)));
-  BEM_CUDA(ctx, cudaMemset(W.lhat, 0, lrows * kKPitch * sizeof(float)));
-  BEM_CUDA(ctx, cudaMemset(W.ure, 0, urows * kKPitch * sizeof(float)));
-  BEM_CUDA(ctx, cudaMemset(W.uim, 0, urows * kKPitch * sizeof(float)));
+  BEM_CUDA(ctx, cudaMemsetAsync(W.lhat, 0, lrows * kKPitch * sizeof(float), ctx->stream));
+  BEM_CUDA(ctx, cudaMemsetAsync(W.ure, 0, urows * kKPitch * sizeof(float), ctx->stream));
+  BEM_CUDA(ctx, cudaMemsetAsync(W.uim, 0, urows * kKPitch * sizeof(float), ctx->stream));
   // maps: 0 Lhat, 1-2 U_re/U_im (128-row boxes), 3 C (made per system), 4-5 U_re/U_im in
   // the 64-row boxes of the CTA-pair kernel
   W.maps = new CUtensorMap[6];

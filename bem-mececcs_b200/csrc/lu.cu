@@ -153,6 +153,7 @@ struct PanelArgs {
   int* pstart;     // panel starts for the later solves: [pidx] = k, [pidx + 1] = k + w
   int pidx;
   int async_mail;  // k_panel_push: mailboxes filled by st.async (mbarrier complete_tx), no per-column cluster barrier
+  int no_singular;  // a tournament round of a tall panel: a zero pivot is not an error here
   // grid fallback only:
   void* slot_val;
   int* slot_row;
@@ -490,7 +491,7 @@ __global__ void __launch_bounds__(NT, 1) k_panel_cluster(PanelArgs a) {
       for (int c = 1; c < SW; ++c)
         if (c == jj) pj = piv[c];
       const bool zero = (pj.re == R(0) && pj.im == R(0));
-      if (zero && rank == 0 && tid == 0) atomicCAS(&a.status[ST_SINGULAR], 0, gj + 1);
+      if (zero && rank == 0 && tid == 0 && !a.no_singular) atomicCAS(&a.status[ST_SINGULAR], 0, gj + 1);
       const C rpv = zero ? C{R(0), R(0)} : crcp(pj);
 #pragma unroll
       for (int q = 0; q < RPT; ++q) {
@@ -974,7 +975,7 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
       // 5. Multipliers and the rank-1 update of the sub-panel, in registers.
       const C pj = piv[jj];
       const bool zero = pj.re == R(0) && pj.im == R(0);
-      if (zero && rank == 0 && tid == 0) atomicCAS(&a.status[ST_SINGULAR], 0, gj + 1);
+      if (zero && rank == 0 && tid == 0 && !a.no_singular) atomicCAS(&a.status[ST_SINGULAR], 0, gj + 1);
       const C rpv = zero ? czero : crcp(pj);
       if (grow != INT_MAX && grow > gj) {
         const C l = v[jj] * rpv;
@@ -1759,6 +1760,187 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel_grid(PanelArgs a) {
       a.perm[1 + 2 * e] = s_pdst[e];
       a.perm[2 + 2 * e] = s_psrc[e];
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tall FP32 panels by tournament pivoting (TSLU; option "panel_tslu").  A
+// panel taller than one cluster holds (more than about 6900 rows of 64
+// complex64 columns) is factored in three rounds instead of by the
+// grid-barrier kernel, which pays a software grid barrier per column and takes
+// the problems one at a time:
+//   1. its rows are split into chunks of at most one cluster's rows; every
+//      chunk (of every problem) is factored with partial pivoting by the
+//      cluster kernel on a copy, in one launch, only to see which 64 rows it
+//      picks;
+//   2. those candidates (64 per chunk, their rows as they are in A) are
+//      factored the same way: its 64 pivots are the panel's pivot rows;
+//   3. the winners are brought to the top of the panel by the same sequence of
+//      row interchanges partial pivoting would record (ipiv, gather list), the
+//      64 x 64 top block is factored without pivoting and L21 = A21 U11^-1.
+// The factors satisfy A = P L U as every other panel's do, so the
+// interchange, update and solve kernels are unchanged; the pivots may differ
+// from per-column partial pivoting, which is why this is used for the FP32
+// factors only (a preconditioner of the FP64 refinement).
+// ---------------------------------------------------------------------------
+constexpr int kTsluW = 64;
+
+// Chunk c of problem b (rows k + c*chunk.. of the panel's 64 columns) into
+// scratch problem b*nch + c, column-major chunk x 64; rows past nn are zero.
+__global__ void __launch_bounds__(256) k_tslu_copy(const float2* __restrict__ Abase, size_t lda, size_t bstride,
+                                                   int nn, int k, int chunk, int nch, float2* S) {
+  const int c = blockIdx.y, b = blockIdx.z;
+  const float2* A = Abase + (size_t)b * bstride;
+  float2* Sp = S + (size_t)(b * nch + c) * chunk * kTsluW;
+  const int r0 = k + c * chunk;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < chunk * kTsluW; idx += gridDim.x * blockDim.x) {
+    const int col = idx / chunk, r = idx - col * chunk;
+    const int gr = r0 + r;
+    Sp[(size_t)col * chunk + r] = gr < nn ? A[(size_t)(k + col) * lda + gr] : make_float2(0.f, 0.f);
+  }
+}
+
+// Candidate i = c*64 + e of problem b: the chunk row that chunk c's
+// factorisation brought to its position e (entry e of its gather list), read
+// from A as it is; cgid = that row's index in A, or -1 for a row past nn.
+__global__ void __launch_bounds__(256) k_tslu_gather(const float2* __restrict__ Abase, size_t lda, size_t bstride,
+                                                     int nn, int k, int chunk, int nch,
+                                                     const int* __restrict__ cperm, float2* Cm, int* cgid) {
+  const int b = blockIdx.y;
+  const int ncand = nch * kTsluW;
+  const float2* A = Abase + (size_t)b * bstride;
+  float2* Cb = Cm + (size_t)b * ncand * kTsluW;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ncand * kTsluW; idx += gridDim.x * blockDim.x) {
+    const int col = idx / ncand, i = idx - col * ncand;
+    const int c = i / kTsluW, e = i - c * kTsluW;
+    const int src = cperm[(size_t)(b * nch + c) * kPermStride + 2 + 2 * e];
+    const int g = k + c * chunk + src;
+    const bool ok = g < nn;
+    Cb[(size_t)col * ncand + i] = ok ? A[(size_t)(k + col) * lda + g] : make_float2(0.f, 0.f);
+    if (col == 0) cgid[(size_t)b * ncand + i] = ok ? g : -1;
+  }
+}
+
+// One CTA per problem: the winners (entries 0..63 of the candidates' gather
+// list) become the pivot rows of columns k..k+63 in order, recorded as
+// partial pivoting records them (ipiv, the panel's gather list); the panel's
+// rows are interchanged accordingly and the 64 x 64 top block is factored
+// without pivoting.  Dynamic shared memory: 128 x 64 interchanged rows, then
+// the 64 x 65 top block.
+__global__ void __launch_bounds__(256) k_tslu_apply(float2* Abase, size_t lda, size_t bstride, int nn, int k,
+                                                    int ncand, const int* __restrict__ wperm,
+                                                    const int* __restrict__ cgid, int* ipiv, int ipiv_stride,
+                                                    int* perm, int* pstart, int pidx, int* status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  zf* s_rows = reinterpret_cast<zf*>(smem_raw);       // [2*64][64]
+  zf* s_t = s_rows + 2 * kTsluW * kTsluW;             // [64][65]
+  __shared__ int s_pdst[2 * kTsluW], s_psrc[2 * kTsluW];
+  __shared__ int s_pcount;
+  const int b = blockIdx.x, tid = threadIdx.x;
+  float2* A = Abase + (size_t)b * bstride;
+  const int* wp = wperm + (size_t)b * kPermStride;
+  const int* gid = cgid + (size_t)b * ncand;
+  int* pl = perm + (size_t)b * kPermStride;
+  if (tid == 0) {
+    int pcount = kTsluW;
+    for (int e = 0; e < kTsluW; ++e) s_pdst[e] = s_psrc[e] = k + e;
+    for (int j = 0; j < kTsluW; ++j) {
+      const int g = gid[wp[2 + 2 * j]];
+      int prow = k + j;  // no candidate row (past nn): the panel is singular there, keep the row
+      if (g >= 0) {
+        prow = g;  // where the winner's row is now: where an earlier interchange put it, else its own row
+        for (int e = 0; e < pcount; ++e)
+          if (s_psrc[e] == g) {
+            prow = s_pdst[e];
+            break;
+          }
+      }
+      ipiv[(size_t)b * ipiv_stride + k + j] = prow + 1;
+      perm_swap(s_pdst, s_psrc, pcount, k, kTsluW, j, prow);
+    }
+    s_pcount = pcount;
+    pl[0] = pcount;
+    if (b == 0 && pstart) {
+      pstart[pidx] = k;
+      pstart[pidx + 1] = k + kTsluW;
+    }
+  }
+  __syncthreads();
+  const int pc = s_pcount;
+  for (int e = tid; e < pc; e += blockDim.x) {
+    pl[1 + 2 * e] = s_pdst[e];
+    pl[2 + 2 * e] = s_psrc[e];
+  }
+  // the interchanges on the panel's columns: every moved row read, then written
+  for (int idx = tid; idx < pc * kTsluW; idx += blockDim.x) {
+    const int e = idx / kTsluW, c = idx - e * kTsluW;
+    const float2 v = A[(size_t)(k + c) * lda + s_psrc[e]];
+    s_rows[e * kTsluW + c] = zf{v.x, v.y};
+  }
+  __syncthreads();
+  for (int idx = tid; idx < pc * kTsluW; idx += blockDim.x) {
+    const int e = idx / kTsluW, c = idx - e * kTsluW;
+    const zf v = s_rows[e * kTsluW + c];
+    if (e >= kTsluW) A[(size_t)(k + c) * lda + s_pdst[e]] = make_float2(v.re, v.im);
+    else s_t[e * 65 + c] = v;  // rows k..k+63: the top block, factored below
+  }
+  // LU of the top block without pivoting (its rows are partial pivoting's choice)
+  for (int j = 0; j < kTsluW; ++j) {
+    __syncthreads();
+    const zf pv = s_t[j * 65 + j];
+    const bool zero = pv.re == 0.f && pv.im == 0.f;
+    if (zero && tid == 0) atomicCAS(&status[ST_SINGULAR], 0, k + j + 1);
+    const zf rpv = zero ? zf{0.f, 0.f} : crcp(pv);
+    for (int i = j + 1 + tid; i < kTsluW; i += blockDim.x) s_t[i * 65 + j] = s_t[i * 65 + j] * rpv;
+    __syncthreads();
+    const int n1 = kTsluW - j - 1;
+    for (int idx = tid; idx < n1 * n1; idx += blockDim.x) {
+      const int i = j + 1 + idx / n1, c = j + 1 + idx % n1;
+      cfms(s_t[i * 65 + c], s_t[i * 65 + j], s_t[j * 65 + c]);
+    }
+  }
+  __syncthreads();
+  for (int idx = tid; idx < kTsluW * kTsluW; idx += blockDim.x) {
+    const int c = idx / kTsluW, i = idx - c * kTsluW;
+    const zf v = s_t[i * 65 + c];
+    A[(size_t)(k + c) * lda + k + i] = make_float2(v.re, v.im);
+  }
+}
+
+// L21 = A21 U11^-1 for rows k+64..nn-1 of problem blockIdx.y: one row per
+// thread, its 64 values in registers, U11 (and the reciprocals of its
+// diagonal) in shared memory.
+__global__ void __launch_bounds__(128) k_tslu_trsm(float2* Abase, size_t lda, size_t bstride, int nn, int k) {
+  __shared__ zf s_u[kTsluW][kTsluW + 1];
+  __shared__ zf s_rd[kTsluW];
+  float2* A = Abase + (size_t)blockIdx.y * bstride;
+  for (int idx = threadIdx.x; idx < kTsluW * kTsluW; idx += blockDim.x) {
+    const int c = idx / kTsluW, i = idx - c * kTsluW;
+    const float2 v = A[(size_t)(k + c) * lda + k + i];
+    s_u[i][c] = zf{v.x, v.y};
+  }
+  __syncthreads();
+  if (threadIdx.x < kTsluW) {
+    const zf d = s_u[threadIdx.x][threadIdx.x];
+    s_rd[threadIdx.x] = (d.re == 0.f && d.im == 0.f) ? zf{0.f, 0.f} : crcp(d);
+  }
+  __syncthreads();
+  for (int r = k + kTsluW + blockIdx.x * blockDim.x + threadIdx.x; r < nn; r += gridDim.x * blockDim.x) {
+    zf x[kTsluW];
+#pragma unroll
+    for (int c = 0; c < kTsluW; ++c) {
+      const float2 v = A[(size_t)(k + c) * lda + r];
+      x[c] = zf{v.x, v.y};
+    }
+#pragma unroll
+    for (int j = 0; j < kTsluW; ++j) {
+      zf acc = x[j];
+#pragma unroll
+      for (int i = 0; i < j; ++i) cfms(acc, x[i], s_u[i][j]);
+      x[j] = acc * s_rd[j];
+    }
+#pragma unroll
+    for (int c = 0; c < kTsluW; ++c) A[(size_t)(k + c) * lda + r] = make_float2(x[c].re, x[c].im);
   }
 }
 
@@ -3393,6 +3575,101 @@ int lu_lockstep_capacity(bem_ctx* ctx, int nn, bool fp32) {
   return cap;
 }
 
+template <typename T>
+static int ts_ensure(bem_ctx* ctx, T*& p, size_t& cap, size_t need) {
+  if (p && cap >= need) return BEM_OK;
+  dev_free(ctx, p);
+  p = nullptr;
+  cap = 0;
+  BEM_CUDA(ctx, dev_alloc(ctx, &p, need * sizeof(T)));
+  cap = need;
+  return BEM_OK;
+}
+
+// The 64-column FP32 panel at column k of `batch` problems, taller than one
+// cluster holds, by tournament pivoting (the kernels k_tslu_*): its factors go
+// into A, its pivots into ipiv, its gather list to perm_p and its start to
+// the panel starts (index pidx), as the cluster kernels leave them.
+static int tslu_panel(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int nn, int k, int batch, int* perm_p,
+                      int pidx) {
+  LuWork& L = ctx->lu;
+  const int m = nn - k;
+  // as few chunks as let one cluster hold a chunk's 64 columns
+  const int cs1 = cluster_size(ctx);
+  int nch = 1, chunk = 0;
+  for (;; ++nch) {
+    chunk = ((m + nch - 1) / nch + 15) & ~15;
+    const int rp = (chunk + cs1 - 1) / cs1;
+    if (rp <= 512 && cluster_panel_fits_any<float>(kTsluW, rp)) break;
+    if (nch >= 64) return fail(ctx, BEM_ERR_ARG, "panel too tall for the tournament");
+  }
+  const int ncand = nch * kTsluW;
+  const int cs2 = cluster_size_for(ctx, ncand);
+  const int rp2 = (ncand + cs2 - 1) / cs2;
+  if (rp2 > 512 || !cluster_panel_fits_any<float>(kTsluW, rp2))
+    return fail(ctx, BEM_ERR_ARG, "too many tournament candidates for one cluster");
+  const size_t nprob1 = (size_t)batch * nch;
+  int rc = ts_ensure(ctx, L.ts_s, L.ts_cap[0], nprob1 * chunk * kTsluW);
+  if (!rc) rc = ts_ensure(ctx, L.ts_ipiv, L.ts_cap[1], nprob1 * chunk);
+  if (!rc) rc = ts_ensure(ctx, L.ts_perm, L.ts_cap[2], nprob1 * kPermStride);
+  if (!rc) rc = ts_ensure(ctx, L.ts_c, L.ts_cap[3], (size_t)batch * ncand * kTsluW);
+  if (!rc) rc = ts_ensure(ctx, L.ts_gid, L.ts_cap[4], (size_t)batch * ncand);
+  if (!rc) rc = ts_ensure(ctx, L.ts_cipiv, L.ts_cap[5], (size_t)batch * ncand);
+  if (!rc) rc = ts_ensure(ctx, L.ts_cperm, L.ts_cap[6], (size_t)batch * kPermStride);
+  if (rc) return rc;
+  cudaStream_t st = ctx->stream;
+  // round 1: every chunk of every problem factored on a copy, in one launch
+  k_tslu_copy<<<dim3(std::min(64, (chunk * kTsluW + 255) / 256), nch, batch), 256, 0, st>>>(A, lda, bstride, nn, k,
+                                                                                         chunk, nch, L.ts_s);
+  PanelArgs p1{};
+  p1.A = L.ts_s;
+  p1.lda = (size_t)chunk;
+  p1.bstride = (size_t)chunk * kTsluW;
+  p1.nn = chunk;
+  p1.k = 0;
+  p1.w = kTsluW;
+  p1.cs = cs1;
+  p1.rp = (chunk + cs1 - 1) / cs1;
+  p1.ipiv = L.ts_ipiv;
+  p1.ipiv_stride = chunk;
+  p1.perm = L.ts_perm;
+  p1.perm_stride = kPermStride;
+  p1.status = ctx->d_status;
+  p1.pstart = nullptr;
+  p1.async_mail = ctx->panel_async ? 1 : 0;
+  p1.no_singular = 1;
+  rc = launch_cluster_panel_any<float>(ctx, p1, (int)nprob1, kTsluW);
+  if (rc) return rc;
+  // round 2: the chunks' choices, as they are in A, factored the same way
+  k_tslu_gather<<<dim3(std::min(64, (ncand * kTsluW + 255) / 256), batch), 256, 0, st>>>(
+      A, lda, bstride, nn, k, chunk, nch, L.ts_perm, L.ts_c, L.ts_gid);
+  PanelArgs p2 = p1;
+  p2.A = L.ts_c;
+  p2.lda = (size_t)ncand;
+  p2.bstride = (size_t)ncand * kTsluW;
+  p2.nn = ncand;
+  p2.cs = cs2;
+  p2.rp = rp2;
+  p2.ipiv = L.ts_cipiv;
+  p2.ipiv_stride = ncand;
+  p2.perm = L.ts_cperm;
+  rc = launch_cluster_panel_any<float>(ctx, p2, batch, kTsluW);
+  if (rc) return rc;
+  // round 3: the winners to the top in partial pivoting's record, the top
+  // block's LU, then L21
+  const size_t asmem = (size_t)(2 * kTsluW * kTsluW + kTsluW * 65) * sizeof(zf);
+  BEM_CUDA(ctx, cudaFuncSetAttribute(k_tslu_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asmem));
+  k_tslu_apply<<<batch, 256, asmem, st>>>(A, lda, bstride, nn, k, ncand, L.ts_cperm, L.ts_gid, L.ipiv, nn, perm_p,
+                                          L.pstart, pidx, ctx->d_status);
+  const int rows = nn - k - kTsluW;
+  if (rows > 0)
+    k_tslu_trsm<<<dim3(std::min((rows + 127) / 128, std::max(1, 4 * ctx->num_sms / batch)), batch), 128, 0, st>>>(
+        A, lda, bstride, nn, k);
+  ctx->launches += 6;
+  BEM_CUDA(ctx, cudaGetLastError());
+  return BEM_OK;
+}
+
 // One cooperative k_trsv launch over `batch` problems: forward (with the
 // interchanges of the last factorisation) and back substitution, or back
 // substitution only.
@@ -3593,6 +3870,11 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
       int rc = calu ? launch_calu_panel_any(ctx, pa, batch, nb) : launch_cluster_panel_any<R>(ctx, pa, batch, nb);
       if (rc) return rc;
       ctx->launches++;
+    } else if (sizeof(R) == 4 && ctx->panel_tslu && m > kTsluW) {
+      // FP32 panel taller than one cluster holds: tournament pivoting.
+      w = kTsluW;
+      int rc = tslu_panel(ctx, static_cast<float2*>(A), lda, bstride, nn, k, batch, perm_p, (int)L.panels.size());
+      if (rc) return rc;
     } else {
       // Panel taller than one cluster holds: cooperative grid, one problem at a time.
       int G = std::min({ctx->num_sms, kMaxGrid, (m + 15) / 16});

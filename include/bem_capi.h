@@ -131,6 +131,9 @@ int bem_ctx_set_stream(bem_ctx *ctx, void *stream);
  * trailing update by CTA pairs on tcgen05 cta_group::2, M = 256 per pair),
  * "small_clusters" (panel clusters of 2, 4 or 8 CTAs for systems whose
  * panel rows fit them at <= 256 rows per CTA, instead of always 16),
+ * "panel_tslu" (FP32 panels taller than a 16-CTA cluster holds, about 6900
+ * rows: tournament pivoting over cluster-sized chunks instead of the
+ * grid-barrier kernel),
  * "panel_calu" (FP32 panels with
  * tournament pivoting), "panel_push" (cluster panels push their pivot
  * candidates by remote stores), "panel_async" (... as st.async into
@@ -138,8 +141,8 @@ int bem_ctx_set_stream(bem_ctx *ctx, void *stream);
  * "laswp_tc" (FP32 row interchanges + U12 on the tensor cores), "trsv_inv"
  * (FP32 solves with inverted diagonal blocks), "graphs" (bem_sweep replays a
  * captured step).  Defaults: tcgen05, trsv_coop, lu_pairs, lu_quads,
- * f64_pairs, small_clusters, panel_push, panel_async, laswp_tc, trsv_inv and
- * graphs on; panel_calu and tc_pair off.
+ * f64_pairs, small_clusters, panel_tslu, panel_push, panel_async, laswp_tc,
+ * trsv_inv and graphs on; panel_calu and tc_pair off.
  * Integer budgets for a context that shares the GPU with another one running
  * at the same time (0, the default, means the whole device): "gemm_ctas"
  * (CTAs of the persistent FP32 trailing update) and "trsv_ctas" (CTAs of one

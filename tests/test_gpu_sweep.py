@@ -131,3 +131,28 @@ def test_small_clusters_same_factors(c1):
     for i, fr in enumerate(FREQS[:3]):
         assert rel(xs[True][i], _oracle_x(p, fr)) < 1e-10
         assert rel(xs[True][i], xs[False][i]) < 1e-13
+
+
+@pytest.mark.parametrize("tslu", [True, False], ids=["tournament", "grid_panel"])
+def test_tall_fp32_panels(tslu):
+    """n = 7500: the first FP32 panels are taller than one 16-CTA cluster
+    holds (about 6900 rows), so they are factored by tournament pivoting
+    (panel_tslu) or by the grid-barrier kernel.  Either way the refined mixed
+    solution reaches the FP64 level of the plain path, which keeps partial
+    pivoting."""
+    from bem_mececcs_b200 import serve
+    nx, ny = serve.grid_for(2500)
+    m = meshgen.enclosed_grid(nx, ny, jitter=0.10, seed=9, depth=2.5, layers=4)
+    d = meshgen.traction_patch(m, radius=2.0)
+    sol = BemSolver(m)
+    sol.ghmatece()
+    sol.set_bc(d.kode, d.bc, d.dam, d.rho)
+    assert sol.nn > 7000
+    freqs = [0.7, 3.1]
+    xp, _ = sol.sweep(freqs, form="plain", batch=2)
+    sol.ctx.set_option("panel_tslu", tslu)
+    xm, corr = sol.sweep(freqs, form="mixed", batch=2, refine=3)
+    for i in range(len(freqs)):
+        assert rel(xm[i], xp[i]) < 1e-10, (tslu, freqs[i])
+        assert corr[i] < 1e-9
+    sol.close()
