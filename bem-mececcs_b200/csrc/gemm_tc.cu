@@ -109,15 +109,19 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
+// 64 consecutive columns of this warp's 32 lanes (four x16 loads, no wait).
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64]) {
 #pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+  for (int q = 0; q < 4; ++q) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr + 16u * q));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[16 * q + i] = __uint_as_float(r[i]);
+  }
 }
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
@@ -292,19 +296,21 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
       const uint32_t tbase = tmem + (uint32_t)buf * 256u + ((uint32_t)(32 * e) << 16);
       for (int hc = 0; hc < 2; ++hc) {
         float* ct = stage_c + (size_t)hc * (kHalfBytes / 4);
+        // the half's 64 columns of both products in one go (one wait), while
+        // this half's previous reduce may still be leaving shared memory
+        float v1[64], v2[64];
+        tmem_ld64(tbase + (uint32_t)(64 * hc), v1);
+        tmem_ld64(tbase + 128u + (uint32_t)(64 * hc), v2);
+        tmem_ld_wait();
         if (issuer) tma_wait_read_1();  // this half's previous reduce has left shared memory
         epi_bar_sync();
-        for (int c = 0; c < 64; c += 16) {
-          float v1[16], v2[16];
-          tmem_ld16(tbase + (uint32_t)(64 * hc + c), v1);
-          tmem_ld16(tbase + 128u + (uint32_t)(64 * hc + c), v2);
-          tmem_ld_wait();
-          const int colbase = a.c0 + tn * kTcCols + 64 * hc + c;
+        {
+          const int colbase = a.c0 + tn * kTcCols + 64 * hc;
 #pragma unroll
-          for (int i = 0; i < 16; ++i) {
+          for (int i = 0; i < 64; ++i) {
             const float x = __shfl_xor_sync(0xffffffffu, v2[i], 1);
             const float val = p ? (v1[i] + x) : (v1[i] - x);
-            ct[(c + i) * 128 + rho] = colbase + i < a.cend ? -val : 0.0f;
+            ct[i * 128 + rho] = colbase + i < a.cend ? -val : 0.0f;
           }
         }
         if (hc == 1) {
@@ -521,19 +527,19 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc2(const __grid_constant__ CUt
       const uint32_t tbase = tmem + (uint32_t)buf * 256u + ((uint32_t)(32 * e) << 16);
       for (int hc = 0; hc < 2; ++hc) {
         float* ct = stage_c + (size_t)hc * (kHalfBytes / 4);
+        float v1[64], v2[64];
+        tmem_ld64(tbase + (uint32_t)(64 * hc), v1);
+        tmem_ld64(tbase + 128u + (uint32_t)(64 * hc), v2);
+        tmem_ld_wait();
         if (issuer) tma_wait_read_1();
         epi_bar_sync();
-        for (int c = 0; c < 64; c += 16) {
-          float v1[16], v2[16];
-          tmem_ld16(tbase + (uint32_t)(64 * hc + c), v1);
-          tmem_ld16(tbase + 128u + (uint32_t)(64 * hc + c), v2);
-          tmem_ld_wait();
-          const int colbase = a.c0 + tn * kTcCols + 64 * hc + c;
+        {
+          const int colbase = a.c0 + tn * kTcCols + 64 * hc;
 #pragma unroll
-          for (int i = 0; i < 16; ++i) {
+          for (int i = 0; i < 64; ++i) {
             const float x = __shfl_xor_sync(0xffffffffu, v2[i], 1);
             const float val = p ? (v1[i] + x) : (v1[i] - x);
-            ct[(c + i) * 128 + rho] = colbase + i < a.cend ? -val : 0.0f;
+            ct[i * 128 + rho] = colbase + i < a.cend ? -val : 0.0f;
           }
         }
         if (hc == 1) {

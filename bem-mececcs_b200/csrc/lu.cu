@@ -1776,8 +1776,9 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel_grid(PanelArgs a) {
 //   2. those candidates (64 per chunk, their rows as they are in A) are
 //      factored the same way: its 64 pivots are the panel's pivot rows;
 //   3. the winners are brought to the top of the panel by the same sequence of
-//      row interchanges partial pivoting would record (ipiv, gather list), the
-//      64 x 64 top block is factored without pivoting and L21 = A21 U11^-1.
+//      row interchanges partial pivoting would record (ipiv, gather list); the
+//      top block is the winners' L11\U11 from round 2 (they were factored in
+//      this order there) and L21 = A21 U11^-1.
 // The factors satisfy A = P L U as every other panel's do, so the
 // interchange, update and solve kernels are unchanged; the pivots may differ
 // from per-column partial pivoting, which is why this is used for the FP32
@@ -1824,16 +1825,16 @@ __global__ void __launch_bounds__(256) k_tslu_gather(const float2* __restrict__ 
 // One CTA per problem: the winners (entries 0..63 of the candidates' gather
 // list) become the pivot rows of columns k..k+63 in order, recorded as
 // partial pivoting records them (ipiv, the panel's gather list); the panel's
-// rows are interchanged accordingly and the 64 x 64 top block is factored
-// without pivoting.  Dynamic shared memory: 128 x 64 interchanged rows, then
-// the 64 x 65 top block.
+// rows are interchanged accordingly and the top block takes the winners'
+// L11\U11 from the candidates' factorisation.  Dynamic shared memory: the
+// 128 x 64 interchanged rows.
 __global__ void __launch_bounds__(256) k_tslu_apply(float2* Abase, size_t lda, size_t bstride, int nn, int k,
                                                     int ncand, const int* __restrict__ wperm,
-                                                    const int* __restrict__ cgid, int* ipiv, int ipiv_stride,
-                                                    int* perm, int* pstart, int pidx, int* status) {
+                                                    const int* __restrict__ cgid, const float2* __restrict__ cfac,
+                                                    int* ipiv, int ipiv_stride, int* perm, int* pstart, int pidx,
+                                                    int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   zf* s_rows = reinterpret_cast<zf*>(smem_raw);       // [2*64][64]
-  zf* s_t = s_rows + 2 * kTsluW * kTsluW;             // [64][65]
   __shared__ int s_pdst[2 * kTsluW], s_psrc[2 * kTsluW];
   __shared__ int s_pcount;
   const int b = blockIdx.x, tid = threadIdx.x;
@@ -1882,28 +1883,15 @@ __global__ void __launch_bounds__(256) k_tslu_apply(float2* Abase, size_t lda, s
     const int e = idx / kTsluW, c = idx - e * kTsluW;
     const zf v = s_rows[e * kTsluW + c];
     if (e >= kTsluW) A[(size_t)(k + c) * lda + s_pdst[e]] = make_float2(v.re, v.im);
-    else s_t[e * 65 + c] = v;  // rows k..k+63: the top block, factored below
   }
-  // LU of the top block without pivoting (its rows are partial pivoting's choice)
-  for (int j = 0; j < kTsluW; ++j) {
-    __syncthreads();
-    const zf pv = s_t[j * 65 + j];
-    const bool zero = pv.re == 0.f && pv.im == 0.f;
-    if (zero && tid == 0) atomicCAS(&status[ST_SINGULAR], 0, k + j + 1);
-    const zf rpv = zero ? zf{0.f, 0.f} : crcp(pv);
-    for (int i = j + 1 + tid; i < kTsluW; i += blockDim.x) s_t[i * 65 + j] = s_t[i * 65 + j] * rpv;
-    __syncthreads();
-    const int n1 = kTsluW - j - 1;
-    for (int idx = tid; idx < n1 * n1; idx += blockDim.x) {
-      const int i = j + 1 + idx / n1, c = j + 1 + idx % n1;
-      cfms(s_t[i * 65 + c], s_t[i * 65 + j], s_t[j * 65 + c]);
-    }
-  }
-  __syncthreads();
+  // rows k..k+63: L11\U11 of the winners in pivot order, which is the top
+  // block of the candidates' factorisation (round 2) as it stands
+  const float2* cf = cfac + (size_t)b * ncand * kTsluW;
   for (int idx = tid; idx < kTsluW * kTsluW; idx += blockDim.x) {
     const int c = idx / kTsluW, i = idx - c * kTsluW;
-    const zf v = s_t[i * 65 + c];
-    A[(size_t)(k + c) * lda + k + i] = make_float2(v.re, v.im);
+    const float2 v = cf[(size_t)c * ncand + i];
+    A[(size_t)(k + c) * lda + k + i] = v;
+    if (i == c && v.x == 0.f && v.y == 0.f) atomicCAS(&status[ST_SINGULAR], 0, k + c + 1);
   }
 }
 
@@ -3657,10 +3645,10 @@ static int tslu_panel(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int n
   if (rc) return rc;
   // round 3: the winners to the top in partial pivoting's record, the top
   // block's LU, then L21
-  const size_t asmem = (size_t)(2 * kTsluW * kTsluW + kTsluW * 65) * sizeof(zf);
+  const size_t asmem = (size_t)(2 * kTsluW * kTsluW) * sizeof(zf);
   BEM_CUDA(ctx, cudaFuncSetAttribute(k_tslu_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asmem));
-  k_tslu_apply<<<batch, 256, asmem, st>>>(A, lda, bstride, nn, k, ncand, L.ts_cperm, L.ts_gid, L.ipiv, nn, perm_p,
-                                          L.pstart, pidx, ctx->d_status);
+  k_tslu_apply<<<batch, 256, asmem, st>>>(A, lda, bstride, nn, k, ncand, L.ts_cperm, L.ts_gid, L.ts_c, L.ipiv, nn,
+                                          perm_p, L.pstart, pidx, ctx->d_status);
   const int rows = nn - k - kTsluW;
   if (rows > 0)
     k_tslu_trsm<<<dim3(std::min((rows + 127) / 128, std::max(1, 4 * ctx->num_sms / batch)), batch), 128, 0, st>>>(
@@ -4007,9 +3995,15 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     // its row map.  A keeps the factors of the one-panel-at-a-time LU (L in
     // panel order), so the solves are unchanged.
     const bool tcg = tc && sizeof(R) == 4;
-    const bool fit4 = m > 256 && panel_nb(m) == 64 && panel_nb(m - 64) == 64 && panel_nb(m - 128) == 64 &&
-                      panel_nb(m - 192) == 64;
-    const bool fit2 = m > 128 && panel_nb(m) == 64 && panel_nb(m - 64) == 64;
+    // panel width at m remaining rows: the cluster kernels', or 64 for a tall
+    // FP32 panel (the tournament and the grid kernel both factor 64 columns
+    // of FP32 panels up to 60000 rows), so that tall panels form groups too
+    auto pw = [&](int mm) {
+      const int nb = panel_nb(mm);
+      return nb ? nb : ((sizeof(R) == 4 && mm > kTsluW && mm <= 60000) ? kTsluW : 0);
+    };
+    const bool fit4 = m > 256 && pw(m) == 64 && pw(m - 64) == 64 && pw(m - 128) == 64 && pw(m - 192) == 64;
+    const bool fit2 = m > 128 && pw(m) == 64 && pw(m - 64) == 64;
     const int G = (tcg && ctx->lu_quads && ctx->laswp_tc && fit4) ? 4 : ((tcg && ctx->lu_pairs && fit2) ? 2 : 1);
     if (G > 1) {
       const int kG = k + 64 * G, ubase = k + 64;
