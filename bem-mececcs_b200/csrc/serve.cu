@@ -35,12 +35,16 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
-// Solves in flight at once.  Every LU keeps one 16-CTA cluster per panel and
-// the device holds about 9 of those at a time; admitting more than that only
-// queues their kernels behind each other on the GPU (measured: 94 concurrent
-// 6480-unknown solves ran 4x slower in total than 16), so a request that
-// fits the memory budget still waits here until a solve finishes.
-constexpr int kMaxInflight = 8;
+// Work in flight at once: at most 8 slots (independent solves or lockstep
+// batches) and 16 problems.  Every LU keeps one panel cluster per problem and
+// the device holds about 9 16-CTA clusters at a time; admitting more than
+// that only queues kernels behind each other (measured: 94 concurrent
+// 6480-unknown solves ran 4x slower in total than 16), so a request that fits
+// the memory budget still waits here until a solve finishes.  16 problems let
+// two lockstep batches of a sweep run side by side, one's panels overlapping
+// the other's updates.
+constexpr int kMaxInflight = 16;
+constexpr int kMaxSlotsBusy = 8;
 
 double ms_between(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
@@ -217,7 +221,7 @@ class Server {
     std::unique_lock<std::mutex> lk(mu_);
     while (!stop_) {
       bool progress = false;
-      int busy = 0;  // problems in flight
+      int busy = 0, busy_slots = 0;  // problems and slots in flight
       for (Slot& s : slots_)
         if (s.busy) {
           if (cudaEventQuery(s.done) == cudaSuccess) {
@@ -225,11 +229,13 @@ class Server {
             progress = true;
           } else {
             busy += (int)s.reqs.size();
+            ++busy_slots;
           }
         }
-      for (auto it = queue_.begin(); it != queue_.end() && busy < kMaxInflight;) {
+      for (auto it = queue_.begin(); it != queue_.end() && busy < kMaxInflight && busy_slots < kMaxSlotsBusy;) {
         const int st = try_start(*it, kMaxInflight - busy);
         if (st > 0) {  // the request and any batched with it leave the queue
+          ++busy_slots;
           queue_.erase(std::remove_if(queue_.begin(), queue_.end(),
                                       [](const std::shared_ptr<SrvRequest>& q) { return q->started; }),
                        queue_.end());

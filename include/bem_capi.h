@@ -353,9 +353,11 @@ int bem_interior(bem_ctx *ctx, const double zge[2], const double zcs[2],
  * problem stays resident (H, its factors and the post-swap G): a later
  * request with the same mesh, material, omega and KODE but a new right-hand
  * side is solved with the cached factors (GEMV + solves).  Idle problems are
- * evicted least-recently-used when a new one needs room.  At most 8 solves
- * run at once (more would only queue their kernels behind each other on the
- * GPU); a request that fits the budget waits for one to finish.  form:
+ * evicted least-recently-used when a new one needs room.  Queued requests
+ * with the same mesh, material, boundary values and KODE (a sweep over omega)
+ * are solved together as one lockstep batch.  At most 8 slots and 16
+ * problems are in flight at once (more would only queue their kernels behind
+ * each other on the GPU); a request that fits the budget waits.  form:
  * BEM_FORM_PLAIN or BEM_FORM_MIXED (with `refine` refinement steps). */
 typedef struct bem_server bem_server;
 int bem_server_create(int device, double budget_bytes, int form, int refine,
