@@ -2545,15 +2545,24 @@ __global__ void __launch_bounds__(256, 2) k_gemm_f64(double2* Abase, size_t lda,
       for (int mt = 0; mt < 4; ++mt) af[mt] = As[st][ks * 4 + t][wm * 32 + mt * 8 + g];
 #pragma unroll
       for (int nt = 0; nt < 2; ++nt) bf[nt] = Bs[st][wn * 16 + nt * 8 + g][ks * 4 + t];
+      // four passes over the 8 tiles: an accumulator's next product is 16
+      // independent DMMAs away (each still takes its terms in the same order)
 #pragma unroll
       for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
-        for (int nt = 0; nt < 2; ++nt) {
-          dmma(acc_re[mt][nt][0], acc_re[mt][nt][1], af[mt].x, bf[nt].x);
-          dmma(acc_re[mt][nt][0], acc_re[mt][nt][1], -af[mt].y, bf[nt].y);
-          dmma(acc_im[mt][nt][0], acc_im[mt][nt][1], af[mt].x, bf[nt].y);
-          dmma(acc_im[mt][nt][0], acc_im[mt][nt][1], af[mt].y, bf[nt].x);
-        }
+        for (int nt = 0; nt < 2; ++nt) dmma(acc_re[mt][nt][0], acc_re[mt][nt][1], af[mt].x, bf[nt].x);
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) dmma(acc_im[mt][nt][0], acc_im[mt][nt][1], af[mt].x, bf[nt].y);
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) dmma(acc_re[mt][nt][0], acc_re[mt][nt][1], -af[mt].y, bf[nt].y);
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) dmma(acc_im[mt][nt][0], acc_im[mt][nt][1], af[mt].y, bf[nt].x);
     }
     __syncthreads();
   }
