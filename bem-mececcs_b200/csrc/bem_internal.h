@@ -17,7 +17,7 @@ namespace bem {
 // Largest Gauss rule per direction (the reference's fixtures use 8).
 constexpr int kMaxNpg = 8;
 // Largest number of problems assembled or factored in lockstep.
-constexpr int kMaxBatch = 16;
+constexpr int kMaxBatch = 64;
 // Largest number of iterative-refinement steps of the mixed form.
 constexpr int kMaxRefine = 8;
 
@@ -217,7 +217,7 @@ struct bem_ctx {
   bool f64_pairs = true;      // FP64 LU: two panels per trailing update (K = 2 x panel width)
   bool tc_pair = false;       // FP32 trailing update by CTA pairs (k_gemm_tc2, tcgen05 cta_group::2)
   bool small_clusters = true; // panel clusters sized to the system (<= 256 rows per CTA), not always 16
-  bool panel_tslu = true;     // FP32 panels taller than a cluster: tournament pivoting instead of the grid kernel
+  bool panel_tslu = false;    // FP32 panels taller than a cluster: tournament pivoting instead of the grid kernel
   // SM shares for contexts that run concurrently on one GPU (0: the whole device)
   int gemm_ctas = 0;          // CTAs of the persistent tensor-core trailing update
   int trsv_ctas = 0;          // CTAs of one cooperative triangular solve (all problems together)

@@ -141,8 +141,9 @@ int bem_ctx_set_stream(bem_ctx *ctx, void *stream);
  * "laswp_tc" (FP32 row interchanges + U12 on the tensor cores), "trsv_inv"
  * (FP32 solves with inverted diagonal blocks), "graphs" (bem_sweep replays a
  * captured step).  Defaults: tcgen05, trsv_coop, lu_pairs, lu_quads,
- * f64_pairs, small_clusters, panel_tslu, panel_push, panel_async, laswp_tc,
- * trsv_inv and graphs on; panel_calu and tc_pair off.
+ * f64_pairs, small_clusters, panel_push, panel_async, laswp_tc, trsv_inv
+ * and graphs on; panel_calu, panel_tslu and tc_pair off (measured no faster
+ * on B200).
  * Integer budgets for a context that shares the GPU with another one running
  * at the same time (0, the default, means the whole device): "gemm_ctas"
  * (CTAs of the persistent FP32 trailing update) and "trsv_ctas" (CTAs of one
@@ -254,7 +255,7 @@ int bem_sync(bem_ctx *ctx);
 int bem_linsolve_async(bem_ctx *ctx);
 
 /* Frequency sweep on the resident mesh (the batching and precision forms).
- * Assembles and solves nfreq frequencies, `batch` (1..16) problems at a
+ * Assembles and solves nfreq frequencies, `batch` (1..64) problems at a
  * time in lockstep.  form BEM_FORM_PLAIN: FP64 assembly and FP64 LU.
  * form BEM_FORM_MIXED: FP64 assembly plus a complex64 copy, FP32 LU with
  * TF32 tensor-core updates, then `refine` (0..8) steps of FP64 iterative
@@ -291,7 +292,7 @@ int bem_batch_solve(bem_ctx *driver, int nprob, bem_ctx *const *probs,
 
 /* Largest lockstep batch bem_sweep uses for this mesh and form: the number
  * of panel-factorisation thread-block clusters the device keeps resident at
- * once (7 for n = 6480 on a 148-SM B200), capped at 16. */
+ * once (7 for n = 6480 on a 148-SM B200), capped at 64. */
 int bem_sweep_batch_limit(bem_ctx *ctx, int form, int *limit);
 
 /* Kernel-class timing with CUDA events on ctx's stream.  Classes:
