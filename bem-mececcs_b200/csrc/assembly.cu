@@ -248,7 +248,7 @@ __global__ void k_gest(int nbe, const double* __restrict__ corner, const double4
 // ---------------------------------------------------------------------------
 // Dynamic assembly.
 // ---------------------------------------------------------------------------
-struct DynParams {
+struct DynCore {
   int nbe, nn, ng, jc, chunks;
   size_t lda;
   size_t a_stride;  // elements between the systems of consecutive problems
@@ -271,7 +271,17 @@ struct DynParams {
   double2* diag_g;
   double2* rhs_part;  // [batch][chunks][nn]
   int* status;
+};
+// One mesh, `batch` frequencies (bem_ghmatecd, bem_sweep).
+struct DynParams : DynCore {
   StokesConsts<double> kb[kMaxBatch];  // per problem (frequency)
+};
+// One problem of a grouped launch (bem_batch_solve): its own mesh, BCs and
+// constants; its system is padded to npad unknowns, the right-hand side in
+// column npad.
+struct DynProblem : DynCore {
+  StokesConsts<double> kc;
+  int npad;
 };
 
 __device__ __forceinline__ zd ld(const double2* p) {
@@ -283,11 +293,9 @@ __device__ __forceinline__ void st(double2* p, zd z) { *p = make_double2(z.re, z
 // Diagonal blocks (I == J): SING_DE (src/Sing_de.for:13-113) with SOLFUNDIF
 // (src/Solfundif.for:18-69), Stokes minus Kelvin per Gauss point, plus the
 // static diagonals (src/Ghmatecd.for:150-153).  One thread per element.
-__global__ void __launch_bounds__(128) k_dyn_diag(DynParams p) {
+__device__ __forceinline__ void dyn_diag_body(const DynCore& p, const StokesConsts<double>& kc, int prob) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= p.nbe) return;
-  const int prob = blockIdx.z;
-  const StokesConsts<double>& kc = p.kb[prob];
   double2* diag_h = p.diag_h + (size_t)prob * p.nbe * 9;
   double2* diag_g = p.diag_g + (size_t)prob * p.nbe * 9;
   const double4 P = p.colloc[j];
@@ -334,6 +342,15 @@ __global__ void __launch_bounds__(128) k_dyn_diag(DynParams p) {
   }
 }
 
+__global__ void __launch_bounds__(128) k_dyn_diag(DynParams p) { dyn_diag_body(p, p.kb[blockIdx.z], blockIdx.z); }
+
+// Grouped form: blockIdx.z is the problem; its descriptor is in global memory.
+__global__ void __launch_bounds__(128) k_dyn_diag_grp(const DynProblem* __restrict__ g) {
+  const DynProblem& p = g[blockIdx.z];
+  const StokesConsts<double> kc = p.kc;
+  dyn_diag_body(p, kc, 0);
+}
+
 // Off-diagonal pairs with the boundary-condition swap (src/Ghmatecd.for:316-333
 // as called at :168: column j with KODE=0 gets H <- -G, G <- -H*ZGE) and the
 // right-hand side ZFI = G*ZDFI (src/Ghmatecd.for:172-181) fused; G itself is
@@ -346,16 +363,17 @@ __host__ __device__ constexpr int sym3(int i, int j) {
 }
 constexpr int kWarpsPerCta = 4;
 
-__global__ void __launch_bounds__(128) k_dyn_offdiag(DynParams p) {
+__device__ __forceinline__ void dyn_offdiag_body(const DynCore& p, const StokesConsts<double>& kc, int prob) {
   extern __shared__ __align__(128) double4 s_gq[];  // [jc][ng]
   __shared__ uint64_t s_bar;
   __shared__ zd s_rhs[kWarpsPerCta][3 * kRowsPerCta];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int I = blockIdx.x * kRowsPerCta + lane;
   const int J0 = blockIdx.y * p.jc;
+  // a grouped launch covers its largest member: CTAs past this one's rows or
+  // element columns leave at once (uniform per CTA, before any barrier)
+  if (J0 >= p.nbe || (int)blockIdx.x * kRowsPerCta >= p.nbe) return;
   const int jn = min(p.jc, p.nbe - J0);
-  const int prob = blockIdx.z;
-  const StokesConsts<double>& kc = p.kb[prob];
   double2* A = p.A + (size_t)prob * p.a_stride;
   float2* A32 = p.A32 ? p.A32 + (size_t)prob * p.a_stride : nullptr;
   double2* Gp = p.G ? p.G + (size_t)prob * p.a_stride : nullptr;
@@ -493,6 +511,53 @@ __global__ void __launch_bounds__(128) k_dyn_offdiag(DynParams p) {
   }
 }
 
+__global__ void __launch_bounds__(128) k_dyn_offdiag(DynParams p) {
+  dyn_offdiag_body(p, p.kb[blockIdx.z], blockIdx.z);
+}
+
+__global__ void __launch_bounds__(128) k_dyn_offdiag_grp(const DynProblem* __restrict__ g) {
+  const DynProblem& p = g[blockIdx.z];
+  dyn_offdiag_body(p, p.kc, 0);
+}
+
+// Grouped form of the right-hand-side reduction and the padding of a class
+// (blockIdx.y = problem): the RHS (chunk partials summed in chunk order, as
+// k_rhs_reduce) goes to column npad with zeros below row nn; columns < nn
+// get zero rows nn..npad-1; columns nn..npad-1 become the identity.  The
+// padding never pivots and stays untouched by the updates.
+__global__ void __launch_bounds__(256) k_rhs_pad_grp(const DynProblem* __restrict__ g) {
+  const DynProblem& p = g[blockIdx.y];
+  const int n = p.nn, npad = p.npad, e = npad - n, chunks = p.chunks;
+  const size_t lda = p.lda;
+  double2* A = p.A;
+  float2* A32 = p.A32;
+  const double2* part = p.rhs_part;
+  const long long live = (long long)e * n, total = (long long)npad + live + (long long)e * npad;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    int row, col;
+    zd v{0.0, 0.0};
+    if (i < npad) {
+      row = (int)i;
+      col = npad;
+      if (row < n)
+        for (int c = 0; c < chunks; ++c) v = v + ld(&part[(size_t)c * n + row]);
+    } else if (i < npad + live) {
+      const long long k = i - npad;
+      col = (int)(k / e);
+      row = n + (int)(k % e);
+    } else {
+      const long long k = i - npad - live;
+      col = n + (int)(k / npad);
+      row = (int)(k % npad);
+      if (row == col) v.re = 1.0;
+    }
+    const size_t idx = (size_t)col * lda + row;
+    st(&A[idx], v);
+    if (A32) A32[idx] = make_float2((float)v.re, (float)v.im);
+  }
+}
+
 // RHS column of A: sum of the per-chunk partials in chunk order.
 __global__ void k_rhs_reduce(int nn, int chunks, size_t lda, size_t a_stride, const double2* __restrict__ part,
                              double2* A, float2* A32) {
@@ -613,11 +678,11 @@ StokesConsts<double> make_consts(const double zge_[2], const double zcs_[2],
   return k;
 }
 
-static DynParams dyn_params(bem_ctx* ctx, const DynBatch& b) {
+static DynCore dyn_core(bem_ctx* ctx, const DynBatch& b) {
   Mesh& m = ctx->mesh;
   const int jc = jc_for(m.ng);
   const int chunks = (m.nbe + jc - 1) / jc;
-  DynParams p{};
+  DynCore p{};
   p.nbe = m.nbe;
   p.nn = 3 * m.nbe;
   p.ng = m.ng;
@@ -647,8 +712,73 @@ static DynParams dyn_params(bem_ctx* ctx, const DynBatch& b) {
   p.rhs_part = b.rhs_part;
   p.G = b.G;
   p.status = ctx->d_status;
+  return p;
+}
+
+static DynParams dyn_params(bem_ctx* ctx, const DynBatch& b) {
+  DynParams p{};
+  static_cast<DynCore&>(p) = dyn_core(ctx, b);
   for (int i = 0; i < b.batch; ++i) p.kb[i] = make_consts(b.zge, b.zcs, b.zcp, b.freqs[i]);
   return p;
+}
+
+size_t dyn_problem_bytes() { return sizeof(DynProblem); }
+
+int launch_dynamic_group(bem_ctx* wk, const GroupMember* mem, int count, void* h_desc, void* d_desc) {
+  if (count < 1 || count > 65535) return fail(wk, BEM_ERR_ARG, "group size out of range");
+  DynProblem* hd = static_cast<DynProblem*>(h_desc);
+  int max_nbe = 0, max_chunks = 0;
+  long long max_pad = 0;
+  size_t smem = 0;
+  double work = 0.0, bytes = 0.0;
+  for (int i = 0; i < count; ++i) {
+    const GroupMember& g = mem[i];
+    bem_ctx* pc = g.pc;
+    std::lock_guard<std::mutex> lk(pc->mu);
+    DynBatch b{};
+    b.zge = g.zge;
+    b.zcs = g.zcs;
+    b.zcp = g.zcp;
+    b.c = g.c;
+    b.freqs = &g.fr;
+    b.batch = 1;
+    b.flags = BEM_FAST_SINGULAR;
+    b.A = g.A;
+    b.lda = g.lda;
+    b.a_stride = 0;
+    b.A32 = g.A32;
+    b.diag_h = g.diag_h;
+    b.diag_g = g.diag_g;
+    b.rhs_part = g.rhs_part;
+    DynProblem q{};
+    static_cast<DynCore&>(q) = dyn_core(pc, b);
+    q.status = wk->d_status;  // the group reports through the worker
+    q.kc = make_consts(g.zge, g.zcs, g.zcp, g.fr);
+    q.npad = g.npad;
+    if (q.npad < q.nn) return fail(wk, BEM_ERR_ARG, "padded size below the problem size");
+    hd[i] = q;
+    const Mesh& m = pc->mesh;
+    max_nbe = std::max(max_nbe, m.nbe);
+    max_chunks = std::max(max_chunks, q.chunks);
+    smem = std::max(smem, (size_t)q.jc * m.ng * sizeof(double4));
+    const long long e = q.npad - q.nn;
+    max_pad = std::max(max_pad, (long long)q.npad + e * q.nn + e * q.npad);
+    work += (double)m.nbe * (double)m.nbe * (double)m.ng;
+    bytes += (double)q.nn * (q.nn + 1) * (16.0 + (g.A32 ? 8.0 : 0.0));
+  }
+  const DynProblem* dd = static_cast<const DynProblem*>(d_desc);
+  BEM_CUDA(wk, cudaMemcpyAsync(d_desc, hd, (size_t)count * sizeof(DynProblem), cudaMemcpyHostToDevice, wk->stream));
+  ProfScope ps(wk, 0, work, bytes);
+  k_dyn_diag_grp<<<dim3((max_nbe + 127) / 128, 1, count), 128, 0, wk->stream>>>(dd);
+  BEM_CUDA(wk, cudaGetLastError());
+  k_dyn_offdiag_grp<<<dim3((max_nbe + kRowsPerCta - 1) / kRowsPerCta, max_chunks, count), 128, smem, wk->stream>>>(
+      dd);
+  BEM_CUDA(wk, cudaGetLastError());
+  const int pb = (int)std::min<long long>((max_pad + 255) / 256, 256);
+  k_rhs_pad_grp<<<dim3(pb, count), 256, 0, wk->stream>>>(dd);
+  BEM_CUDA(wk, cudaGetLastError());
+  wk->launches += 3;
+  return BEM_OK;
 }
 
 // The per-frequency constants of a captured step: every k_dyn_diag and

@@ -208,7 +208,9 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 // Bounded wait for phase `parity` of the mbarrier; false on timeout.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity,
                                           unsigned long long limit_ns = kWaitLimitNs) {
-  const unsigned long long t0 = globaltimer_ns();
+  // the clock is read only once the first try has failed: a wait that is
+  // already satisfied (the common case in a full pipeline) costs one try
+  unsigned long long t0 = 0;
   unsigned spins = 0;
   while (true) {
     uint32_t done;
@@ -218,6 +220,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity,
         : "r"(smem_u32(bar)), "r"(parity)
         : "memory");
     if (done) return true;
+    if (spins == 0) t0 = globaltimer_ns();
     if ((++spins & 63u) == 0 && globaltimer_ns() - t0 > limit_ns) return false;
   }
 }

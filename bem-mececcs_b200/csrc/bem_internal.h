@@ -195,8 +195,10 @@ struct bem_ctx {
   size_t int_cap_l = 0, int_cap_nn = 0;
   bem::SweepBuf bbuf;  // padded systems of bem_batch_solve
   std::vector<bem_ctx*> workers;   // bem_batch_solve: contexts whose streams run classes concurrently
-  void* pinned = nullptr;          // bem_batch_solve: pinned staging of solutions and norms
+  void* pinned = nullptr;          // bem_batch_solve: pinned staging of descriptors, solutions, norms
   size_t pinned_bytes = 0;
+  unsigned char* grp_desc = nullptr;  // bem_batch_solve: assembly descriptors on the device
+  size_t grp_desc_bytes = 0;
   bool use_tcgen05 = true;  // FP32 trailing update on tcgen05 (else TF32 mma.sync)
   bool use_trsv_coop = true;
   bool trsv_inv = true;        // FP32 cooperative solves apply inverted diagonal blocks (k_trsv_f32)
@@ -278,6 +280,23 @@ int dyn_graph_update(bem_ctx* ctx, cudaGraphExec_t exec, const std::vector<cudaG
                      const DynBatch& b);
 int dyn_graph_nodes(bem_ctx* ctx, cudaGraph_t g, std::vector<cudaGraphNode_t>& out);
 int launch_dynamic_batch(bem_ctx* ctx, const DynBatch& b);
+// One member of a grouped assembly (bem_batch_solve).
+struct GroupMember {
+  bem_ctx* pc;  // the problem's context: mesh, static diagonals, BCs
+  const double *zge, *zcs, *zcp, *c;
+  double fr;
+  double2* A;    // its padded slot (npad x (npad + 1), RHS in column npad)
+  float2* A32;   // optional complex64 copy, same layout
+  size_t lda;
+  int npad;
+  double2 *diag_h, *diag_g;  // [nbe][9] scratch
+  double2* rhs_part;         // [chunks][nn] scratch
+};
+// Assembles and pads `count` problems in three launches on wk's stream; the
+// descriptors go through h_desc (pinned, count x dyn_problem_bytes(), left
+// untouched until the stream has passed) to d_desc (device, same size).
+int launch_dynamic_group(bem_ctx* wk, const GroupMember* mem, int count, void* h_desc, void* d_desc);
+size_t dyn_problem_bytes();
 int rhs_chunks(bem_ctx* ctx);
 
 // LU (lu.cu).

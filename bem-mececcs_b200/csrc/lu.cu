@@ -771,6 +771,7 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
   // bytes arriving in a CTA per column: every CTA's candidate (1 + KW words) and row gj (KW words)
   const unsigned mail_bytes = (unsigned)(cs * (1 + KW) + KW) * 16u;
   unsigned mph = 0;  // phase bits of s_mb[0], s_mb[1]
+  bool gave_up = false;  // this thread's mailbox wait ran out: later waits are skipped
 
   const int grow = tid < rcount ? rbase + tid : INT_MAX;  // my row (position)
   const C czero{R(0), R(0)};
@@ -919,10 +920,14 @@ __global__ void __launch_bounds__(NT, 1) k_panel_push(PanelArgs a) {
       }
       if (amail) {
         // the column's mailboxes are full when the mbarrier's phase completes; a
-        // wait that runs out sets the status and later waits are skipped (the
-        // kernel still meets every cluster barrier)
-        if (*(volatile int*)&a.status[ST_TIMEOUT] == 0 && !mbar_wait(&s_mb[par], (mph >> par) & 1u, wlim))
+        // wait that runs out sets the status and this thread skips its later
+        // waits (the kernel still meets every cluster barrier), so a kernel
+        // waits at most one limit in all.  No global read on this path: the
+        // wait is on the critical path of every column.
+        if (!gave_up && !mbar_wait(&s_mb[par], (mph >> par) & 1u, wlim)) {
+          gave_up = true;
           atomicExch(&a.status[ST_TIMEOUT], 1);
+        }
         mph ^= 1u << par;
       } else {
         cluster_sync();

@@ -373,21 +373,23 @@ int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double z
 // classes whose largest member is at most 1.25 x the smallest and whose count
 // fits the lockstep limit; each class is embedded in one padded size (the
 // problem, then the identity) and runs through the lockstep LU of bem_sweep.
-// Every problem is assembled from its own context (mesh, static diagonals,
-// BCs) straight into its padded slot, on the driver's stream.
+// A class is assembled in three launches (launch_dynamic_group: every member
+// from its own context's mesh, static diagonals and BCs, straight into its
+// padded slot) and its solutions come back in one copy, so the host issues a
+// few dozen calls per class, not per problem.
 // ---------------------------------------------------------------------------
 namespace {
 
 struct BatchNeed {
-  size_t a_elems = 0, vec_elems = 0, resid_elems = 0, rhs_elems = 0;
-  int max_nbe = 0, norm_batch = 0;
-  void add(int npad, int batch, int nbe, int chunks) {
+  size_t a_elems = 0, vec_elems = 0, resid_elems = 0, rhs_elems = 0, diag_elems = 0;
+  int norm_batch = 0;
+  void add(int npad, int batch, size_t diag, size_t rhs) {
     const size_t lda = (size_t)((npad + 1) & ~1), a_stride = lda * (size_t)(npad + 1);
     a_elems = std::max(a_elems, a_stride * batch);
     vec_elems = std::max(vec_elems, (size_t)npad * batch);
     resid_elems = std::max(resid_elems, (size_t)((npad + kResidCols - 1) / kResidCols) * npad * batch);
-    rhs_elems = std::max(rhs_elems, (size_t)chunks * 3 * nbe);
-    max_nbe = std::max(max_nbe, nbe);
+    rhs_elems = std::max(rhs_elems, rhs);
+    diag_elems = std::max(diag_elems, diag);
     norm_batch = std::max(norm_batch, batch);
   }
 };
@@ -397,7 +399,7 @@ int ensure_batchbuf(bem_ctx* d, const BatchNeed& q, bool mixed) {
   SweepBuf& S = d->bbuf;
   const bool fits = S.A64 && q.a_elems <= S.a_stride && (!mixed || S.A32) && q.vec_elems <= (size_t)S.nn &&
                     q.resid_elems <= (size_t)S.resid_chunks && q.rhs_elems <= (size_t)S.rhs_chunks &&
-                    q.max_nbe <= S.batch && (size_t)q.norm_batch <= S.norm_cap;
+                    q.diag_elems <= (size_t)S.batch && (size_t)q.norm_batch <= S.norm_cap;
   if (fits) return BEM_OK;
   free_sweep(d, S);
   BEM_CUDA(d, dev_alloc(d, &S.A64, q.a_elems * sizeof(double2)));
@@ -405,8 +407,8 @@ int ensure_batchbuf(bem_ctx* d, const BatchNeed& q, bool mixed) {
   BEM_CUDA(d, dev_alloc(d, &S.x64, q.vec_elems * sizeof(double2)));
   BEM_CUDA(d, dev_alloc(d, &S.v32, q.vec_elems * sizeof(float2)));
   BEM_CUDA(d, dev_alloc(d, &S.part, q.resid_elems * sizeof(double2)));
-  BEM_CUDA(d, dev_alloc(d, &S.diag_h, (size_t)q.max_nbe * 9 * sizeof(double2)));
-  BEM_CUDA(d, dev_alloc(d, &S.diag_g, (size_t)q.max_nbe * 9 * sizeof(double2)));
+  BEM_CUDA(d, dev_alloc(d, &S.diag_h, q.diag_elems * sizeof(double2)));
+  BEM_CUDA(d, dev_alloc(d, &S.diag_g, q.diag_elems * sizeof(double2)));
   BEM_CUDA(d, dev_alloc(d, &S.rhs_part, q.rhs_elems * sizeof(double2)));
   BEM_CUDA(d, dev_alloc(d, &S.norm, (size_t)2 * q.norm_batch * (kMaxRefine + 1) * sizeof(unsigned long long)));
   // capacities, in elements (this buffer set is only read through views)
@@ -414,10 +416,12 @@ int ensure_batchbuf(bem_ctx* d, const BatchNeed& q, bool mixed) {
   S.nn = (int)q.vec_elems;
   S.resid_chunks = (int)q.resid_elems;
   S.rhs_chunks = (int)q.rhs_elems;
-  S.batch = q.max_nbe;
+  S.batch = (int)q.diag_elems;
   S.norm_cap = (size_t)q.norm_batch;
   return BEM_OK;
 }
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 }  // namespace
 
@@ -439,33 +443,16 @@ int batch_solve(bem_ctx* d, int nprob, bem_ctx* const* probs, const double* freq
     if (rc) return fail(d, rc, "bem_batch_solve: worker context");
     d->workers.push_back(w);
   }
-  // Pinned staging: solutions, then per-class refinement norms.
-  size_t xoff_total = 0;
-  std::vector<size_t> xoff(nprob);
-  for (int p = 0; p < nprob; ++p) {
-    xoff[p] = xoff_total;
-    xoff_total += (size_t)3 * probs[p]->mesh.nbe;
-  }
-  const size_t norm_words = (size_t)nprob * 2 * (kMaxRefine + 1);
-  const size_t need = xoff_total * sizeof(double2) + norm_words * sizeof(unsigned long long);
-  if (d->pinned_bytes < need) {
-    if (d->pinned) cudaFreeHost(d->pinned);
-    d->pinned = nullptr;
-    d->pinned_bytes = 0;
-    BEM_CUDA(d, cudaMallocHost(&d->pinned, need));
-    d->pinned_bytes = need;
-  }
-  double2* hx = static_cast<double2*>(d->pinned);
-  unsigned long long* hnorm = reinterpret_cast<unsigned long long*>(hx + xoff_total);
-  std::vector<int> class_of(nprob), slot_of(nprob);
   // Plan: size classes in sorted order, round-robin over the workers, each
   // worker's buffers sized once for all its classes (no allocation between
   // launches).
   struct Cls {
     int g0, g1, npad;
+    size_t sol;  // offset of its solutions in the pinned staging, in double2
   };
   std::vector<Cls> plan;
   std::vector<BatchNeed> need_w(kBatchWorkers);
+  size_t sol_total = 0;
   for (int g0 = 0; g0 < nprob;) {
     const int n0 = 3 * probs[order[g0]]->mesh.nbe;
     int g1 = g0 + 1, npad = n0;
@@ -476,13 +463,14 @@ int batch_solve(bem_ctx* d, int nprob, bem_ctx* const* probs, const double* freq
       npad = n1;
       ++g1;
     }
-    int max_nbe = 0, max_chunks = 0;
+    size_t diag = 0, rhs = 0;
     for (int k = g0; k < g1; ++k) {
-      max_nbe = std::max(max_nbe, probs[order[k]]->mesh.nbe);
-      max_chunks = std::max(max_chunks, rhs_chunks(probs[order[k]]));
+      diag += (size_t)9 * probs[order[k]]->mesh.nbe;
+      rhs += (size_t)rhs_chunks(probs[order[k]]) * 3 * probs[order[k]]->mesh.nbe;
     }
-    need_w[plan.size() % kBatchWorkers].add(npad, g1 - g0, max_nbe, max_chunks);
-    plan.push_back({g0, g1, npad});
+    need_w[plan.size() % kBatchWorkers].add(npad, g1 - g0, diag, rhs);
+    plan.push_back({g0, g1, npad, sol_total});
+    sol_total += (size_t)(g1 - g0) * npad;
     g0 = g1;
   }
   for (int w = 0; w < kBatchWorkers; ++w) {
@@ -490,7 +478,34 @@ int batch_solve(bem_ctx* d, int nprob, bem_ctx* const* probs, const double* freq
     const int rc = ensure_batchbuf(d->workers[w], need_w[w], mixed);
     if (rc) return fail(d, rc, std::string("bem_batch_solve: ") + d->workers[w]->last_error);
   }
+  // Pinned staging: assembly descriptors, solutions, refinement norms.
+  const size_t desc_bytes = dyn_problem_bytes();
+  const size_t desc_total = align256((size_t)nprob * desc_bytes);
+  const size_t norm_words = (size_t)nprob * 2 * (kMaxRefine + 1);
+  const size_t need = desc_total + align256(sol_total * sizeof(double2)) + norm_words * sizeof(unsigned long long);
+  if (d->pinned_bytes < need) {
+    if (d->pinned) cudaFreeHost(d->pinned);
+    d->pinned = nullptr;
+    d->pinned_bytes = 0;
+    BEM_CUDA(d, cudaMallocHost(&d->pinned, need));
+    d->pinned_bytes = need;
+  }
+  if (d->grp_desc_bytes < desc_total) {
+    dev_free(d, d->grp_desc);
+    d->grp_desc = nullptr;
+    d->grp_desc_bytes = 0;
+    BEM_CUDA(d, dev_alloc(d, &d->grp_desc, desc_total));
+    BEM_CUDA(d, cudaStreamSynchronize(d->stream));  // the workers' streams use it next
+    d->grp_desc_bytes = desc_total;
+  }
+  unsigned char* hdesc = static_cast<unsigned char*>(d->pinned);
+  unsigned char* ddesc = static_cast<unsigned char*>(d->grp_desc);
+  double2* hsol = reinterpret_cast<double2*>(hdesc + desc_total);
+  unsigned long long* hnorm = reinterpret_cast<unsigned long long*>(
+      reinterpret_cast<unsigned char*>(hsol) + align256(sol_total * sizeof(double2)));
+  std::vector<int> class_of(nprob), slot_of(nprob);
   for (bem_ctx* w : d->workers) BEM_CUDA(w, cudaMemsetAsync(w->d_status, 0, ST_COUNT * sizeof(int), w->stream));
+  std::vector<GroupMember> mem;
   for (int ncls = 0; ncls < (int)plan.size(); ++ncls) {
     bem_ctx* wk = d->workers[ncls % kBatchWorkers];
     const int g0 = plan[ncls].g0, g1 = plan[ncls].g1, npad = plan[ncls].npad;
@@ -498,49 +513,35 @@ int batch_solve(bem_ctx* d, int nprob, bem_ctx* const* probs, const double* freq
     int rc = BEM_OK;
     SweepBuf& S = wk->bbuf;
     const size_t lda = (size_t)((npad + 1) & ~1), a_stride = lda * (size_t)(npad + 1);
+    mem.assign(B, GroupMember{});
+    size_t diag_off = 0, rhs_off = 0;
     for (int k = g0; k < g1; ++k) {
       const int p = order[k], slot = k - g0;
       class_of[p] = ncls;
       slot_of[p] = slot;
       bem_ctx* pc = probs[p];
-      const int n = 3 * pc->mesh.nbe;
-      std::lock_guard<std::mutex> lk(pc->mu);
-      cudaStream_t keep = pc->stream;
-      pc->stream = wk->stream;
-      DynBatch db{};
-      db.zge = zge + 2 * p;
-      db.zcs = zcs + 2 * p;
-      db.zcp = zcp + 2 * p;
-      db.c = c + 4 * p;
-      db.freqs = freqs + p;
-      db.batch = 1;
-      db.flags = BEM_FAST_SINGULAR;
-      db.A = S.A64 + (size_t)slot * a_stride;
-      db.lda = lda;
-      db.a_stride = 0;
-      db.A32 = mixed ? S.A32 + (size_t)slot * a_stride : nullptr;
-      db.diag_h = S.diag_h;
-      db.diag_g = S.diag_g;
-      db.rhs_part = S.rhs_part;
-      const long long l0 = pc->launches;
-      rc = cudaMemsetAsync(pc->d_status, 0, ST_COUNT * sizeof(int), wk->stream) == cudaSuccess
-               ? launch_dynamic_batch(pc, db)
-               : BEM_ERR_CUDA;
-      pc->stream = keep;
-      d->launches += pc->launches - l0;
-      if (rc) return fail(d, rc, std::string("assembly of a batched problem: ") + pc->last_error);
-      if (n < npad) {
-        const dim3 rg((npad + 255) / 256);
-        k_pad_rhs<<<rg, 256, 0, wk->stream>>>(db.A, lda, n, npad);
-        k_pad_rest<<<dim3(rg.x, npad), 256, 0, wk->stream>>>(db.A, lda, n, npad);
-        d->launches += 2;
-        if (mixed) {
-          k_pad_rhs<<<rg, 256, 0, wk->stream>>>(db.A32, lda, n, npad);
-          k_pad_rest<<<dim3(rg.x, npad), 256, 0, wk->stream>>>(db.A32, lda, n, npad);
-          d->launches += 2;
-        }
-        BEM_CUDA(d, cudaGetLastError());
-      }
+      GroupMember& g = mem[slot];
+      g.pc = pc;
+      g.zge = zge + 2 * p;
+      g.zcs = zcs + 2 * p;
+      g.zcp = zcp + 2 * p;
+      g.c = c + 4 * p;
+      g.fr = freqs[p];
+      g.A = S.A64 + (size_t)slot * a_stride;
+      g.A32 = mixed ? S.A32 + (size_t)slot * a_stride : nullptr;
+      g.lda = lda;
+      g.npad = npad;
+      g.diag_h = S.diag_h + diag_off;
+      g.diag_g = S.diag_g + diag_off;
+      g.rhs_part = S.rhs_part + rhs_off;
+      diag_off += (size_t)9 * pc->mesh.nbe;
+      rhs_off += (size_t)rhs_chunks(pc) * 3 * pc->mesh.nbe;
+    }
+    {
+      const long long l0 = wk->launches;
+      rc = launch_dynamic_group(wk, mem.data(), B, hdesc + (size_t)g0 * desc_bytes, ddesc + (size_t)g0 * desc_bytes);
+      d->launches += wk->launches - l0;
+      if (rc) return fail(d, rc, std::string("assembly of a batched class: ") + wk->last_error);
     }
     // the padded class through the lockstep LU (+ refinement)
     SweepBuf V = S;  // a view with this class's size for refine_steps
@@ -564,13 +565,15 @@ int batch_solve(bem_ctx* d, int nprob, bem_ctx* const* probs, const double* freq
     }
     d->launches += wk->launches - l0;
     if (rc) return fail(d, rc, std::string("bem_batch_solve: ") + wk->last_error);
-    for (int k = g0; k < g1; ++k) {
-      const int p = order[k], slot = k - g0;
-      const int n = 3 * probs[p]->mesh.nbe;
-      const double2* src = mixed ? V.x64 + (size_t)slot * npad : V.A64 + (size_t)slot * a_stride + (size_t)npad * lda;
-      BEM_CUDA(d, cudaMemcpyAsync(hx + xoff[p], src, (size_t)n * sizeof(double2), cudaMemcpyDeviceToHost,
+    // the class's solutions (npad each, padding included) in one copy
+    double2* dst = hsol + plan[ncls].sol;
+    if (mixed)
+      BEM_CUDA(d, cudaMemcpyAsync(dst, V.x64, (size_t)B * npad * sizeof(double2), cudaMemcpyDeviceToHost,
                                   wk->stream));
-    }
+    else
+      BEM_CUDA(d, cudaMemcpy2DAsync(dst, (size_t)npad * sizeof(double2), V.A64 + (size_t)npad * lda,
+                                    a_stride * sizeof(double2), (size_t)npad * sizeof(double2), B,
+                                    cudaMemcpyDeviceToHost, wk->stream));
     if (mixed && iters > 0)
       BEM_CUDA(d, cudaMemcpyAsync(hnorm + (size_t)2 * (kMaxRefine + 1) * g0, V.norm,
                                   (size_t)2 * B * (kMaxRefine + 1) * sizeof(unsigned long long),
@@ -582,23 +585,21 @@ int batch_solve(bem_ctx* d, int nprob, bem_ctx* const* probs, const double* freq
     if (rc) return fail(d, rc, std::string("bem_batch_solve: ") + w->last_error);
   }
   for (int p = 0; p < nprob; ++p) {
-    int rc = check_status(probs[p]);
-    if (rc) return fail(d, rc, std::string("batched problem: ") + probs[p]->last_error);
     if (probs[p]->mesh_flag_bnd) return fail(d, BEM_ERR_DEGENERATE, "Jacobian below 1e-5 on a boundary element");
-    if (x_out && x_out[p]) memcpy(x_out[p], hx + xoff[p], (size_t)3 * probs[p]->mesh.nbe * sizeof(double2));
+    const Cls& k = plan[class_of[p]];
+    if (x_out && x_out[p])
+      memcpy(x_out[p], hsol + k.sol + (size_t)slot_of[p] * k.npad, (size_t)3 * probs[p]->mesh.nbe * sizeof(double2));
   }
   if (corr_out) {
     // class norms were staged at the class's first sorted position
-    for (int k = 0, g0 = 0; k < nprob; ++k) {
-      const int p = order[k];
-      if (slot_of[p] == 0) g0 = k;
+    for (int p = 0; p < nprob; ++p) {
       if (!(mixed && iters > 0)) {
         corr_out[p] = 0.0;
         continue;
       }
-      int B = 0;
-      for (int q = g0; q < nprob && class_of[order[q]] == class_of[p]; ++q) ++B;
-      const unsigned long long* hn = hnorm + (size_t)2 * (kMaxRefine + 1) * g0 + (size_t)2 * B * (iters - 1);
+      const Cls& k = plan[class_of[p]];
+      const int B = k.g1 - k.g0;
+      const unsigned long long* hn = hnorm + (size_t)2 * (kMaxRefine + 1) * k.g0 + (size_t)2 * B * (iters - 1);
       double dm, xm;
       memcpy(&dm, &hn[2 * slot_of[p]], sizeof dm);
       memcpy(&xm, &hn[2 * slot_of[p] + 1], sizeof xm);

@@ -82,6 +82,9 @@ def parse_args():
     ap.add_argument("--profile-case", action="store_true",
                     help="run only warmup+steps headline sweep batches and print a launch count "
                          "(a small, short command to run under ncu); no bench line")
+    ap.add_argument("--profile-plain", action="store_true",
+                    help="run only warmup+steps plain FP64 solves (bem_ghmatecd + bem_linsolve) of the "
+                         "headline mesh and print a launch count (for ncu); no bench line")
     return ap.parse_args()
 
 
@@ -343,6 +346,15 @@ def run_ours(args):
             sweep_step(i)
         ctx.sync()
         print(json.dumps({"profile_case": "mixed sweep", "batch": B, "batches": args.warmup + args.steps,
+                          "launches": ctx.launches}), flush=True)
+        ctx.close()
+        return
+    if args.profile_plain:
+        for i in range(args.warmup + args.steps):
+            sol.ghmatecd(mine[i % len(mine)])
+            sol.linsolve()
+        ctx.sync()
+        print(json.dumps({"profile_case": "plain FP64 solve", "solves": args.warmup + args.steps,
                           "launches": ctx.launches}), flush=True)
         ctx.close()
         return

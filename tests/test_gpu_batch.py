@@ -41,3 +41,30 @@ def test_batch_uneven_matches_alone(form, tol):
         assert rel(disp, da) < tol and rel(trac, ta) < tol, (sol.nn, fr)
     for p in probs:
         p[0].ctx.close()
+
+
+def test_batch_equal_sizes_single_and_reuse():
+    """Classes without padding (members of one size), a batch of one, and a
+    second call on the same driver (its buffers reused, then grown): each
+    result equals the problem solved alone."""
+    meshes = [meshgen.enclosed_grid(8, 7, jitter=0.10, seed=s, depth=2.5, layers=4) for s in (1, 2, 3)]
+    probs = []
+    for k, m in enumerate(meshes):
+        d = meshgen.traction_patch(m, radius=2.0)
+        sol = BemSolver(m)
+        sol.ghmatece()
+        sol.set_bc(d.kode, d.bc, d.dam, d.rho)
+        probs.append((sol, 0.7 + 1.3 * k, d))
+    assert len({p[0].nn for p in probs}) == 1
+    extra = _problems(3, seed=4)
+    driver = capi.Context(0)
+    for form, tol in (("plain", 1e-10), ("mixed", 1e-8)):
+        for sub in (probs[:1], probs, probs + extra):
+            xs, _ = batch_solve(driver, [(p[0], p[1]) for p in sub], form=form, refine=3)
+            for (sol, fr, d), x in zip(sub, xs):
+                disp, trac = unswap_host(x, d.kode, d.bc, sol.material[0])
+                da, ta = sol.solve_frequency(fr)
+                assert rel(disp, da) < tol and rel(trac, ta) < tol, (form, sol.nn, fr)
+    driver.close()
+    for p in probs + extra:
+        p[0].ctx.close()
