@@ -47,10 +47,14 @@ constexpr int kPrefetch = 3;  // C tiles prefetched into L2 ahead of the current
 constexpr int kKPitch = 256;  // floats per packed operand row: K up to 256 (four 64-column panels)
 constexpr size_t kTcSmem = (size_t)kStages * kStageBytes + 2 * kHalfBytes + 1024;
 
-__device__ __forceinline__ uint32_t idesc_tf32_128x128() {
-  // c_format F32 (bit 4), a/b format TF32 = 2 (bits 7, 10), K-major A and B,
-  // N >> 3 at bit 17, M >> 4 at bit 24.
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcCols >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+// Instruction descriptor, M = 128, N = 256: c_format F32 (bit 4), a/b format
+// TF32 = 2 (bits 7, 10), K-major A and B, N >> 3 at bit 17, M >> 4 at bit
+// 24.  U_re and U_im of a stage (128 rows each, adjacent in shared memory in
+// the same swizzled K-major layout) form one 256-row B, so one MMA per K
+// step writes both products into 256 accumulator columns (the U_re part in
+// columns 0..127, the U_im part in 128..255).
+__device__ __forceinline__ uint32_t idesc_tf32_128x256() {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(2 * kTcCols >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
 
 // Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
@@ -97,8 +101,7 @@ __device__ __forceinline__ void umma_tf32(uint32_t dtmem, uint64_t adesc, uint64
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-      : "memory");
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
@@ -156,9 +159,24 @@ __device__ __forceinline__ void tile_of(int t, const TcArgs& a, int& b, int& tm,
   tm = bi * a.band + r2 % bm;
 }
 
-// Bounded wait; on timeout raise the kernel-wide abort flag and the status word.
+// Non-blocking test of an mbarrier phase.
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Bounded wait; on timeout raise the kernel-wide abort flag and the status
+// word.  A phase that has already completed is taken by one test, with no
+// flag read and no suspend: the single MMA-issuing thread waits once per
+// stage, and a blocking wait there cost a large share of the tensor pipe.
 __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* status,
                                               unsigned long long limit_ns) {
+  if (mbar_test(bar, parity)) return true;
   if (*abort_flag) return false;
   if (mbar_wait(bar, parity, limit_ns)) return true;
   *abort_flag = 1;
@@ -244,7 +262,14 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
     }
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer ----
-    const uint32_t idesc = idesc_tf32_128x128();
+    // One thread issues every MMA of the CTA, so its instruction stream is
+    // on the critical path: a K = 8 step of both products is 140 tensor
+    // cycles, and building three descriptors per step from addresses took
+    // about as long.  Descriptors are the stage-0 Lhat descriptor plus
+    // constant offsets (the 14-bit start-address field holds addr >> 4 of a
+    // shared window below 256 KB, so the adds never carry out of it).
+    const uint32_t idesc = idesc_tf32_128x256();
+    const uint64_t dbase = sdesc(smem_u32(ring));
     int s = 0;
     uint32_t ph = 0;
     int it = 0;
@@ -253,23 +278,23 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __grid_constant__ CUte
       const int buf = it & 1;
       if (!wait_or_abort(&t_empty[buf], ((uint32_t)(it >> 1) & 1u) ^ 1u, abort_flag, a.status, wlim)) break;
       tc_fence_after();
-      const uint32_t d1 = tmem + (uint32_t)buf * 256u, d2 = d1 + 128u;
+      const uint32_t d1 = tmem + (uint32_t)buf * 256u;
       for (int h = 0; h < nchunks; ++h) {
         if (!wait_or_abort(&full[s], ph, abort_flag, a.status, wlim)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        const uint32_t sbase = smem_u32(ring + (size_t)s * kStageBytes);
+        const uint64_t da = dbase + (uint64_t)(((uint32_t)s * kStageBytes) >> 4);
+        const uint64_t du = da + (kChunk >> 4);  // U_re then U_im: one N = 256 operand
         const int ks = min(4, (a.kw - 32 * h) / 8);
-        for (int kk = 0; kk < ks; ++kk) {
-          const uint32_t off = (uint32_t)kk * 32u;
-          const uint64_t da = sdesc(sbase + off);
-          const uint64_t dre = sdesc(sbase + kChunk + off);
-          const uint64_t dim = sdesc(sbase + 2 * kChunk + off);
-          const uint32_t acc = (h > 0 || kk > 0) ? 1u : 0u;
-          umma_tf32(d1, da, dre, idesc, acc);
-          umma_tf32(d2, da, dim, idesc, acc);
+        const uint32_t acc0 = h > 0 ? 1u : 0u;
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+          if (kk < ks) {
+            const uint64_t o = (uint64_t)(2 * kk);  // 32 bytes of K
+            umma_tf32(d1, da + o, du + o, idesc, acc0 | (uint32_t)kk);
+          }
         }
         umma_commit(&empty[s]);
         if (++s == kStages) {
@@ -383,8 +408,7 @@ __device__ __forceinline__ void umma_tf32_pair(uint32_t dtmem, uint64_t adesc, u
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-      : "memory");
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 // Arrives on the mbarrier at the same offset in both CTAs of the pair once the
 // MMAs issued so far are complete.
@@ -474,6 +498,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc2(const __grid_constant__ CUt
     // ---- MMA issuer of the pair ----
     const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcCols >> 3) << 17) |
                            ((uint32_t)(256 >> 4) << 24);
+    const uint64_t dbase = sdesc(smem_u32(ring));  // as in k_gemm_tc: constant offsets from one descriptor
     int s = 0;
     uint32_t ph = 0;
     int it = 0;
@@ -489,16 +514,17 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc2(const __grid_constant__ CUt
           break;
         }
         tc_fence_after();
-        const uint32_t sbase = smem_u32(ring + (size_t)s * kStage2Bytes);
+        const uint64_t da = dbase + (uint64_t)(((uint32_t)s * kStage2Bytes) >> 4);
+        const uint64_t dre = da + (kChunk >> 4), dim = da + ((kChunk + kHalfChunk) >> 4);
         const int ks = min(4, (a.kw - 32 * h) / 8);
-        for (int kk = 0; kk < ks; ++kk) {
-          const uint32_t off = (uint32_t)kk * 32u;
-          const uint64_t da = sdesc(sbase + off);
-          const uint64_t dre = sdesc(sbase + kChunk + off);
-          const uint64_t dim = sdesc(sbase + kChunk + kHalfChunk + off);
-          const uint32_t acc = (h > 0 || kk > 0) ? 1u : 0u;
-          umma_tf32_pair(d1, da, dre, idesc, acc);
-          umma_tf32_pair(d2, da, dim, idesc, acc);
+        const uint32_t acc0 = h > 0 ? 1u : 0u;
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+          if (kk < ks) {
+            const uint64_t o = (uint64_t)(2 * kk);
+            umma_tf32_pair(d1, da + o, dre + o, idesc, acc0 | (uint32_t)kk);
+            umma_tf32_pair(d2, da + o, dim + o, idesc, acc0 | (uint32_t)kk);
+          }
         }
         umma_commit_pair(&empty[s]);
         if (++s == kStages2) {
