@@ -217,7 +217,7 @@ struct bem_ctx {
   bool lu_pairs = true;       // FP32 tensor-core LU: two 64-column panels per trailing update (K = 128)
   bool lu_quads = true;       // ... four (K = 256) where four 64-column panels fit
   bool f64_pairs = true;      // FP64 LU: two panels per trailing update (K = 2 x panel width)
-  bool tc_pair = false;       // FP32 trailing update by CTA pairs (k_gemm_tc2, tcgen05 cta_group::2)
+  bool tc_pair = true;        // FP32 trailing update by CTA pairs (k_gemm_tc2, tcgen05 cta_group::2)
   bool small_clusters = true; // panel clusters sized to the system (<= 256 rows per CTA), not always 16
   bool panel_tslu = false;    // FP32 panels taller than a cluster: tournament pivoting instead of the grid kernel
   // SM shares for contexts that run concurrently on one GPU (0: the whole device)

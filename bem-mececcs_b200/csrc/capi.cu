@@ -164,7 +164,7 @@ int bem_ctx_create(int device, bem_ctx** out) {
   if (const char* env = getenv("BEM_LU_QUADS")) ctx->lu_quads = env[0] != '0';
   if (const char* env = getenv("BEM_PANEL_ASYNC")) ctx->panel_async = env[0] != '0';
   if (const char* env = getenv("BEM_F64_PAIRS")) ctx->f64_pairs = env[0] != '0';
-  if (const char* env = getenv("BEM_TC_PAIR")) ctx->tc_pair = env[0] == '1';
+  if (const char* env = getenv("BEM_TC_PAIR")) ctx->tc_pair = env[0] != '0';
   if (const char* env = getenv("BEM_SMALL_CLUSTERS")) ctx->small_clusters = env[0] != '0';
   if (const char* env = getenv("BEM_PANEL_TSLU")) ctx->panel_tslu = env[0] == '1';
   *out = ctx;

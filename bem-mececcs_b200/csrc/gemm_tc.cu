@@ -496,7 +496,11 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc2(const __grid_constant__ CUt
     }
   } else if (warp == 1 && lane == 0 && even) {
     // ---- MMA issuer of the pair ----
-    const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcCols >> 3) << 17) |
+    // M = 256 (the pair's rows), N = 256: each CTA's 64 U_re and 64 U_im rows
+    // of a stage are adjacent, so B is one 128-row operand per CTA and one
+    // MMA per K step fills 256 accumulator columns: [U_re 0..63 | U_im 0..63]
+    // from the even CTA's rows, then [U_re 64..127 | U_im 64..127].
+    const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(2 * kTcCols >> 3) << 17) |
                            ((uint32_t)(256 >> 4) << 24);
     const uint64_t dbase = sdesc(smem_u32(ring));  // as in k_gemm_tc: constant offsets from one descriptor
     int s = 0;
@@ -507,7 +511,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc2(const __grid_constant__ CUt
       const int buf = it & 1;
       if (!wait_or_abort(&t_empty[buf], ((uint32_t)(it >> 1) & 1u) ^ 1u, abort_flag, a.status, wlim)) break;
       tc_fence_after();
-      const uint32_t d1 = tmem + (uint32_t)buf * 256u, d2 = d1 + 128u;
+      const uint32_t d1 = tmem + (uint32_t)buf * 256u;
       for (int h = 0; h < nchunks; ++h) {
         if (!wait_or_abort(&full[s], ph, abort_flag, a.status, wlim)) {
           ok = false;
@@ -515,15 +519,14 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc2(const __grid_constant__ CUt
         }
         tc_fence_after();
         const uint64_t da = dbase + (uint64_t)(((uint32_t)s * kStage2Bytes) >> 4);
-        const uint64_t dre = da + (kChunk >> 4), dim = da + ((kChunk + kHalfChunk) >> 4);
+        const uint64_t du = da + (kChunk >> 4);
         const int ks = min(4, (a.kw - 32 * h) / 8);
         const uint32_t acc0 = h > 0 ? 1u : 0u;
 #pragma unroll
         for (int kk = 0; kk < 4; ++kk) {
           if (kk < ks) {
             const uint64_t o = (uint64_t)(2 * kk);
-            umma_tf32_pair(d1, da + o, dre + o, idesc, acc0 | (uint32_t)kk);
-            umma_tf32_pair(d2, da + o, dim + o, idesc, acc0 | (uint32_t)kk);
+            umma_tf32_pair(d1, da + o, du + o, idesc, acc0 | (uint32_t)kk);
           }
         }
         umma_commit_pair(&empty[s]);
@@ -553,9 +556,11 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc2(const __grid_constant__ CUt
       const uint32_t tbase = tmem + (uint32_t)buf * 256u + ((uint32_t)(32 * e) << 16);
       for (int hc = 0; hc < 2; ++hc) {
         float* ct = stage_c + (size_t)hc * (kHalfBytes / 4);
+        // columns 64 hc .. 64 hc + 63 of the tile: the U_re part at
+        // accumulator columns 128 hc.., the U_im part 64 further
         float v1[64], v2[64];
-        tmem_ld64(tbase + (uint32_t)(64 * hc), v1);
-        tmem_ld64(tbase + 128u + (uint32_t)(64 * hc), v2);
+        tmem_ld64(tbase + (uint32_t)(128 * hc), v1);
+        tmem_ld64(tbase + (uint32_t)(128 * hc + 64), v2);
         tmem_ld_wait();
         if (issuer) tma_wait_read_1();
         epi_bar_sync();

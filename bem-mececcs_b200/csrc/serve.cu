@@ -45,6 +45,7 @@ using Clock = std::chrono::steady_clock;
 // the other's updates.
 constexpr int kMaxInflight = 16;
 constexpr int kMaxSlotsBusy = 8;
+constexpr int kDefer = -2;  // try_start: wait for a fuller lockstep batch
 
 double ms_between(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
@@ -126,6 +127,7 @@ class Server {
     worker_.join();
     cudaSetDevice(device_);
     for (Slot& s : slots_) destroy_slot(s);
+    if (probe_) bem_ctx_destroy(probe_);
     for (auto& b : pinned_free_) cudaFreeHost(b.second);
     // hand the device memory the slots held back from the stream-ordered pool
     cudaMemPool_t pool;
@@ -234,6 +236,7 @@ class Server {
         }
       for (auto it = queue_.begin(); it != queue_.end() && busy < kMaxInflight && busy_slots < kMaxSlotsBusy;) {
         const int st = try_start(*it, kMaxInflight - busy);
+        if (st == kDefer) break;  // the queue's head waits for a fuller batch
         if (st > 0) {  // the request and any batched with it leave the queue
           ++busy_slots;
           queue_.erase(std::remove_if(queue_.begin(), queue_.end(),
@@ -365,8 +368,23 @@ class Server {
     return out;
   }
 
+  // Problems in lockstep on one slot for an nn-unknown mesh: the panel
+  // kernel's resident limit, at most kMaxBatch (a context of the server's
+  // own answers the occupancy query and caches it per size).
+  int lockstep_cap(int nn) {
+    if (!probe_ && bem_ctx_create(device_, &probe_) != BEM_OK) {
+      probe_ = nullptr;
+      return 1;
+    }
+    std::lock_guard<std::mutex> g(probe_->mu);
+    return std::max(1, std::min(kMaxBatch, lu_lockstep_capacity(probe_, nn, mixed_)));
+  }
+
   // Problems started (the request, and those batched with it), 0 not yet
-  // (waits for memory or a slot), -1 failed.  `room`: problems that may start.
+  // (waits for memory or a slot), -1 failed, kDefer: the request has more
+  // lockstep companions queued than the in-flight limit lets start now
+  // while other solves run, so it waits for a fuller batch (the queue scan
+  // stops there: first come, first served).  `room`: problems that may start.
   int try_start(const std::shared_ptr<SrvRequest>& r, int room) {
     const SrvMesh& m = meshes_[r->mesh];
     const int nn = 3 * m.nbe;
@@ -380,7 +398,12 @@ class Server {
       }
     std::vector<std::shared_ptr<SrvRequest>> batch{r};
     if (!rhs_only) {
-      auto more = companions(r, std::min(room, kMaxBatch));
+      // companions up to the lockstep limit, before any memory is reserved
+      auto more = companions(r, lockstep_cap(nn));
+      if ((int)more.size() + 1 > room) {
+        if (room < kMaxInflight) return kDefer;
+        more.resize(room - 1);
+      }
       batch.insert(batch.end(), more.begin(), more.end());
     }
     const size_t per = slot_footprint(nn, m.nbe, m.npg * m.npg, mixed_) +
@@ -510,6 +533,7 @@ class Server {
   }
 
   int device_;
+  bem_ctx* probe_ = nullptr;  // lockstep-limit queries (loop thread)
   size_t budget_;
   bool mixed_;
   int refine_;

@@ -140,9 +140,9 @@ int bem_ctx_set_stream(bem_ctx *ctx, void *stream);
  * mbarrier-counted mailboxes, without a cluster barrier per column),
  * "laswp_tc" (FP32 row interchanges + U12 on the tensor cores), "trsv_inv"
  * (FP32 solves with inverted diagonal blocks), "graphs" (bem_sweep replays a
- * captured step).  Defaults: tcgen05, trsv_coop, lu_pairs, lu_quads,
- * f64_pairs, small_clusters, panel_push, panel_async, laswp_tc, trsv_inv
- * and graphs on; panel_calu, panel_tslu and tc_pair off (measured no faster
+ * captured step).  Defaults: tcgen05, tc_pair, trsv_coop, lu_pairs,
+ * lu_quads, f64_pairs, small_clusters, panel_push, panel_async, laswp_tc,
+ * trsv_inv and graphs on; panel_calu and panel_tslu off (measured no faster
  * on B200).
  * Integer budgets for a context that shares the GPU with another one running
  * at the same time (0, the default, means the whole device): "gemm_ctas"

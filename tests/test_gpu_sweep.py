@@ -102,13 +102,15 @@ def test_sweep_mixed_cta_pair_update(c1, batch):
     solution at the FP64 level, as the one-CTA update does, and its
     unrefined FP32 solution is as close to the oracle's."""
     s, d, p, sol = c1
-    x1, _ = sol.sweep(FREQS, form="mixed", batch=batch, refine=0)
-    sol.ctx.set_option("tc_pair", True)
+    default = sol.ctx.get_option("tc_pair")
     try:
+        sol.ctx.set_option("tc_pair", False)
+        x1, _ = sol.sweep(FREQS, form="mixed", batch=batch, refine=0)
+        sol.ctx.set_option("tc_pair", True)
         x2, _ = sol.sweep(FREQS, form="mixed", batch=batch, refine=0)
         x3, corr = sol.sweep(FREQS, form="mixed", batch=batch, refine=3)
     finally:
-        sol.ctx.set_option("tc_pair", False)
+        sol.ctx.set_option("tc_pair", default)
     for i, fr in enumerate(FREQS):
         ox = _oracle_x(p, fr)
         e1, e2 = rel(x1[i], ox), rel(x2[i], ox)
