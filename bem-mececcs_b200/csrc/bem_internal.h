@@ -217,6 +217,9 @@ struct bem_ctx {
   bool lu_pairs = true;       // FP32 tensor-core LU: two 64-column panels per trailing update (K = 128)
   bool lu_quads = true;       // ... four (K = 256) where four 64-column panels fit
   bool f64_pairs = true;      // FP64 LU: two panels per trailing update (K = 2 x panel width)
+  bool f64_cublas = true;     // FP64 LU: trailing update by cuBLAS ZGEMM (one panel per update)
+  void* cublas = nullptr;     // cuBLAS handle (f64_cublas), created on first use
+  void* cublas_ws = nullptr;  // its workspace (stream-ordered, so graph capture allocates nothing)
   bool tc_pair = true;        // FP32 trailing update by CTA pairs (k_gemm_tc2, tcgen05 cta_group::2)
   bool small_clusters = true; // panel clusters sized to the system (<= 256 rows per CTA), not always 16
   bool panel_tslu = false;    // FP32 panels taller than a cluster: tournament pivoting instead of the grid kernel
@@ -280,6 +283,7 @@ int dyn_graph_update(bem_ctx* ctx, cudaGraphExec_t exec, const std::vector<cudaG
                      const DynBatch& b);
 int dyn_graph_nodes(bem_ctx* ctx, cudaGraph_t g, std::vector<cudaGraphNode_t>& out);
 int launch_dynamic_batch(bem_ctx* ctx, const DynBatch& b);
+void release_cublas(bem_ctx* ctx);
 // One member of a grouped assembly (bem_batch_solve).
 struct GroupMember {
   bem_ctx* pc;  // the problem's context: mesh, static diagonals, BCs

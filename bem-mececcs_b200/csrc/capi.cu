@@ -164,6 +164,7 @@ int bem_ctx_create(int device, bem_ctx** out) {
   if (const char* env = getenv("BEM_LU_QUADS")) ctx->lu_quads = env[0] != '0';
   if (const char* env = getenv("BEM_PANEL_ASYNC")) ctx->panel_async = env[0] != '0';
   if (const char* env = getenv("BEM_F64_PAIRS")) ctx->f64_pairs = env[0] != '0';
+  if (const char* env = getenv("BEM_F64_CUBLAS")) ctx->f64_cublas = env[0] != '0';
   if (const char* env = getenv("BEM_TC_PAIR")) ctx->tc_pair = env[0] != '0';
   if (const char* env = getenv("BEM_SMALL_CLUSTERS")) ctx->small_clusters = env[0] != '0';
   if (const char* env = getenv("BEM_PANEL_TSLU")) ctx->panel_tslu = env[0] == '1';
@@ -213,6 +214,7 @@ int bem_ctx_destroy(bem_ctx* ctx) {
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   release_sweep(ctx);
   release_interior(ctx);
+  release_cublas(ctx);
   tc_release(ctx);
   for (cudaEvent_t e : ctx->prof.pool) cudaEventDestroy(e);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -577,6 +579,7 @@ static bool* option_slot(bem_ctx* ctx, const char* name) {
   if (!strcmp(name, "lu_pairs")) return &ctx->lu_pairs;
   if (!strcmp(name, "lu_quads")) return &ctx->lu_quads;
   if (!strcmp(name, "f64_pairs")) return &ctx->f64_pairs;
+  if (!strcmp(name, "f64_cublas")) return &ctx->f64_cublas;
   if (!strcmp(name, "tc_pair")) return &ctx->tc_pair;
   if (!strcmp(name, "small_clusters")) return &ctx->small_clusters;
   if (!strcmp(name, "panel_tslu")) return &ctx->panel_tslu;

@@ -32,6 +32,7 @@
 // Row interchanges are never applied to columns left of a panel; each panel's
 // interchanges are kept (ipiv and a dst/src gather list) so that later solves
 // can replay them in panel order.
+#include <cublas_v2.h>
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -3567,6 +3568,45 @@ static int lockstep_capacity_t(bem_ctx* ctx, int nn) {
 
 // Problems whose panels run in one wave: the first (tallest) panel's cluster
 // kernel, as many clusters as can be resident at once.
+// FP64 trailing update by cuBLAS (option f64_cublas): C -= L21 U12 for rows
+// [c0, nn) and columns [c0, ncols) of `batch` systems, one strided-batched
+// ZGEMM (the plain library GEMM, FP64 tensor cores).  The handle and a fixed
+// workspace are made once per context, so a captured graph allocates nothing.
+constexpr size_t kCublasWorkspace = (size_t)32 << 20;
+
+int f64_update_cublas(bem_ctx* ctx, double2* A, size_t lda, size_t bstride, int nn, int k, int w, int c0, int ncols,
+                      int batch) {
+  if (!ctx->cublas) {
+    cublasHandle_t h = nullptr;
+    if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) return fail(ctx, BEM_ERR_CUDA, "cublasCreate failed");
+    ctx->cublas = h;
+    BEM_CUDA(ctx, dev_alloc(ctx, reinterpret_cast<unsigned char**>(&ctx->cublas_ws), kCublasWorkspace));
+    BEM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (cublasSetWorkspace(h, ctx->cublas_ws, kCublasWorkspace) != CUBLAS_STATUS_SUCCESS)
+      return fail(ctx, BEM_ERR_CUDA, "cublasSetWorkspace failed");
+  }
+  cublasHandle_t h = static_cast<cublasHandle_t>(ctx->cublas);
+  if (cublasSetStream(h, ctx->stream) != CUBLAS_STATUS_SUCCESS) return fail(ctx, BEM_ERR_CUDA, "cublasSetStream failed");
+  const cuDoubleComplex minus_one = make_cuDoubleComplex(-1.0, 0.0), one = make_cuDoubleComplex(1.0, 0.0);
+  cuDoubleComplex* a = reinterpret_cast<cuDoubleComplex*>(A);
+  const int m = nn - c0, n = ncols - c0;
+  if (m <= 0 || n <= 0 || w <= 0) return BEM_OK;
+  const cublasStatus_t st = cublasZgemmStridedBatched(
+      h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, w, &minus_one, a + (size_t)k * lda + c0, (int)lda, (long long)bstride,
+      a + (size_t)c0 * lda + k, (int)lda, (long long)bstride, &one, a + (size_t)c0 * lda + c0, (int)lda,
+      (long long)bstride, batch);
+  if (st != CUBLAS_STATUS_SUCCESS) return fail(ctx, BEM_ERR_CUDA, "cublasZgemmStridedBatched failed");
+  ctx->launches++;
+  return BEM_OK;
+}
+
+void release_cublas(bem_ctx* ctx) {
+  if (ctx->cublas) cublasDestroy(static_cast<cublasHandle_t>(ctx->cublas));
+  ctx->cublas = nullptr;
+  dev_free(ctx, ctx->cublas_ws);
+  ctx->cublas_ws = nullptr;
+}
+
 int lu_lockstep_capacity(bem_ctx* ctx, int nn, bool fp32) {
   // occupancy queries are host calls of tens of microseconds: remember each answer
   const long long key = 4LL * nn + (fp32 ? 1 : 0) + (ctx->small_clusters ? 2 : 0);
@@ -4059,7 +4099,7 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     // rest is one K = 2 nb update whose first nb columns read panel 1's L
     // through the same list.  A keeps the factors of the one-panel-at-a-time
     // LU, so the solves are unchanged.
-    const int nbp = sizeof(R) == 8 && ctx->f64_pairs ? panel_nb(m) : 0;
+    const int nbp = sizeof(R) == 8 && ctx->f64_pairs && !ctx->f64_cublas ? panel_nb(m) : 0;
     if (nbp > 0 && m > 2 * nbp && panel_nb(m - nbp) == nbp) {
       double2* A2 = static_cast<double2*>(A);
       int w1 = 0, w2 = 0, *p1 = nullptr, *p2 = nullptr;
@@ -4113,6 +4153,9 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
             rc = tc_gemm(ctx, static_cast<float2*>(A), lda, bstride, nn, c0, c0, nn + 1, w, 0, batch, 0);
           else
             rc = tc_trailing_update(ctx, static_cast<float2*>(A), lda, bstride, nn, k, w, batch);
+          if (rc) return rc;
+        } else if (sizeof(R) == 8 && ctx->f64_cublas) {
+          rc = f64_update_cublas(ctx, static_cast<double2*>(A), lda, bstride, nn, k, w, c0, ncols, batch);
           if (rc) return rc;
         } else if (sizeof(R) == 8) {
           dim3 grid((nn - c0 + GBM - 1) / GBM, (cols + GBN - 1) / GBN, batch);

@@ -52,7 +52,8 @@ WORKLOAD = ("2160 boundary elements (48x45 quads over [-5,5]^2 at z=0, +-10% int
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40,
+                    help="timed lockstep steps (40: about 2 s, so the clock sampler sees the timed region)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -126,8 +126,11 @@ int bem_ctx_set_stream(bem_ctx *ctx, void *stream);
  * autotuner: "tcgen05" (FP32 trailing update on tcgen05, else TF32
  * mma.sync), "trsv_coop" (one cooperative launch per triangular solve),
  * "lu_pairs" (two 64-column panels per FP32 trailing update, K = 128),
- * "lu_quads" (four, K = 256, where they fit), "f64_pairs" (FP64 LU: two
- * panels per trailing update, K = twice the panel width), "tc_pair" (the FP32
+ * "lu_quads" (four, K = 256, where they fit), "f64_cublas" (FP64 LU: the
+ * trailing update by cuBLAS ZGEMM, one panel per update; the plain FP64
+ * form's library GEMM), "f64_pairs" (FP64 LU with f64_cublas off: two
+ * panels per trailing update on the DMMA kernel, K = twice the panel
+ * width), "tc_pair" (the FP32
  * trailing update by CTA pairs on tcgen05 cta_group::2, M = 256 per pair),
  * "small_clusters" (panel clusters of 2, 4 or 8 CTAs for systems whose
  * panel rows fit them at <= 256 rows per CTA, instead of always 16),
@@ -141,9 +144,9 @@ int bem_ctx_set_stream(bem_ctx *ctx, void *stream);
  * "laswp_tc" (FP32 row interchanges + U12 on the tensor cores), "trsv_inv"
  * (FP32 solves with inverted diagonal blocks), "graphs" (bem_sweep replays a
  * captured step).  Defaults: tcgen05, tc_pair, trsv_coop, lu_pairs,
- * lu_quads, f64_pairs, small_clusters, panel_push, panel_async, laswp_tc,
- * trsv_inv and graphs on; panel_calu and panel_tslu off (measured no faster
- * on B200).
+ * lu_quads, f64_cublas, f64_pairs, small_clusters, panel_push, panel_async,
+ * laswp_tc, trsv_inv and graphs on; panel_calu and panel_tslu off (measured
+ * no faster on B200).
  * Integer budgets for a context that shares the GPU with another one running
  * at the same time (0, the default, means the whole device): "gemm_ctas"
  * (CTAs of the persistent FP32 trailing update) and "trsv_ctas" (CTAs of one
