@@ -112,6 +112,8 @@ struct LuWork {
   float2* tinv = nullptr;        // FP32 solves: inverted diagonal blocks of the last factors
   size_t tinv_bytes = 0;
   bool tinv_valid = false;
+  double2* lg = nullptr;         // FP64 panel pairs on cuBLAS: both panels' L, the first gathered
+  size_t lg_cap = 0;             // elements
 };
 
 constexpr int kMaxGrid = 160;

@@ -208,6 +208,7 @@ int bem_ctx_destroy(bem_ctx* ctx) {
   dev_free(ctx, L.ts_gid);
   dev_free(ctx, L.ts_cipiv);
   dev_free(ctx, L.ts_cperm);
+  dev_free(ctx, L.lg);
   dev_free(ctx, ctx->grp_desc);
   for (bem_ctx* w : ctx->workers) bem_ctx_destroy(w);
   ctx->workers.clear();

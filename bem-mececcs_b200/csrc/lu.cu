@@ -3561,21 +3561,25 @@ static int lockstep_capacity_t(bem_ctx* ctx, int nn) {
     if (nb == 64) n = big ? cluster_capacity<R, 64, 512>(cs, rp) : cluster_capacity<R, 64, 256>(cs, rp);
     if (nb == 32) n = big ? cluster_capacity<R, 32, 512>(cs, rp) : cluster_capacity<R, 32, 256>(cs, rp);
     if (nb == 16) n = big ? cluster_capacity<R, 16, 512>(cs, rp) : cluster_capacity<R, 16, 256>(cs, rp);
-    return n >= 1 ? std::min(n, kMaxBatch) : kMaxBatch;
+    // At most one CTA per SM: clusters that share SMs (the occupancy query
+    // allows two CTAs per SM for short panels) measured 2.75x the time of a
+    // one-per-SM launch, where two launches of half the problems take 2x.
+    const int one_per_sm = std::max(1, ctx->num_sms / cs);
+    return n >= 1 ? std::min({n, one_per_sm, kMaxBatch}) : std::min(one_per_sm, kMaxBatch);
   }
   return kMaxBatch;
 }
 
-// Problems whose panels run in one wave: the first (tallest) panel's cluster
-// kernel, as many clusters as can be resident at once.
-// FP64 trailing update by cuBLAS (option f64_cublas): C -= L21 U12 for rows
-// [c0, nn) and columns [c0, ncols) of `batch` systems, one strided-batched
-// ZGEMM (the plain library GEMM, FP64 tensor cores).  The handle and a fixed
+// FP64 trailing update by cuBLAS (option f64_cublas): C -= L U for rows
+// [r0, nn) and columns [c0, cend) of `batch` systems, one strided-batched
+// ZGEMM (the plain library GEMM, FP64 tensor cores).  L is A's columns
+// kcol..kcol+kw-1 at rows r0.., or `lg` (ld nn - r0, lg_stride per problem);
+// U is A's rows kcol..kcol+kw-1 at columns c0...  The handle and a fixed
 // workspace are made once per context, so a captured graph allocates nothing.
 constexpr size_t kCublasWorkspace = (size_t)32 << 20;
 
-int f64_update_cublas(bem_ctx* ctx, double2* A, size_t lda, size_t bstride, int nn, int k, int w, int c0, int ncols,
-                      int batch) {
+int f64_gemm_cublas(bem_ctx* ctx, double2* A, size_t lda, size_t bstride, int nn, int kcol, int kw, int r0, int c0,
+                    int cend, int batch, const double2* lg, size_t lg_stride) {
   if (!ctx->cublas) {
     cublasHandle_t h = nullptr;
     if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) return fail(ctx, BEM_ERR_CUDA, "cublasCreate failed");
@@ -3587,17 +3591,53 @@ int f64_update_cublas(bem_ctx* ctx, double2* A, size_t lda, size_t bstride, int 
   }
   cublasHandle_t h = static_cast<cublasHandle_t>(ctx->cublas);
   if (cublasSetStream(h, ctx->stream) != CUBLAS_STATUS_SUCCESS) return fail(ctx, BEM_ERR_CUDA, "cublasSetStream failed");
+  const int m = nn - r0, n = cend - c0;
+  if (m <= 0 || n <= 0 || kw <= 0) return BEM_OK;
   const cuDoubleComplex minus_one = make_cuDoubleComplex(-1.0, 0.0), one = make_cuDoubleComplex(1.0, 0.0);
   cuDoubleComplex* a = reinterpret_cast<cuDoubleComplex*>(A);
-  const int m = nn - c0, n = ncols - c0;
-  if (m <= 0 || n <= 0 || w <= 0) return BEM_OK;
+  const cuDoubleComplex* l = lg ? reinterpret_cast<const cuDoubleComplex*>(lg) : a + (size_t)kcol * lda + r0;
+  const int ldl = lg ? m : (int)lda;
+  const long long sl = lg ? (long long)lg_stride : (long long)bstride;
   const cublasStatus_t st = cublasZgemmStridedBatched(
-      h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, w, &minus_one, a + (size_t)k * lda + c0, (int)lda, (long long)bstride,
-      a + (size_t)c0 * lda + k, (int)lda, (long long)bstride, &one, a + (size_t)c0 * lda + c0, (int)lda,
-      (long long)bstride, batch);
+      h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, kw, &minus_one, l, ldl, sl, a + (size_t)c0 * lda + kcol, (int)lda,
+      (long long)bstride, &one, a + (size_t)c0 * lda + r0, (int)lda, (long long)bstride, batch);
   if (st != CUBLAS_STATUS_SUCCESS) return fail(ctx, BEM_ERR_CUDA, "cublasZgemmStridedBatched failed");
   ctx->launches++;
   return BEM_OK;
+}
+
+int f64_update_cublas(bem_ctx* ctx, double2* A, size_t lda, size_t bstride, int nn, int k, int w, int c0, int ncols,
+                      int batch) {
+  return f64_gemm_cublas(ctx, A, lda, bstride, nn, k, w, c0, c0, ncols, batch, nullptr, 0);
+}
+
+// L of an FP64 panel pair for its update past the pair (rows r0.. of columns
+// k..k+w1+w2-1): the first panel's columns read through the second panel's
+// gather list (count, then dst/src pairs; row dst of C takes L from row src,
+// as k_gemm_f64 with gperm does), the second panel's as they are.  Out:
+// column-major, ld nn - r0, problem b at out + b * ostride.
+__global__ void __launch_bounds__(256) k_gather_l_pair(const double2* __restrict__ Abase, size_t lda, size_t bstride,
+                                                       int nn, int k, int w1, int w2, int r0,
+                                                       const int* __restrict__ gperm, int gperm_stride,
+                                                       double2* __restrict__ out, size_t ostride) {
+  __shared__ int s_map[256];
+  const int b = blockIdx.y, tid = threadIdx.x;
+  const int row0 = r0 + blockIdx.x * 256, r = row0 + tid;
+  const double2* A = Abase + (size_t)b * bstride;
+  double2* o = out + (size_t)b * ostride;
+  const int m = nn - r0;
+  s_map[tid] = r;
+  __syncthreads();
+  const int* pl = gperm + (size_t)b * gperm_stride;
+  const int cnt = pl[0];
+  for (int e = tid; e < cnt; e += blockDim.x) {
+    const int dst = pl[1 + 2 * e];
+    if (dst >= row0 && dst < row0 + 256) s_map[dst - row0] = pl[2 + 2 * e];
+  }
+  __syncthreads();
+  if (r >= nn) return;
+  const int src = s_map[tid];
+  for (int c = 0; c < w1 + w2; ++c) o[(size_t)c * m + (r - r0)] = A[(size_t)(k + c) * lda + (c < w1 ? src : r)];
 }
 
 void release_cublas(bem_ctx* ctx) {
@@ -3607,6 +3647,8 @@ void release_cublas(bem_ctx* ctx) {
   ctx->cublas_ws = nullptr;
 }
 
+// Problems whose panels run in one wave: the first (tallest) panel's cluster
+// kernel, as many clusters as can be resident at once.
 int lu_lockstep_capacity(bem_ctx* ctx, int nn, bool fp32) {
   // occupancy queries are host calls of tens of microseconds: remember each answer
   const long long key = 4LL * nn + (fp32 ? 1 : 0) + (ctx->small_clusters ? 2 : 0);
@@ -4099,7 +4141,7 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
     // rest is one K = 2 nb update whose first nb columns read panel 1's L
     // through the same list.  A keeps the factors of the one-panel-at-a-time
     // LU, so the solves are unchanged.
-    const int nbp = sizeof(R) == 8 && ctx->f64_pairs && !ctx->f64_cublas ? panel_nb(m) : 0;
+    const int nbp = sizeof(R) == 8 && ctx->f64_pairs ? panel_nb(m) : 0;
     if (nbp > 0 && m > 2 * nbp && panel_nb(m - nbp) == nbp) {
       double2* A2 = static_cast<double2*>(A);
       int w1 = 0, w2 = 0, *p1 = nullptr, *p2 = nullptr;
@@ -4112,11 +4154,16 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
       {  // panel 1's update of panel 2's columns
         ProfScope ps(ctx, 3, 8.0 * (double)(nn - k2) * (double)nbp * (double)w1 * batch,
                      2.0 * (double)(nn - k2) * (double)nbp * es * batch);
-        dim3 grid((nn - k2 + GBM - 1) / GBM, (nbp + GBN - 1) / GBN, batch);
-        k_gemm_f64<<<grid, 256, kGemmSmem, ctx->stream>>>(A2, lda, bstride, nn, k, w1, k2, k2, k2 + nbp, nullptr,
-                                                         0, 0);
-        ctx->launches++;
-        BEM_CUDA(ctx, cudaGetLastError());
+        if (ctx->f64_cublas) {
+          rc = f64_gemm_cublas(ctx, A2, lda, bstride, nn, k, w1, k2, k2, k2 + nbp, batch, nullptr, 0);
+          if (rc) return rc;
+        } else {
+          dim3 grid((nn - k2 + GBM - 1) / GBM, (nbp + GBN - 1) / GBN, batch);
+          k_gemm_f64<<<grid, 256, kGemmSmem, ctx->stream>>>(A2, lda, bstride, nn, k, w1, k2, k2, k2 + nbp, nullptr,
+                                                           0, 0);
+          ctx->launches++;
+          BEM_CUDA(ctx, cudaGetLastError());
+        }
       }
       rc = run_panel(k2, w2, p2);
       if (rc) return rc;
@@ -4127,11 +4174,31 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
         const int cols = ncols - kG;
         ProfScope ps(ctx, 3, 8.0 * (double)(nn - kG) * (double)cols * (double)(w1 + w2) * batch,
                      2.0 * (double)(nn - kG) * (double)cols * es * batch);
-        dim3 grid((nn - kG + GBM - 1) / GBM, (cols + GBN - 1) / GBN, batch);
-        k_gemm_f64<<<grid, 256, kGemmSmem, ctx->stream>>>(A2, lda, bstride, nn, k, w1 + w2, kG, kG, ncols, p2,
-                                                         kPermStride, w1);
-        ctx->launches++;
-        BEM_CUDA(ctx, cudaGetLastError());
+        if (ctx->f64_cublas) {
+          // both panels' L in one buffer (the first through the second's
+          // gather list), then one ZGEMM with K = w1 + w2
+          LuWork& LW = ctx->lu;
+          const size_t per = (size_t)(nn - kG) * (w1 + w2), need = per * batch;
+          if (LW.lg_cap < need) {
+            dev_free(ctx, LW.lg);
+            LW.lg = nullptr;
+            LW.lg_cap = 0;
+            BEM_CUDA(ctx, dev_alloc(ctx, &LW.lg, need * sizeof(double2)));
+            LW.lg_cap = need;
+          }
+          k_gather_l_pair<<<dim3((nn - kG + 255) / 256, batch), 256, 0, ctx->stream>>>(
+              A2, lda, bstride, nn, k, w1, w2, kG, p2, kPermStride, LW.lg, per);
+          ctx->launches++;
+          BEM_CUDA(ctx, cudaGetLastError());
+          rc = f64_gemm_cublas(ctx, A2, lda, bstride, nn, k, w1 + w2, kG, kG, ncols, batch, LW.lg, per);
+          if (rc) return rc;
+        } else {
+          dim3 grid((nn - kG + GBM - 1) / GBM, (cols + GBN - 1) / GBN, batch);
+          k_gemm_f64<<<grid, 256, kGemmSmem, ctx->stream>>>(A2, lda, bstride, nn, k, w1 + w2, kG, kG, ncols, p2,
+                                                           kPermStride, w1);
+          ctx->launches++;
+          BEM_CUDA(ctx, cudaGetLastError());
+        }
       }
       k = kG;
       continue;

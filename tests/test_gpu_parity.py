@@ -43,22 +43,23 @@ def test_lu_random(ctx, n):
     assert rel(x, ref) < 1e-11 * max(1.0, np.linalg.cond(a) / 100)
 
 
-@pytest.mark.parametrize("scheme", ["cublas", "f64_pairs", "one_panel"])
+@pytest.mark.parametrize("scheme", ["cublas_pairs", "cublas", "f64_pairs", "one_panel"])
 def test_lu_tall_panels_pairs(ctx, scheme):
     """n = 4000: the FP64 panels above 3440 rows are 32 columns wide, so two
-    of them share one K = 64 trailing update (f64_pairs, own DMMA kernel),
-    the first panel's L read through the second's gather list.  Rows are
-    shuffled so that every panel pivots across the pair; the result must not
-    depend on the scheme: cuBLAS ZGEMM per panel (f64_cublas, the default),
-    pairs on the DMMA kernel, or one panel at a time on it."""
+    of them share one K = 64 trailing update (f64_pairs), the first panel's L
+    read through the second's gather list.  Rows are shuffled so that every
+    panel pivots across the pair; the result must not depend on the scheme:
+    pairs on cuBLAS ZGEMM with the gathered L in a buffer (the default), one
+    panel per cuBLAS update, pairs on the own DMMA kernel, or one panel at a
+    time on it."""
     n = 4000
     rng = np.random.default_rng(40)
     a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
     a = a[rng.permutation(n)] * np.exp(rng.uniform(-3, 3, n))[:, None]  # uneven row scales: real pivoting
     b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
     defaults = {k: ctx.get_option(k) for k in ("f64_cublas", "f64_pairs")}
-    ctx.set_option("f64_cublas", scheme == "cublas")
-    ctx.set_option("f64_pairs", scheme == "f64_pairs")
+    ctx.set_option("f64_cublas", scheme.startswith("cublas"))
+    ctx.set_option("f64_pairs", scheme in ("cublas_pairs", "f64_pairs"))
     try:
         x = solve_dense(ctx, a, b)
     finally:
