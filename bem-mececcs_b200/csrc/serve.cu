@@ -46,6 +46,11 @@ using Clock = std::chrono::steady_clock;
 constexpr int kMaxInflight = 16;
 constexpr int kMaxSlotsBusy = 8;
 constexpr int kDefer = -2;  // try_start: wait for a fuller lockstep batch
+// A request that could lead a lockstep batch (same mesh, material, BCs and
+// KODE, other omegas) but has fewer companions queued than the batch holds
+// waits this long after its submission for more to arrive: a sweep submitted
+// request by request then forms full batches instead of a first batch of one.
+constexpr double kBatchWindowMs = 2.0;
 
 double ms_between(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
@@ -399,10 +404,13 @@ class Server {
     std::vector<std::shared_ptr<SrvRequest>> batch{r};
     if (!rhs_only) {
       // companions up to the lockstep limit, before any memory is reserved
-      auto more = companions(r, lockstep_cap(nn));
+      const int cap = lockstep_cap(nn);
+      auto more = companions(r, cap);
       if ((int)more.size() + 1 > room) {
         if (room < kMaxInflight) return kDefer;
         more.resize(room - 1);
+      } else if ((int)more.size() + 1 < cap && ms_between(r->t_submit, Clock::now()) < kBatchWindowMs) {
+        return 0;
       }
       batch.insert(batch.end(), more.begin(), more.end());
     }

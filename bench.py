@@ -527,12 +527,14 @@ def run_ours(args):
                      "frequencies_checked": len(errs), "refinement_steps": R, "tolerance": 1e-8,
                      "last_correction": float(max(corr))},
         "plain_fp64": {"value": round(value_plain, 3), "unit": UNIT,
-                       "form": "one frequency at a time: bem_ghmatecd + bem_linsolve (the reference's order)",
+                       "form": "one frequency at a time: bem_ghmatecd + bem_linsolve (the reference's order); "
+                               "FP64 LU with panel pairs, trailing update by cuBLAS ZGEMM",
                        "ms_per_solve": round(ms_plain / kp, 3), "steps": kp,
                        "gemm_tflops": round(plain_gemm, 3) if plain_gemm else None,
                        "kernel_share": {k: round(v["ms"] / t_plain["ms"], 4) for k, v in pp.items()}},
         "plain_fp64_batched": {"value": round(value_plain_b, 3), "unit": UNIT,
-                               "form": f"bem_sweep PLAIN, {Bp} frequencies per step in lockstep, FP64 LU",
+                               "form": f"bem_sweep PLAIN, {Bp} frequencies per step in lockstep, FP64 LU "
+                                       "(panel pairs, trailing update by strided-batched cuBLAS ZGEMM)",
                                "ms_per_step": round(ms_plain_b / kpb, 3), "steps": kpb},
         "speedup_vs_plain_fp64": round(value / value_plain, 3),
         "speedup_vs_plain_fp64_batched": round(value / value_plain_b, 3),
