@@ -46,11 +46,6 @@ using Clock = std::chrono::steady_clock;
 constexpr int kMaxInflight = 16;
 constexpr int kMaxSlotsBusy = 8;
 constexpr int kDefer = -2;  // try_start: wait for a fuller lockstep batch
-// A request that could lead a lockstep batch (same mesh, material, BCs and
-// KODE, other omegas) but has fewer companions queued than the batch holds
-// waits this long after its submission for more to arrive: a sweep submitted
-// request by request then forms full batches instead of a first batch of one.
-constexpr double kBatchWindowMs = 2.0;
 
 double ms_between(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
@@ -70,6 +65,7 @@ struct SrvRequest {
   std::vector<double> bc;  // 3 nbe complex
   std::vector<int> kode;   // 3 nbe
   Clock::time_point t_submit, t_start, t_done;
+  long long pkey = 0;  // problem key: equal for equal (mesh, material, BCs, KODE)
   bool started = false, done = false, rhs_only = false;
   int status = BEM_OK;
   size_t bytes = 0;
@@ -157,6 +153,7 @@ class Server {
     r->fr = fr;
     r->bc.assign(bc, bc + 2 * (size_t)nn);
     r->kode.assign(kode, kode + nn);
+    r->pkey = problem_key(r);
     r->t_submit = Clock::now();
     if (!have_first_) {
       first_submit_ = r->t_submit;
@@ -241,7 +238,6 @@ class Server {
         }
       for (auto it = queue_.begin(); it != queue_.end() && busy < kMaxInflight && busy_slots < kMaxSlotsBusy;) {
         const int st = try_start(*it, kMaxInflight - busy);
-        if (st == kDefer) break;  // the queue's head waits for a fuller batch
         if (st > 0) {  // the request and any batched with it leave the queue
           ++busy_slots;
           queue_.erase(std::remove_if(queue_.begin(), queue_.end(),
@@ -250,6 +246,8 @@ class Server {
           it = queue_.begin();
           progress = true;
           busy += st;
+        } else if (st == kDefer) {
+          ++it;  // waits for a fuller lockstep batch; later requests may start
         } else if (st < 0) {
           it = queue_.erase(it);  // failed at admission: reported through wait()
           progress = true;
@@ -359,15 +357,47 @@ class Server {
     return true;
   }
 
+  static uint64_t bits(double v) {
+    uint64_t u;
+    std::memcpy(&u, &v, sizeof u);
+    return u;
+  }
+
+  // Key of a request's problem (mesh, material, boundary conditions, KODE):
+  // requests with equal data get the same key.  A hash of the data picks the
+  // bucket, one full comparison against a live request of the bucket decides,
+  // so the queue scans compare keys only.  Buckets hold weak references: a
+  // key outlives its requests only while one of them is alive.
+  long long problem_key(const std::shared_ptr<SrvRequest>& r) {
+    uint64_t h = 1469598103934665603ull;  // FNV-1a over 64- and 32-bit words
+    auto mix = [&h](uint64_t w) { h = (h ^ w) * 1099511628211ull; };
+    mix((uint64_t)r->mesh);
+    for (double v : r->mat) mix(bits(v));
+    for (double v : r->bc) mix(bits(v));
+    for (int v : r->kode) mix((uint32_t)v);
+    auto& bucket = pkeys_[h];
+    for (auto it = bucket.begin(); it != bucket.end();) {
+      auto q = it->lock();
+      if (!q) {
+        it = bucket.erase(it);
+        continue;
+      }
+      if (q->mesh == r->mesh && std::memcmp(q->mat, r->mat, sizeof q->mat) == 0 && q->kode == r->kode &&
+          q->bc == r->bc)
+        return q->pkey;
+      ++it;
+    }
+    bucket.push_back(r);
+    return ++next_pkey_;
+  }
+
   // Queued requests that can run in lockstep with r: same mesh, material,
   // boundary conditions and KODE, any omega (a frequency sweep).
   std::vector<std::shared_ptr<SrvRequest>> companions(const std::shared_ptr<SrvRequest>& r, int room) {
     std::vector<std::shared_ptr<SrvRequest>> out;
     for (const auto& q : queue_) {
       if ((int)out.size() + 1 >= room) break;
-      if (q == r || q->started || q->mesh != r->mesh || std::memcmp(q->mat, r->mat, sizeof q->mat) != 0 ||
-          q->kode != r->kode || q->bc != r->bc)
-        continue;
+      if (q == r || q->started || q->pkey != r->pkey) continue;
       out.push_back(q);
     }
     return out;
@@ -388,8 +418,8 @@ class Server {
   // Problems started (the request, and those batched with it), 0 not yet
   // (waits for memory or a slot), -1 failed, kDefer: the request has more
   // lockstep companions queued than the in-flight limit lets start now
-  // while other solves run, so it waits for a fuller batch (the queue scan
-  // stops there: first come, first served).  `room`: problems that may start.
+  // while other solves run, so it waits for a fuller batch (other requests
+  // behind it may start meanwhile).  `room`: problems that may start.
   int try_start(const std::shared_ptr<SrvRequest>& r, int room) {
     const SrvMesh& m = meshes_[r->mesh];
     const int nn = 3 * m.nbe;
@@ -409,8 +439,6 @@ class Server {
       if ((int)more.size() + 1 > room) {
         if (room < kMaxInflight) return kDefer;
         more.resize(room - 1);
-      } else if ((int)more.size() + 1 < cap && ms_between(r->t_submit, Clock::now()) < kBatchWindowMs) {
-        return 0;
       }
       batch.insert(batch.end(), more.begin(), more.end());
     }
@@ -554,7 +582,8 @@ class Server {
   std::vector<std::pair<size_t, double*>> pinned_free_;  // pinned buffers of destroyed slots
   std::deque<std::shared_ptr<SrvRequest>> queue_;
   std::unordered_map<long long, std::shared_ptr<SrvRequest>> reqs_;
-  long long next_id_ = 0;
+  std::unordered_map<uint64_t, std::vector<std::weak_ptr<SrvRequest>>> pkeys_;  // problem_key's buckets
+  long long next_id_ = 0, next_pkey_ = 0;
   unsigned long long tick_ = 0;
   size_t used_bytes_ = 0, peak_bytes_ = 0;
   long long n_rhs_only_ = 0, n_evict_ = 0;
