@@ -286,6 +286,11 @@ int dyn_graph_update(bem_ctx* ctx, cudaGraphExec_t exec, const std::vector<cudaG
 int dyn_graph_nodes(bem_ctx* ctx, cudaGraph_t g, std::vector<cudaGraphNode_t>& out);
 int launch_dynamic_batch(bem_ctx* ctx, const DynBatch& b);
 void release_cublas(bem_ctx* ctx);
+// A kernel's dynamic shared-memory limit is a process-wide attribute, and
+// contexts in other host threads launch the same kernel with other sizes:
+// the limit is only ever raised (under a lock), so no launch finds it lowered
+// by another thread between setting it and launching.
+cudaError_t raise_smem_limit(const void* func, size_t bytes);
 // One member of a grouped assembly (bem_batch_solve).
 struct GroupMember {
   bem_ctx* pc;  // the problem's context: mesh, static diagonals, BCs

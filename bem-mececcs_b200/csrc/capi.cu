@@ -5,6 +5,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <utility>
 #include <vector>
 
 #include "bem_internal.h"
@@ -26,6 +29,20 @@ int cuda_fail(bem_ctx* ctx, cudaError_t e, const char* what) {
 }
 
 // Reads the device status words after a synchronisation.
+cudaError_t raise_smem_limit(const void* func, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> limit;
+  int dev = 0;
+  const cudaError_t de = cudaGetDevice(&dev);
+  if (de != cudaSuccess) return de;
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& cur = limit[{dev, func}];
+  if (bytes <= cur) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
+}
+
 int check_status(bem_ctx* ctx) {
   int st[ST_COUNT] = {0};
   BEM_CUDA(ctx, cudaMemcpyAsync(st, ctx->d_status, sizeof st, cudaMemcpyDeviceToHost, ctx->stream));

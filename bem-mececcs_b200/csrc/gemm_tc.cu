@@ -718,7 +718,7 @@ __global__ void __launch_bounds__(128, 1) k_umma_peak(int iters, int n, int* sta
 int measure_tf32_peak(bem_ctx* ctx, int n, double* tflops) {
   if (n != 128 && n != 256) return fail(ctx, BEM_ERR_ARG, "UMMA peak probe: N must be 128 or 256");
   const size_t smem = kChunk + (size_t)n * 128 + 1024;
-  BEM_CUDA(ctx, cudaFuncSetAttribute(k_umma_peak, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_umma_peak), smem));
   const int iters = 2048;
   cudaEvent_t e0, e1;
   BEM_CUDA(ctx, cudaEventCreate(&e0));
@@ -757,8 +757,8 @@ int tc_ensure(bem_ctx* ctx, int nn, int batch) {
     return fail(ctx, BEM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   W.lrows_cap = lrows;
   W.urows_cap = urows;
-  BEM_CUDA(ctx, cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
-  BEM_CUDA(ctx, cudaFuncSetAttribute(k_gemm_tc2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTc2Smem));
+  BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_gemm_tc), kTcSmem));
+  BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_gemm_tc2), kTc2Smem));
   return BEM_OK;
 }
 

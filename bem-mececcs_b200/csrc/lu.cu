@@ -3367,7 +3367,7 @@ static int launch_cluster_panel(bem_ctx* ctx, const PanelArgs& pa, int batch) {
   const bool push = ctx->panel_push;
   const size_t smem = push ? push_panel_smem<R, NB>(pa.rp) : ((size_t)NB * pa.rp + 4 * NB + 2 * 8 * NB) * sizeof(cpx<R>);
   auto kern = push ? k_panel_push<R, NB, NT> : k_panel_cluster<R, NB, NT>;
-  BEM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(kern), smem));
   BEM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(pa.cs, batch, 1);
@@ -3436,7 +3436,7 @@ template <int NB, int NT>
 static int launch_calu_panel(bem_ctx* ctx, const PanelArgs& pa, int batch) {
   const size_t smem = calu_dyn_smem<NB>(pa.rp);
   auto kern = k_panel_calu<NB, NT>;
-  BEM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(kern), smem));
   BEM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(pa.cs, batch, 1);
@@ -3476,7 +3476,7 @@ template <typename R, int NB>
 static int launch_grid_panel(bem_ctx* ctx, PanelArgs pa) {
   auto kern = k_panel_grid<R, NB>;
   const size_t smem = (size_t)pa.rp * NB * sizeof(cpx<R>);
-  BEM_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(kern), smem));
   BEM_CUDA(ctx, cudaMemsetAsync(pa.bar, 0, sizeof(unsigned), ctx->stream));
   void* args[] = {&pa};
   BEM_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)kern, dim3(pa.cs), dim3(kPanelThreads), args, smem,
@@ -3489,7 +3489,7 @@ static int cluster_size(bem_ctx* ctx) {
   if (ctx->lu.cluster_cs) return ctx->lu.cluster_cs;
   int cs = 8;
   auto kern = k_panel_cluster<double, 32, 512>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemBudget);
+  raise_smem_limit(reinterpret_cast<const void*>(kern), kPanelSmemBudget);
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(16, 1, 1);
@@ -3530,7 +3530,7 @@ static int cluster_capacity(int cs, int rp) {
   const size_t smem = ((size_t)NB * rp + 4 * NB + 2 * 8 * NB) * sizeof(cpx<R>);
   auto kern = k_panel_cluster<R, NB, NT>;
   int n = 0;
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+  if (raise_smem_limit(reinterpret_cast<const void*>(kern), smem) == cudaSuccess &&
       cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(cs, 1, 1);
@@ -3742,7 +3742,7 @@ static int tslu_panel(bem_ctx* ctx, float2* A, size_t lda, size_t bstride, int n
   // round 3: the winners to the top in partial pivoting's record, the top
   // block's LU, then L21
   const size_t asmem = (size_t)(2 * kTsluW * kTsluW) * sizeof(zf);
-  BEM_CUDA(ctx, cudaFuncSetAttribute(k_tslu_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asmem));
+  BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_tslu_apply), asmem));
   k_tslu_apply<<<batch, 256, asmem, st>>>(A, lda, bstride, nn, k, ncand, L.ts_cperm, L.ts_gid, L.ts_c, L.ipiv, nn,
                                           perm_p, L.pstart, pidx, ctx->d_status);
   const int rows = nn - k - kTsluW;
@@ -3777,7 +3777,7 @@ static int trsv_f32(bem_ctx* ctx, const void* A, size_t lda, size_t bstride, int
     const int l = (per + 3) & ~1;  // rows of a share rounded out to even ends
     const size_t sm = (size_t)kTrsvBlk * l * sizeof(float2) + (size_t)l * sizeof(int) + 128;
     if (sm > kTrsvF32SmemMax || l > 256) break;  // smaller groups only need more; TMA boxes <= 256 rows
-    BEM_CUDA(ctx, cudaFuncSetAttribute(k_trsv_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_trsv_f32), sm));
     int occ = 0;
     BEM_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trsv_f32, 256, sm));
     int slots = occ * ctx->num_sms;
@@ -3802,7 +3802,7 @@ static int trsv_f32(bem_ctx* ctx, const void* A, size_t lda, size_t bstride, int
     ProfScope ps(ctx, 4, 8.0 * (double)(npan + nblk) * kTrsvBlk * kTrsvBlk * kTrsvBlk / 3.0 * batch,
                  2.0 * (double)(npan + nblk) * kTrsvBlk * kTrsvBlk * sizeof(float2) * batch);
     constexpr size_t kInvSmem = (size_t)2 * 64 * 65 * sizeof(float2);
-    BEM_CUDA(ctx, cudaFuncSetAttribute(k_tri_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
+    BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_tri_inv), kInvSmem));
     k_tri_inv<<<dim3(npan + nblk, batch), 64, kInvSmem, ctx->stream>>>(static_cast<const float2*>(A), lda, bstride,
                                                                        nn, npan, L.pstart, L.tinv);
     ctx->launches++;
@@ -3860,7 +3860,7 @@ static int trsv_coop(bem_ctx* ctx, const void* A, size_t lda, size_t bstride, in
     }
   }
   const size_t smem = (size_t)kTrsvBlk * kTrsvBlk * sizeof(cpx<R>);
-  BEM_CUDA(ctx, cudaFuncSetAttribute(k_trsv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_trsv<R>), smem));
   int occ = 0;
   BEM_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trsv<R>, 256, smem));
   int slots = occ * ctx->num_sms;
@@ -3900,13 +3900,11 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
   const int cs = cluster_size_for(ctx, nn);
   const size_t lsmem = 64 * 64 * es;
   const size_t bsmem = 64 * 64 * es;
-  BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_trsm<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)lsmem));
-  BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_trsm<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(2 * lsmem)));
-  BEM_CUDA(ctx, cudaFuncSetAttribute(k_backsub<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem));
-  BEM_CUDA(ctx, cudaFuncSetAttribute(k_gemm_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
-  BEM_CUDA(ctx, cudaFuncSetAttribute(k_gemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmTf32Smem));
+  BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_laswp_trsm<R, false>), lsmem));
+  BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_laswp_trsm<R, true>), 2 * lsmem));
+  BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_backsub<R>), bsmem));
+  BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_gemm_f64), kGemmSmem));
+  BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_gemm_tf32), kGemmTf32Smem));
   if (sizeof(R) == 4 && ctx->use_tcgen05) {
     int rc = tc_ensure(ctx, nn, batch);
     if (rc) return rc;
@@ -4010,7 +4008,7 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
       BEM_CUDA(ctx, dev_alloc(ctx, &LW.gmap, mbytes));
       LW.gmap_bytes = mbytes;
     }
-    BEM_CUDA(ctx, cudaFuncSetAttribute(k_l11_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * kLtTile)));
+    BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_l11_inv), (2 * kLtTile)));
     k_l11_inv<<<batch, 1024, 2 * kLtTile, ctx->stream>>>(static_cast<const float2*>(A), lda, bstride, k, w, LW.linv,
                                                          perm_p, kPermStride, LW.gmap, nn, gi, gsize);
     ctx->launches++;
@@ -4047,12 +4045,12 @@ static int lu_run(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int
       const int pk = (ure && pack_r0 >= 0) ? pack_r0 : -1;
       float* lhat = ctx->tc.lhat;
       if (pre) {
-        BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_laswp_tc<true>), sm));
         k_laswp_tc<true><<<dim3(tb, batch), 256, sm, ctx->stream>>>(
             A2, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kfirst, nprev,
             cdefer, LW.gmap, nn, LW.linv, lhat, 2 * nn, pk);
       } else {
-        BEM_CUDA(ctx, cudaFuncSetAttribute(k_laswp_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_laswp_tc<false>), sm));
         k_laswp_tc<false><<<dim3(tb, batch), 256, sm, ctx->stream>>>(
             A2, lda, bstride, k, w, c0, ncols, perm_p, kPermStride, ure, uim, nn + 1, ubase, koff, kfirst, 0, ncols,
             LW.gmap, nn, LW.linv, lhat, 2 * nn, pk);
@@ -4323,8 +4321,8 @@ static int lu_solve_vec_t(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int
   LuWork& L = ctx->lu;
   const size_t es = sizeof(cpx<R>);
   const size_t lsmem = 64 * 64 * es;
-  BEM_CUDA(ctx, cudaFuncSetAttribute(k_fwd_panel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem));
-  BEM_CUDA(ctx, cudaFuncSetAttribute(k_backsub<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem));
+  BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_fwd_panel<R>), lsmem));
+  BEM_CUDA(ctx, raise_smem_limit(reinterpret_cast<const void*>(k_backsub<R>), lsmem));
   ProfScope ps(ctx, 4, 8.0 * (double)nn * nn * batch, (double)nn * nn * sizeof(cpx<R>) * batch);
   if (ctx->use_trsv_coop) return trsv_coop<R>(ctx, A, lda, bstride, nn, batch, v, vstride, true);
   for (size_t p = 0; p < L.panels.size(); ++p) {

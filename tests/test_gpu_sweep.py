@@ -158,3 +158,44 @@ def test_tall_fp32_panels(tslu):
         assert rel(xm[i], xp[i]) < 1e-10, (tslu, freqs[i])
         assert corr[i] < 1e-9
     sol.close()
+
+
+def test_two_contexts_two_threads_other_sizes():
+    """Two contexts driven from two host threads at once, on meshes of other
+    sizes, so that the same kernels launch concurrently with other dynamic
+    shared-memory sizes (the limit is a process-wide kernel attribute; it is
+    only ever raised).  Every sweep must succeed and equal the same sweep run
+    alone."""
+    import threading
+    meshes = [meshgen.enclosed_grid(nx, ny, jitter=0.10, seed=sd, depth=2.5, layers=4)
+              for nx, ny, sd in ((16, 15, 21), (30, 27, 22))]
+    sols, alone = [], []
+    freqs = [0.6, 1.9, 3.3]
+    for m in meshes:
+        d = meshgen.traction_patch(m, radius=2.0)
+        sol = BemSolver(m)
+        sol.ghmatece()
+        sol.set_bc(d.kode, d.bc, d.dam, d.rho)
+        sols.append(sol)
+        for form in ("mixed", "plain"):
+            alone.append(sol.sweep(freqs, form=form, batch=3, refine=2)[0])
+    errors, got = [], {}
+
+    def run(i):
+        try:
+            for rnd in range(4):
+                for j, form in enumerate(("mixed", "plain")):
+                    got[(i, j, rnd)] = sols[i].sweep(freqs, form=form, batch=3, refine=2)[0]
+        except Exception as e:  # reported below
+            errors.append(e)
+
+    th = [threading.Thread(target=run, args=(i,)) for i in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for s in sols:
+        s.close()
+    assert not errors, errors[0]
+    for (i, j, rnd), x in got.items():
+        assert rel(x, alone[2 * i + j]) < 1e-12, (i, j, rnd)
