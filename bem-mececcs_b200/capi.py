@@ -93,6 +93,7 @@ def lib():
     L.bem_batch_solve.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, ip, ip, vp, vp]
     L.bem_interior.argtypes = [vp, vp, vp, vp, dp, dp, ip, vp, vp, vp, vp, vp, vp, vp]
     L.bem_sweep.argtypes = [vp, vp, vp, vp, vp, vp, ip, ip, ip, ip, vp, vp]
+    L.bem_sweep_async.argtypes = [vp, vp, vp, vp, vp, vp, ip, ip, ip, ip, vp]
     L.bem_sweep_batch_limit.argtypes = [vp, ip, P(ip)]
     _lib = L
     return L

@@ -323,8 +323,11 @@ int lu_solve_vec(bem_ctx* ctx, void* A, size_t lda, size_t bstride, int nn, int 
                  bool fp32);
 
 // Frequency sweep (mixed.cu).
+// wait_out: with x_out, return once the solutions are in host memory (else
+// their copies are only enqueued and errors wait for the next bem_sync).
 int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], const double c[4],
-          const double* freqs, int nfreq, int form, int batch, int iters, double* x_out, double* corr_out);
+          const double* freqs, int nfreq, int form, int batch, int iters, double* x_out, double* corr_out,
+          bool wait_out = true);
 void release_sweep(bem_ctx* ctx);
 void release_sweep_graph(bem_ctx* ctx);
 // Lockstep solve of problems of uneven size (bem_batch_solve).

@@ -572,6 +572,17 @@ int bem_sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const doub
   return BEM_OK;
 }
 
+int bem_sweep_async(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], const double c[4],
+                    const double* freqs, int nfreq, int form, int batch, int refine, double* x_out) {
+  if (!ctx || !zge || !zcs || !zcp || !c || (nfreq > 0 && !freqs)) return BEM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!ctx->have_mesh || !ctx->have_dyn || !ctx->have_hest || !ctx->have_gest)
+    return fail(ctx, BEM_ERR_STATE, "bem_sweep_async needs the mesh, BCs and static diagonals");
+  if (ctx->mesh_flag_bnd) return fail(ctx, BEM_ERR_DEGENERATE, "Jacobian below 1e-5 on a boundary element");
+  cudaSetDevice(ctx->device);
+  return sweep(ctx, zge, zcs, zcp, c, freqs, nfreq, form, batch, refine, x_out, nullptr, false);
+}
+
 int bem_batch_solve(bem_ctx* driver, int nprob, bem_ctx* const* probs, const double* freqs, const double* zge,
                     const double* zcs, const double* zcp, const double* c, int form, int refine,
                     double* const* x_out, double* corr_out) {

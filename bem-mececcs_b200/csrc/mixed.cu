@@ -235,7 +235,8 @@ void release_sweep(bem_ctx* ctx) {
 }
 
 int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double zcp[2], const double c[4],
-          const double* freqs, int nfreq, int form, int batch, int iters, double* x_out, double* corr_out) {
+          const double* freqs, int nfreq, int form, int batch, int iters, double* x_out, double* corr_out,
+          bool wait_out) {
   const bool mixed = form == BEM_FORM_MIXED;
   if (!mixed && form != BEM_FORM_PLAIN) return fail(ctx, BEM_ERR_ARG, "unknown form");
   if (batch < 1 || batch > kMaxBatch || nfreq < 0 || iters < 0 || iters > kMaxRefine)
@@ -364,7 +365,7 @@ int sweep(bem_ctx* ctx, const double zge[2], const double zcs[2], const double z
       }
     }
   }
-  if (x_out || corr_out) return check_status(ctx);
+  if ((x_out && wait_out) || corr_out) return check_status(ctx);
   return BEM_OK;
 }
 

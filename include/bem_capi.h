@@ -276,6 +276,18 @@ int bem_sweep(bem_ctx *ctx, const double zge[2], const double zcs[2],
               int nfreq, int form, int batch, int refine, double *x_out,
               double *corr_out);
 
+/* bem_sweep that returns once its work and the copies of its solutions into
+ * x_out are enqueued on ctx's stream (no corrections).  x_out should be
+ * page-locked host memory (or device memory) for the copies to overlap; it
+ * must stay untouched until the stream has passed them: record an event on
+ * the stream given to bem_ctx_set_stream, or call bem_sync, which also
+ * reports the errors of this call.  A client keeps several sweeps of one
+ * context in flight this way, each into its own output buffer. */
+int bem_sweep_async(bem_ctx *ctx, const double zge[2], const double zcs[2],
+                    const double zcp[2], const double c[4],
+                    const double *freqs, int nfreq, int form, int batch,
+                    int refine, double *x_out);
+
 /* Many problems of uneven size in lockstep (the batching form for small
  * meshes).  probs[p] is a context holding problem p's mesh, static
  * diagonals (bem_ghmatece) and BCs (bem_dyn_upload); p is solved at

@@ -199,3 +199,28 @@ def test_two_contexts_two_threads_other_sizes():
     assert not errors, errors[0]
     for (i, j, rnd), x in got.items():
         assert rel(x, alone[2 * i + j]) < 1e-12, (i, j, rnd)
+
+
+@pytest.mark.parametrize("form", ["mixed", "plain"])
+def test_sweep_async_matches_sweep(c1, form):
+    """bem_sweep_async: three sweeps in flight on one context, each into its
+    own page-locked buffer, then one bem_sync; every buffer equals what
+    bem_sweep returns for the same frequencies."""
+    import torch
+    from bem_mececcs_b200 import capi
+    s, d, p, sol = c1
+    groups = [FREQS[0:3], FREQS[3:6], FREQS[4:7]]
+    want = [sol.sweep(g, form=form, batch=3, refine=2)[0] for g in groups]
+    zge, zcs, zcp = sol.material
+    zg, zc, zp = (capi.f64([z.real, z.imag]) for z in (zge, zcs, zcp))
+    cc = capi.f64(sol.c)
+    fm = capi.BEM_FORM_MIXED if form == "mixed" else capi.BEM_FORM_PLAIN
+    bufs = [torch.empty(3 * sol.nn * 16, dtype=torch.uint8, pin_memory=True).numpy().view(np.complex128)
+            for _ in groups]
+    frs = [capi.f64(g) for g in groups]
+    for fr, b in zip(frs, bufs):
+        sol.ctx.check(sol.ctx.L.bem_sweep_async(sol.ctx.h, capi.ptr(zg), capi.ptr(zc), capi.ptr(zp), capi.ptr(cc),
+                                                capi.ptr(fr), 3, fm, 3, 2, capi.ptr(b)), "bem_sweep_async")
+    sol.ctx.sync()
+    for w, b in zip(want, bufs):
+        assert rel(b.reshape(3, sol.nn), w) < 1e-12
