@@ -388,6 +388,15 @@ class Server {
       ++it;
     }
     bucket.push_back(r);
+    // a long-running server sees ever new problems: drop the buckets whose
+    // requests are all gone, now and then
+    if ((++pkey_inserts_ & 1023u) == 0)
+      for (auto b = pkeys_.begin(); b != pkeys_.end();) {
+        auto& v = b->second;
+        v.erase(std::remove_if(v.begin(), v.end(), [](const std::weak_ptr<SrvRequest>& w) { return w.expired(); }),
+                v.end());
+        b = v.empty() ? pkeys_.erase(b) : std::next(b);
+      }
     return ++next_pkey_;
   }
 
@@ -584,6 +593,7 @@ class Server {
   std::unordered_map<long long, std::shared_ptr<SrvRequest>> reqs_;
   std::unordered_map<uint64_t, std::vector<std::weak_ptr<SrvRequest>>> pkeys_;  // problem_key's buckets
   long long next_id_ = 0, next_pkey_ = 0;
+  unsigned pkey_inserts_ = 0;
   unsigned long long tick_ = 0;
   size_t used_bytes_ = 0, peak_bytes_ = 0;
   long long n_rhs_only_ = 0, n_evict_ = 0;
