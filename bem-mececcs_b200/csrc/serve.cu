@@ -46,6 +46,9 @@ using Clock = std::chrono::steady_clock;
 constexpr int kMaxInflight = 16;
 constexpr int kMaxSlotsBusy = 8;
 constexpr int kDefer = -2;  // try_start: wait for a fuller lockstep batch
+// A request waits for a fuller batch at most this long after its submission,
+// so that a busy server cannot starve it (it then starts with what fits).
+constexpr double kDeferLimitMs = 1000.0;
 
 double ms_between(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
@@ -428,7 +431,8 @@ class Server {
   // (waits for memory or a slot), -1 failed, kDefer: the request has more
   // lockstep companions queued than the in-flight limit lets start now
   // while other solves run, so it waits for a fuller batch (other requests
-  // behind it may start meanwhile).  `room`: problems that may start.
+  // behind it may start meanwhile), for up to kDeferLimitMs.  `room`:
+  // problems that may start.
   int try_start(const std::shared_ptr<SrvRequest>& r, int room) {
     const SrvMesh& m = meshes_[r->mesh];
     const int nn = 3 * m.nbe;
@@ -446,7 +450,8 @@ class Server {
       const int cap = lockstep_cap(nn);
       auto more = companions(r, cap);
       if ((int)more.size() + 1 > room) {
-        if (room < kMaxInflight) return kDefer;
+        const int target = std::min(cap, kMaxInflight);
+        if (room < target && ms_between(r->t_submit, Clock::now()) < kDeferLimitMs) return kDefer;
         more.resize(room - 1);
       }
       batch.insert(batch.end(), more.begin(), more.end());
