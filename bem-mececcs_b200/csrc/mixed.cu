@@ -118,31 +118,6 @@ __global__ void k_ir_update(double2* x, size_t x_stride, const float2* __restric
   }
 }
 
-// Padded embedding of a problem of size n in an npad system (bem_batch_solve):
-// the right-hand side moves from column n to column npad, rows n..npad-1 of
-// it are zero.
-template <typename T>
-__global__ void k_pad_rhs(T* A, size_t lda, int n, int npad) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= npad) return;
-  T v;
-  v.x = 0;
-  v.y = 0;
-  if (r < n) v = A[(size_t)n * lda + r];
-  A[(size_t)npad * lda + r] = v;
-}
-// Then columns < n get zero rows n..npad-1 and columns n..npad-1 become the
-// identity, so the padding never pivots and stays untouched by the updates.
-template <typename T>
-__global__ void k_pad_rest(T* A, size_t lda, int n, int npad) {
-  const int col = blockIdx.y;
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= npad || col >= npad) return;
-  T v;
-  v.x = (col >= n && r == col) ? 1 : 0;
-  v.y = 0;
-  if (col >= n || r >= n) A[(size_t)col * lda + r] = v;
-}
 
 void free_sweep(bem_ctx* ctx, SweepBuf& S) {
   dev_free(ctx, S.A64);
