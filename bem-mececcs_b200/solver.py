@@ -180,6 +180,22 @@ class BemSolver:
             ptr(x), ptr(corr)), "bem_sweep")
         return x, corr
 
+    def sweep_async(self, freqs, x_out, *, form: str = "mixed", batch: int = 8, refine: int = 3):
+        """bem_sweep_async: enqueues the sweep and the copy of its raw
+        solutions into x_out (complex128, len(freqs) x nn, page-locked for
+        the copy to overlap) and returns at once.  x_out must stay alive and
+        untouched until the context's stream has passed the copy (an event
+        on that stream, or self.ctx.sync(), which also reports errors)."""
+        freqs = f64(freqs)
+        if x_out.dtype != np.complex128 or x_out.size < freqs.size * self.nn or not x_out.flags.c_contiguous:
+            raise ValueError("x_out: contiguous complex128 with len(freqs) * nn entries")
+        zge, zcs, zcp = self.material
+        fm = BEM_FORM_MIXED if form == "mixed" else BEM_FORM_PLAIN
+        self.ctx.check(self.ctx.L.bem_sweep_async(
+            self.ctx.h, ptr(f64([zge.real, zge.imag])), ptr(f64([zcs.real, zcs.imag])),
+            ptr(f64([zcp.real, zcp.imag])), ptr(f64(self.c)), ptr(freqs), freqs.size, fm, batch, refine,
+            ptr(x_out)), "bem_sweep_async")
+
     def sweep_batch_limit(self, form: str = "mixed") -> int:
         """Largest lockstep batch bem_sweep uses for this mesh and form."""
         out = ctypes.c_int(0)
