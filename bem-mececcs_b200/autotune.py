@@ -3,7 +3,8 @@
 The choices it makes are the library's algorithm switches and the lockstep
 batch: the FP32 panel's pivoting (per column, or tournament per 8-column
 sub-panel), four, two or one panels per tensor-core trailing update
-(K = 256, 128 or 64; four take precedence where they fit), CUDA-graph replay
+(K = 256, 128 or 64; four take precedence where they fit), the update by CTA
+pairs or by single CTAs, CUDA-graph replay
 of the batch step, and the number of problems in lockstep (up to
 bem_sweep_batch_limit).  Each candidate is timed on the
 resident mesh on real frequencies (after one untimed batch) and the fastest
@@ -26,6 +27,7 @@ DEFAULT_SPACE = {
     "lu_quads": (True, False),
     "panel_calu": (False, True),
     "lu_pairs": (True, False),
+    "tc_pair": (True, False),
     "graphs": (True, False),
 }
 

@@ -30,7 +30,7 @@ class FakeClock:
 class FakeCtx:
     def __init__(self, clock):
         self.clock = clock
-        self.opts = {"lu_quads": True, "panel_calu": False, "lu_pairs": True, "graphs": True}
+        self.opts = {"lu_quads": True, "panel_calu": False, "lu_pairs": True, "tc_pair": True, "graphs": True}
         self.synced = 0
 
     def set_option(self, k, v):
@@ -65,6 +65,7 @@ class FakeSolver:
         per *= 1.0 if o["lu_quads"] else 1.3
         per *= 1.0 if o["lu_pairs"] else 1.2
         per *= 1.1 if o["panel_calu"] else 1.0
+        per *= 1.0 if o["tc_pair"] else 1.1
         per *= 0.95 if not o["graphs"] else 1.0
         per *= 1.0 + 0.05 * (7 - batch)
         self.calls.append((form, batch, dict(o), len(freqs)))
@@ -82,7 +83,7 @@ def test_picks_the_fastest_candidate_and_restores_the_switches(fake):
     before = dict(fake.ctx.opts)
     best = autotune.tune_sweep(fake, [1.0, 2.0, 3.0], form="mixed", steps=2)
     assert best["options"] == {"lu_quads": True, "panel_calu": False, "lu_pairs": True,
-                               "graphs": False}
+                               "tc_pair": True, "graphs": False}
     assert best["batch"] == 7
     assert best["solves_per_s"] == pytest.approx(1 / (0.1 * 0.95), rel=1e-3)
     # every combination of the default space x the batches {7, 6, 3}
